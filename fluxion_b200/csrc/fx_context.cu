@@ -1,0 +1,396 @@
+// fx_context.cu -- context, buffers, host<->device transfers and the shared host helpers.
+//
+// The context plays the role of the reference's process-wide HIP backend singleton
+// (crates/backend-hip/src/backend.rs:61-79, :103-264): one device, one stream, the
+// reduction scratch.  Buffers play HipBuffer (crates/backend-hip/src/buffer.rs:16-123).
+#include <cstring>
+#include <mutex>
+
+#include "fx_internal.cuh"
+
+namespace fx {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+int check_launch(fx_ctx *ctx, const char *what) {
+    ctx->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(FX_ERR_BACKEND, std::string(what) + ": " + cudaGetErrorString(e));
+    return FX_OK;
+}
+
+int check_buf(const fx_buf *b, const char *name) {
+    if (!b) return fail(FX_ERR_INVALID_ARGUMENT, std::string("null buffer: ") + name);
+    return FX_OK;
+}
+
+int check_same(const fx_buf *a, const fx_buf *b) {
+    if (a->len != b->len) {
+        return fail(FX_ERR_DIMENSION_MISMATCH, "dimension mismatch: expected " +
+                                                   std::to_string(a->len) + ", got " +
+                                                   std::to_string(b->len));
+    }
+    if (a->dtype != b->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
+    return FX_OK;
+}
+
+int check_grid(const fx_grid *g) {
+    if (!g) return fail(FX_ERR_INVALID_ARGUMENT, "null grid");
+    if (g->rows < 3 || g->cols < 3)
+        return fail(FX_ERR_INVALID_GRID, "invalid grid: minimum 3x3, got " + std::to_string(g->rows) +
+                                             "x" + std::to_string(g->cols));
+    if (!(g->dx > 0.0) || !(g->dy > 0.0) || !std::isfinite(g->dx) || !std::isfinite(g->dy))
+        return fail(FX_ERR_INVALID_GRID, "invalid grid: spacing must be finite and positive");
+    if (g->rows > (size_t)0x7fffffff || g->cols > (size_t)0x7fffffff ||
+        g->rows * g->cols > ((size_t)1 << 40))
+        return fail(FX_ERR_INVALID_GRID, "invalid grid: too large");
+    return FX_OK;
+}
+
+int check_grid_len(const fx_grid *g, const fx_buf *b) {
+    const size_t n = g->rows * g->cols;
+    if (b->len != n)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "dimension mismatch: expected " + std::to_string(n) +
+                                                   ", got " + std::to_string(b->len));
+    return FX_OK;
+}
+
+int make_stencil(const fx_stencil *s, StencilP *P) {
+    std::memset(P, 0, sizeof(*P));
+    if (!s || s->n < 1 || !s->dr || !s->dc || !s->w)
+        return fail(FX_ERR_INVALID_STENCIL, "invalid stencil: stencil must have at least one entry");
+    const int n = s->n;
+    if (n == 5 || n == 9) {  // ops.rs:898-916, :953-975: weights by offset, others ignored
+        P->mode = n;
+        for (int k = 0; k < n; k++) {
+            const int r = s->dr[k], c = s->dc[k];
+            const double w = s->w[k];
+            if (r == 0 && c == 0) P->c = w;
+            else if (r == -1 && c == 0) P->n = w;
+            else if (r == 1 && c == 0) P->s = w;
+            else if (r == 0 && c == -1) P->w = w;
+            else if (r == 0 && c == 1) P->e = w;
+            else if (n == 9 && r == -1 && c == -1) P->nw = w;
+            else if (n == 9 && r == -1 && c == 1) P->ne = w;
+            else if (n == 9 && r == 1 && c == -1) P->sw = w;
+            else if (n == 9 && r == 1 && c == 1) P->se = w;
+        }
+        return FX_OK;
+    }
+    if (n > kMaxGeneric)
+        return fail(FX_ERR_INVALID_STENCIL, "invalid stencil: more than 27 entries");
+    for (int k = 0; k < n; k++) {
+        if (s->dr[k] < -1 || s->dr[k] > 1 || s->dc[k] < -1 || s->dc[k] > 1)
+            return fail(FX_ERR_INVALID_STENCIL, "invalid stencil: offsets beyond radius 1");
+        P->gi[k] = (signed char)((s->dr[k] + 1) * 3 + (s->dc[k] + 1));
+        P->gw[k] = s->w[k];
+    }
+    P->mode = 0;
+    P->ne_ = n;
+    return FX_OK;
+}
+
+int make_bc(const fx_boundaries *bc, double dx, double dy, BcP *P, bool reject_periodic) {
+    std::memset(P, 0, sizeof(*P));
+    P->dx = dx;
+    P->dy = dy;
+    if (!bc) {
+        for (int i = 0; i < 4; i++) P->kind[i] = FX_BC_DIRICHLET;
+        return FX_OK;
+    }
+    for (int i = 0; i < 4; i++) {
+        const int k = bc->side[i].kind;
+        if (k < 0 || k > 3) return fail(FX_ERR_INVALID_ARGUMENT, "unknown boundary kind");
+        if (k == FX_BC_PERIODIC && reject_periodic)  // ops.rs:9-23
+            return fail(FX_ERR_UNSUPPORTED, "backend error: periodic boundaries are not yet implemented");
+        P->kind[i] = k;
+        P->a[i] = bc->side[i].a;
+        P->b[i] = bc->side[i].b;
+        P->g[i] = bc->side[i].g;
+    }
+    return FX_OK;
+}
+
+MarchGeom march_geom(fx_ctx *ctx, size_t rows, size_t cols, int U) {
+    MarchGeom G;
+    G.rows = (int)rows;
+    G.cols = (int)cols;
+    G.nstrips = (int)((cols + 31) / 32);
+    // Aim for about 64 resident warps per SM worth of work items; chunks at least 2U rows.
+    const long target = (long)ctx->num_sms * 64;
+    long chunks = target / G.nstrips;
+    if (chunks < 1) chunks = 1;
+    long cr = ((long)rows + chunks - 1) / chunks;
+    const long min_rows = 2 * U;
+    if (cr < min_rows) cr = min_rows;
+    cr = ((cr + U - 1) / U) * U;
+    G.chunk_rows = (int)cr;
+    const long nchunks = ((long)rows + cr - 1) / cr;
+    G.nwarps = (int)(nchunks * G.nstrips);
+    return G;
+}
+
+FlatGeom flat_geom(fx_ctx *ctx, size_t n) {
+    FlatGeom g;
+    g.n = n;
+    size_t b = (n + kBlock - 1) / kBlock;
+    const size_t cap = (size_t)ctx->num_sms * 8;
+    if (b > cap) b = cap;
+    g.blocks = (int)b;
+    return g;
+}
+
+int read_results(fx_ctx *ctx, int k, double *out) {
+    FX_CUDA(cudaMemcpyAsync(ctx->h_result, ctx->d_result, k * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < k; i++) out[i] = ctx->h_result[i];
+    return FX_OK;
+}
+
+}  // namespace fx
+
+using namespace fx;
+
+extern "C" {
+
+const char *fx_last_error(void) { return g_err.c_str(); }
+
+int fx_version(void) { return 10000; }
+
+const char *fx_backend_name(void) { return "cuda"; }
+
+int fx_device_count(int *count) {
+    if (!count) return fail(FX_ERR_INVALID_ARGUMENT, "null out");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *count = 0;
+        return fail(FX_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    *count = n;
+    return FX_OK;
+}
+
+int fx_ctx_create(int device, fx_ctx **out) {
+    if (!out) return fail(FX_ERR_INVALID_ARGUMENT, "null out");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(FX_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= n) return fail(FX_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    FX_CUDA(cudaSetDevice(device));
+    fx_ctx *c = new fx_ctx();
+    c->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c->d_partials, sizeof(double) * 2 * kMaxSums * (size_t)kMaxRedBlocks) != cudaSuccess ||
+        cudaMalloc(&c->d_counter, sizeof(unsigned) * 4) != cudaSuccess ||
+        cudaMalloc(&c->d_result, sizeof(double) * 8) != cudaSuccess ||
+        cudaMallocHost(&c->h_result, sizeof(double) * 8) != cudaSuccess ||
+        cudaMemset(c->d_counter, 0, sizeof(unsigned) * 4) != cudaSuccess) {
+        std::string m = cudaGetErrorString(cudaGetLastError());
+        fx_ctx_destroy(c);
+        return fail(FX_ERR_BACKEND, "context allocation failed: " + m);
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return FX_OK;
+}
+
+int fx_ctx_destroy(fx_ctx *c) {
+    if (!c) return FX_OK;
+    cudaSetDevice(c->device);
+    if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+    if (c->d_partials) cudaFree(c->d_partials);
+    if (c->d_counter) cudaFree(c->d_counter);
+    if (c->d_result) cudaFree(c->d_result);
+    if (c->h_result) cudaFreeHost(c->h_result);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return FX_OK;
+}
+
+int fx_ctx_synchronize(fx_ctx *c) {
+    if (!c) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    FX_CUDA(cudaStreamSynchronize(c->stream));
+    return FX_OK;
+}
+
+int fx_ctx_set_stream(fx_ctx *c, void *stream) {
+    if (!c) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return FX_OK;
+}
+
+void *fx_ctx_get_stream(fx_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+unsigned long long fx_ctx_launch_count(fx_ctx *c) { return c ? c->launches : 0ull; }
+
+int fx_alloc(fx_ctx *ctx, size_t len, int dtype, fx_buf **out) {
+    if (!ctx || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (dtype != FX_F32 && dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "unknown dtype");
+    *out = nullptr;
+    fx_buf *b = new fx_buf();
+    b->ctx = ctx;
+    b->len = len;
+    b->dtype = dtype;
+    const size_t bytes = len * elem_size(dtype);
+    if (bytes) {
+        if (cudaMalloc(&b->ptr, bytes) != cudaSuccess) {
+            delete b;
+            return fail(FX_ERR_BACKEND, std::string("backend error: allocation failed: ") +
+                                            cudaGetErrorString(cudaGetLastError()));
+        }
+        if (cudaMemsetAsync(b->ptr, 0, bytes, ctx->stream) != cudaSuccess) {
+            cudaFree(b->ptr);
+            delete b;
+            return fail(FX_ERR_BACKEND, "backend error: memset failed");
+        }
+    }
+    *out = b;
+    return FX_OK;
+}
+
+int fx_wrap(fx_ctx *ctx, void *ptr, size_t len, int dtype, fx_buf **out) {
+    if (!ctx || !out || (!ptr && len)) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (dtype != FX_F32 && dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "unknown dtype");
+    fx_buf *b = new fx_buf();
+    b->ctx = ctx;
+    b->ptr = ptr;
+    b->len = len;
+    b->dtype = dtype;
+    b->owned = false;
+    *out = b;
+    return FX_OK;
+}
+
+int fx_free(fx_buf *b) {
+    if (!b) return FX_OK;
+    if (b->owned && b->ptr) {
+        cudaStreamSynchronize(b->ctx->stream);
+        cudaFree(b->ptr);
+    }
+    delete b;
+    return FX_OK;
+}
+
+size_t fx_buf_len(const fx_buf *b) { return b ? b->len : 0; }
+int fx_buf_dtype(const fx_buf *b) { return b ? b->dtype : -1; }
+void *fx_buf_device_ptr(const fx_buf *b) { return b ? b->ptr : nullptr; }
+
+}  // extern "C"
+
+// Conversion kernels for uploads / downloads across dtypes.
+namespace {
+__global__ void k_f64_to_f32(const double *__restrict__ s, float *__restrict__ d, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        d[i] = (float)s[i];
+}
+__global__ void k_f32_to_f64(const float *__restrict__ s, double *__restrict__ d, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        d[i] = (double)s[i];
+}
+
+int write_host(fx_ctx *ctx, fx_buf *b, const void *src, int src_dtype, size_t len) {
+    if (!ctx || !b || (!src && len)) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (len != b->len)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "dimension mismatch: expected " + std::to_string(b->len) +
+                                                   ", got " + std::to_string(len));
+    if (!len) return FX_OK;
+    if (src_dtype == b->dtype) {
+        FX_CUDA(cudaMemcpyAsync(b->ptr, src, len * elem_size(b->dtype), cudaMemcpyHostToDevice, ctx->stream));
+        FX_CUDA(cudaStreamSynchronize(ctx->stream));
+        return FX_OK;
+    }
+    void *tmp = nullptr;
+    FX_CUDA(cudaMallocAsync(&tmp, len * elem_size(src_dtype), ctx->stream));
+    FX_CUDA(cudaMemcpyAsync(tmp, src, len * elem_size(src_dtype), cudaMemcpyHostToDevice, ctx->stream));
+    FlatGeom g = flat_geom(ctx, len);
+    if (src_dtype == FX_F64)
+        k_f64_to_f32<<<g.blocks, kBlock, 0, ctx->stream>>>((const double *)tmp, (float *)b->ptr, len);
+    else
+        k_f32_to_f64<<<g.blocks, kBlock, 0, ctx->stream>>>((const float *)tmp, (double *)b->ptr, len);
+    int st = check_launch(ctx, "convert");
+    cudaFreeAsync(tmp, ctx->stream);
+    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return st;
+}
+
+int read_host(fx_ctx *ctx, const fx_buf *b, void *dst, int dst_dtype, size_t len) {
+    if (!ctx || !b || (!dst && len)) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (len != b->len)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "destination length mismatch: expected " +
+                                                   std::to_string(b->len) + ", got " + std::to_string(len));
+    if (!len) return FX_OK;
+    if (dst_dtype == b->dtype) {
+        FX_CUDA(cudaMemcpyAsync(dst, b->ptr, len * elem_size(b->dtype), cudaMemcpyDeviceToHost, ctx->stream));
+        FX_CUDA(cudaStreamSynchronize(ctx->stream));
+        return FX_OK;
+    }
+    void *tmp = nullptr;
+    FX_CUDA(cudaMallocAsync(&tmp, len * elem_size(dst_dtype), ctx->stream));
+    FlatGeom g = flat_geom(ctx, len);
+    if (dst_dtype == FX_F32)
+        k_f64_to_f32<<<g.blocks, kBlock, 0, ctx->stream>>>((const double *)b->ptr, (float *)tmp, len);
+    else
+        k_f32_to_f64<<<g.blocks, kBlock, 0, ctx->stream>>>((const float *)b->ptr, (double *)tmp, len);
+    int st = check_launch(ctx, "convert");
+    FX_CUDA(cudaMemcpyAsync(dst, tmp, len * elem_size(dst_dtype), cudaMemcpyDeviceToHost, ctx->stream));
+    cudaFreeAsync(tmp, ctx->stream);
+    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return st;
+}
+}  // namespace
+
+extern "C" {
+
+int fx_upload_f64(fx_ctx *ctx, const double *data, size_t len, fx_buf **out) {
+    FX_TRY(fx_alloc(ctx, len, FX_F64, out));
+    int st = write_host(ctx, *out, data, FX_F64, len);
+    if (st) {
+        fx_free(*out);
+        *out = nullptr;
+    }
+    return st;
+}
+
+int fx_upload_f32(fx_ctx *ctx, const float *data, size_t len, fx_buf **out) {
+    FX_TRY(fx_alloc(ctx, len, FX_F32, out));
+    int st = write_host(ctx, *out, data, FX_F32, len);
+    if (st) {
+        fx_free(*out);
+        *out = nullptr;
+    }
+    return st;
+}
+
+int fx_write_f64(fx_ctx *ctx, fx_buf *b, const double *src, size_t len) {
+    return write_host(ctx, b, src, FX_F64, len);
+}
+
+int fx_write_f32(fx_ctx *ctx, fx_buf *b, const float *src, size_t len) {
+    return write_host(ctx, b, src, FX_F32, len);
+}
+
+int fx_copy_to_host_f64(fx_ctx *ctx, const fx_buf *b, double *dst, size_t len) {
+    return read_host(ctx, b, dst, FX_F64, len);
+}
+
+int fx_copy_to_host_f32(fx_ctx *ctx, const fx_buf *b, float *dst, size_t len) {
+    return read_host(ctx, b, dst, FX_F32, len);
+}
+
+}  // extern "C"

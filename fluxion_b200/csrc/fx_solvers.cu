@@ -1,0 +1,1726 @@
+// fx_solvers.cu -- preconditioners, multigrid and the Krylov solver loops.
+//
+// The solver loops restate crates/runtime/src/{cg,pipelined_cg,bicgstab,gmres}.rs with
+// the same scalar recurrences, stop tests and iteration counts, but the vector work is
+// fused: each kernel applies the operator on the fly, updates several vectors and emits
+// the next inner products in the same pass.  The scalars (alpha, beta, rho, omega, ...)
+// live in device memory and are updated by the last block of each reduction, so an
+// iteration needs no host round trip; the host enqueues iterations in batches and a
+// `done` word in device memory turns the surplus launches into no-ops once the stop
+// test (evaluated on the device, exactly as the reference evaluates it) has fired.
+#include <cmath>
+#include <vector>
+
+#include "fx_points.cuh"
+
+using namespace fx;
+
+// ---------------------------------------------------------------- device solver state
+
+namespace fx {
+
+struct DevState {
+    double tol;
+    long long max_iter;
+    long long iter;
+    int done;     // solve finished: every later kernel is a no-op
+    int halt;     // done, or a pending early exit (BiCGSTAB): kernels that must skip read this
+    int reason;
+    int pending;  // BiCGSTAB: 1 = converged on s, 2 = breakdown on t.t (x += alpha*p still due)
+    double resid, r0;
+    // CG / PCG
+    double rs_old, alpha, beta, rr;
+    // pipelined CG
+    double gamma, delta, gamma_prev, alpha_prev;
+    // BiCGSTAB
+    double rho, rho_new, omega, r_norm, s_norm;
+};
+
+__device__ __forceinline__ void st_finish(DevState *S, int reason, long long iters, double resid) {
+    S->done = 1;
+    S->halt = 1;
+    S->reason = reason;
+    S->iter = iters;
+    S->resid = resid;
+}
+
+}  // namespace fx
+
+// ---------------------------------------------------------------- preconditioners
+
+struct fx_precond {
+    fx_ctx *ctx = nullptr;
+    bool borrowed = false;
+    virtual ~fx_precond() {}
+    // z <- M^-1 r.  z_zero: z holds zeros on entry (the solvers zero-fill z first, as the
+    // reference does); skip: device word, nonzero means the solve is over.
+    virtual int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) = 0;
+};
+
+namespace {
+
+
+// ---------------------------------------------------------------- operator A v = v + coeff*S v
+
+template <typename T, int MODE>
+struct OpA {
+    StencilP P;
+    T coeff;
+    int rows, cols;
+    __device__ __forceinline__ bool ring(int r, int c) const {
+        return r == 0 || r == rows - 1 || c == 0 || c == cols - 1;
+    }
+    // copy_from + stencil_axpy (cg.rs:106-109): interior fma(coeff, S v, v), ring = v
+    __device__ __forceinline__ T apply(int r, int c, const Nb<T> &nb) const {
+        return ring(r, c) ? nb.c : fx_fma(coeff, stencil_eval<T, MODE>(P, nb), nb.c);
+    }
+};
+
+template <typename T>
+struct Ld1 {
+    const T *p;
+    __device__ __forceinline__ T operator()(size_t i) const { return p[i]; }
+};
+
+// r + beta*p, rounded as p.scale(beta); p.axpy(1.0, r) (cg.rs:153-154)
+template <typename T>
+struct LdAypx {
+    const T *r, *p;
+    const DevState *S;
+    __device__ __forceinline__ T operator()(size_t i) const {
+        const T beta = (T)S->beta;
+        return r[i] + p[i] * beta;
+    }
+};
+
+// ------------------------------------------------ flat (pointwise) functors
+
+template <typename T>
+struct FlatCopy {
+    T *dst;
+    const T *src;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const { dst[i] = src[i]; }
+};
+
+template <typename T>
+struct FlatZero {
+    T *p;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const { p[i] = (T)0; }
+};
+
+template <typename S, typename D>
+struct FlatConvert {
+    const S *src;
+    D *dst;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const { dst[i] = (D)src[i]; }
+};
+
+template <typename T>
+struct FlatDot {
+    const T *a, *b;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        csum_add_prod(acc[0], (double)a[i], (double)b[i]);
+    }
+};
+
+template <typename T>
+struct FlatScaleInto {  // dst = src * f (copy_from + scale)
+    T *dst;
+    const T *src;
+    T f;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const { dst[i] = src[i] * f; }
+};
+
+template <typename T>
+struct FlatRestrictFW {
+    const T *f;
+    T *c;
+    size_t fcols, crows, ccols;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const {
+        const size_t I = i / ccols, J = i % ccols;
+        if (I == 0 || J == 0 || I == crows - 1 || J == ccols - 1) {
+            c[i] = (T)0;
+            return;
+        }
+        const size_t k = (2 * I) * fcols + 2 * J;
+        const T e = (f[k - fcols] + f[k + fcols]) + (f[k - 1] + f[k + 1]);
+        const T d = (f[k - fcols - 1] + f[k - fcols + 1]) + (f[k + fcols - 1] + f[k + fcols + 1]);
+        c[i] = ((T)4 * f[k] + ((T)2 * e + d)) * (T)0.0625;
+    }
+};
+
+template <typename T>
+struct FlatProlongBil {
+    const T *c;
+    T *f;
+    size_t ccols, fcols, iw;
+    __device__ __forceinline__ void operator()(size_t q, CSum *) const {
+        const size_t i = 1 + q / iw, j = 1 + q % iw;
+        const size_t k = (i / 2) * ccols + (j / 2);
+        T e;
+        if (!(i & 1) && !(j & 1)) e = c[k];
+        else if ((i & 1) && !(j & 1)) e = (T)0.5 * (c[k] + c[k + ccols]);
+        else if (!(i & 1) && (j & 1)) e = (T)0.5 * (c[k] + c[k + 1]);
+        else e = (T)0.25 * ((c[k] + c[k + ccols]) + (c[k + 1] + c[k + ccols + 1]));
+        f[i * fcols + j] += e;
+    }
+};
+
+struct IdentityPc : fx_precond {
+    int apply(fx_buf *z, const fx_buf *r, const int *skip, bool) override {
+        FX_TRY(check_same(z, r));
+        FX_DISPATCH(z->dtype, {
+            return launch_flat<0>(ctx, z->len, FlatCopy<T>{(T *)z->ptr, (const T *)r->ptr}, NoFin{}, skip,
+                                  "identity_pc");
+        });
+    }
+};
+
+// ------------------------------------------------ generic kernels used by several solvers
+
+// out = A v (no reduction) or with <v, out> / <out, y> reductions.
+template <typename T, int MODE>
+struct PtApplyOp {
+    OpA<T, MODE> A;
+    T *out;
+    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *) const {
+        out[idx] = A.apply(r, c, nb);
+    }
+};
+
+// Finalisers -------------------------------------------------------------------------
+
+struct FinStore1 {
+    double *dst;
+    __device__ void operator()(const double *v) const { *dst = v[0]; }
+};
+
+}  // namespace
+
+// ================================================================ multigrid
+
+namespace {
+
+struct MgLevel {
+    size_t rows = 0, cols = 0;
+    double dx = 0, dy = 0;
+    double a5[5] = {0, 0, 0, 0, 0};    // vertex: operator on this level
+    double lap5[5] = {0, 0, 0, 0, 0};  // reference: Laplacian weights
+    fx_buf *u = nullptr, *rhs = nullptr, *tmp = nullptr;
+};
+
+}  // namespace
+
+struct fx_mg {
+    fx_ctx *ctx = nullptr;
+    int mode = 0;  // 0 reference, 1 vertex
+    int dtype = FX_F64;
+    size_t n_pre = 2, n_post = 2, coarse_sweeps = 200;
+    double omega = 2.0 / 3.0;
+    fx_boundaries bc{};
+    std::vector<MgLevel> lv;
+    fx_buf *tmp0 = nullptr;  // level-0 ping-pong partner (vertex mode)
+    fx_buf *x32 = nullptr, *b32 = nullptr;  // level-0 single-precision copies (F32 cycle)
+    struct View : fx_precond {
+        fx_mg *mg = nullptr;
+        int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) override;
+    } view;
+    ~fx_mg() {
+        for (auto &L : lv) {
+            fx_free(L.u);
+            fx_free(L.rhs);
+            fx_free(L.tmp);
+        }
+        fx_free(tmp0);
+        fx_free(x32);
+        fx_free(b32);
+    }
+};
+
+namespace {
+
+const int LAP_DR[5] = {0, -1, 1, 0, 0};
+const int LAP_DC[5] = {0, 0, 0, -1, 1};
+
+void lap5_of(double dx, double dy, double *a) {  // stencil.rs:152-168
+    const double inv_dx2 = 1.0 / (dx * dx), inv_dy2 = 1.0 / (dy * dy);
+    a[0] = -2.0 * (inv_dx2 + inv_dy2);
+    a[1] = inv_dy2;
+    a[2] = inv_dy2;
+    a[3] = inv_dx2;
+    a[4] = inv_dx2;
+}
+
+// Vertex hierarchy: off-diagonal (diffusion) weights scale by 1/4 when h doubles; the
+// reaction part sigma (sum of all weights) is kept.
+void coarse_op(const double *fine, double sigma, double *coarse) {
+    coarse[1] = fine[1] * 0.25;
+    coarse[2] = fine[2] * 0.25;
+    coarse[3] = fine[3] * 0.25;
+    coarse[4] = fine[4] * 0.25;
+    coarse[0] = sigma - ((coarse[1] + coarse[2]) + (coarse[3] + coarse[4]));
+}
+
+// ---- vertex-cycle kernels (with skip support)
+
+template <typename T>
+int sweep(fx_ctx *ctx, const T *in, T *out, const T *b, const double *a5, double omega, size_t rows, size_t cols,
+          const int *skip) {
+    constexpr int U = unroll_for<T>();
+    MarchGeom G = march_geom(ctx, rows, cols, U);
+    PtJacobi<T> pt{out, b, make_a5<T>(a5), (T)(omega / a5[0]), G.rows, G.cols};
+    return launch_march<T, U, 0>(ctx, G, LoadArr<T>{in}, pt, NoFin{}, skip, "mg_sweep");
+}
+
+template <typename T>
+int residual(fx_ctx *ctx, const T *x, const T *b, T *r, const double *a5, size_t rows, size_t cols,
+             const int *skip) {
+    constexpr int U = unroll_for<T>();
+    MarchGeom G = march_geom(ctx, rows, cols, U);
+    PtResidual<T> pt{r, b, make_a5<T>(a5), G.rows, G.cols};
+    return launch_march<T, U, 0>(ctx, G, LoadArr<T>{x}, pt, NoFin{}, skip, "mg_residual");
+}
+
+template <typename T>
+int restrict_fw(fx_ctx *ctx, const T *f, T *c, size_t fcols, size_t crows, size_t ccols, const int *skip) {
+    return launch_flat<0>(ctx, crows * ccols, FlatRestrictFW<T>{f, c, fcols, crows, ccols}, NoFin{}, skip,
+                          "mg_restrict_fw");
+}
+
+template <typename T>
+int prolong_bilinear(fx_ctx *ctx, const T *c, T *f, size_t ccols, size_t frows, size_t fcols, const int *skip) {
+    return launch_flat<0>(ctx, (frows - 2) * (fcols - 2), FlatProlongBil<T>{c, f, ccols, fcols, fcols - 2}, NoFin{},
+                          skip, "mg_prolong_bilinear");
+}
+
+template <typename T>
+int zero_fill(fx_ctx *ctx, T *p, size_t n, const int *skip) {
+    return launch_flat<0>(ctx, n, FlatZero<T>{p}, NoFin{}, skip, "mg_zero");
+}
+
+// Coarsest level: all sweeps in one block, the grid held in shared memory.  Each point
+// evaluates exactly the expression of the sweep kernel, so the result is bitwise equal
+// to running `nsweeps` separate sweeps.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_coarse_solve(T *u, const T *__restrict__ b, int rows, int cols,
+                                                       A5<T> a, T wd, int nsweeps, const int *skip) {
+    if (skip && *(volatile const int *)skip) return;
+    extern __shared__ unsigned char smem_raw[];
+    T *s0 = reinterpret_cast<T *>(smem_raw);
+    T *s1 = s0 + rows * cols;
+    T *sb = s1 + rows * cols;
+    const int n = rows * cols;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        s0[i] = u[i];
+        s1[i] = u[i];
+        sb[i] = b[i];
+    }
+    __syncthreads();
+    for (int k = 0; k < nsweeps; k++) {
+        const T *src = (k & 1) ? s1 : s0;
+        T *dst = (k & 1) ? s0 : s1;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int r = i / cols, c = i % cols;
+            if (r == 0 || c == 0 || r == rows - 1 || c == cols - 1) continue;
+            Nb<T> nb;
+            nb.c = src[i];
+            nb.n = src[i - cols];
+            nb.s = src[i + cols];
+            nb.w = src[i - 1];
+            nb.e = src[i + 1];
+            dst[i] = fx_fma(wd, sb[i] - op5<T>(a, nb), nb.c);
+        }
+        __syncthreads();
+    }
+    const T *fin = (nsweeps & 1) ? s1 : s0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) u[i] = fin[i];
+}
+
+template <typename T>
+int vertex_cycle(fx_mg *mg, T *x, const T *b, const int *skip, bool x_zero) {
+    fx_ctx *ctx = mg->ctx;
+    const int nl = (int)mg->lv.size();
+    MgLevel &L0 = mg->lv[0];
+    // Level 0 iterates between x and tmp0; the ring is homogeneous Dirichlet.
+    if (!x_zero) {
+        fx_buf xb;
+        xb.ctx = ctx;
+        xb.ptr = x;
+        xb.len = L0.rows * L0.cols;
+        xb.dtype = mg->dtype;
+        xb.owned = false;
+        FX_TRY(fx_zero_boundaries(ctx, &xb, L0.rows, L0.cols));
+    }
+    std::vector<T *> cur(nl), oth(nl);
+    std::vector<const T *> rhs(nl);
+    cur[0] = x;
+    oth[0] = (T *)mg->tmp0->ptr;
+    rhs[0] = b;
+    for (int l = 1; l < nl; l++) {
+        cur[l] = (T *)mg->lv[l].u->ptr;
+        oth[l] = (T *)mg->lv[l].tmp->ptr;
+        rhs[l] = (const T *)mg->lv[l].rhs->ptr;
+    }
+    auto smooth = [&](int l, size_t n) -> int {
+        MgLevel &L = mg->lv[l];
+        for (size_t k = 0; k < n; k++) {
+            FX_TRY(sweep<T>(ctx, cur[l], oth[l], rhs[l], L.a5, mg->omega, L.rows, L.cols, skip));
+            std::swap(cur[l], oth[l]);
+        }
+        return FX_OK;
+    };
+    for (int l = 0; l < nl - 1; l++) {
+        MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
+        FX_TRY(smooth(l, mg->n_pre));
+        FX_TRY(residual<T>(ctx, cur[l], rhs[l], oth[l], L.a5, L.rows, L.cols, skip));
+        FX_TRY(restrict_fw<T>(ctx, oth[l], (T *)C.rhs->ptr, L.cols, C.rows, C.cols, skip));
+        FX_TRY(zero_fill<T>(ctx, cur[l + 1], C.rows * C.cols, skip));
+    }
+    {
+        const int l = nl - 1;
+        MgLevel &L = mg->lv[l];
+        const size_t n = L.rows * L.cols;
+        const size_t smem = 3 * n * sizeof(T);
+        if (smem <= 48 * 1024 && mg->coarse_sweeps > 0) {
+            k_coarse_solve<T><<<1, 1024, smem, ctx->stream>>>(cur[l], rhs[l], (int)L.rows, (int)L.cols,
+                                                              make_a5<T>(L.a5), (T)(mg->omega / L.a5[0]),
+                                                              (int)mg->coarse_sweeps, skip);
+            FX_TRY(check_launch(ctx, "mg_coarse_solve"));
+            // the kernel writes the final iterate back into cur[l]; cur/oth roles unchanged
+        } else {
+            FX_TRY(smooth(l, mg->coarse_sweeps));
+        }
+    }
+    for (int l = nl - 2; l >= 0; l--) {
+        MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
+        FX_TRY(prolong_bilinear<T>(ctx, cur[l + 1], cur[l], C.cols, L.rows, L.cols, skip));
+        FX_TRY(smooth(l, mg->n_post));
+    }
+    if (cur[0] != x) {
+        FX_CUDA(cudaMemcpyAsync(x, cur[0], L0.rows * L0.cols * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return FX_OK;
+}
+
+// F64 <-> F32 conversion with skip, for a single-precision cycle inside an F64 solve.
+template <typename S, typename D>
+int convert(fx_ctx *ctx, const S *src, D *dst, size_t n, const int *skip) {
+    return launch_flat<0>(ctx, n, FlatConvert<S, D>{src, dst}, NoFin{}, skip, "mg_convert");
+}
+
+// Reference-semantics cycle (multigrid.rs:188-230), built from the trait ops.
+int reference_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b, bool x_zero) {
+    fx_ctx *ctx = mg->ctx;
+    const int nl = (int)mg->lv.size();
+    MgLevel &L0 = mg->lv[0];
+    FX_TRY(fx_copy(ctx, b, L0.rhs));
+    if (x_zero) FX_TRY(fx_fill(ctx, L0.u, 0.0));
+    else FX_TRY(fx_copy(ctx, x, L0.u));
+    auto smooth = [&](int l, size_t n) -> int {
+        MgLevel &L = mg->lv[l];
+        fx_grid g{L.rows, L.cols, L.dx, L.dy};
+        fx_stencil s{5, LAP_DR, LAP_DC, L.lap5};
+        for (size_t k = 0; k < n; k++) FX_TRY(fx_weighted_jacobi(ctx, L.u, L.rhs, mg->omega, &g, &s, &mg->bc));
+        return FX_OK;
+    };
+    for (int l = 0; l < nl - 1; l++) {
+        MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
+        FX_TRY(smooth(l, mg->n_pre));
+        fx_grid g{L.rows, L.cols, L.dx, L.dy}, cg{C.rows, C.cols, C.dx, C.dy};
+        fx_stencil s{5, LAP_DR, LAP_DC, L.lap5};
+        FX_TRY(fx_apply_stencil(ctx, L.u, L.tmp, &g, &s, &mg->bc));  // multigrid.rs:476-491
+        FX_TRY(fx_scale(ctx, L.tmp, -1.0));
+        FX_TRY(fx_axpy(ctx, 1.0, L.rhs, L.tmp));
+        FX_TRY(fx_restrict(ctx, L.tmp, C.rhs, &g, &cg));
+        FX_TRY(fx_fill(ctx, C.u, 0.0));
+    }
+    FX_TRY(smooth(nl - 1, mg->n_pre + mg->n_post + 10));
+    for (int l = nl - 2; l >= 0; l--) {
+        MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
+        fx_grid g{L.rows, L.cols, L.dx, L.dy}, cg{C.rows, C.cols, C.dx, C.dy};
+        FX_TRY(fx_prolong(ctx, C.u, L.u, &cg, &g));
+        FX_TRY(smooth(l, mg->n_post));
+    }
+    return fx_copy(ctx, L0.u, x);
+}
+
+}  // namespace
+
+int fx_mg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) {
+    fx_mg *m = mg;
+    const MgLevel &L0 = m->lv[0];
+    if (z->len != L0.rows * L0.cols || r->len != z->len)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "dimension mismatch: expected " +
+                                                   std::to_string(L0.rows * L0.cols) + ", got " +
+                                                   std::to_string(z->len));
+    if (z->dtype != r->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
+    if (m->mode == 0) return reference_cycle(m, z, r, z_zero);
+    if (m->dtype == z->dtype) {
+        if (z->dtype == FX_F64) return vertex_cycle<double>(m, (double *)z->ptr, (const double *)r->ptr, skip, z_zero);
+        return vertex_cycle<float>(m, (float *)z->ptr, (const float *)r->ptr, skip, z_zero);
+    }
+    // single-precision cycle on double-precision vectors
+    if (m->dtype == FX_F32 && z->dtype == FX_F64) {
+        const size_t n = z->len;
+        float *x32 = (float *)m->x32->ptr, *b32 = (float *)m->b32->ptr;
+        FX_TRY(convert<double, float>(m->ctx, (const double *)r->ptr, b32, n, skip));
+        if (z_zero) FX_TRY(zero_fill<float>(m->ctx, x32, n, skip));
+        else FX_TRY(convert<double, float>(m->ctx, (const double *)z->ptr, x32, n, skip));
+        FX_TRY(vertex_cycle<float>(m, x32, b32, skip, z_zero));
+        return convert<float, double>(m->ctx, x32, (double *)z->ptr, n, skip);
+    }
+    return fail(FX_ERR_UNSUPPORTED, "multigrid dtype combination not supported");
+}
+
+// ================================================================ Krylov solvers
+
+namespace {
+
+struct SolverBase {
+    fx_ctx *ctx = nullptr;
+    fx_grid g{};
+    double tol = 0;
+    size_t max_iter = 0;
+    DevState *d_st = nullptr;
+    DevState *h_st = nullptr;
+    std::vector<fx_buf *> bufs;
+
+    int init_base(fx_ctx *c, const fx_grid *grid, double t, size_t mi, int nvec) {
+        ctx = c;
+        g = *grid;
+        tol = t;
+        max_iter = mi;
+        FX_CUDA(cudaMalloc(&d_st, sizeof(DevState)));
+        FX_CUDA(cudaMallocHost(&h_st, sizeof(DevState)));
+        for (int i = 0; i < nvec; i++) {
+            fx_buf *b = nullptr;
+            FX_TRY(fx_alloc(ctx, g.rows * g.cols, FX_F64, &b));
+            bufs.push_back(b);
+        }
+        return FX_OK;
+    }
+    virtual ~SolverBase() {
+        if (ctx) cudaStreamSynchronize(ctx->stream);
+        for (auto *b : bufs) fx_free(b);
+        if (d_st) cudaFree(d_st);
+        if (h_st) cudaFreeHost(h_st);
+    }
+    int reset_state() {
+        DevState s;
+        std::memset(&s, 0, sizeof(s));
+        s.tol = tol;
+        s.max_iter = (long long)max_iter;
+        *h_st = s;
+        FX_CUDA(cudaMemcpyAsync(d_st, h_st, sizeof(DevState), cudaMemcpyHostToDevice, ctx->stream));
+        return FX_OK;
+    }
+    int read_state() {
+        FX_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+        FX_CUDA(cudaStreamSynchronize(ctx->stream));
+        return FX_OK;
+    }
+    int check_io(const fx_buf *x, const fx_buf *b) {
+        FX_TRY(check_buf(x, "x"));
+        FX_TRY(check_buf(b, "b"));
+        FX_TRY(check_grid_len(&g, x));
+        FX_TRY(check_grid_len(&g, b));
+        if (x->dtype != FX_F64 || b->dtype != FX_F64)
+            return fail(FX_ERR_INVALID_ARGUMENT, "solver vectors must be F64");
+        return FX_OK;
+    }
+    // Run `step(i)` for i = 0, 1, ... until the device says done.  Iterations are enqueued
+    // in batches sized from the observed convergence rate; surplus iterations are no-ops.
+    template <typename Step>
+    int drive(Step step, size_t max_launch, bool expensive) {
+        FX_TRY(read_state());
+        if (h_st->done) return FX_OK;
+        size_t launched = 0;
+        const double r0 = h_st->resid > 0 ? h_st->resid : 1.0;
+        size_t batch = expensive ? 1 : 4;
+        while (launched < max_launch) {
+            const size_t nb = std::min(batch, max_launch - launched);
+            for (size_t k = 0; k < nb; k++) FX_TRY(step(launched + k));
+            launched += nb;
+            FX_TRY(read_state());
+            if (h_st->done) return FX_OK;
+            // predict the iterations still needed from the mean reduction rate so far
+            const double rk = h_st->resid;
+            size_t pred = 1;
+            if (rk > 0 && rk < r0 && launched > 0 && h_st->tol > 0) {
+                const double rate = std::log(rk / r0) / (double)launched;
+                const double need = std::log(h_st->tol / rk) / rate;
+                if (need > 1 && need < 1e6) pred = (size_t)std::ceil(need);
+            } else {
+                pred = batch * 2;
+            }
+            batch = std::max<size_t>(1, std::min<size_t>(pred, expensive ? 8 : 128));
+        }
+        return read_state();
+    }
+    void stats(fx_stats *out) {
+        out->iterations = (size_t)h_st->iter;
+        out->residual = h_st->resid;
+        out->reason = h_st->reason;
+    }
+};
+
+#define SOLVER_MODE_DISPATCH(P, ...)     \
+    do {                                 \
+        if ((P).mode == 5) {             \
+            constexpr int MODE = 5;      \
+            __VA_ARGS__;                 \
+        } else if ((P).mode == 9) {      \
+            constexpr int MODE = 9;      \
+            __VA_ARGS__;                 \
+        } else {                         \
+            constexpr int MODE = 0;      \
+            __VA_ARGS__;                 \
+        }                                \
+    } while (0)
+
+int prep_op(const fx_grid &g, const fx_stencil *st, const fx_boundaries *bc, StencilP *P) {
+    BcP B;
+    FX_TRY(make_bc(bc, g.dx, g.dy, &B, true));
+    return make_stencil(st, P);
+}
+
+// ------------------------------------------------ CG / PCG kernels (cg.rs:96-256)
+
+// r = b - A x (cg.rs:104-111); reduction r.r
+template <typename T, int MODE>
+struct PtInitResid {
+    OpA<T, MODE> A;
+    const T *b;
+    T *r;
+    T *r2;  // optional second copy (BiCGSTAB r_hat)
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        const T ax = A.apply(rr, c, nb);
+        const T rv = fx_fma((T)-1, ax, b[idx]);
+        r[idx] = rv;
+        if (r2) r2[idx] = rv;
+        csum_add_prod(acc[0], (double)rv, (double)rv);
+    }
+};
+
+struct FinCgInit {  // unpreconditioned: rs_old = r.r; loop-top test of iteration 0
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->rs_old = v[0];
+        S->beta = 0.0;
+        S->iter = 0;
+        S->resid = sqrt(v[0]);
+        S->r0 = S->resid;
+        if (S->max_iter == 0) st_finish(S, FX_MAX_ITERATIONS, 0, sqrt(v[0]));
+        else if (sqrt(v[0]) < S->tol) st_finish(S, FX_CONVERGED, 0, sqrt(v[0]));
+    }
+};
+
+// p_new = (r|z) + beta p_old; ap = A p_new; reduction p.ap
+template <typename T, int MODE>
+struct PtCgDir {
+    OpA<T, MODE> A;
+    T *p_new;
+    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        p_new[idx] = nb.c;
+        const T ap = A.apply(r, c, nb);
+        csum_add_prod(acc[0], (double)nb.c, (double)ap);
+    }
+};
+
+struct FinCgDir {  // alpha = rs_old / p.ap, breakdown test (cg.rs:133-142)
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        const double p_ap = v[0];
+        if (fabs(p_ap) < 1e-30) {
+            st_finish(S, FX_BREAKDOWN, S->iter, S->resid);
+            return;
+        }
+        S->alpha = S->rs_old / p_ap;
+    }
+};
+
+// x += alpha p; r -= alpha A p (A p recomputed from p); reduction r.r
+template <typename T, int MODE>
+struct PtCgUpd {
+    OpA<T, MODE> A;
+    T *x, *r;
+    const DevState *S;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        const T alpha = (T)S->alpha;
+        const T ap = A.apply(rr, c, nb);
+        x[idx] = fx_fma(alpha, nb.c, x[idx]);
+        const T rv = fx_fma(-alpha, ap, r[idx]);
+        r[idx] = rv;
+        csum_add_prod(acc[0], (double)rv, (double)rv);
+    }
+};
+
+struct FinCgUpd {  // beta = rs_new / rs_old; loop-top test of the next iteration
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        const double rs_new = v[0];
+        S->beta = rs_new / S->rs_old;
+        S->rs_old = rs_new;
+        S->iter += 1;
+        S->resid = sqrt(rs_new);
+        if (S->iter >= S->max_iter) st_finish(S, FX_MAX_ITERATIONS, S->max_iter, sqrt(rs_new));
+        else if (sqrt(rs_new) < S->tol) st_finish(S, FX_CONVERGED, S->iter, sqrt(rs_new));
+    }
+};
+
+// PCG: after r update, rr stored; stop test; then z = M^-1 r; rz = r.z -> beta
+struct FinPcgResid {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->rr = v[0];
+        S->resid = sqrt(v[0]);
+    }
+};
+
+struct FinPcgUpd {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->rr = v[0];
+        S->iter += 1;
+        S->resid = sqrt(v[0]);
+        if (S->iter >= S->max_iter) st_finish(S, FX_MAX_ITERATIONS, S->max_iter, sqrt(v[0]));
+        else if (sqrt(v[0]) < S->tol) st_finish(S, FX_CONVERGED, S->iter, sqrt(v[0]));
+    }
+};
+
+struct FinPcgRzInit {  // rz_old = r.z, beta = 0, loop-top test of iteration 0 (cg.rs:202-212)
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->rs_old = v[0];
+        S->beta = 0.0;
+        S->iter = 0;
+        S->r0 = S->resid;
+        if (S->max_iter == 0) st_finish(S, FX_MAX_ITERATIONS, 0, S->resid);
+        else if (S->resid < S->tol) st_finish(S, FX_CONVERGED, 0, S->resid);
+    }
+};
+
+struct FinPcgRz {  // beta = rz_new / rz_old (cg.rs:240-247)
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->beta = v[0] / S->rs_old;
+        S->rs_old = v[0];
+    }
+};
+
+}  // namespace
+
+struct fx_cg : SolverBase {
+    // bufs: 0 r, 1 z, 2 p0, 3 p1
+};
+
+namespace {
+
+template <int MODE>
+int cg_solve_impl(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
+    using T = double;
+    fx_ctx *ctx = s->ctx;
+    constexpr int U = unroll_for<T>();
+    MarchGeom G = march_geom(ctx, s->g.rows, s->g.cols, U);
+    OpA<T, MODE> A{P, (T)coeff, G.rows, G.cols};
+    T *r = (T *)s->bufs[0]->ptr, *z = (T *)s->bufs[1]->ptr;
+    T *pb[2] = {(T *)s->bufs[2]->ptr, (T *)s->bufs[3]->ptr};
+    T *xp = (T *)x->ptr;
+    const T *bp = (const T *)b->ptr;
+    const size_t n = s->g.rows * s->g.cols;
+    DevState *S = s->d_st;
+    const int *halt = &S->halt;
+    FX_TRY(s->reset_state());
+    FX_CUDA(cudaMemsetAsync(pb[0], 0, n * sizeof(T), ctx->stream));
+    FX_CUDA(cudaMemsetAsync(pb[1], 0, n * sizeof(T), ctx->stream));
+    if (!pc) {
+        FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, r, nullptr}, FinCgInit{S},
+                                      nullptr, "cg_init")));
+        auto step = [&](size_t i) -> int {
+            T *po = pb[i & 1], *pn = pb[(i + 1) & 1];
+            FX_TRY((launch_march<T, U, 1>(ctx, G, LdAypx<T>{r, po, S}, PtCgDir<T, MODE>{A, pn}, FinCgDir{S}, halt,
+                                          "cg_dir")));
+            return launch_march<T, U, 1>(ctx, G, Ld1<T>{pn}, PtCgUpd<T, MODE>{A, xp, r, S}, FinCgUpd{S}, halt,
+                                         "cg_update");
+        };
+        return s->drive(step, s->max_iter + 1, n >= (1u << 20));
+    }
+    // preconditioned (cg.rs:178-256)
+    FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, r, nullptr}, FinPcgResid{S},
+                                  nullptr, "pcg_init")));
+    fx_buf rb{ctx, r, n, FX_F64, false}, zb{ctx, z, n, FX_F64, false};
+    FX_TRY(zero_fill<T>(ctx, z, n, nullptr));
+    FX_TRY(pc->apply(&zb, &rb, halt, true));
+    FX_TRY(launch_flat<1>(ctx, n, FlatDot<T>{r, z}, FinPcgRzInit{S}, halt, "pcg_rz"));
+    auto step = [&](size_t i) -> int {
+        T *po = pb[i & 1], *pn = pb[(i + 1) & 1];
+        FX_TRY((launch_march<T, U, 1>(ctx, G, LdAypx<T>{z, po, S}, PtCgDir<T, MODE>{A, pn}, FinCgDir{S}, halt,
+                                      "pcg_dir")));
+        FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{pn}, PtCgUpd<T, MODE>{A, xp, r, S}, FinPcgUpd{S}, halt,
+                                      "pcg_update")));
+        FX_TRY(zero_fill<T>(ctx, z, n, halt));
+        FX_TRY(pc->apply(&zb, &rb, halt, true));
+        return launch_flat<1>(ctx, n, FlatDot<T>{r, z}, FinPcgRz{S}, halt, "pcg_rz");
+    };
+    return s->drive(step, s->max_iter + 1, true);
+}
+
+// ------------------------------------------------ pipelined CG (pipelined_cg.rs:353-424)
+
+template <typename T, int MODE>
+struct PtPipeInitQ {  // q = A x; r = b - q
+    OpA<T, MODE> A;
+    const T *b;
+    T *r;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *) const {
+        r[idx] = fx_fma((T)-1, A.apply(rr, c, nb), b[idx]);
+    }
+};
+
+template <typename T, int MODE>
+struct PtPipeInitW {  // w = A r; p = t = z = 0; reductions (r.r, r.w)
+    OpA<T, MODE> A;
+    T *w, *p, *t, *z;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        const T wv = A.apply(rr, c, nb);
+        w[idx] = wv;
+        p[idx] = (T)0;
+        t[idx] = (T)0;
+        z[idx] = (T)0;
+        csum_add_prod(acc[0], (double)nb.c, (double)nb.c);
+        csum_add_prod(acc[1], (double)nb.c, (double)wv);
+    }
+};
+
+__device__ __forceinline__ void pipe_scalars(DevState *S) {
+    const double beta = S->gamma / S->gamma_prev;
+    S->beta = beta;
+    S->alpha = S->gamma / (S->delta - beta * S->gamma / S->alpha_prev);
+}
+
+struct FinPipeInit {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->gamma = v[0];
+        S->delta = v[1];
+        S->gamma_prev = INFINITY;
+        S->alpha_prev = INFINITY;
+        S->iter = 0;
+        S->resid = sqrt(v[0]);
+        S->r0 = S->resid;
+        if (S->max_iter == 0) st_finish(S, FX_MAX_ITERATIONS, 0, sqrt(v[0]));
+        else if (sqrt(v[0]) < S->tol) st_finish(S, FX_CONVERGED, 0, sqrt(v[0]));
+        else pipe_scalars(S);
+    }
+};
+
+// One whole iteration: q = A w (on the fly), the 6-way update, and (r.r, r.w) of the
+// updated vectors for the next iteration's scalars.
+template <typename T, int MODE>
+struct PtPipeIter {
+    OpA<T, MODE> A;
+    T *z, *t, *p, *x, *r, *w_new;
+    const DevState *S;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        const T alpha = (T)S->alpha, beta = (T)S->beta;
+        const T q = A.apply(rr, c, nb);
+        const T w = nb.c;
+        const T zn = q + z[idx] * beta;
+        const T tn = w + t[idx] * beta;
+        const T pn = r[idx] + p[idx] * beta;
+        z[idx] = zn;
+        t[idx] = tn;
+        p[idx] = pn;
+        x[idx] = fx_fma(alpha, pn, x[idx]);
+        const T rn = fx_fma(-alpha, tn, r[idx]);
+        const T wn = fx_fma(-alpha, zn, w);
+        r[idx] = rn;
+        w_new[idx] = wn;
+        csum_add_prod(acc[0], (double)rn, (double)rn);
+        csum_add_prod(acc[1], (double)rn, (double)wn);
+    }
+};
+
+struct FinPipeIter {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->gamma_prev = S->gamma;
+        S->alpha_prev = S->alpha;
+        S->gamma = v[0];
+        S->delta = v[1];
+        S->iter += 1;
+        S->resid = sqrt(v[0]);
+        if (S->iter >= S->max_iter) st_finish(S, FX_MAX_ITERATIONS, S->max_iter, sqrt(v[0]));
+        else if (sqrt(v[0]) < S->tol) st_finish(S, FX_CONVERGED, S->iter, sqrt(v[0]));
+        else pipe_scalars(S);
+    }
+};
+
+}  // namespace
+
+struct fx_pipelined_cg : SolverBase {
+    // bufs: 0 r, 1 p, 2 t, 3 z, 4 w0, 5 w1
+};
+
+namespace {
+
+template <int MODE>
+int pipe_solve_impl(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P) {
+    using T = double;
+    fx_ctx *ctx = s->ctx;
+    constexpr int U = unroll_for<T>();
+    MarchGeom G = march_geom(ctx, s->g.rows, s->g.cols, U);
+    OpA<T, MODE> A{P, (T)coeff, G.rows, G.cols};
+    T *r = (T *)s->bufs[0]->ptr, *p = (T *)s->bufs[1]->ptr, *t = (T *)s->bufs[2]->ptr, *z = (T *)s->bufs[3]->ptr;
+    T *w[2] = {(T *)s->bufs[4]->ptr, (T *)s->bufs[5]->ptr};
+    T *xp = (T *)x->ptr;
+    const T *bp = (const T *)b->ptr;
+    DevState *S = s->d_st;
+    const int *halt = &S->halt;
+    FX_TRY(s->reset_state());
+    FX_TRY((launch_march<T, U, 0>(ctx, G, Ld1<T>{xp}, PtPipeInitQ<T, MODE>{A, bp, r}, NoFin{}, nullptr, "pipe_init_q")));
+    FX_TRY((launch_march<T, U, 2>(ctx, G, Ld1<T>{r}, PtPipeInitW<T, MODE>{A, w[0], p, t, z}, FinPipeInit{S}, nullptr,
+                                  "pipe_init_w")));
+    auto step = [&](size_t i) -> int {
+        T *wo = w[i & 1], *wn = w[(i + 1) & 1];
+        return launch_march<T, U, 2>(ctx, G, Ld1<T>{wo}, PtPipeIter<T, MODE>{A, z, t, p, xp, r, wn, S},
+                                     FinPipeIter{S}, halt, "pipe_iter");
+    };
+    return s->drive(step, s->max_iter + 1, s->g.rows * s->g.cols >= (1u << 22));
+}
+
+// ------------------------------------------------ BiCGSTAB (bicgstab.rs:90-346)
+
+__device__ __forceinline__ void bicg_top(DevState *S, double rr, double rho_new) {
+    // loop-top of iteration S->iter: ||r|| test, rho = r_hat.r breakdown test, beta
+    const double r_norm = sqrt(rr);
+    S->r_norm = r_norm;
+    S->resid = r_norm;
+    if (S->iter >= S->max_iter) {
+        st_finish(S, FX_MAX_ITERATIONS, S->max_iter, r_norm);
+        return;
+    }
+    if (r_norm < S->tol) {
+        st_finish(S, FX_CONVERGED, S->iter, r_norm);
+        return;
+    }
+    S->rho_new = rho_new;
+    if (fabs(rho_new) < 1e-30) {
+        st_finish(S, FX_BREAKDOWN, S->iter, r_norm);
+        return;
+    }
+    S->beta = (rho_new / S->rho) * (S->alpha / S->omega);
+}
+
+struct FinBicgInit {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->rho = 1.0;
+        S->alpha = 1.0;
+        S->omega = 1.0;
+        S->iter = 0;
+        S->r0 = sqrt(v[0]);
+        bicg_top(S, v[0], v[1]);
+    }
+};
+
+// p_new = r + beta (p_old - omega v_old), rounded as p.axpy(-omega, v); p.scale(beta); p.axpy(1, r)
+template <typename T>
+struct LdBicgP {
+    const T *r, *p, *v;
+    const DevState *S;
+    __device__ __forceinline__ T operator()(size_t i) const {
+        const T beta = (T)S->beta, omega = (T)S->omega;
+        return r[i] + fx_fma(-omega, v[i], p[i]) * beta;
+    }
+};
+
+// v = A (p or p_hat); store p_new when marching the fused p; reduction r_hat.v
+template <typename T, int MODE>
+struct PtBicgV {
+    OpA<T, MODE> A;
+    T *p_store;  // null when the marched field is already stored (p_hat)
+    T *v;
+    const T *r_hat;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        if (p_store) p_store[idx] = nb.c;
+        const T vv = A.apply(rr, c, nb);
+        v[idx] = vv;
+        csum_add_prod(acc[0], (double)r_hat[idx], (double)vv);
+    }
+};
+
+struct FinBicgRv {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        const double rv = v[0];
+        if (fabs(rv) < 1e-30) {
+            st_finish(S, FX_BREAKDOWN, S->iter, S->r_norm);
+            return;
+        }
+        S->alpha = S->rho_new / rv;
+    }
+};
+
+struct FinBicgS {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->s_norm = sqrt(v[0]);
+        if (S->s_norm < S->tol) {
+            S->pending = 1;
+            S->halt = 1;
+        }
+    }
+};
+
+// t = A (s or s_hat); reductions (t.s, t.t)
+template <typename T, int MODE>
+struct PtBicgT {
+    OpA<T, MODE> A;
+    T *t;
+    const T *s;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        const T tv = A.apply(rr, c, nb);
+        t[idx] = tv;
+        csum_add_prod(acc[0], (double)tv, (double)s[idx]);
+        csum_add_prod(acc[1], (double)tv, (double)tv);
+    }
+};
+
+struct FinBicgT {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        const double ts = v[0], tt = v[1];
+        if (fabs(tt) < 1e-30) {
+            S->pending = 2;
+            S->halt = 1;
+            return;
+        }
+        S->omega = ts / tt;
+    }
+};
+
+struct FinBicgEnd {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        if (S->pending) {
+            st_finish(S, S->pending == 1 ? FX_CONVERGED : FX_BREAKDOWN, S->iter, S->s_norm);
+            return;
+        }
+        S->rho = S->rho_new;
+        S->iter += 1;
+        bicg_top(S, v[0], v[1]);
+    }
+};
+
+// s = r - alpha v; reduction s.s (bicgstab.rs:159-164)
+template <typename T>
+struct FlatBicgS {
+    const T *r, *v;
+    T *s;
+    const DevState *S;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        const T sv = fx_fma(-(T)S->alpha, v[i], r[i]);
+        s[i] = sv;
+        csum_add_prod(acc[0], (double)sv, (double)sv);
+    }
+};
+
+// x += alpha pp + omega ss; r = s - omega t; reductions (r.r, r_hat.r) (bicgstab.rs:193-201).
+// With a pending early exit only x += alpha pp is due (bicgstab.rs:165-172, :183-190).
+template <typename T>
+struct FlatBicgFinish {
+    T *x, *r;
+    const T *pp, *ss, *t, *s, *rh;
+    const DevState *S;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        const T alpha = (T)S->alpha;
+        if (S->pending) {
+            x[i] = fx_fma(alpha, pp[i], x[i]);
+            return;
+        }
+        const T omega = (T)S->omega;
+        x[i] = fx_fma(omega, ss[i], fx_fma(alpha, pp[i], x[i]));
+        const T rv = fx_fma(-omega, t[i], s[i]);
+        r[i] = rv;
+        csum_add_prod(acc[0], (double)rv, (double)rv);
+        csum_add_prod(acc[1], (double)rh[i], (double)rv);
+    }
+};
+
+// p = r + beta (p - omega v) in place (bicgstab.rs:266-269)
+template <typename T>
+struct FlatBicgP {
+    T *p;
+    const T *r, *v;
+    const DevState *S;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const {
+        const T beta = (T)S->beta, omega = (T)S->omega;
+        p[i] = r[i] + fx_fma(-omega, v[i], p[i]) * beta;
+    }
+};
+
+// r = b - A x; r_hat = r; reductions (r.r, r_hat.r)
+template <typename T, int MODE>
+struct PtBicgInit {
+    OpA<T, MODE> A;
+    const T *b;
+    T *r, *rh;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        const T rv = fx_fma((T)-1, A.apply(rr, c, nb), b[idx]);
+        r[idx] = rv;
+        rh[idx] = rv;
+        csum_add_prod(acc[0], (double)rv, (double)rv);
+        csum_add_prod(acc[1], (double)rv, (double)rv);
+    }
+};
+
+}  // namespace
+
+struct fx_bicgstab : SolverBase {
+    // bufs: 0 r, 1 r_hat, 2 p0, 3 p1, 4 v0, 5 v1, 6 s, 7 t, 8 ph, 9 sh
+};
+
+namespace {
+
+template <int MODE>
+int bicg_solve_impl(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
+    using T = double;
+    fx_ctx *ctx = s->ctx;
+    constexpr int U = unroll_for<T>();
+    MarchGeom G = march_geom(ctx, s->g.rows, s->g.cols, U);
+    OpA<T, MODE> A{P, (T)coeff, G.rows, G.cols};
+    const size_t n = s->g.rows * s->g.cols;
+    T *r = (T *)s->bufs[0]->ptr, *rh = (T *)s->bufs[1]->ptr;
+    T *pb[2] = {(T *)s->bufs[2]->ptr, (T *)s->bufs[3]->ptr};
+    T *vb[2] = {(T *)s->bufs[4]->ptr, (T *)s->bufs[5]->ptr};
+    T *sv = (T *)s->bufs[6]->ptr, *tv = (T *)s->bufs[7]->ptr, *ph = (T *)s->bufs[8]->ptr, *sh = (T *)s->bufs[9]->ptr;
+    T *xp = (T *)x->ptr;
+    const T *bp = (const T *)b->ptr;
+    DevState *S = s->d_st;
+    const int *halt = &S->halt;
+    const int *done = &S->done;
+    FX_TRY(s->reset_state());
+    for (int k = 0; k < 2; k++) {
+        FX_CUDA(cudaMemsetAsync(pb[k], 0, n * sizeof(T), ctx->stream));
+        FX_CUDA(cudaMemsetAsync(vb[k], 0, n * sizeof(T), ctx->stream));
+    }
+    // r = b - A x; r_hat = r; (r.r, r_hat.r)
+    FX_TRY((launch_march<T, U, 2>(ctx, G, Ld1<T>{xp}, PtBicgInit<T, MODE>{A, bp, r, rh}, FinBicgInit{S}, nullptr,
+                                  "bicg_init")));
+    auto s_update = [&](const T *v) -> int {
+        return launch_flat<1>(ctx, n, FlatBicgS<T>{r, v, sv, S}, FinBicgS{S}, halt, "bicg_s");
+    };
+    auto finish = [&](const T *pp, const T *ss) -> int {
+        return launch_flat<2>(ctx, n, FlatBicgFinish<T>{xp, r, pp, ss, tv, sv, rh, S}, FinBicgEnd{S}, done,
+                              "bicg_finish");
+    };
+    if (!pc) {
+        auto step = [&](size_t i) -> int {
+            T *po = pb[i & 1], *pn = pb[(i + 1) & 1], *vo = vb[i & 1], *vn = vb[(i + 1) & 1];
+            FX_TRY((launch_march<T, U, 1>(ctx, G, LdBicgP<T>{r, po, vo, S}, PtBicgV<T, MODE>{A, pn, vn, rh},
+                                          FinBicgRv{S}, halt, "bicg_pv")));
+            FX_TRY(s_update(vn));
+            FX_TRY((launch_march<T, U, 2>(ctx, G, Ld1<T>{sv}, PtBicgT<T, MODE>{A, tv, sv}, FinBicgT{S}, halt,
+                                          "bicg_t")));
+            return finish(pn, sv);
+        };
+        return s->drive(step, s->max_iter + 1, n >= (1u << 21));
+    }
+    T *p = pb[0], *v = vb[0];
+    fx_buf pbuf{ctx, p, n, FX_F64, false}, phb{ctx, ph, n, FX_F64, false};
+    fx_buf sbuf{ctx, sv, n, FX_F64, false}, shb{ctx, sh, n, FX_F64, false};
+    auto step = [&](size_t) -> int {
+        FX_TRY(launch_flat<0>(ctx, n, FlatBicgP<T>{p, r, v, S}, NoFin{}, halt, "bicg_p"));
+        FX_TRY(zero_fill<T>(ctx, ph, n, halt));
+        FX_TRY(pc->apply(&phb, &pbuf, halt, true));
+        FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{ph}, PtBicgV<T, MODE>{A, nullptr, v, rh}, FinBicgRv{S}, halt,
+                                      "bicg_v")));
+        FX_TRY(s_update(v));
+        FX_TRY(zero_fill<T>(ctx, sh, n, halt));
+        FX_TRY(pc->apply(&shb, &sbuf, halt, true));
+        FX_TRY((launch_march<T, U, 2>(ctx, G, Ld1<T>{sh}, PtBicgT<T, MODE>{A, tv, sv}, FinBicgT{S}, halt, "bicg_t")));
+        return finish(ph, sh);
+    };
+    return s->drive(step, s->max_iter + 1, true);
+}
+
+}  // namespace
+
+// ------------------------------------------------ GMRES (gmres.rs:463-837)
+
+struct fx_gmres : SolverBase {
+    size_t restart = 30;
+    double *d_h = nullptr;  // device column of dots
+    double *h_h = nullptr;
+    std::vector<double> hh, cc, ss, grs;
+    std::vector<fx_buf *> vv;  // m+1 basis vectors (bufs[0..m]); w = bufs[m+1]
+    ~fx_gmres() {
+        if (d_h) cudaFree(d_h);
+        if (h_h) cudaFreeHost(h_h);
+    }
+};
+
+namespace {
+
+struct FinSlot {
+    double *dst;
+    __device__ void operator()(const double *v) const { *dst = v[0]; }
+};
+
+template <typename T, int MODE>
+struct PtGmResid {  // out = b - A x (gmres.rs:477-485); reduction out.out
+    OpA<T, MODE> A;
+    const T *b;
+    T *out;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        const T ax = A.apply(rr, c, nb);
+        const T v = fx_fma((T)1, b[idx], -ax);
+        out[idx] = v;
+        csum_add_prod(acc[0], (double)v, (double)v);
+    }
+};
+
+template <typename T, int MODE>
+struct PtGmAv {  // w = A v; reduction w.v0 (when v0 given)
+    OpA<T, MODE> A;
+    T *w;
+    const T *v0;
+    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+        const T wv = A.apply(rr, c, nb);
+        w[idx] = wv;
+        if (v0) csum_add_prod(acc[0], (double)wv, (double)v0[idx]);
+    }
+};
+
+template <typename T>
+struct FlatGmBuild {  // x += y_j v_j, j in order (gmres.rs:832-835)
+    T *x;
+    const T *v[8];
+    T y[8];
+    int cnt;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const {
+        T xv = x[i];
+        for (int j = 0; j < cnt; j++) xv = fx_fma(y[j], v[j][i], xv);
+        x[i] = xv;
+    }
+};
+
+template <typename T>
+struct FlatGmPcCopy {  // w = M^-1 A v_k (held in src); reduction w.v0
+    T *w;
+    const T *src, *v0;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        const T wv = src[i];
+        w[i] = wv;
+        csum_add_prod(acc[0], (double)wv, (double)v0[i]);
+    }
+};
+
+template <typename T>
+struct FlatGmMgs {  // w -= h_j v_j; reduction w.v_{j+1} (or w.w after the last)
+    T *w;
+    const T *vj, *vn;
+    const double *hj;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        const T wv = fx_fma(-(T)(*hj), vj[i], w[i]);
+        w[i] = wv;
+        if (vn) csum_add_prod(acc[0], (double)wv, (double)vn[i]);
+        else csum_add_prod(acc[0], (double)wv, (double)wv);
+    }
+};
+
+template <int MODE>
+int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
+    using T = double;
+    fx_ctx *ctx = s->ctx;
+    constexpr int U = unroll_for<T>();
+    MarchGeom G = march_geom(ctx, s->g.rows, s->g.cols, U);
+    OpA<T, MODE> A{P, (T)coeff, G.rows, G.cols};
+    const size_t n = s->g.rows * s->g.cols, m = s->restart, mp1 = m + 1;
+    std::vector<T *> V(mp1);
+    for (size_t i = 0; i < mp1; i++) V[i] = (T *)s->bufs[i]->ptr;
+    T *w = (T *)s->bufs[mp1]->ptr;
+    T *xp = (T *)x->ptr;
+    const T *bp = (const T *)b->ptr;
+    double *dh = s->d_h;
+    auto H = [&](size_t i, size_t j) -> double & { return s->hh[j * mp1 + i]; };
+    size_t total_its = 0;
+    fx_stats st{0, 0.0, FX_CONVERGED};
+
+    auto read_h = [&](size_t k) -> int {
+        FX_CUDA(cudaMemcpyAsync(s->h_h, dh, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        FX_CUDA(cudaStreamSynchronize(ctx->stream));
+        return FX_OK;
+    };
+    auto scale_into = [&](T *dst, const T *src, double f) -> int {  // copy_from + scale(f)
+        return launch_flat<0>(ctx, n, FlatScaleInto<T>{dst, src, (T)f}, NoFin{}, nullptr, "gmres_scale");
+    };
+    auto build_solution = [&](size_t k) -> int {  // gmres.rs:808-837
+        if (k == 0) return FX_OK;
+        std::vector<double> y(k, 0.0);
+        for (size_t ii = k; ii-- > 0;) {
+            double sacc = s->grs[ii];
+            for (size_t j = ii + 1; j < k; j++) sacc -= s->hh[j * mp1 + ii] * y[j];
+            const double diag = s->hh[ii * mp1 + ii];
+            if (std::fabs(diag) < 1e-30) break;
+            y[ii] = sacc / diag;
+        }
+        // x += y_i v_i in order i = 0..k-1, one pass (same per-element sequence of fma)
+        for (size_t i0 = 0; i0 < k; i0 += 8) {
+            const size_t cnt = std::min<size_t>(8, k - i0);
+            FlatGmBuild<T> fb;
+            fb.x = xp;
+            for (size_t j = 0; j < cnt; j++) {
+                fb.v[j] = V[i0 + j];
+                fb.y[j] = (T)y[i0 + j];
+            }
+            fb.cnt = (int)cnt;
+            FX_TRY(launch_flat<0>(ctx, n, fb, NoFin{}, nullptr, "gmres_build"));
+        }
+        return FX_OK;
+    };
+    fx_buf wb{ctx, w, n, FX_F64, false};
+    for (;;) {
+        double beta;
+        if (!pc) {
+            FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{xp}, PtGmResid<T, MODE>{A, bp, V[0]}, FinSlot{dh}, nullptr,
+                                          "gmres_resid")));
+            FX_TRY(read_h(0));
+            beta = std::sqrt(s->h_h[0]);
+        } else {
+            FX_TRY((launch_march<T, U, 0>(ctx, G, Ld1<T>{xp}, PtGmResid<T, MODE>{A, bp, w}, NoFin{}, nullptr, "gmres_resid")));
+            fx_buf v0b{ctx, V[0], n, FX_F64, false};
+            FX_TRY(zero_fill<T>(ctx, V[0], n, nullptr));
+            FX_TRY(pc->apply(&v0b, &wb, nullptr, true));
+            T *v0 = V[0];
+            FX_TRY(launch_flat<1>(ctx, n, FlatDot<T>{v0, v0}, FinSlot{dh}, nullptr, "gmres_beta"));
+            FX_TRY(read_h(0));
+            beta = std::sqrt(s->h_h[0]);
+        }
+        if (beta < s->tol) {
+            st = {total_its, beta, FX_CONVERGED};
+            break;
+        }
+        FX_TRY(scale_into(V[0], V[0], 1.0 / beta));
+        std::fill(s->grs.begin(), s->grs.end(), 0.0);
+        s->grs[0] = beta;
+        std::fill(s->hh.begin(), s->hh.end(), 0.0);
+        double cur_resid = beta;
+        size_t k = 0;
+        bool finished = false;
+        while (k < m) {
+            if (total_its >= s->max_iter) {
+                FX_TRY(build_solution(k));
+                st = {total_its, cur_resid, FX_MAX_ITERATIONS};
+                finished = true;
+                break;
+            }
+            // w = A v_k (+ left preconditioning), then modified Gram-Schmidt with every dot
+            // fused into the preceding AXPY
+            if (!pc) {
+                FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{V[k]}, PtGmAv<T, MODE>{A, w, V[0]}, FinSlot{dh + 0}, nullptr,
+                                              "gmres_av")));
+            } else {
+                FX_TRY((launch_march<T, U, 0>(ctx, G, Ld1<T>{V[k]}, PtGmAv<T, MODE>{A, w, nullptr}, NoFin{}, nullptr,
+                                              "gmres_av")));
+                fx_buf vk1{ctx, V[k + 1], n, FX_F64, false};
+                FX_TRY(zero_fill<T>(ctx, V[k + 1], n, nullptr));
+                FX_TRY(pc->apply(&vk1, &wb, nullptr, true));
+                T *src = V[k + 1], *v0 = V[0];
+                FX_TRY(launch_flat<1>(ctx, n, FlatGmPcCopy<T>{w, src, v0}, FinSlot{dh + 0}, nullptr, "gmres_pc_copy"));
+            }
+            for (size_t j = 0; j <= k; j++) {
+                const T *vj = V[j];
+                const T *vn = j < k ? V[j + 1] : nullptr;
+                const double *hj = dh + j;
+                FX_TRY(launch_flat<1>(ctx, n, FlatGmMgs<T>{w, vj, vn, hj}, FinSlot{dh + j + 1}, nullptr, "gmres_mgs"));
+            }
+            FX_TRY(read_h(k));
+            for (size_t j = 0; j <= k; j++) H(j, k) = s->h_h[j];
+            const double h_kp1_k = std::sqrt(s->h_h[k + 1]);
+            H(k + 1, k) = h_kp1_k;
+            if (h_kp1_k > 1e-30) FX_TRY(scale_into(V[k + 1], w, 1.0 / h_kp1_k));
+            for (size_t j = 0; j < k; j++) {
+                const double h_j = H(j, k), h_jp1 = H(j + 1, k), cj = s->cc[j], sj = s->ss[j];
+                H(j, k) = std::fma(cj, h_j, sj * h_jp1);
+                H(j + 1, k) = std::fma(cj, h_jp1, -sj * h_j);
+            }
+            const double a = H(k, k), bv = H(k + 1, k);
+            const double rr = std::hypot(a, bv);
+            if (std::fabs(rr) < 1e-30) {
+                FX_TRY(build_solution(k));
+                st = {total_its, cur_resid, FX_BREAKDOWN};
+                finished = true;
+                break;
+            }
+            s->cc[k] = a / rr;
+            s->ss[k] = bv / rr;
+            H(k, k) = rr;
+            H(k + 1, k) = 0.0;
+            const double g_k = s->grs[k];
+            s->grs[k] = s->cc[k] * g_k;
+            s->grs[k + 1] = -s->ss[k] * g_k;
+            cur_resid = std::fabs(s->grs[k + 1]);
+            total_its++;
+            k++;
+            if (cur_resid < s->tol) break;
+            if (h_kp1_k <= 1e-30) break;
+        }
+        if (finished) break;
+        FX_TRY(build_solution(k));
+        if (cur_resid < s->tol) {
+            st = {total_its, cur_resid, FX_CONVERGED};
+            break;
+        }
+        if (total_its >= s->max_iter) {
+            st = {total_its, cur_resid, FX_MAX_ITERATIONS};
+            break;
+        }
+    }
+    s->h_st->iter = (long long)st.iterations;
+    s->h_st->resid = st.residual;
+    s->h_st->reason = st.reason;
+    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FX_OK;
+}
+
+template <typename Solver>
+int create_solver(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, int nvec, Solver **out) {
+    if (!ctx || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(check_grid(g));
+    *out = nullptr;
+    Solver *s = new Solver();
+    int st = s->init_base(ctx, g, tol, max_iter, nvec);
+    if (st) {
+        delete s;
+        return st;
+    }
+    *out = s;
+    return FX_OK;
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+
+extern "C" {
+
+int fx_precond_identity(fx_ctx *ctx, fx_precond **out) {
+    if (!ctx || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    IdentityPc *p = new IdentityPc();
+    p->ctx = ctx;
+    *out = p;
+    return FX_OK;
+}
+
+int fx_precond_destroy(fx_precond *pc) {
+    if (!pc) return FX_OK;
+    if (pc->borrowed) return fail(FX_ERR_INVALID_ARGUMENT, "borrowed preconditioner: destroy its owner");
+    delete pc;
+    return FX_OK;
+}
+
+int fx_precond_apply(fx_precond *pc, fx_buf *z, const fx_buf *r) {
+    if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
+    FX_TRY(check_buf(z, "z"));
+    FX_TRY(check_buf(r, "r"));
+    return pc->apply(z, r, nullptr, false);
+}
+
+int fx_mg_create(fx_ctx *ctx, const fx_grid *g, const fx_boundaries *bc, size_t n_pre, size_t n_post, double omega,
+                 int smoother, fx_mg **out) {
+    if (!ctx || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(check_grid(g));
+    if (smoother != 0) return fail(FX_ERR_UNSUPPORTED, "Chebyshev smoother is not implemented");
+    *out = nullptr;
+    fx_mg *mg = new fx_mg();
+    mg->ctx = ctx;
+    mg->mode = 0;
+    mg->n_pre = n_pre;
+    mg->n_post = n_post;
+    mg->omega = omega;
+    if (bc) mg->bc = *bc;
+    mg->view.mg = mg;
+    mg->view.ctx = ctx;
+    mg->view.borrowed = true;
+    size_t r = g->rows, c = g->cols;
+    double hx = g->dx, hy = g->dy;
+    for (;;) {  // multigrid.rs:101-136
+        MgLevel L;
+        L.rows = r;
+        L.cols = c;
+        L.dx = hx;
+        L.dy = hy;
+        lap5_of(hx, hy, L.lap5);
+        int st = fx_alloc(ctx, r * c, FX_F64, &L.u);
+        if (!st) st = fx_alloc(ctx, r * c, FX_F64, &L.rhs);
+        if (!st) st = fx_alloc(ctx, r * c, FX_F64, &L.tmp);
+        mg->lv.push_back(L);
+        if (st) {
+            delete mg;
+            return st;
+        }
+        if (r <= 4 || c <= 4) break;
+        const size_t cr = r / 2, cc = c / 2;
+        if (cr < 3 || cc < 3) break;
+        r = cr;
+        c = cc;
+        hx *= 2.0;
+        hy *= 2.0;
+    }
+    *out = mg;
+    return FX_OK;
+}
+
+int fx_mg_create_vertex(fx_ctx *ctx, const fx_grid *g, const fx_boundaries *bc, const fx_mg_vertex_opts *o,
+                        fx_mg **out) {
+    if (!ctx || !out || !o) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(check_grid(g));
+    if (bc) {
+        for (int i = 0; i < 4; i++)
+            if (bc->side[i].kind != FX_BC_DIRICHLET || bc->side[i].a != 0.0)
+                return fail(FX_ERR_UNSUPPORTED, "vertex multigrid needs homogeneous Dirichlet boundaries");
+    }
+    if (o->dtype != FX_F32 && o->dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "unknown dtype");
+    StencilP P;
+    FX_TRY(make_stencil(&o->op_stencil, &P));
+    if (P.mode != 5) return fail(FX_ERR_UNSUPPORTED, "vertex multigrid needs a 5-point operator");
+    *out = nullptr;
+    fx_mg *mg = new fx_mg();
+    mg->ctx = ctx;
+    mg->mode = 1;
+    mg->dtype = o->dtype;
+    mg->n_pre = o->n_pre;
+    mg->n_post = o->n_post;
+    mg->omega = o->omega;
+    mg->coarse_sweeps = o->coarse_sweeps;
+    if (bc) mg->bc = *bc;
+    mg->view.mg = mg;
+    mg->view.ctx = ctx;
+    mg->view.borrowed = true;
+    double a5[5];
+    const double cf = o->op_coeff;
+    a5[0] = 1.0 + cf * P.c;
+    a5[1] = cf * P.n;
+    a5[2] = cf * P.s;
+    a5[3] = cf * P.w;
+    a5[4] = cf * P.e;
+    const double sigma = a5[0] + ((a5[1] + a5[2]) + (a5[3] + a5[4]));
+    size_t r = g->rows, c = g->cols;
+    double hx = g->dx, hy = g->dy;
+    int st = FX_OK;
+    for (int l = 0;; l++) {
+        MgLevel L;
+        L.rows = r;
+        L.cols = c;
+        L.dx = hx;
+        L.dy = hy;
+        if (l == 0) std::memcpy(L.a5, a5, sizeof(a5));
+        else coarse_op(mg->lv[l - 1].a5, sigma, L.a5);
+        if (l > 0) {
+            st = fx_alloc(ctx, r * c, o->dtype, &L.u);
+            if (!st) st = fx_alloc(ctx, r * c, o->dtype, &L.rhs);
+            if (!st) st = fx_alloc(ctx, r * c, o->dtype, &L.tmp);
+        }
+        mg->lv.push_back(L);
+        if (st) break;
+        if (!(r - 2 > o->coarse_max && c - 2 > o->coarse_max && (r - 1) % 2 == 0 && (c - 1) % 2 == 0)) break;
+        r = (r - 1) / 2 + 1;
+        c = (c - 1) / 2 + 1;
+        hx *= 2.0;
+        hy *= 2.0;
+    }
+    const size_t n0 = g->rows * g->cols;
+    if (!st) st = fx_alloc(ctx, n0, o->dtype, &mg->tmp0);
+    if (!st && o->dtype == FX_F32) {
+        st = fx_alloc(ctx, n0, FX_F32, &mg->x32);
+        if (!st) st = fx_alloc(ctx, n0, FX_F32, &mg->b32);
+    }
+    if (st) {
+        delete mg;
+        return st;
+    }
+    *out = mg;
+    return FX_OK;
+}
+
+int fx_mg_destroy(fx_mg *mg) {
+    if (!mg) return FX_OK;
+    cudaStreamSynchronize(mg->ctx->stream);
+    delete mg;
+    return FX_OK;
+}
+
+int fx_mg_depth(const fx_mg *mg, size_t *depth) {
+    if (!mg || !depth) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    *depth = mg->lv.size();
+    return FX_OK;
+}
+
+int fx_mg_level_dims(const fx_mg *mg, size_t level, size_t *rows, size_t *cols) {
+    if (!mg || !rows || !cols) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (level >= mg->lv.size()) return fail(FX_ERR_INVALID_ARGUMENT, "level out of range");
+    *rows = mg->lv[level].rows;
+    *cols = mg->lv[level].cols;
+    return FX_OK;
+}
+
+int fx_mg_v_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b) {
+    if (!mg) return fail(FX_ERR_INVALID_ARGUMENT, "null multigrid");
+    FX_TRY(check_buf(x, "x"));
+    FX_TRY(check_buf(b, "b"));
+    return mg->view.apply(x, b, nullptr, false);
+}
+
+fx_precond *fx_mg_as_precond(fx_mg *mg) { return mg ? &mg->view : nullptr; }
+
+// ---- CG
+
+int fx_cg_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, fx_cg **out) {
+    return create_solver(ctx, g, tol, max_iter, 4, out);
+}
+int fx_cg_destroy(fx_cg *s) {
+    delete s;
+    return FX_OK;
+}
+int fx_cg_set_params(fx_cg *s, double tol, size_t max_iter) {
+    if (!s) return fail(FX_ERR_INVALID_ARGUMENT, "null solver");
+    s->tol = tol;
+    s->max_iter = max_iter;
+    return FX_OK;
+}
+
+static int cg_entry(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st, const fx_boundaries *bc,
+                    fx_precond *pc, fx_stats *out) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(s->check_io(x, b));
+    StencilP P;
+    FX_TRY(prep_op(s->g, st, bc, &P));
+    SOLVER_MODE_DISPATCH(P, FX_TRY(cg_solve_impl<MODE>(s, x, b, coeff, P, pc)));
+    s->stats(out);
+    return FX_OK;
+}
+
+int fx_cg_solve(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st, const fx_boundaries *bc,
+                fx_stats *out) {
+    return cg_entry(s, x, b, coeff, st, bc, nullptr, out);
+}
+
+int fx_cg_solve_preconditioned(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                               const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
+    return cg_entry(s, x, b, coeff, st, bc, pc, out);
+}
+
+// ---- pipelined CG
+
+int fx_pipelined_cg_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, fx_pipelined_cg **out) {
+    return create_solver(ctx, g, tol, max_iter, 6, out);
+}
+int fx_pipelined_cg_destroy(fx_pipelined_cg *s) {
+    delete s;
+    return FX_OK;
+}
+int fx_pipelined_cg_set_params(fx_pipelined_cg *s, double tol, size_t max_iter) {
+    if (!s) return fail(FX_ERR_INVALID_ARGUMENT, "null solver");
+    s->tol = tol;
+    s->max_iter = max_iter;
+    return FX_OK;
+}
+int fx_pipelined_cg_solve(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                          const fx_boundaries *bc, fx_stats *out) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(s->check_io(x, b));
+    StencilP P;
+    FX_TRY(prep_op(s->g, st, bc, &P));
+    SOLVER_MODE_DISPATCH(P, FX_TRY(pipe_solve_impl<MODE>(s, x, b, coeff, P)));
+    s->stats(out);
+    return FX_OK;
+}
+
+// ---- BiCGSTAB
+
+int fx_bicgstab_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, fx_bicgstab **out) {
+    return create_solver(ctx, g, tol, max_iter, 10, out);
+}
+int fx_bicgstab_destroy(fx_bicgstab *s) {
+    delete s;
+    return FX_OK;
+}
+int fx_bicgstab_set_params(fx_bicgstab *s, double tol, size_t max_iter) {
+    if (!s) return fail(FX_ERR_INVALID_ARGUMENT, "null solver");
+    s->tol = tol;
+    s->max_iter = max_iter;
+    return FX_OK;
+}
+static int bicg_entry(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                      const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(s->check_io(x, b));
+    StencilP P;
+    FX_TRY(prep_op(s->g, st, bc, &P));
+    SOLVER_MODE_DISPATCH(P, FX_TRY(bicg_solve_impl<MODE>(s, x, b, coeff, P, pc)));
+    s->stats(out);
+    return FX_OK;
+}
+int fx_bicgstab_solve(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                      const fx_boundaries *bc, fx_stats *out) {
+    return bicg_entry(s, x, b, coeff, st, bc, nullptr, out);
+}
+int fx_bicgstab_solve_preconditioned(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                                     const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
+    return bicg_entry(s, x, b, coeff, st, bc, pc, out);
+}
+
+// ---- GMRES
+
+int fx_gmres_create(fx_ctx *ctx, const fx_grid *g, size_t restart, double tol, size_t max_iter, fx_gmres **out) {
+    if (restart < 1) return fail(FX_ERR_INVALID_ARGUMENT, "restart must be at least 1");
+    FX_TRY(create_solver(ctx, g, tol, max_iter, (int)restart + 2, out));
+    fx_gmres *s = *out;
+    s->restart = restart;
+    s->hh.assign((restart + 1) * restart, 0.0);
+    s->cc.assign(restart, 0.0);
+    s->ss.assign(restart, 0.0);
+    s->grs.assign(restart + 1, 0.0);
+    if (cudaMalloc(&s->d_h, (restart + 2) * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&s->h_h, (restart + 2) * sizeof(double)) != cudaSuccess) {
+        delete s;
+        *out = nullptr;
+        return fail(FX_ERR_BACKEND, "gmres scratch allocation failed");
+    }
+    return FX_OK;
+}
+int fx_gmres_destroy(fx_gmres *s) {
+    delete s;
+    return FX_OK;
+}
+int fx_gmres_set_params(fx_gmres *s, double tol, size_t max_iter) {
+    if (!s) return fail(FX_ERR_INVALID_ARGUMENT, "null solver");
+    s->tol = tol;
+    s->max_iter = max_iter;
+    return FX_OK;
+}
+static int gmres_entry(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                       const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(s->check_io(x, b));
+    StencilP P;
+    FX_TRY(prep_op(s->g, st, bc, &P));
+    SOLVER_MODE_DISPATCH(P, FX_TRY(gmres_solve_impl<MODE>(s, x, b, coeff, P, pc)));
+    s->stats(out);
+    return FX_OK;
+}
+int fx_gmres_solve(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                   const fx_boundaries *bc, fx_stats *out) {
+    return gmres_entry(s, x, b, coeff, st, bc, nullptr, out);
+}
+int fx_gmres_solve_preconditioned(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                                  const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
+    return gmres_entry(s, x, b, coeff, st, bc, pc, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,348 @@
+// fx_stencil.cu -- stencil apply / fused stencil+AXPY / variable-coefficient stencil,
+// upwind convection-diffusion, boundary ring, and the multigrid grid-transfer and
+// smoothing primitives.  All grid kernels use the row-marching framework
+// (fx_internal.cuh): one HBM read per element of the marched field.
+#include "fx_points.cuh"
+
+using namespace fx;
+
+namespace {
+
+// Reference weighted_jacobi (ops.rs:425-473): an in-place lexicographic sweep.  Executed
+// as a wavefront over hyperplanes 2r + c = t: for radius-1 stencils every neighbour that
+// the lexicographic order updates first lies on an earlier hyperplane and every later one
+// on a later hyperplane, so each point sees exactly the values the sequential sweep sees.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_lex_jacobi(T *x, const T *__restrict__ b, int rows, int cols,
+                                                     StencilP P, double omega, double inv_diag) {
+    const int tmin = 3, tmax = 2 * (rows - 2) + (cols - 2);
+    const T om = (T)omega, id = (T)inv_diag;
+    for (int t = tmin; t <= tmax; t++) {
+        int rlo = (t - (cols - 2) + 1) / 2;
+        if (rlo < 1) rlo = 1;
+        int rhi = (t - 1) / 2;
+        if (rhi > rows - 2) rhi = rows - 2;
+        for (int r = rlo + (int)threadIdx.x; r <= rhi; r += blockDim.x) {
+            const int c = t - 2 * r;
+            const size_t idx = (size_t)r * cols + c;
+            T ax = (T)0;
+            for (int k = 0; k < P.ne_; k++) {
+                const int dr = P.gi[k] / 3 - 1, dc = P.gi[k] % 3 - 1;
+                ax = fx_fma((T)P.gw[k], x[idx + (long)dr * cols + dc], ax);
+            }
+            const T residual = b[idx] - ax;
+            x[idx] = fx_fma(om, id * residual, x[idx]);
+        }
+        __syncthreads();
+    }
+}
+
+int pre_grid2(fx_ctx *ctx, const fx_buf *a, const fx_buf *b, const fx_grid *g) {
+    if (!ctx) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    FX_TRY(check_grid(g));
+    FX_TRY(check_buf(a, "input"));
+    FX_TRY(check_buf(b, "output"));
+    FX_TRY(check_grid_len(g, a));
+    FX_TRY(check_grid_len(g, b));
+    if (a->dtype != b->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
+    if (a->ptr == b->ptr) return fail(FX_ERR_INVALID_ARGUMENT, "input and output must be distinct buffers");
+    return FX_OK;
+}
+
+int pre_vec(const fx_buf *ref, const fx_buf *b, const char *name) {
+    FX_TRY(check_buf(b, name));
+    return check_same(ref, b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fx_apply_stencil(fx_ctx *ctx, const fx_buf *in, fx_buf *out, const fx_grid *g, const fx_stencil *s,
+                     const fx_boundaries *bc) {
+    FX_TRY(pre_grid2(ctx, in, out, g));
+    BcP B;
+    FX_TRY(make_bc(bc, g->dx, g->dy, &B, true));
+    StencilP P;
+    FX_TRY(make_stencil(s, &P));
+    FX_DISPATCH(in->dtype, {
+        constexpr int U = unroll_for<T>();
+        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        FX_MODE_DISPATCH(P.mode, {
+            PtApply<T, MODE, false> pt{(T *)out->ptr, nullptr, P, B, G.rows, G.cols};
+            return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)in->ptr}, pt, NoFin{}, nullptr,
+                                         "apply_stencil");
+        });
+    });
+}
+
+int fx_apply_stencil_var(fx_ctx *ctx, const fx_buf *in, fx_buf *out, const fx_buf *coeff, const fx_grid *g,
+                         const fx_stencil *s, const fx_boundaries *bc) {
+    FX_TRY(pre_grid2(ctx, in, out, g));
+    FX_TRY(pre_vec(in, coeff, "coeff"));
+    BcP B;
+    FX_TRY(make_bc(bc, g->dx, g->dy, &B, true));
+    StencilP P;
+    FX_TRY(make_stencil(s, &P));
+    FX_DISPATCH(in->dtype, {
+        constexpr int U = unroll_for<T>();
+        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        FX_MODE_DISPATCH(P.mode, {
+            PtApply<T, MODE, true> pt{(T *)out->ptr, (const T *)coeff->ptr, P, B, G.rows, G.cols};
+            return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)in->ptr}, pt, NoFin{}, nullptr,
+                                         "apply_stencil_var");
+        });
+    });
+}
+
+int fx_stencil_axpy(fx_ctx *ctx, double alpha, const fx_buf *x, fx_buf *y, const fx_grid *g,
+                    const fx_stencil *s, const fx_boundaries *bc) {
+    FX_TRY(pre_grid2(ctx, x, y, g));
+    BcP B;
+    FX_TRY(make_bc(bc, g->dx, g->dy, &B, true));
+    StencilP P;
+    FX_TRY(make_stencil(s, &P));
+    FX_DISPATCH(x->dtype, {
+        constexpr int U = unroll_for<T>();
+        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        FX_MODE_DISPATCH(P.mode, {
+            PtAxpy<T, MODE> pt{(T *)y->ptr, P, (T)alpha, G.rows, G.cols};
+            return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)x->ptr}, pt, NoFin{}, nullptr,
+                                         "stencil_axpy");
+        });
+    });
+}
+
+int fx_zero_boundaries(fx_ctx *ctx, fx_buf *buf, size_t rows, size_t cols) {
+    if (!ctx) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    FX_TRY(check_buf(buf, "buf"));
+    if (rows < 1 || cols < 1 || rows * cols != buf->len)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "dimension mismatch: expected " + std::to_string(rows * cols) +
+                                                   ", got " + std::to_string(buf->len));
+    const size_t nring = 2 * cols + 2 * (rows > 2 ? rows - 2 : 0);
+    FX_DISPATCH(buf->dtype, {
+        T *p = (T *)buf->ptr;
+        return launch_flat<0>(ctx, nring,
+                              [=] __device__(size_t i, CSum *) {
+                                  size_t idx;
+                                  if (i < cols) idx = i;
+                                  else if (i < 2 * cols) idx = (rows - 1) * cols + (i - cols);
+                                  else {
+                                      const size_t j = i - 2 * cols;
+                                      const size_t r = 1 + j / 2;
+                                      idx = r * cols + ((j & 1) ? cols - 1 : 0);
+                                  }
+                                  p[idx] = (T)0;
+                              },
+                              NoFin{}, nullptr, "zero_boundaries");
+    });
+}
+
+int fx_apply_conv_diff(fx_ctx *ctx, const fx_buf *u, fx_buf *out, const fx_buf *kappa, const fx_buf *vx,
+                       const fx_buf *vy, const fx_grid *g, const fx_boundaries *) {
+    FX_TRY(pre_grid2(ctx, u, out, g));
+    FX_TRY(pre_vec(u, kappa, "kappa"));
+    FX_TRY(pre_vec(u, vx, "vx"));
+    FX_TRY(pre_vec(u, vy, "vy"));
+    FX_DISPATCH(u->dtype, {
+        constexpr int U = unroll_for<T>();
+        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        PtConvDiff<T, false> pt{(T *)out->ptr, (const T *)kappa->ptr, (const T *)vx->ptr, (const T *)vy->ptr,
+                                conv_consts<T>(g->dx, g->dy), (T)0, G.rows, G.cols};
+        return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)u->ptr}, pt, NoFin{}, nullptr,
+                                     "apply_conv_diff");
+    });
+}
+
+int fx_conv_diff_axpy(fx_ctx *ctx, double alpha, const fx_buf *u, fx_buf *out, const fx_buf *kappa,
+                      const fx_buf *vx, const fx_buf *vy, const fx_grid *g, const fx_boundaries *) {
+    FX_TRY(pre_grid2(ctx, u, out, g));
+    FX_TRY(pre_vec(u, kappa, "kappa"));
+    FX_TRY(pre_vec(u, vx, "vx"));
+    FX_TRY(pre_vec(u, vy, "vy"));
+    FX_DISPATCH(u->dtype, {
+        constexpr int U = unroll_for<T>();
+        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        PtConvDiff<T, true> pt{(T *)out->ptr, (const T *)kappa->ptr, (const T *)vx->ptr, (const T *)vy->ptr,
+                               conv_consts<T>(g->dx, g->dy), (T)alpha, G.rows, G.cols};
+        return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)u->ptr}, pt, NoFin{}, nullptr,
+                                     "conv_diff_axpy");
+    });
+}
+
+// ---------------------------------------------------------------- multigrid, reference semantics
+
+int fx_restrict(fx_ctx *ctx, const fx_buf *fine, fx_buf *coarse, const fx_grid *fg, const fx_grid *cg) {
+    if (!ctx || !fg || !cg) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(check_buf(fine, "fine"));
+    FX_TRY(check_buf(coarse, "coarse"));
+    FX_TRY(check_grid_len(fg, fine));
+    FX_TRY(check_grid_len(cg, coarse));
+    if (fine->dtype != coarse->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
+    const size_t frows = fg->rows, fcols = fg->cols, crows = cg->rows, ccols = cg->cols;
+    // ops.rs:380-395 indexes fine[2*row] unchecked (a panic past the fine grid).
+    if (crows == 0 || ccols == 0 || 2 * (crows - 1) > frows - 1 || 2 * (ccols - 1) > fcols - 1)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "restrict: coarse grid does not fit the fine grid");
+    FX_DISPATCH(fine->dtype, {
+        const T *f = (const T *)fine->ptr;
+        T *c = (T *)coarse->ptr;
+        return launch_flat<0>(ctx, crows * ccols,
+                              [=] __device__(size_t i, CSum *) {
+                                  const size_t row = i / ccols, col = i % ccols;
+                                  const size_t fr = row * 2, fcc = col * 2;
+                                  const size_t fr1 = fr + 1 < frows - 1 ? fr + 1 : frows - 1;
+                                  const size_t fc1 = fcc + 1 < fcols - 1 ? fcc + 1 : fcols - 1;
+                                  c[i] = (T)0.25 * (((f[fr * fcols + fcc] + f[fr1 * fcols + fcc]) +
+                                                     f[fr * fcols + fc1]) + f[fr1 * fcols + fc1]);
+                              },
+                              NoFin{}, nullptr, "restrict");
+    });
+}
+
+int fx_prolong(fx_ctx *ctx, const fx_buf *coarse, fx_buf *fine, const fx_grid *cg, const fx_grid *fg) {
+    if (!ctx || !fg || !cg) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(check_buf(fine, "fine"));
+    FX_TRY(check_buf(coarse, "coarse"));
+    FX_TRY(check_grid_len(fg, fine));
+    FX_TRY(check_grid_len(cg, coarse));
+    if (fine->dtype != coarse->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
+    const size_t frows = fg->rows, fcols = fg->cols, crows = cg->rows, ccols = cg->cols;
+    // ops.rs:413-420 indexes coarse[row/2] unchecked (a panic past the coarse grid).
+    if ((frows - 1) / 2 > crows - 1 || (fcols - 1) / 2 > ccols - 1)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "prolong: fine grid maps outside the coarse grid");
+    FX_DISPATCH(fine->dtype, {
+        const T *c = (const T *)coarse->ptr;
+        T *f = (T *)fine->ptr;
+        return launch_flat<0>(ctx, frows * fcols,
+                              [=] __device__(size_t i, CSum *) {
+                                  const size_t row = i / fcols, col = i % fcols;
+                                  f[i] += c[(row / 2) * ccols + col / 2];
+                              },
+                              NoFin{}, nullptr, "prolong");
+    });
+}
+
+int fx_weighted_jacobi(fx_ctx *ctx, fx_buf *x, const fx_buf *b, double omega, const fx_grid *g,
+                       const fx_stencil *s, const fx_boundaries *) {
+    if (!ctx) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    FX_TRY(check_grid(g));
+    FX_TRY(check_buf(x, "x"));
+    FX_TRY(check_buf(b, "b"));
+    FX_TRY(check_grid_len(g, x));
+    FX_TRY(check_grid_len(g, b));
+    if (x->dtype != b->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
+    if (!s || s->n < 1) return fail(FX_ERR_INVALID_STENCIL, "invalid stencil: stencil must have at least one entry");
+    // ops.rs:440-457 uses the entry list in order (no 5/9-point fast path) -> generic form.
+    StencilP P;
+    std::memset(&P, 0, sizeof(P));
+    if (s->n > kMaxGeneric) return fail(FX_ERR_INVALID_STENCIL, "invalid stencil: more than 27 entries");
+    double diag = -4.0;
+    bool found = false;
+    for (int k = 0; k < s->n; k++) {
+        if (s->dr[k] < -1 || s->dr[k] > 1 || s->dc[k] < -1 || s->dc[k] > 1)
+            return fail(FX_ERR_INVALID_STENCIL, "invalid stencil: offsets beyond radius 1");
+        P.gi[k] = (signed char)((s->dr[k] + 1) * 3 + (s->dc[k] + 1));
+        P.gw[k] = s->w[k];
+        if (!found && s->dr[k] == 0 && s->dc[k] == 0) {
+            diag = s->w[k];
+            found = true;
+        }
+    }
+    P.ne_ = s->n;
+    const double inv_diag = 1.0 / diag;
+    FX_DISPATCH(x->dtype, {
+        k_lex_jacobi<T><<<1, 1024, 0, ctx->stream>>>((T *)x->ptr, (const T *)b->ptr, (int)g->rows,
+                                                      (int)g->cols, P, omega, inv_diag);
+        return check_launch(ctx, "weighted_jacobi");
+    });
+}
+
+// ---------------------------------------------------------------- vertex-centred primitives
+
+int fx_jacobi_sweep(fx_ctx *ctx, const fx_buf *x_in, fx_buf *x_out, const fx_buf *b, double omega, size_t rows,
+                    size_t cols, const double a5[5]) {
+    if (!ctx || !a5) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    fx_grid g{rows, cols, 1.0, 1.0};
+    FX_TRY(pre_grid2(ctx, x_in, x_out, &g));
+    FX_TRY(pre_vec(x_in, b, "b"));
+    const double wd = omega / a5[0];
+    FX_DISPATCH(x_in->dtype, {
+        constexpr int U = unroll_for<T>();
+        MarchGeom G = march_geom(ctx, rows, cols, U);
+        PtJacobi<T> pt{(T *)x_out->ptr, (const T *)b->ptr, make_a5<T>(a5), (T)wd, G.rows, G.cols};
+        return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)x_in->ptr}, pt, NoFin{}, nullptr,
+                                     "jacobi_sweep");
+    });
+}
+
+int fx_residual5(fx_ctx *ctx, const fx_buf *x, const fx_buf *b, fx_buf *r, size_t rows, size_t cols,
+                 const double a5[5]) {
+    if (!ctx || !a5) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    fx_grid g{rows, cols, 1.0, 1.0};
+    FX_TRY(pre_grid2(ctx, x, r, &g));
+    FX_TRY(pre_vec(x, b, "b"));
+    FX_DISPATCH(x->dtype, {
+        constexpr int U = unroll_for<T>();
+        MarchGeom G = march_geom(ctx, rows, cols, U);
+        PtResidual<T> pt{(T *)r->ptr, (const T *)b->ptr, make_a5<T>(a5), G.rows, G.cols};
+        return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)x->ptr}, pt, NoFin{}, nullptr, "residual5");
+    });
+}
+
+int fx_restrict_fw(fx_ctx *ctx, const fx_buf *fine, fx_buf *coarse, size_t frows, size_t fcols, size_t crows,
+                   size_t ccols) {
+    if (!ctx) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    FX_TRY(check_buf(fine, "fine"));
+    FX_TRY(check_buf(coarse, "coarse"));
+    if (crows < 3 || ccols < 3 || frows != 2 * (crows - 1) + 1 || fcols != 2 * (ccols - 1) + 1 ||
+        fine->len != frows * fcols || coarse->len != crows * ccols)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "restrict_fw: grids are not a vertex-centred pair");
+    if (fine->dtype != coarse->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
+    FX_DISPATCH(fine->dtype, {
+        const T *f = (const T *)fine->ptr;
+        T *c = (T *)coarse->ptr;
+        return launch_flat<0>(ctx, crows * ccols,
+                              [=] __device__(size_t i, CSum *) {
+                                  const size_t I = i / ccols, J = i % ccols;
+                                  if (I == 0 || J == 0 || I == crows - 1 || J == ccols - 1) {
+                                      c[i] = (T)0;
+                                      return;
+                                  }
+                                  const size_t k = (2 * I) * fcols + 2 * J;
+                                  const T e = (f[k - fcols] + f[k + fcols]) + (f[k - 1] + f[k + 1]);
+                                  const T d = (f[k - fcols - 1] + f[k - fcols + 1]) + (f[k + fcols - 1] + f[k + fcols + 1]);
+                                  c[i] = ((T)4 * f[k] + ((T)2 * e + d)) * (T)0.0625;
+                              },
+                              NoFin{}, nullptr, "restrict_fw");
+    });
+}
+
+int fx_prolong_bilinear(fx_ctx *ctx, const fx_buf *coarse, fx_buf *fine, size_t crows, size_t ccols, size_t frows,
+                        size_t fcols) {
+    if (!ctx) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    FX_TRY(check_buf(fine, "fine"));
+    FX_TRY(check_buf(coarse, "coarse"));
+    if (crows < 3 || ccols < 3 || frows != 2 * (crows - 1) + 1 || fcols != 2 * (ccols - 1) + 1 ||
+        fine->len != frows * fcols || coarse->len != crows * ccols)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "prolong_bilinear: grids are not a vertex-centred pair");
+    if (fine->dtype != coarse->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
+    FX_DISPATCH(fine->dtype, {
+        const T *c = (const T *)coarse->ptr;
+        T *f = (T *)fine->ptr;
+        const size_t iw = fcols - 2;
+        return launch_flat<0>(ctx, (frows - 2) * (fcols - 2),
+                              [=] __device__(size_t q, CSum *) {
+                                  const size_t i = 1 + q / iw, j = 1 + q % iw;
+                                  const size_t k = (i / 2) * ccols + (j / 2);
+                                  T e;
+                                  if (!(i & 1) && !(j & 1)) e = c[k];
+                                  else if ((i & 1) && !(j & 1)) e = (T)0.5 * (c[k] + c[k + ccols]);
+                                  else if (!(i & 1) && (j & 1)) e = (T)0.5 * (c[k] + c[k + 1]);
+                                  else e = (T)0.25 * ((c[k] + c[k + ccols]) + (c[k + 1] + c[k + ccols + 1]));
+                                  f[i * fcols + j] += e;
+                              },
+                              NoFin{}, nullptr, "prolong_bilinear");
+    });
+}
+
+}  // extern "C"

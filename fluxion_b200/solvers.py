@@ -1,0 +1,289 @@
+"""Solver structs of fluxion's runtime, executed by the native C++/CUDA solver loops.
+
+``CgSolver`` (crates/runtime/src/cg.rs:52-256), ``PipelinedCgSolver``
+(pipelined_cg.rs:25-237), ``BiCgStabSolver`` (bicgstab.rs:19-346),
+``GmresSolver`` (gmres.rs:24-491), ``Multigrid`` (multigrid.rs:39-608),
+``Identity`` / ``Preconditioner`` (preconditioner.rs:10-37), ``LinearSolver``
+(linear_solver.rs:13-102), ``SolveStats`` / ``ConvergenceReason`` (cg.rs:9-41).
+Same constructor arguments, public fields and solve signatures as the
+reference; each ``solve`` is one call into ``libfluxion_cuda.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass
+from typing import Optional
+
+from . import _lib as L
+from .backend import StencilC, bcs_c, check, grid_c
+from .core import Boundaries, DType, Grid, Stencil
+from .field import Device, Field
+
+
+class ConvergenceReason(enum.IntEnum):
+    """cg.rs:9-18"""
+
+    Converged = 0
+    MaxIterations = 1
+    Breakdown = 2
+
+
+@dataclass
+class SolveStats:
+    """cg.rs:20-38"""
+
+    iterations: int
+    residual: float
+    reason: ConvergenceReason
+
+    def converged(self) -> bool:
+        return self.reason == ConvergenceReason.Converged
+
+
+CgStats = SolveStats
+
+
+def _stats(st: L.FxStats) -> SolveStats:
+    return SolveStats(int(st.iterations), float(st.residual), ConvergenceReason(st.reason))
+
+
+# ------------------------------------------------------------------ preconditioners
+
+class Preconditioner:
+    """preconditioner.rs:10-29: ``apply(z, r)`` approximately solves M z = r."""
+
+    def _handle(self, device: Device) -> int:
+        raise NotImplementedError
+
+    def apply(self, z: Field, r: Field) -> None:
+        check(L.lib().fx_precond_apply(self._handle(z.device()), z.storage.handle, r.storage.handle))
+
+
+class Identity(Preconditioner):
+    """preconditioner.rs:31-37: z = r."""
+
+    def __init__(self):
+        self._h = {}
+
+    def _handle(self, device: Device) -> int:
+        h = self._h.get(device)
+        if h is None:
+            out = C.c_void_p()
+            check(L.lib().fx_precond_identity(device.backend().ctx, C.byref(out)))
+            h = out.value
+            self._h[device] = h
+        return h
+
+    def __del__(self):
+        try:
+            for h in self._h.values():
+                L.lib().fx_precond_destroy(h)
+        except Exception:
+            pass
+
+
+class SmootherKind(enum.IntEnum):
+    """multigrid.rs:11-20"""
+
+    Jacobi = 0
+    Chebyshev = 1
+
+
+class Multigrid(Preconditioner):
+    """Geometric multigrid V-cycle preconditioner.
+
+    ``Multigrid(grid, boundaries, device, n_pre, n_post, omega)`` / ``Multigrid.build(...)`` give
+    the reference hierarchy and operators (multigrid.rs:61-146).  ``Multigrid.vertex(...)`` gives
+    the vertex-centred cycle for the operator actually solved (full weighting, bilinear
+    prolongation, true weighted Jacobi, dense coarsest solve), which is the one the Poisson and
+    convection-diffusion configurations use.
+    """
+
+    def __init__(self, grid: Grid, boundaries: Boundaries, device: Optional[Device] = None, n_pre: int = 2,
+                 n_post: int = 2, omega: float = 2.0 / 3.0, smoother: SmootherKind = SmootherKind.Jacobi,
+                 _handle: Optional[int] = None):
+        self.device = device or Device.best()
+        self.grid = grid
+        if _handle is not None:
+            self.h = _handle
+            return
+        out = C.c_void_p()
+        g, b = grid_c(grid), bcs_c(boundaries)
+        check(L.lib().fx_mg_create(self.device.backend().ctx, C.byref(g), C.byref(b), int(n_pre), int(n_post),
+                                   float(omega), int(smoother), C.byref(out)))
+        self.h = out.value
+
+    @staticmethod
+    def new(grid, boundaries, device=None, n_pre=2, n_post=2, omega=2.0 / 3.0) -> "Multigrid":
+        return Multigrid(grid, boundaries, device, n_pre, n_post, omega)
+
+    @staticmethod
+    def build(grid, boundaries, device=None, n_pre=2, n_post=2, omega=2.0 / 3.0,
+              smoother=SmootherKind.Jacobi) -> "Multigrid":
+        return Multigrid(grid, boundaries, device, n_pre, n_post, omega, smoother)
+
+    @staticmethod
+    def vertex(grid: Grid, boundaries: Optional[Boundaries] = None, device: Optional[Device] = None,
+               n_pre: int = 2, n_post: int = 2, omega: float = 0.8, coarse_max: int = 15,
+               coarse_sweeps: int = 200, dtype: DType = DType.F64, op_coeff: float = 1.0,
+               op_stencil: Optional[Stencil] = None) -> "Multigrid":
+        device = device or Device.best()
+        op_stencil = op_stencil or Stencil.poisson_neg_laplacian(grid.dx, grid.dy)
+        sc = StencilC(op_stencil)
+        opts = L.FxMgVertexOpts(int(n_pre), int(n_post), float(omega), int(coarse_max), int(coarse_sweeps),
+                                int(dtype), float(op_coeff), sc.s)
+        out = C.c_void_p()
+        g, b = grid_c(grid), bcs_c(boundaries)
+        check(L.lib().fx_mg_create_vertex(device.backend().ctx, C.byref(g), C.byref(b), C.byref(opts),
+                                          C.byref(out)))
+        return Multigrid(grid, boundaries, device, _handle=out.value)
+
+    def depth(self) -> int:
+        d = C.c_size_t()
+        check(L.lib().fx_mg_depth(self.h, C.byref(d)))
+        return d.value
+
+    def level_dims(self, level: int):
+        r, c = C.c_size_t(), C.c_size_t()
+        check(L.lib().fx_mg_level_dims(self.h, int(level), C.byref(r), C.byref(c)))
+        return r.value, c.value
+
+    def v_cycle(self, x: Field, b: Field) -> None:
+        check(L.lib().fx_mg_v_cycle(self.h, x.storage.handle, b.storage.handle))
+
+    def _handle(self, device: Device) -> int:
+        return L.lib().fx_mg_as_precond(self.h)
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().fx_mg_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ solvers
+
+class LinearSolver:
+    """linear_solver.rs:13-36"""
+
+    def solve(self, x: Field, b: Field, coeff: float, stencil: Stencil, boundaries: Boundaries) -> SolveStats:
+        raise NotImplementedError
+
+    def name(self) -> str:
+        raise NotImplementedError
+
+
+class _Native(LinearSolver):
+    _prefix = ""
+
+    def __init__(self, grid: Grid, device: Optional[Device], tol: float, max_iter: int, *extra):
+        self.device = device or Device.best()
+        self.grid = grid
+        self._tol = float(tol)
+        self._max_iter = int(max_iter)
+        out = C.c_void_p()
+        g = grid_c(grid)
+        create = getattr(L.lib(), f"fx_{self._prefix}_create")
+        check(create(self.device.backend().ctx, C.byref(g), *extra, self._tol, self._max_iter, C.byref(out)))
+        self.h = out.value
+
+    # public fields `tol` / `max_iter`, as in the reference structs
+    @property
+    def tol(self) -> float:
+        return self._tol
+
+    @tol.setter
+    def tol(self, v: float) -> None:
+        self._tol = float(v)
+        self._push()
+
+    @property
+    def max_iter(self) -> int:
+        return self._max_iter
+
+    @max_iter.setter
+    def max_iter(self, v: int) -> None:
+        self._max_iter = int(v)
+        self._push()
+
+    def _push(self):
+        check(getattr(L.lib(), f"fx_{self._prefix}_set_params")(self.h, self._tol, self._max_iter))
+
+    def _run(self, fn, x: Field, b: Field, coeff, stencil, boundaries, *extra) -> SolveStats:
+        sc = StencilC(stencil)
+        bc = bcs_c(boundaries)
+        st = L.FxStats()
+        check(fn(self.h, x.storage.handle, b.storage.handle, float(coeff), sc.ptr, C.byref(bc), *extra,
+                 C.byref(st)))
+        return _stats(st)
+
+    def solve(self, x, b, coeff, stencil, boundaries) -> SolveStats:
+        return self._run(getattr(L.lib(), f"fx_{self._prefix}_solve"), x, b, coeff, stencil, boundaries)
+
+    def solve_preconditioned(self, x, b, coeff, stencil, boundaries, pc: Preconditioner) -> SolveStats:
+        fn = getattr(L.lib(), f"fx_{self._prefix}_solve_preconditioned")
+        return self._run(fn, x, b, coeff, stencil, boundaries, pc._handle(self.device))
+
+    def __del__(self):
+        try:
+            if self.h:
+                getattr(L.lib(), f"fx_{self._prefix}_destroy")(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class CgSolver(_Native):
+    """cg.rs:52-256: matrix-free (P)CG on A v = v + coeff * S v."""
+
+    _prefix = "cg"
+
+    def __init__(self, grid: Grid, device: Optional[Device] = None, tol: float = 1e-8, max_iter: int = 500):
+        super().__init__(grid, device, tol, max_iter)
+
+    def name(self) -> str:
+        return "CG"
+
+
+class PipelinedCgSolver(_Native):
+    """pipelined_cg.rs:25-237 (Ghysels-Vanroose)."""
+
+    _prefix = "pipelined_cg"
+
+    def __init__(self, grid: Grid, device: Optional[Device] = None, tol: float = 1e-8, max_iter: int = 500):
+        super().__init__(grid, device, tol, max_iter)
+
+    def solve_preconditioned(self, *a, **k):
+        raise NotImplementedError("PipelinedCgSolver has no preconditioned variant (pipelined_cg.rs)")
+
+    def name(self) -> str:
+        return "PipelinedCG"
+
+
+class BiCgStabSolver(_Native):
+    """bicgstab.rs:19-346."""
+
+    _prefix = "bicgstab"
+
+    def __init__(self, grid: Grid, device: Optional[Device] = None, tol: float = 1e-8, max_iter: int = 500):
+        super().__init__(grid, device, tol, max_iter)
+
+    def name(self) -> str:
+        return "BiCGSTAB"
+
+
+class GmresSolver(_Native):
+    """gmres.rs:24-491: restarted GMRES(m) with modified Gram-Schmidt."""
+
+    _prefix = "gmres"
+
+    def __init__(self, grid: Grid, device: Optional[Device] = None, restart: int = 30, tol: float = 1e-8,
+                 max_iter: int = 500):
+        self.restart = int(restart)
+        super().__init__(grid, device, tol, max_iter, C.c_size_t(self.restart))
+
+    def name(self) -> str:
+        return "GMRES"

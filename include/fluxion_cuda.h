@@ -1,0 +1,312 @@
+/*
+ * fluxion_cuda.h -- C ABI of the B200 (sm_100a) backend for fluxion's
+ * matrix-free solve path.
+ *
+ * One `extern "C"` entry point per operation of the reference's backend
+ * trait `fluxion_core::Backend` (crates/core/src/backend.rs:43-406), plus
+ * the non-trait fast paths the reference runtime already calls on its GPU
+ * backend (crates/backend-hip/src/backend.rs:463-668) and the solver
+ * structs of crates/runtime.  Every function returns an `int` status
+ * (FX_OK == 0) and writes results through out-pointers; on error,
+ * fx_last_error() returns a message for the calling thread.
+ *
+ * Conventions
+ *  - Buffers are opaque handles owned by the library (the reference's
+ *    `BackendBuffer`, crates/core/src/backend.rs:13-36): fx_alloc returns a
+ *    zero-filled buffer, fx_free releases it (HipBuffer's Drop,
+ *    crates/backend-hip/src/buffer.rs:81-87).
+ *  - A grid is rows x cols INCLUDING the boundary ring, row-major
+ *    (crates/core/src/grid.rs:4-9, :59-61).
+ *  - Every operation is enqueued on the context's stream in call order.
+ *    Calls that return a host scalar (reductions, solves) synchronise.
+ *  - F64 buffers compute in double precision, F32 buffers in single
+ *    precision; all reductions accumulate in compensated double precision
+ *    and are bitwise deterministic for a given length.
+ *  - Status codes map onto the reference's `CoreError` variants
+ *    (crates/core/src/error.rs:4-20).
+ */
+#ifndef FLUXION_CUDA_H
+#define FLUXION_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Status, dtypes, descriptors                                        */
+/* ------------------------------------------------------------------ */
+
+enum {
+    FX_OK = 0,
+    FX_ERR_DIMENSION_MISMATCH = 1, /* CoreError::DimensionMismatch */
+    FX_ERR_INVALID_GRID = 2,       /* CoreError::InvalidGrid */
+    FX_ERR_INVALID_STENCIL = 3,    /* CoreError::InvalidStencil */
+    FX_ERR_BACKEND = 4,            /* CoreError::BackendError (CUDA failure) */
+    FX_ERR_INVALID_ARGUMENT = 5,   /* null handle, dtype mismatch, bad parameter */
+    FX_ERR_UNSUPPORTED = 6,        /* e.g. periodic boundaries (ops.rs:9-23) */
+    FX_ERR_NO_DEVICE = 7           /* no CUDA device / driver */
+};
+
+enum { FX_F32 = 0, FX_F64 = 1 }; /* crates/core/src/dtype.rs:2-5 */
+
+/* crates/core/src/boundary.rs:2-15 */
+enum { FX_BC_DIRICHLET = 0, FX_BC_NEUMANN = 1, FX_BC_ROBIN = 2, FX_BC_PERIODIC = 3 };
+
+typedef struct {
+    int kind;
+    double a; /* Dirichlet value | Neumann flux | Robin alpha */
+    double b; /* Robin beta */
+    double g; /* Robin g */
+} fx_bc;
+
+/* Boundaries {top, bottom, left, right} (crates/core/src/boundary.rs:17-24). */
+typedef struct {
+    fx_bc side[4];
+} fx_boundaries;
+
+/* crates/core/src/grid.rs:3-9 */
+typedef struct {
+    size_t rows, cols;
+    double dx, dy;
+} fx_grid;
+
+/* crates/core/src/stencil.rs:1-14: n entries of (dr, dc, weight). */
+typedef struct {
+    int n;
+    const int *dr;
+    const int *dc;
+    const double *w;
+} fx_stencil;
+
+/* SolveStats (crates/runtime/src/cg.rs:9-29). */
+enum { FX_CONVERGED = 0, FX_MAX_ITERATIONS = 1, FX_BREAKDOWN = 2 };
+typedef struct {
+    size_t iterations;
+    double residual;
+    int reason;
+} fx_stats;
+
+typedef struct fx_ctx fx_ctx;
+typedef struct fx_buf fx_buf;
+typedef struct fx_precond fx_precond;
+typedef struct fx_mg fx_mg;
+typedef struct fx_cg fx_cg;
+typedef struct fx_pipelined_cg fx_pipelined_cg;
+typedef struct fx_bicgstab fx_bicgstab;
+typedef struct fx_gmres fx_gmres;
+
+/* ------------------------------------------------------------------ */
+/* Context (HipBackend::new / singleton, backend-hip/src/backend.rs:103-264) */
+/* ------------------------------------------------------------------ */
+
+const char *fx_last_error(void);
+int fx_version(void);
+int fx_device_count(int *count);
+/* Backend::name (backend.rs:47) -> "cuda" */
+const char *fx_backend_name(void);
+int fx_ctx_create(int device, fx_ctx **out);
+int fx_ctx_destroy(fx_ctx *ctx);
+int fx_ctx_synchronize(fx_ctx *ctx);
+/* Use an external cudaStream_t (e.g. the caller's); NULL restores the context's own. */
+int fx_ctx_set_stream(fx_ctx *ctx, void *stream);
+void *fx_ctx_get_stream(fx_ctx *ctx);
+/* Number of kernels this context has launched (for launch accounting). */
+unsigned long long fx_ctx_launch_count(fx_ctx *ctx);
+
+/* ------------------------------------------------------------------ */
+/* Memory (Backend::allocate / upload_f64 / upload_f32, backend.rs:49-77;
+ * BackendBuffer::copy_to_host_*, :25-35)                             */
+/* ------------------------------------------------------------------ */
+
+int fx_alloc(fx_ctx *ctx, size_t len, int dtype, fx_buf **out);
+int fx_upload_f64(fx_ctx *ctx, const double *data, size_t len, fx_buf **out);
+int fx_upload_f32(fx_ctx *ctx, const float *data, size_t len, fx_buf **out);
+/* Non-owning view of existing device memory (interop); fx_free releases only the handle. */
+int fx_wrap(fx_ctx *ctx, void *device_ptr, size_t len, int dtype, fx_buf **out);
+int fx_free(fx_buf *buf);
+size_t fx_buf_len(const fx_buf *buf);
+int fx_buf_dtype(const fx_buf *buf);
+void *fx_buf_device_ptr(const fx_buf *buf);
+/* Length mismatch is an error here (the reference panics, buffer.rs:100-110). */
+int fx_copy_to_host_f64(fx_ctx *ctx, const fx_buf *buf, double *dst, size_t len);
+int fx_copy_to_host_f32(fx_ctx *ctx, const fx_buf *buf, float *dst, size_t len);
+/* Host -> existing buffer (no reallocation), converting to the buffer's dtype. */
+int fx_write_f64(fx_ctx *ctx, fx_buf *buf, const double *src, size_t len);
+int fx_write_f32(fx_ctx *ctx, fx_buf *buf, const float *src, size_t len);
+
+/* ------------------------------------------------------------------ */
+/* Backend trait ops (crates/core/src/backend.rs)                      */
+/* ------------------------------------------------------------------ */
+
+/* apply_stencil :88-95 -- out = S(in); ring = boundary values. */
+int fx_apply_stencil(fx_ctx *ctx, const fx_buf *in, fx_buf *out, const fx_grid *g,
+                     const fx_stencil *s, const fx_boundaries *bc);
+/* apply_stencil_var :148-156 -- out = coeff .* S(in) (whole array). */
+int fx_apply_stencil_var(fx_ctx *ctx, const fx_buf *in, fx_buf *out, const fx_buf *coeff,
+                         const fx_grid *g, const fx_stencil *s, const fx_boundaries *bc);
+/* stencil_axpy :166-174 -- y[interior] += alpha * S(x); ring untouched. */
+int fx_stencil_axpy(fx_ctx *ctx, double alpha, const fx_buf *x, fx_buf *y, const fx_grid *g,
+                    const fx_stencil *s, const fx_boundaries *bc);
+int fx_copy(fx_ctx *ctx, const fx_buf *src, fx_buf *dst);                      /* :101-105 */
+int fx_fill(fx_ctx *ctx, fx_buf *buf, double value);                            /* :111-115 */
+int fx_axpy(fx_ctx *ctx, double alpha, const fx_buf *x, fx_buf *y);             /* :121-126 */
+int fx_scale(fx_ctx *ctx, fx_buf *buf, double alpha);                           /* :132-136 */
+int fx_norm_l2(fx_ctx *ctx, const fx_buf *buf, double *out);                    /* :180 */
+int fx_reduce_sum(fx_ctx *ctx, const fx_buf *buf, double *out);                 /* :188 */
+int fx_reduce_max(fx_ctx *ctx, const fx_buf *buf, double *out);                 /* :194 */
+int fx_reduce_min(fx_ctx *ctx, const fx_buf *buf, double *out);                 /* :200 */
+int fx_dot(fx_ctx *ctx, const fx_buf *x, const fx_buf *y, double *out);         /* :206-210 */
+/* dot2 :219-230 -- (a.b, c.d) in one pass. */
+int fx_dot2(fx_ctx *ctx, const fx_buf *a, const fx_buf *b, const fx_buf *c, const fx_buf *d,
+            double *ab, double *cd);
+/* restrict :240-246 (reference semantics: clamped 2x2 average). */
+int fx_restrict(fx_ctx *ctx, const fx_buf *fine, fx_buf *coarse, const fx_grid *fine_grid,
+                const fx_grid *coarse_grid);
+/* prolong :254-260 (reference semantics: fine[i,j] += coarse[i/2,j/2]). */
+int fx_prolong(fx_ctx *ctx, const fx_buf *coarse, fx_buf *fine, const fx_grid *coarse_grid,
+               const fx_grid *fine_grid);
+/* weighted_jacobi :269-277 -- reference CPU semantics: one in-place lexicographic sweep
+ * (ops.rs:425-473), bitwise equal to it. */
+int fx_weighted_jacobi(fx_ctx *ctx, fx_buf *x, const fx_buf *b, double omega, const fx_grid *g,
+                       const fx_stencil *s, const fx_boundaries *bc);
+int fx_pointwise_mult(fx_ctx *ctx, const fx_buf *x, const fx_buf *y, fx_buf *z); /* :285-290 */
+int fx_pointwise_div(fx_ctx *ctx, const fx_buf *x, const fx_buf *y, fx_buf *z);  /* :296-301 */
+int fx_waxpy(fx_ctx *ctx, double alpha, const fx_buf *x, double beta, const fx_buf *y,
+             fx_buf *w);                                                          /* :309-316 */
+int fx_aypx(fx_ctx *ctx, double alpha, const fx_buf *x, fx_buf *y);              /* :322-327 */
+int fx_reciprocal(fx_ctx *ctx, fx_buf *buf);                                     /* :333-336 */
+int fx_abs_val(fx_ctx *ctx, fx_buf *buf);                                        /* :342-345 */
+int fx_pointwise_max(fx_ctx *ctx, const fx_buf *x, const fx_buf *y, fx_buf *z);  /* :348-353 */
+int fx_pointwise_min(fx_ctx *ctx, const fx_buf *x, const fx_buf *y, fx_buf *z);  /* :356-361 */
+/* apply_conv_diff :375-384 -- out = kappa .* Lap(u) + v . grad(u) (upwind); ring = 0. */
+int fx_apply_conv_diff(fx_ctx *ctx, const fx_buf *u, fx_buf *out, const fx_buf *kappa,
+                       const fx_buf *vx, const fx_buf *vy, const fx_grid *g,
+                       const fx_boundaries *bc);
+/* conv_diff_axpy :395-405 -- out[interior] += alpha * (...); ring untouched. */
+int fx_conv_diff_axpy(fx_ctx *ctx, double alpha, const fx_buf *u, fx_buf *out,
+                      const fx_buf *kappa, const fx_buf *vx, const fx_buf *vy, const fx_grid *g,
+                      const fx_boundaries *bc);
+
+/* ------------------------------------------------------------------ */
+/* Non-trait fast paths (HipBackend extras, backend-hip/src/backend.rs:463-668) */
+/* ------------------------------------------------------------------ */
+
+/* zero_boundaries (backend.rs:510-531; field.rs:386-431) */
+int fx_zero_boundaries(fx_ctx *ctx, fx_buf *buf, size_t rows, size_t cols);
+/* pipelined_cg_fused (backend.rs:469-504): z=q+b*z; t=w+b*t; p=r+b*p; x+=a*p; r-=a*t; w-=a*z */
+int fx_pcg_fused_update(fx_ctx *ctx, double alpha, double beta, fx_buf *z, fx_buf *t, fx_buf *p,
+                        fx_buf *x, fx_buf *r, fx_buf *w, const fx_buf *q);
+/* Same update plus (r.r, r.w) of the updated r, w in the same pass. */
+int fx_pcg_fused_update_dot2(fx_ctx *ctx, double alpha, double beta, fx_buf *z, fx_buf *t,
+                             fx_buf *p, fx_buf *x, fx_buf *r, fx_buf *w, const fx_buf *q,
+                             double *rr, double *rw);
+
+/* ------------------------------------------------------------------ */
+/* Vertex-centred multigrid primitives (full weighting, bilinear prolongation, true weighted
+ * Jacobi).  Grids are (2^k+1) x (2^k+1)-style: fine = 2*(coarse-1)+1 in each direction.
+ * a5 = {centre, north, south, west, east} weights of the level operator.
+ * ------------------------------------------------------------------ */
+int fx_jacobi_sweep(fx_ctx *ctx, const fx_buf *x_in, fx_buf *x_out, const fx_buf *b,
+                    double omega, size_t rows, size_t cols, const double a5[5]);
+int fx_residual5(fx_ctx *ctx, const fx_buf *x, const fx_buf *b, fx_buf *r, size_t rows,
+                 size_t cols, const double a5[5]);
+int fx_restrict_fw(fx_ctx *ctx, const fx_buf *fine, fx_buf *coarse, size_t frows, size_t fcols,
+                   size_t crows, size_t ccols);
+int fx_prolong_bilinear(fx_ctx *ctx, const fx_buf *coarse, fx_buf *fine, size_t crows,
+                        size_t ccols, size_t frows, size_t fcols);
+
+/* ------------------------------------------------------------------ */
+/* Preconditioners (crates/runtime/src/preconditioner.rs:10-37; multigrid.rs) */
+/* ------------------------------------------------------------------ */
+
+/* Identity: z = r (preconditioner.rs:31-37). */
+int fx_precond_identity(fx_ctx *ctx, fx_precond **out);
+int fx_precond_destroy(fx_precond *pc);
+/* Preconditioner::apply(z, r) (preconditioner.rs:19-29).  The solvers zero-fill z first. */
+int fx_precond_apply(fx_precond *pc, fx_buf *z, const fx_buf *r);
+
+/* Multigrid::new / ::build (multigrid.rs:61-146): reference hierarchy (rows/2 per level,
+ * Laplacian on each level, clamped 2x2 restriction, piecewise-constant prolongation,
+ * lexicographic weighted-Jacobi smoother, coarsest level n_pre+n_post+10 sweeps).
+ * smoother: 0 = Jacobi (the Chebyshev smoother is not implemented: FX_ERR_UNSUPPORTED). */
+int fx_mg_create(fx_ctx *ctx, const fx_grid *g, const fx_boundaries *bc, size_t n_pre,
+                 size_t n_post, double omega, int smoother, fx_mg **out);
+
+/* Vertex-centred V-cycle for the operator actually solved, A = I + coeff*S with S a 5-point
+ * stencil: coarsening (rows-1)/2 per level down to an interior of at most coarse_max, full
+ * weighting, bilinear prolongation, n_pre/n_post true weighted-Jacobi sweeps (omega), and
+ * coarse_sweeps sweeps on the coarsest level.  dtype FX_F32 runs the cycle in single
+ * precision (inputs/outputs stay in their own dtype).  Homogeneous Dirichlet ring. */
+typedef struct {
+    size_t n_pre, n_post;
+    double omega;
+    size_t coarse_max;
+    size_t coarse_sweeps;
+    int dtype;
+    double op_coeff;
+    fx_stencil op_stencil;
+} fx_mg_vertex_opts;
+int fx_mg_create_vertex(fx_ctx *ctx, const fx_grid *g, const fx_boundaries *bc,
+                        const fx_mg_vertex_opts *opts, fx_mg **out);
+int fx_mg_destroy(fx_mg *mg);
+/* Multigrid::depth (multigrid.rs:174-178) */
+int fx_mg_depth(const fx_mg *mg, size_t *depth);
+int fx_mg_level_dims(const fx_mg *mg, size_t level, size_t *rows, size_t *cols);
+/* Multigrid::v_cycle (multigrid.rs:188-230): x (initial guess, in/out), b (rhs). */
+int fx_mg_v_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b);
+/* Borrowed view of the multigrid as a preconditioner (impl Preconditioner, :600-608).
+ * Valid until fx_mg_destroy; do not pass it to fx_precond_destroy. */
+fx_precond *fx_mg_as_precond(fx_mg *mg);
+
+/* ------------------------------------------------------------------ */
+/* Krylov solvers.  Operator A v = v + coeff * S v (linear_solver.rs:7-22).  `tol` is the
+ * absolute tolerance on ||r||_2 (cg.rs:61-64).  Solver parameters are fixed at creation, as
+ * the reference's `tol` / `max_iter` fields are; fx_*_set_params changes them.
+ * ------------------------------------------------------------------ */
+
+/* CgSolver (cg.rs:52-256) */
+int fx_cg_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, fx_cg **out);
+int fx_cg_destroy(fx_cg *s);
+int fx_cg_set_params(fx_cg *s, double tol, size_t max_iter);
+int fx_cg_solve(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                const fx_boundaries *bc, fx_stats *out);
+int fx_cg_solve_preconditioned(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff,
+                               const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
+                               fx_stats *out);
+
+/* PipelinedCgSolver (pipelined_cg.rs:25-237) */
+int fx_pipelined_cg_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter,
+                           fx_pipelined_cg **out);
+int fx_pipelined_cg_destroy(fx_pipelined_cg *s);
+int fx_pipelined_cg_set_params(fx_pipelined_cg *s, double tol, size_t max_iter);
+int fx_pipelined_cg_solve(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff,
+                          const fx_stencil *st, const fx_boundaries *bc, fx_stats *out);
+
+/* BiCgStabSolver (bicgstab.rs:19-346) */
+int fx_bicgstab_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter,
+                       fx_bicgstab **out);
+int fx_bicgstab_destroy(fx_bicgstab *s);
+int fx_bicgstab_set_params(fx_bicgstab *s, double tol, size_t max_iter);
+int fx_bicgstab_solve(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff,
+                      const fx_stencil *st, const fx_boundaries *bc, fx_stats *out);
+int fx_bicgstab_solve_preconditioned(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff,
+                                     const fx_stencil *st, const fx_boundaries *bc,
+                                     fx_precond *pc, fx_stats *out);
+
+/* GmresSolver (gmres.rs:24-491) */
+int fx_gmres_create(fx_ctx *ctx, const fx_grid *g, size_t restart, double tol, size_t max_iter,
+                    fx_gmres **out);
+int fx_gmres_destroy(fx_gmres *s);
+int fx_gmres_set_params(fx_gmres *s, double tol, size_t max_iter);
+int fx_gmres_solve(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                   const fx_boundaries *bc, fx_stats *out);
+int fx_gmres_solve_preconditioned(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff,
+                                  const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
+                                  fx_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLUXION_CUDA_H */

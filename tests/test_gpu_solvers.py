@@ -1,0 +1,258 @@
+"""GPU solver parity: the reference's solver known-answer tests through the CUDA path, the same
+solves run by the oracle (iteration counts and solutions), bitwise V-cycles, and solution-level
+checks against the exact FP64 DST-I Poisson solve."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import gaussian_ic, rel_err, sin_sin_field
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    from fluxion_b200 import Device
+    return Device.best()
+
+
+def _cn(n, coeff, dev):
+    """b = u + coeff*Lap(u), u the Gaussian IC (solvers.rs:53-63)."""
+    from fluxion_b200 import Boundaries, DType, Field, Grid, Stencil
+    h = 1.0 / (n - 1)
+    g = Grid.square(n, h)
+    st = Stencil.laplacian_2d_5pt(h, h)
+    bc = Boundaries.zero_dirichlet()
+    u = Field.from_f64(g, gaussian_ic(n, h), dev)
+    b = Field.zeros(g, DType.F64, dev)
+    b.copy_from(u)
+    tmp = Field.zeros(g, DType.F64, dev)
+    tmp.copy_from(u)
+    b.stencil_axpy(coeff, tmp, st, bc)
+    return g, st, bc, b
+
+
+# ---------------------------------------------------------------- reference known answers
+
+def test_cg_known_answers(dev):
+    from fluxion_b200 import CgSolver, ConvergenceReason, DType, Field, Identity
+    g, st, bc, b = _cn(32, -0.01, dev)
+    x = Field.zeros(g, DType.F64, dev)
+    s = CgSolver(g, dev, 1e-8, 500).solve(x, b, -0.01, st, bc)
+    assert s.converged() and s.iterations < 200  # solvers.rs:43-76
+    x0 = Field.zeros(g, DType.F64, dev)
+    s0 = CgSolver(g, dev, 1e-10, 100).solve(x0, Field.zeros(g, DType.F64, dev), -0.01, st, bc)
+    assert s0.converged() and s0.iterations == 0  # solvers.rs:79-97
+    x2 = Field.zeros(g, DType.F64, dev)
+    s2 = CgSolver(g, dev, 1e-8, 500).solve_preconditioned(x2, b, -0.01, st, bc, Identity())
+    assert s2.converged() and abs(s.iterations - s2.iterations) <= 2  # solvers.rs:101-154
+    h = 1.0 / 31
+    bb = Field.from_f64(g, gaussian_ic(32, h), dev)
+    xm = Field.zeros(g, DType.F64, dev)
+    sm = CgSolver(g, dev, 1e-15, 2).solve(xm, bb, -0.01, st, bc)
+    assert sm.reason == ConvergenceReason.MaxIterations and sm.iterations == 2  # solvers.rs:1151-1176
+    cg = CgSolver(g, dev, 1e-8, 500)
+    for _ in range(5):  # solvers.rs:1180-1218 (reuse)
+        assert cg.solve(Field.zeros(g, DType.F64, dev), b, -0.01, st, bc).converged()
+
+
+def test_pipelined_cg_matches_cg(dev):
+    from fluxion_b200 import CgSolver, DType, Field, PipelinedCgSolver
+    g, st, bc, b = _cn(32, -0.01, dev)
+    x1, x2 = Field.zeros(g, DType.F64, dev), Field.zeros(g, DType.F64, dev)
+    assert CgSolver(g, dev, 1e-8, 500).solve(x1, b, -0.01, st, bc).converged()
+    assert PipelinedCgSolver(g, dev, 1e-8, 500).solve(x2, b, -0.01, st, bc).converged()
+    assert np.max(np.abs(x1.to_vec_f64() - x2.to_vec_f64())) < 1e-6  # solvers.rs:322-379
+
+
+@pytest.mark.parametrize("coeff,tol,maxit,pc", [(-0.01, 1e-8, 500, False), (-0.01, 1e-8, 500, True),
+                                                (-0.5, 1e-6, 1000, False)])
+def test_bicgstab_converges(dev, coeff, tol, maxit, pc):
+    from fluxion_b200 import BiCgStabSolver, DType, Field, Identity
+    g, st, bc, b = _cn(32, coeff, dev)
+    x = Field.zeros(g, DType.F64, dev)
+    s = BiCgStabSolver(g, dev, tol, maxit)
+    stats = s.solve_preconditioned(x, b, coeff, st, bc, Identity()) if pc else s.solve(x, b, coeff, st, bc)
+    assert stats.converged()
+
+
+def test_gmres_known_answers(dev):
+    from fluxion_b200 import CgSolver, DType, Field, GmresSolver, Identity, LinearSolver
+    g, st, bc, b = _cn(32, -0.01, dev)
+    x = Field.zeros(g, DType.F64, dev)
+    assert GmresSolver(g, dev, 30, 1e-8, 500).solve(x, b, -0.01, st, bc).converged()
+    xc, xg = Field.zeros(g, DType.F64, dev), Field.zeros(g, DType.F64, dev)
+    CgSolver(g, dev, 1e-8, 500).solve(xc, b, -0.01, st, bc)
+    GmresSolver(g, dev, 50, 1e-8, 500).solve(xg, b, -0.01, st, bc)
+    assert np.max(np.abs(xc.to_vec_f64() - xg.to_vec_f64())) < 1e-6
+    x = Field.zeros(g, DType.F64, dev)
+    assert GmresSolver(g, dev, 30, 1e-8, 500).solve_preconditioned(x, b, -0.01, st, bc, Identity()).converged()
+    solver: LinearSolver = GmresSolver(g, dev, 30, 1e-8, 500)
+    assert solver.name() == "GMRES"
+    x = Field.zeros(g, DType.F64, dev)
+    s5 = GmresSolver(g, dev, 5, 1e-8, 500).solve(x, b, -0.01, st, bc)
+    assert s5.converged() and s5.iterations > 5
+    g2, st2, bc2, b2 = _cn(32, -0.5, dev)
+    x = Field.zeros(g2, DType.F64, dev)
+    assert GmresSolver(g2, dev, 100, 1e-6, 1000).solve(x, b2, -0.5, st2, bc2).converged()
+
+
+def test_multigrid_known_answers(dev):
+    from fluxion_b200 import Boundaries, DType, Field, Grid, Multigrid, Stencil
+    for n, depth in ((64, 5), (32, 4), (8, 2)):  # solvers.rs:813-841
+        assert Multigrid(Grid.square(n, 1.0 / (n - 1)), Boundaries.zero_dirichlet(), dev, 2, 2,
+                         2.0 / 3.0).depth() == depth
+    n = 64  # analytical.rs:447-521
+    h = 1.0 / (n - 1)
+    g = Grid.square(n, h)
+    bc = Boundaries.zero_dirichlet()
+    b = Field.from_f64(g, sin_sin_field(n, h), dev)
+    mg = Multigrid(g, bc, dev, 3, 3, 2.0 / 3.0)
+    x = Field.zeros(g, DType.F64, dev)
+    st = Stencil.laplacian_2d_5pt(h, h)
+    prev = np.inf
+    for _ in range(10):
+        mg.v_cycle(x, b)
+        ax = Field.zeros(g, DType.F64, dev)
+        x.apply_stencil_into(st, bc, ax)
+        r = Field.zeros(g, DType.F64, dev)
+        r.copy_from(b)
+        r.axpy(-1.0, ax)
+        res = np.sqrt(r.dot(r))
+        assert res < prev
+        prev = res
+    assert prev < 10.0
+
+
+# ---------------------------------------------------------------- parity with the oracle
+
+def _oracle_cn(n, coeff):
+    h = 1.0 / (n - 1)
+    st = O.laplacian_5pt(h, h)
+    u = gaussian_ic(n, h)
+    b = u.copy()
+    O.stencil_axpy(coeff, u.copy(), b, n, n, st)
+    return st, b
+
+
+@pytest.mark.parametrize("n,coeff", [(32, -0.01), (67, -0.05), (130, -0.002)])
+def test_solver_parity_with_oracle(dev, n, coeff):
+    from fluxion_b200 import BiCgStabSolver, CgSolver, DType, Field, GmresSolver, PipelinedCgSolver
+    g, st, bc, b = _cn(n, coeff, dev)
+    ost, ob = _oracle_cn(n, coeff)
+    assert np.array_equal(b.to_vec_f64(), ob)  # the rhs itself is bitwise equal
+    runs = {
+        "cg": (lambda x: CgSolver(g, dev, 1e-9, 2000).solve(x, b, coeff, st, bc),
+               lambda x: O.cg_solve(x, ob, n, n, coeff, ost, 1e-9, 2000)),
+        "pipelined": (lambda x: PipelinedCgSolver(g, dev, 1e-9, 2000).solve(x, b, coeff, st, bc),
+                      lambda x: O.pipelined_cg_solve(x, ob, n, n, coeff, ost, 1e-9, 2000)),
+        "bicgstab": (lambda x: BiCgStabSolver(g, dev, 1e-9, 2000).solve(x, b, coeff, st, bc),
+                     lambda x: O.bicgstab_solve(x, ob, n, n, coeff, ost, 1e-9, 2000)),
+        "gmres": (lambda x: GmresSolver(g, dev, 30, 1e-9, 2000).solve(x, b, coeff, st, bc),
+                  lambda x: O.gmres_solve(x, ob, n, n, coeff, ost, 30, 1e-9, 2000)),
+    }
+    for name, (gpu, ora) in runs.items():
+        x = Field.zeros(g, DType.F64, dev)
+        sg = gpu(x)
+        xo = np.zeros(n * n)
+        it, res, reason = ora(xo)
+        assert sg.converged() and reason == 0, name
+        assert abs(sg.iterations - it) <= 1, (name, sg.iterations, it)
+        # both solves stop at ||r|| < 1e-9; their solutions agree to that level
+        assert rel_err(x.to_vec_f64(), xo) < 1e-7, (name, rel_err(x.to_vec_f64(), xo))
+
+
+def test_reference_mg_vcycle_bitwise(dev):
+    """multigrid.rs V-cycle (reference semantics) is built from bitwise-exact ops."""
+    from fluxion_b200 import Boundaries, DType, Field, Grid, Multigrid
+    n = 64
+    h = 1.0 / (n - 1)
+    g = Grid.square(n, h)
+    rng = np.random.default_rng(4)
+    bvec = rng.uniform(-1, 1, n * n)
+    mg = Multigrid(g, Boundaries.zero_dirichlet(), dev, 2, 2, 2.0 / 3.0)
+    omg = O.Multigrid(n, n, h, h, 2, 2, 2.0 / 3.0, mode=0)
+    x = Field.zeros(g, DType.F64, dev)
+    b = Field.from_f64(g, bvec, dev)
+    xo = np.zeros(n * n)
+    for _ in range(3):
+        mg.v_cycle(x, b)
+        omg.v_cycle(xo, bvec)
+    assert np.array_equal(x.to_vec_f64(), xo)
+
+
+@pytest.mark.parametrize("n", [15, 63, 255])
+def test_vertex_mg_vcycle_bitwise(dev, n):
+    from fluxion_b200 import DType, Field, Multigrid
+    from fluxion_b200.workloads import poisson_problem
+    P = poisson_problem(n)
+    N = n + 2
+    mg = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200)
+    omg = O.Multigrid(N, N, P.h, P.h, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=P.stencil.as_triples(),
+                      coarse_max=15, coarse_sweeps=200)
+    assert mg.depth() == omg.depth()
+    rng = np.random.default_rng(n)
+    bvec = rng.uniform(-1, 1, N * N)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    b = Field.from_f64(P.grid, bvec, dev)
+    xo = np.zeros(N * N)
+    for _ in range(2):
+        mg.v_cycle(x, b)
+        omg.v_cycle(xo, bvec)
+    assert np.array_equal(x.to_vec_f64(), xo)
+
+
+# ---------------------------------------------------------------- solution level
+
+@pytest.mark.parametrize("n,pipelined", [(255, False), (255, True), (511, False)])
+def test_mg_pcg_poisson_matches_direct_solve(dev, n, pipelined):
+    from fluxion_b200 import CgSolver, DType, Field, Multigrid
+    from fluxion_b200.workloads import dst_poisson_solve, neg_laplacian_residual, poisson_problem, \
+        poisson_modes_rhs
+    P = poisson_problem(n)
+    f = poisson_modes_rhs(n, seed=12)
+    u_ref = dst_poisson_solve(f, n)
+    b = Field.from_f64(P.grid, f, dev)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    tol = 1e-10 * np.linalg.norm(f)
+    mg = Multigrid.vertex(P.grid, None, dev)
+    s = CgSolver(P.grid, dev, tol, 200).solve_preconditioned(x, b, P.coeff, P.stencil, None, mg)
+    assert s.converged() and s.iterations < 30
+    u = x.to_vec_f64()
+    assert neg_laplacian_residual(u, f, n) < 1.01e-10 * np.linalg.norm(f)
+    assert rel_err(u, u_ref) < 1e-8
+
+
+def test_f32_vcycle_preconditions_f64_pcg(dev):
+    from fluxion_b200 import CgSolver, DType, Field, Multigrid
+    from fluxion_b200.workloads import dst_poisson_solve, poisson_problem, poisson_uniform_rhs
+    n = 511
+    P = poisson_problem(n)
+    f = poisson_uniform_rhs(n, seed=3)
+    b = Field.from_f64(P.grid, f, dev)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    mg = Multigrid.vertex(P.grid, None, dev, dtype=DType.F32)
+    s = CgSolver(P.grid, dev, 1e-10 * np.linalg.norm(f), 200).solve_preconditioned(x, b, 1.0, P.stencil, None, mg)
+    assert s.converged()
+    assert rel_err(x.to_vec_f64(), dst_poisson_solve(f, n)) < 1e-8
+
+
+def test_config1_cg_on_gpu(dev):
+    """512^2 interior Poisson, f ~ U[-1,1], unpreconditioned CG to rel. residual 1e-8."""
+    from fluxion_b200 import CgSolver, DType, Field
+    from fluxion_b200.workloads import dst_poisson_solve, neg_laplacian_residual, poisson_problem, \
+        poisson_uniform_rhs
+    n = 512
+    P = poisson_problem(n)
+    f = poisson_uniform_rhs(n, seed=1)
+    b = Field.from_f64(P.grid, f, dev)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    s = CgSolver(P.grid, dev, 1e-8 * np.linalg.norm(f), 5000).solve(x, b, P.coeff, P.stencil, None)
+    assert s.converged()
+    u = x.to_vec_f64()
+    assert neg_laplacian_residual(u, f, n) < 1.01e-8 * np.linalg.norm(f)
+    ob = f.copy()
+    xo = np.zeros_like(f)
+    it, res, reason = O.cg_solve(xo, ob, n + 2, n + 2, 1.0, P.stencil.as_triples(), 1e-8 * np.linalg.norm(f), 5000)
+    assert reason == 0 and abs(it - s.iterations) <= 2
+    assert rel_err(u, xo) < 1e-6
