@@ -1,0 +1,443 @@
+#!/usr/bin/env python
+"""Benchmark: time to relative residual 1e-10 for the 4095^2 Poisson solve on one B200.
+
+Workload (one "step"): -Lap u = f on the unit square, 4095 x 4095 interior nodes (4097^2 grid
+with the Dirichlet ring), f = 32 seeded sin-sin modes (k, l in 1..64, N(0,1) amplitudes) plus
+1e-3 * U[-1,1] noise, u0 = 0, CG preconditioned by one V(2,2)-cycle per iteration (full
+weighting, bilinear prolongation, weighted Jacobi omega = 0.8, coarsest 15^2 with 200 sweeps)
+to ||r|| < 1e-10 ||f|| (verified in FP64 against the plain operator and against the exact
+DST-I solve).  Two variants are timed: the plain FP64 solve and the mixed one (FP64 CG,
+residual, update and inner products; FP32 V-cycle); `value` is the mixed one.
+
+Also reported: e2e time through the public API with the source and the solution in pinned host
+memory; the live roofline of the dominant kernel (CUDA events on its launching stream over the
+timed region); stencil / AXPY / dual-dot microbenchmarks on a 16384^2 grid; the CPU oracle on
+the host cores; SM clocks sampled during the timed region; the number of our kernel launches.
+
+`--impl reference` times the reference algorithm's CPU restatement (the oracle: the reference
+itself is Rust and cannot be built here) on all host cores, on a bounded sample of the same
+workload.  Under torchrun (N > 1) every rank solves its own replica (no data-path exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to rel-resid 1e-10: learned/mixed vs plain (1 B200); stencil GB/s"
+N_INTERIOR = 4095
+SEED = 2024
+
+# algorithmic bytes per grid point of each kernel (F64 sizes; F32 kernels carry a _f32 tag)
+BYTES_PER_POINT = {
+    "mg_sweep": 3, "mg_residual": 3, "mg_prolong_bilinear": 2.25, "mg_restrict_fw": 5, "mg_zero": 1,
+    "pcg_dir": 3, "pcg_update": 5, "pcg_rz": 2, "pcg_init": 3,
+}
+# element-size multiplier is applied per dtype: F64 -> 8 bytes, F32 -> 4 bytes (see roofline())
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=N_INTERIOR, help="interior nodes per direction")
+    p.add_argument("--no-micro", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu_index)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU oracle timing
+
+def cpu_oracle_estimate(n: int, f: np.ndarray, iters_needed: int):
+    """Time the oracle's MG-PCG (same algorithm, FP64) on all host threads on a bounded sample:
+    solves stopped after 1 and 3 iterations; extrapolate to `iters_needed` iterations."""
+    from oracle import oracle as O
+    from fluxion_b200.workloads import poisson_problem
+
+    O.set_threads(os.cpu_count() or 1)
+    P = poisson_problem(n)
+    N = n + 2
+    mg = O.Multigrid(N, N, P.h, P.h, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=P.stencil.as_triples(),
+                     coarse_max=15, coarse_sweeps=200)
+    tol = 1e-10 * float(np.linalg.norm(f))
+    times = {}
+    for k in (1, 3):
+        x = np.zeros(N * N)
+        t0 = time.perf_counter()
+        O.cg_solve(x, f, N, N, 1.0, P.stencil.as_triples(), tol, k, pc=mg)
+        times[k] = time.perf_counter() - t0
+    per_iter = (times[3] - times[1]) / 2.0
+    est = times[1] + per_iter * max(iters_needed - 1, 0)
+    return est, O.get_threads(), (f"MG-PCG solves of the {n}^2 problem stopped after 1 and 3 iterations "
+                                  f"({times[1]:.2f} s, {times[3]:.2f} s), extrapolated to the {iters_needed} "
+                                  f"iterations the solve needs")
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from fluxion_b200.workloads import poisson_modes_rhs
+    from oracle import oracle as O
+    from fluxion_b200.workloads import poisson_problem
+
+    n = args.n
+    f = poisson_modes_rhs(n, SEED)
+    O.set_threads(os.cpu_count() or 1)
+    P = poisson_problem(n)
+    N = n + 2
+    mg = O.Multigrid(N, N, P.h, P.h, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=P.stencil.as_triples(),
+                     coarse_max=15, coarse_sweeps=200)
+    tol = 1e-10 * float(np.linalg.norm(f))
+    # iterations the CPU solve needs: one full solve on a 1023^2 copy of the problem class (the
+    # V-cycle makes the count grid-independent); each timed step is a bounded 1- and 3-iteration
+    # sample of the full-size solve.
+    nsm = 1023
+    Ps = poisson_problem(nsm)
+    fs = poisson_modes_rhs(nsm, SEED)
+    mgs = O.Multigrid(nsm + 2, nsm + 2, Ps.h, Ps.h, 2, 2, 0.8, mode=1, op_coeff=1.0,
+                      entries=Ps.stencil.as_triples(), coarse_max=15, coarse_sweeps=200)
+    xs = np.zeros((nsm + 2) ** 2)
+    iters, _, _ = O.cg_solve(xs, fs, nsm + 2, nsm + 2, 1.0, Ps.stencil.as_triples(),
+                             1e-10 * float(np.linalg.norm(fs)), 200, pc=mgs)
+    samples = []
+    for step in range(args.warmup + args.steps):
+        t = {}
+        for k in (1, 3):
+            x = np.zeros(N * N)
+            t0 = time.perf_counter()
+            O.cg_solve(x, f, N, N, 1.0, P.stencil.as_triples(), tol, k, pc=mg)
+            t[k] = time.perf_counter() - t0
+        est = t[1] + (t[3] - t[1]) / 2.0 * max(iters - 1, 0)
+        if step >= args.warmup:
+            samples.append(est)
+    v = float(np.mean(samples))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"poisson_{n}sq_mg_pcg_rel1e-10", "grid": f"{N}x{N} incl. ring",
+                   "solver": "CG + V(2,2) FW/bilinear/weighted-Jacobi 0.8, coarsest 15^2 x 200 (CPU restatement)"},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": O.get_threads(), "kind": "port",
+                         "sample": f"per step: full-size MG-PCG stopped after 1 and 3 iterations, extrapolated "
+                                   f"to the {iters} iterations the solve needs (counted on the 1023^2 problem)"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference is Rust (no cargo/rustc here); its CPU backend is timed as the C restatement",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from fluxion_b200 import CgSolver, DType, Device, Field, Multigrid
+    from fluxion_b200 import _lib as L
+    from fluxion_b200.workloads import dst_poisson_solve, neg_laplacian_residual, poisson_modes_rhs, \
+        poisson_problem
+
+    peak, peak_kind = measured_peaks()
+    dev = Device.Cuda(local)
+    be = dev.backend()
+    stream = torch.cuda.Stream(device=local)
+    be.set_stream(stream.cuda_stream)
+
+    n = args.n
+    P = poisson_problem(n)
+    N = n + 2
+    f = poisson_modes_rhs(n, SEED + rank)
+    fnorm = float(np.linalg.norm(f))
+    tol = 1e-10 * fnorm
+    b = Field.from_f64(P.grid, f, dev)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    cg = CgSolver(P.grid, dev, tol, 100)
+    mg64 = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200, DType.F64)
+    mg32 = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200, DType.F32)
+
+    def solve(mg):
+        x.fill(0.0)
+        return cg.solve_preconditioned(x, b, P.coeff, P.stencil, None, mg)
+
+    def timed(mg, k, w, kernel=None):
+        for _ in range(w):
+            solve(mg)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = be.launch_count()
+        if kernel:
+            L.lib().fx_ctx_timing_begin(be.ctx, kernel.encode())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = None
+        for _ in range(k):
+            st = solve(mg)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ktime = None
+        if kernel:
+            import ctypes as C
+            ms, cnt, pts = C.c_double(), C.c_ulonglong(), C.c_double()
+            L.lib().fx_ctx_timing_end(be.ctx, C.byref(ms), C.byref(cnt), C.byref(pts))
+            ktime = (ms.value, cnt.value, pts.value)
+        launches = be.launch_count() - l0
+        ms_total = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms_total], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_total = float(t.item())
+        return ms_total / k, st, launches, ktime
+
+    # which kernel dominates the mixed solve? (one untimed solve per candidate)
+    import ctypes as C
+    candidates = ["mg_sweep", "pcg_update", "pcg_dir", "mg_residual", "mg_restrict_fw",
+                  "mg_prolong_bilinear", "pcg_rz", "mg_convert", "mg_zero", "mg_coarse_solve"]
+    solve(mg32)
+    shares = {}
+    for kname in candidates:
+        L.lib().fx_ctx_timing_begin(be.ctx, kname.encode())
+        solve(mg32)
+        ms, cnt, pts = C.c_double(), C.c_ulonglong(), C.c_double()
+        L.lib().fx_ctx_timing_end(be.ctx, C.byref(ms), C.byref(cnt), C.byref(pts))
+        shares[kname] = ms.value
+    dom = max(shares, key=shares.get)
+
+    # plain FP64 and mixed solves
+    plain_ms, st64, _, _ = timed(mg64, args.steps, args.warmup)
+    u64 = x.to_vec_f64()
+    with ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else
+                      int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])) as clk:
+        mixed_ms, st32, launches, ktime = timed(mg32, args.steps, args.warmup, kernel=dom)
+    u32 = x.to_vec_f64()
+
+    # verification in FP64 (plain operator) and against the exact DST-I solve
+    u_ref = dst_poisson_solve(f, n)
+    err32 = float(np.linalg.norm(u32 - u_ref) / np.linalg.norm(u_ref))
+    err64 = float(np.linalg.norm(u64 - u_ref) / np.linalg.norm(u_ref))
+    rr32 = neg_laplacian_residual(u32, f, n) / fnorm
+    rr64 = neg_laplacian_residual(u64, f, n) / fnorm
+
+    # e2e: host f (pinned) -> solve -> host u (pinned), through the public API
+    f_host = torch.empty(N * N, dtype=torch.float64, pin_memory=True).numpy()
+    f_host[:] = f
+    u_host = torch.empty(N * N, dtype=torch.float64, pin_memory=True).numpy()
+
+    def e2e_step():
+        b.write(f_host)
+        x.fill(0.0)
+        cg.solve_preconditioned(x, b, P.coeff, P.stencil, None, mg32)
+        x.storage.copy_to_host_f64(u_host)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - w0) * 1e3) / args.steps
+    if dist:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_ok = bool(np.array_equal(u_host, u32))
+
+    # roofline of the dominant kernel, live over the timed mixed solves
+    roof = None
+    if ktime and ktime[1] > 0:
+        esize = 4 if dom.startswith("mg_") and dom not in ("mg_convert",) else 8
+        bpp = BYTES_PER_POINT.get(dom, 3) * esize
+        if dom == "mg_convert":
+            bpp = 12
+        avg_ms = ktime[0] / ktime[1]
+        bytes_per_launch = ktime[2] / ktime[1] * bpp
+        achieved = bytes_per_launch / (avg_ms * 1e-3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", f"{dom}_traffic.txt")
+        if os.path.exists(tp):
+            for ln in open(tp):
+                if ln.startswith("dram_bytes_per_point:"):
+                    traffic = float(ln.split(":")[1]) * ktime[2] / ktime[1]
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_per_launch, "bytes_per_point": bpp,
+                "launches": ktime[1], "avg_launch_ms": avg_ms,
+                "share_of_solve": (ktime[0] / args.steps) / mixed_ms}
+
+    micro = None
+    if not args.no_micro:
+        micro = microbench(be, peak, args, stream)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            est, cores, sample = cpu_oracle_estimate(n, f, int(st64.iterations))
+            cpu = {"value": est, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": mixed_ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mixed_ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 Krylov/residual/update + f32 V-cycle",
+            "data": "synthetic (seeded 32-mode sin-sin source + 1e-3 uniform noise)",
+            "config": {"workload": f"poisson_{n}sq_mg_pcg_rel1e-10", "grid": f"{N}x{N} incl. Dirichlet ring",
+                       "solver": "CG + V(2,2) full weighting / bilinear / weighted Jacobi 0.8, coarsest 15^2 x 200",
+                       "tolerance": "||r||_2 < 1e-10 ||f||_2", "l2": "inputs larger than L2 (134 MB per vector)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "iterations": int(st32.iterations), "rel_residual_fp64": rr32, "err_vs_fp64_direct": err32,
+            "plain_fp64": {"value": plain_ms / 1e3, "unit": "s", "iterations": int(st64.iterations),
+                           "rel_residual_fp64": rr64, "err_vs_fp64_direct": err64},
+            "speedup_mixed_vs_plain": plain_ms / mixed_ms,
+            "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": N * N * 8,
+                    "d2h_bytes_per_step": N * N * 8, "result_matches_device_run": e2e_ok},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "gpu_launches": int(launches), "kernel_time_shares_ms": shares, "microbench": micro,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def microbench(be, peak, args, stream):
+    """Stencil / stencil-AXPY / AXPY / dual-dot on a 16384^2 grid (inputs far above L2)."""
+    import torch
+    from fluxion_b200 import Boundaries, DType, Grid, Stencil
+
+    n = 16384
+    g = Grid.square(n, 1.0 / (n - 1))
+    st = Stencil.laplacian_2d_5pt(g.dx, g.dy)
+    bc = Boundaries.zero_dirichlet()
+    out = {}
+    reps = max(5, args.steps)
+    for dt, es in ((DType.F64, 8), (DType.F32, 4)):
+        a = be.allocate(n * n, dt)
+        c = be.allocate(n * n, dt)
+        be.fill(a, 1.0)
+        cases = {
+            "stencil": (lambda: be.apply_stencil(a, c, g, st, bc), 2 * es),
+            "stencil_axpy": (lambda: be.stencil_axpy(0.5, a, c, g, st, bc), 3 * es),
+            "axpy": (lambda: be.axpy(0.5, a, c), 3 * es),
+            "dot2": (lambda: be.dot2(a, c, c, c), 2 * es),  # (a.c, c.c): 2 distinct vectors read
+        }
+        for name, (fn, bpp) in cases.items():
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)  # the stream every library kernel is launched on
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            gbs = n * n * bpp / (ms * 1e-3) / 1e9
+            out[f"{name}_{dt.name.lower()}"] = {"GBps": gbs, "frac_of_measured_peak": gbs / peak,
+                                                "ms": ms, "bytes_per_point": bpp}
+        a.free()
+        c.free()
+    return out
+
+
+if __name__ == "__main__":
+    sys.exit(main())

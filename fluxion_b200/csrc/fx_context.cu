@@ -26,6 +26,32 @@ int check_launch(fx_ctx *ctx, const char *what) {
     return FX_OK;
 }
 
+void timing_pre(fx_ctx *ctx, const char *what) {
+    if (!ctx->timing || ctx->timing_name != what) return;
+    if (ctx->pool_next + 2 > ctx->event_pool.size()) {
+        for (int i = 0; i < 64; i++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return;
+            ctx->event_pool.push_back(e);
+        }
+    }
+    fx_timing_rec r;
+    r.a = ctx->event_pool[ctx->pool_next++];
+    r.b = ctx->event_pool[ctx->pool_next++];
+    r.points = 0;
+    cudaEventRecord(r.a, ctx->stream);
+    ctx->timing_recs.push_back(r);
+    ctx->timing_open = true;
+}
+
+void timing_post(fx_ctx *ctx, double points) {
+    if (!ctx->timing_open) return;
+    fx_timing_rec &r = ctx->timing_recs.back();
+    cudaEventRecord(r.b, ctx->stream);
+    r.points = points;
+    ctx->timing_open = false;
+}
+
 int check_buf(const fx_buf *b, const char *name) {
     if (!b) return fail(FX_ERR_INVALID_ARGUMENT, std::string("null buffer: ") + name);
     return FX_OK;
@@ -219,6 +245,7 @@ int fx_ctx_destroy(fx_ctx *c) {
     if (c->d_result) cudaFree(c->d_result);
     if (c->h_result) cudaFreeHost(c->h_result);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    for (auto e : c->event_pool) cudaEventDestroy(e);
     delete c;
     return FX_OK;
 }
@@ -238,6 +265,35 @@ int fx_ctx_set_stream(fx_ctx *c, void *stream) {
 void *fx_ctx_get_stream(fx_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 unsigned long long fx_ctx_launch_count(fx_ctx *c) { return c ? c->launches : 0ull; }
+
+int fx_ctx_timing_begin(fx_ctx *c, const char *kernel) {
+    if (!c || !kernel) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    c->timing = true;
+    c->timing_name = kernel;
+    c->timing_recs.clear();
+    c->pool_next = 0;
+    c->timing_open = false;
+    return FX_OK;
+}
+
+int fx_ctx_timing_end(fx_ctx *c, double *total_ms, unsigned long long *launches, double *total_points) {
+    if (!c || !total_ms || !launches || !total_points) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_CUDA(cudaStreamSynchronize(c->stream));
+    double ms = 0.0, pts = 0.0;
+    for (auto &r : c->timing_recs) {
+        float t = 0.f;
+        FX_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+        ms += t;
+        pts += r.points;
+    }
+    *total_ms = ms;
+    *launches = c->timing_recs.size();
+    *total_points = pts;
+    c->timing = false;
+    c->timing_recs.clear();
+    c->pool_next = 0;
+    return FX_OK;
+}
 
 int fx_alloc(fx_ctx *ctx, size_t len, int dtype, fx_buf **out) {
     if (!ctx || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");

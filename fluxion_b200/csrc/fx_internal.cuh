@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/fluxion_cuda.h"
 
@@ -41,6 +42,11 @@ constexpr int kBlock = 256;  // threads per block for grid kernels (8 warps)
 
 }  // namespace fx
 
+struct fx_timing_rec {
+    cudaEvent_t a, b;
+    double points;
+};
+
 struct fx_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -51,6 +57,13 @@ struct fx_ctx {
     double *d_result = nullptr;    // results of standalone reductions [kMaxSums]
     double *h_result = nullptr;    // pinned mirror
     unsigned long long launches = 0;
+    // per-kernel timing (fx_ctx_timing_begin / _end)
+    bool timing = false;
+    std::string timing_name;
+    std::vector<fx_timing_rec> timing_recs;
+    std::vector<cudaEvent_t> event_pool;
+    size_t pool_next = 0;
+    bool timing_open = false;
 };
 
 struct fx_buf {
@@ -64,6 +77,9 @@ struct fx_buf {
 namespace fx {
 
 int check_launch(fx_ctx *ctx, const char *what);
+// Timing hooks around a launch (no-ops unless fx_ctx_timing_begin named this kernel).
+void timing_pre(fx_ctx *ctx, const char *what);
+void timing_post(fx_ctx *ctx, double points);
 
 inline size_t elem_size(int dtype) { return dtype == FX_F32 ? 4 : 8; }
 
@@ -374,7 +390,9 @@ int launch_march(fx_ctx *ctx, const MarchGeom &G, Loader ld, Point pt, Fin fin,
                  const int *skip, const char *what) {
     const int blocks = (G.nwarps + (kBlock / 32) - 1) / (kBlock / 32);
     if (K > 0 && blocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");
+    timing_pre(ctx, what);
     k_march<T, U, K><<<blocks, kBlock, 0, ctx->stream>>>(G, ld, pt, fin, red_args<K>(ctx), skip);
+    timing_post(ctx, (double)G.rows * (double)G.cols);
     return check_launch(ctx, what);
 }
 
@@ -403,7 +421,9 @@ template <int K, typename F, typename Fin>
 int launch_flat(fx_ctx *ctx, size_t n, F f, Fin fin, const int *skip, const char *what) {
     FlatGeom g = flat_geom(ctx, n);
     if (g.blocks == 0) return FX_OK;
+    timing_pre(ctx, what);
     k_flat<K><<<g.blocks, kBlock, 0, ctx->stream>>>(n, f, fin, red_args<K>(ctx), skip);
+    timing_post(ctx, (double)n);
     return check_launch(ctx, what);
 }
 

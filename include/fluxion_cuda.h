@@ -114,6 +114,12 @@ int fx_ctx_set_stream(fx_ctx *ctx, void *stream);
 void *fx_ctx_get_stream(fx_ctx *ctx);
 /* Number of kernels this context has launched (for launch accounting). */
 unsigned long long fx_ctx_launch_count(fx_ctx *ctx);
+/* Per-kernel timing: from fx_ctx_timing_begin until fx_ctx_timing_end, every launch of the
+ * kernel named `kernel` is bracketed by CUDA events on the launching stream.  End returns the
+ * summed device time, the launch count and the summed grid points those launches covered. */
+int fx_ctx_timing_begin(fx_ctx *ctx, const char *kernel);
+int fx_ctx_timing_end(fx_ctx *ctx, double *total_ms, unsigned long long *launches,
+                      double *total_points);
 
 /* ------------------------------------------------------------------ */
 /* Memory (Backend::allocate / upload_f64 / upload_f32, backend.rs:49-77;
