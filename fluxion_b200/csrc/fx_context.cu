@@ -144,22 +144,37 @@ int make_bc(const fx_boundaries *bc, double dx, double dy, BcP *P, bool reject_p
     return FX_OK;
 }
 
-MarchGeom march_geom(fx_ctx *ctx, size_t rows, size_t cols, int U) {
+MarchGeom march_geom(size_t rows, size_t cols, int bx, int d, int capacity) {
     MarchGeom G;
     G.rows = (int)rows;
     G.cols = (int)cols;
-    G.nstrips = (int)((cols + 31) / 32);
-    // Aim for about 64 resident warps per SM worth of work items; chunks at least 2U rows.
-    const long target = (long)ctx->num_sms * 64;
-    long chunks = target / G.nstrips;
-    if (chunks < 1) chunks = 1;
-    long cr = ((long)rows + chunks - 1) / chunks;
-    const long min_rows = 2 * U;
-    if (cr < min_rows) cr = min_rows;
-    cr = ((cr + U - 1) / U) * U;
+    G.nbands = (int)((cols - 1 + bx - 1) / bx);
+    if (G.nbands < 1) G.nbands = 1;
+    // Split the rows into chunks so that bands x chunks fills whole waves of resident CTAs
+    // (one work item per CTA, equal work per item); chunks stay at least 4*d rows long.
+    const long R = (long)rows, B = G.nbands;
+    long best_chunks = 1;
+    double best_eff = -1.0;
+    for (int w = 1; w <= 8; w++) {
+        long chunks = (long)w * capacity / B;
+        if (chunks < 1) chunks = 1;
+        long cr = (R + chunks - 1) / chunks;
+        if (cr < 4 * d) cr = 4 * d;
+        cr = ((cr + d - 1) / d) * d;
+        chunks = (R + cr - 1) / cr;
+        const long nb = chunks * B;
+        const long waves = (nb + capacity - 1) / capacity;
+        const double eff = (double)nb / (double)(waves * capacity);
+        if (eff > best_eff + 0.02) {
+            best_eff = eff;
+            best_chunks = chunks;
+        }
+    }
+    long cr = (R + best_chunks - 1) / best_chunks;
+    if (cr < 4 * d) cr = 4 * d;
+    cr = ((cr + d - 1) / d) * d;
     G.chunk_rows = (int)cr;
-    const long nchunks = ((long)rows + cr - 1) / cr;
-    G.nwarps = (int)(nchunks * G.nstrips);
+    G.nblocks = (int)(((R + cr - 1) / cr) * B);
     return G;
 }
 

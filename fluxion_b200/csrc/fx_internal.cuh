@@ -39,6 +39,7 @@ int fail(int code, const std::string &msg);
 constexpr int kMaxRedBlocks = 1 << 16;
 constexpr int kMaxSums = 4;
 constexpr int kBlock = 256;  // threads per block for grid kernels (8 warps)
+constexpr int kBandThreads = kBlock + 32;  // band kernels: 8 column warps + 1 halo warp
 
 }  // namespace fx
 
@@ -149,7 +150,7 @@ __device__ __forceinline__ void warp_reduce(CSum (&acc)[K]) {
 // Reduce acc over the block; result valid in thread 0.
 template <int K>
 __device__ __forceinline__ void block_reduce(CSum (&acc)[K]) {
-    __shared__ CSum sh[kBlock / 32][K > 0 ? K : 1];
+    __shared__ CSum sh[32][K > 0 ? K : 1];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     warp_reduce<K>(acc);
     if (lane == 0) {
@@ -282,100 +283,167 @@ __device__ __forceinline__ T stencil_eval(const StencilP &P, const Nb<T> &v) {
     }
 }
 
-// ------------------------------------------------------------------ row-marching framework
+// ------------------------------------------------------------------ band-marching framework
 //
-// A warp owns a strip of 32 consecutive columns and marches down a chunk of rows,
-// keeping the rows above, at and below the current one in registers.  Each row of
-// the marched field is loaded exactly once per warp (one coalesced 32-wide load plus
-// two halo values for the strip edges, exchanged by shuffles), so the field costs one
-// HBM read per element instead of five.  U rows are loaded per step so that U
-// independent loads are in flight per thread.
+// A CTA owns a band of BX = 256*CPT consecutive columns (the first band starts at column 1)
+// and marches down a chunk of rows: 8 warps hold the band columns, a 9th warp loads the two
+// halo columns (its lane 0 also computes column 0 in band 0).  The rows above, at and below the current one live in a
+// 4-row shared-memory ring (plus one halo column on each side).  Every value a point needs
+// from HBM -- the marched field row r+1 and the NA per-point "aux" arrays of row r -- is
+// prefetched D rows ahead through a register FIFO, so D rows of loads are always in flight
+// and no load sits on the critical path of the compute.  One __syncthreads per row.
 //
-// Loader  : T operator()(size_t idx) const       -- value of the marched field at idx
-//           (may combine several arrays, e.g. r + beta*p for a fused CG update).
-// Point   : void operator()(int r, int c, size_t idx, const Nb<T>& nb, CSum* acc) const
-//           -- called for every grid point (r, c) of the chunk, ring included.
+// Loader : T operator()(size_t idx) const -- value of the marched field at idx (may
+//          combine several arrays, e.g. r + beta*p for a fused CG update).
+// Point  : static constexpr int NA;  const T *aux(int k) const;
+//          void operator()(bool ring, int r, int c, size_t idx, const Nb<T>& nb, const T *a,
+//                          CSum *acc)
+//          -- called once for every grid point with ring = (point on the boundary ring) and
+//          a[k] = aux(k)[idx].
 // The kernel ends with a grid reduction of K compensated sums and a finaliser.
 
 struct MarchGeom {
     int rows, cols;
-    int nstrips;
-    int chunk_rows;  // multiple of U
-    int nwarps;      // strips * chunks
+    int nbands;
+    int chunk_rows;  // multiple of D
+    int nblocks;     // bands * chunks
 };
 
-MarchGeom march_geom(fx_ctx *ctx, size_t rows, size_t cols, int U);
+// capacity: CTAs of the kernel resident on the whole GPU at once
+MarchGeom march_geom(size_t rows, size_t cols, int bx, int d, int capacity);
 
-template <typename T, int U, int K, typename Loader, typename Point, typename Fin>
-__global__ void __launch_bounds__(kBlock) k_march(MarchGeom G, Loader ld, Point pt, Fin fin,
-                                                  RedArgs<K> ra, const int *skip) {
+template <typename T>
+constexpr int band_cpt() {
+    return sizeof(T) == 8 ? 1 : 2;
+}
+
+template <int NA>
+constexpr int band_depth() {
+    return NA == 0 ? 8 : (NA == 1 ? 4 : 3);
+}
+
+template <typename T, int CPT, int D, int K, typename Loader, typename Point, typename Fin>
+__global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader ld, Point pt, Fin fin,
+                                                           RedArgs<K> ra, const int *skip) {
     if (skip && *(volatile const int *)skip) return;
+    constexpr int BX = kBlock * CPT;
+    constexpr int W = BX + 2;
+    constexpr int NA = Point::NA;
+    __shared__ T ring[4][W];
     CSum acc[K > 0 ? K : 1];
 #pragma unroll
     for (int k = 0; k < (K > 0 ? K : 1); k++) acc[k] = CSum{0.0, 0.0};
 
-    const int lane = threadIdx.x & 31;
-    const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
-    if (gw < G.nwarps) {
-        const int strip = gw % G.nstrips;
-        const int chunk = gw / G.nstrips;
-        const int r0 = chunk * G.chunk_rows;
-        const int r1 = min(r0 + G.chunk_rows, G.rows);
-        const int col0 = strip * 32;
-        const int col = col0 + lane;
-        const bool cin = col < G.cols;
-        const bool has_w = col0 > 0;
-        const bool has_e = col0 + 32 < G.cols;
-        auto load = [&](int r, T &v, T &hw, T &he) {
-            v = (T)0;
-            hw = (T)0;
-            he = (T)0;
-            if (r >= 0 && r < G.rows) {
-                const size_t base = (size_t)r * G.cols;
-                if (cin) v = ld(base + col);
-                if (lane == 0 && has_w) hw = ld(base + col0 - 1);
-                if (lane == 31 && has_e) he = ld(base + col0 + 32);
-            }
-        };
-        // window: index 0 = row r-1, 1 = row r, ..., U+1 = row r+U
-        T v[U + 2], hw[U + 2], he[U + 2];
-        load(r0 - 1, v[0], hw[0], he[0]);
-        load(r0, v[1], hw[1], he[1]);
-        for (int r = r0; r < r1; r += U) {
+    const int t = threadIdx.x;
+    const int band = blockIdx.x % G.nbands;
+    const int chunk = blockIdx.x / G.nbands;
+    const int c0 = 1 + band * BX;
+    const int r0 = chunk * G.chunk_rows;
+    const int r1 = min(r0 + G.chunk_rows, G.rows);
+    const int rows = G.rows, cols = G.cols;
+
+    // column warps: slot s -> column c0 + t + s*256 (smem index 1 + t + s*256)
+    // halo warp (t >= 256): lane 0 -> column c0-1 (smem 0; in band 0 that is column 0, which
+    // this lane also computes), lane 1 -> column c0+BX (smem BX+1, halo only)
+    const bool halo_warp = t >= kBlock;
+    const int hl = t - kBlock;
+    int col[CPT], sidx[CPT];
+    bool valid[CPT], point[CPT], ringcol[CPT];
 #pragma unroll
-            for (int u = 0; u < U; u++) load(r + 1 + u, v[u + 2], hw[u + 2], he[u + 2]);
-            // west / east neighbours of every window row
-            T wv[U + 2], ev[U + 2];
+    for (int s = 0; s < CPT; s++) {
+        if (!halo_warp) {
+            col[s] = c0 + t + s * kBlock;
+            sidx[s] = 1 + t + s * kBlock;
+            valid[s] = col[s] < cols;
+            point[s] = valid[s];
+            ringcol[s] = col[s] == cols - 1;
+        } else {
+            col[s] = (hl == 0) ? c0 - 1 : c0 + BX;
+            sidx[s] = (hl == 0) ? 0 : BX + 1;
+            valid[s] = s == 0 && ((hl == 0) || (hl == 1 && c0 + BX < cols));
+            point[s] = s == 0 && hl == 0 && band == 0;
+            ringcol[s] = true;  // the only computed halo-warp point is column 0
+        }
+    }
+    const bool writes_smem = !halo_warp || hl < 2;
+
+    T fv[D][CPT];                      // marched field, row r+1 (D rows ahead)
+    T fa[D][CPT][NA > 0 ? NA : 1];     // aux arrays, row r (D rows ahead)
+
+    auto load_field = [&](int r, T (&v)[CPT]) {
 #pragma unroll
-            for (int u = 0; u < U + 2; u++) {
-                T up = __shfl_up_sync(0xffffffffu, v[u], 1);
-                T dn = __shfl_down_sync(0xffffffffu, v[u], 1);
-                wv[u] = lane == 0 ? hw[u] : up;
-                ev[u] = lane == 31 ? he[u] : dn;
-            }
+        for (int s = 0; s < CPT; s++) {
+            v[s] = (T)0;
+            if (r >= 0 && r < rows && valid[s]) v[s] = ld((size_t)r * cols + col[s]);
+        }
+    };
+    auto load_aux = [&](int r, T (&a)[CPT][NA > 0 ? NA : 1]) {
+        if constexpr (NA > 0) {
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int rr = r + u;
-                if (rr < r1 && cin) {
-                    Nb<T> nb;
-                    nb.c = v[u + 1];
-                    nb.n = v[u];
-                    nb.s = v[u + 2];
-                    nb.w = wv[u + 1];
-                    nb.e = ev[u + 1];
-                    nb.nw = wv[u];
-                    nb.ne = ev[u];
-                    nb.sw = wv[u + 2];
-                    nb.se = ev[u + 2];
-                    pt(rr, col, (size_t)rr * G.cols + col, nb, acc);
+            for (int s = 0; s < CPT; s++) {
+#pragma unroll
+                for (int k = 0; k < NA; k++) {
+                    a[s][k] = (T)0;
+                    if (point[s] && r < r1) a[s][k] = pt.aux(k)[(size_t)r * cols + col[s]];
                 }
             }
-            v[0] = v[U];
-            hw[0] = hw[U];
-            he[0] = he[U];
-            v[1] = v[U + 1];
-            hw[1] = hw[U + 1];
-            he[1] = he[U + 1];
+        }
+    };
+    auto store_row = [&](int r, const T (&v)[CPT]) {
+        if (!writes_smem) return;
+        T *row = ring[r & 3];
+#pragma unroll
+        for (int s = 0; s < CPT; s++)
+            if (!halo_warp || s == 0) row[sidx[s]] = v[s];
+    };
+
+    {
+        T v[CPT];
+        load_field(r0 - 1, v);
+        store_row(r0 + 3, v);  // (r0 - 1) & 3 without a negative operand
+        load_field(r0, v);
+        store_row(r0, v);
+    }
+#pragma unroll
+    for (int u = 0; u < D; u++) {
+        load_field(r0 + 1 + u, fv[u]);
+        load_aux(r0 + u, fa[u]);
+    }
+
+    for (int rb = r0; rb < r1; rb += D) {
+#pragma unroll
+        for (int u = 0; u < D; u++) {
+            const int r = rb + u;
+            store_row(r + 1, fv[u]);
+            __syncthreads();
+            if (r < r1) {
+                const T *rn = ring[(r + 3) & 3];
+                const T *rc = ring[r & 3];
+                const T *rs = ring[(r + 1) & 3];
+                const bool ringrow = (r == 0) || (r == rows - 1);
+                const size_t rowoff = (size_t)r * cols;
+#pragma unroll
+                for (int s = 0; s < CPT; s++) {
+                    if (point[s]) {
+                        const int i = sidx[s];
+                        const bool edge = i == 0;  // column 0: no west neighbours
+                        Nb<T> nb;
+                        nb.c = rc[i];
+                        nb.n = rn[i];
+                        nb.s = rs[i];
+                        nb.w = edge ? (T)0 : rc[i - 1];
+                        nb.e = rc[i + 1];
+                        nb.nw = edge ? (T)0 : rn[i - 1];
+                        nb.ne = rn[i + 1];
+                        nb.sw = edge ? (T)0 : rs[i - 1];
+                        nb.se = rs[i + 1];
+                        pt(ringrow || ringcol[s], r, col[s], rowoff + col[s], nb, fa[u][s], acc);
+                    }
+                }
+            }
+            // refill this FIFO stage: field row r+1+D, aux row r+D (only rows the chunk needs)
+            if (r + 1 + D <= r1) load_field(r + 1 + D, fv[u]);
+            load_aux(r + D, fa[u]);
         }
     }
     if constexpr (K > 0) grid_reduce<K>(acc, ra, fin);
@@ -385,14 +453,22 @@ struct NoFin {
     __device__ void operator()(const double *) const {}
 };
 
-template <typename T, int U, int K, typename Loader, typename Point, typename Fin>
-int launch_march(fx_ctx *ctx, const MarchGeom &G, Loader ld, Point pt, Fin fin,
-                 const int *skip, const char *what) {
-    const int blocks = (G.nwarps + (kBlock / 32) - 1) / (kBlock / 32);
-    if (K > 0 && blocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");
+template <typename T, int K, typename Loader, typename Point, typename Fin>
+int launch_march(fx_ctx *ctx, size_t rows, size_t cols, Loader ld, Point pt, Fin fin, const int *skip,
+                 const char *what) {
+    constexpr int CPT = band_cpt<T>();
+    constexpr int D = band_depth<Point::NA>();
+    static int occ = 0;  // resident CTAs per SM for this instantiation
+    if (!occ) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_march<T, CPT, D, K, Loader, Point, Fin>,
+                                                          kBandThreads, 0) != cudaSuccess || occ < 1)
+            occ = 1;
+    }
+    const MarchGeom G = march_geom(rows, cols, kBlock * CPT, D, occ * ctx->num_sms);
+    if (K > 0 && G.nblocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");
     timing_pre(ctx, what);
-    k_march<T, U, K><<<blocks, kBlock, 0, ctx->stream>>>(G, ld, pt, fin, red_args<K>(ctx), skip);
-    timing_post(ctx, (double)G.rows * (double)G.cols);
+    k_march<T, CPT, D, K><<<G.nblocks, kBandThreads, 0, ctx->stream>>>(G, ld, pt, fin, red_args<K>(ctx), skip);
+    timing_post(ctx, (double)rows * (double)cols);
     return check_launch(ctx, what);
 }
 

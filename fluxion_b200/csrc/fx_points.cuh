@@ -46,19 +46,18 @@ constexpr int unroll_for() {
 // apply_stencil (ops.rs:76-127 + apply_boundaries :796-843) and apply_stencil_var (:129-154)
 template <typename T, int MODE, bool VAR>
 struct PtApply {
+    static constexpr int NA = VAR ? 1 : 0;
     T *out;
     const T *coeff;
     StencilP P;
     BcP B;
     int rows, cols;
-    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *) const {
-        T v;
-        if (r == 0) v = (T)bc_value(B, 0, (double)nb.c, (double)nb.s, B.dy);
-        else if (r == rows - 1) v = (T)bc_value(B, 1, (double)nb.c, (double)nb.n, B.dy);
-        else if (c == 0) v = (T)bc_value(B, 2, (double)nb.c, (double)nb.e, B.dx);
-        else if (c == cols - 1) v = (T)bc_value(B, 3, (double)nb.c, (double)nb.w, B.dx);
-        else v = stencil_eval<T, MODE>(P, nb);
-        if (VAR) v = v * coeff[idx];
+    __device__ __forceinline__ const T *aux(int) const { return coeff; }
+    __device__ __forceinline__ void operator()(bool ring, int r, int c, size_t idx, const Nb<T> &nb, const T *a,
+                                               CSum *) const {
+        if (ring) return;  // boundary values come from k_ring_values
+        T v = stencil_eval<T, MODE>(P, nb);
+        if (VAR) v = v * a[0];
         out[idx] = v;
     }
 };
@@ -66,13 +65,16 @@ struct PtApply {
 // stencil_axpy (ops.rs:225-269, fused_5pt_axpy_row :1011-1125): ring untouched
 template <typename T, int MODE>
 struct PtAxpy {
+    static constexpr int NA = 1;
     T *y;
     StencilP P;
     T alpha;
     int rows, cols;
-    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *) const {
-        if (r == 0 || r == rows - 1 || c == 0 || c == cols - 1) return;
-        y[idx] = fx_fma(alpha, stencil_eval<T, MODE>(P, nb), y[idx]);
+    __device__ __forceinline__ const T *aux(int) const { return y; }
+    __device__ __forceinline__ void operator()(bool ring, int, int, size_t idx, const Nb<T> &nb, const T *a,
+                                               CSum *) const {
+        if (ring) return;
+        y[idx] = fx_fma(alpha, stencil_eval<T, MODE>(P, nb), a[0]);
     }
 };
 
@@ -95,19 +97,23 @@ __device__ __forceinline__ T conv_diff_at(const ConvDiffC<T> &K, const Nb<T> &nb
 
 template <typename T, bool AXPY>
 struct PtConvDiff {
+    static constexpr int NA = AXPY ? 4 : 3;
     T *out;
     const T *kappa, *vx, *vy;
     ConvDiffC<T> K;
     T alpha;
     int rows, cols;
-    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *) const {
-        const bool ring = (r == 0 || r == rows - 1 || c == 0 || c == cols - 1);
+    __device__ __forceinline__ const T *aux(int k) const {
+        return k == 0 ? kappa : (k == 1 ? vx : (k == 2 ? vy : (const T *)out));
+    }
+    __device__ __forceinline__ void operator()(bool ring, int, int, size_t idx, const Nb<T> &nb, const T *a,
+                                               CSum *) const {
         if (ring) {
             if (!AXPY) out[idx] = (T)0;
             return;
         }
-        const T v = conv_diff_at<T>(K, nb, kappa[idx], vx[idx], vy[idx]);
-        out[idx] = AXPY ? fx_fma(alpha, v, out[idx]) : v;
+        const T v = conv_diff_at<T>(K, nb, a[0], a[1], a[2]);
+        out[idx] = AXPY ? fx_fma(alpha, v, a[AXPY ? 3 : 0]) : v;
     }
 };
 
@@ -137,26 +143,32 @@ __device__ __forceinline__ T op5(const A5<T> &a, const Nb<T> &v) {
 
 template <typename T>
 struct PtJacobi {
+    static constexpr int NA = 1;
     T *out;
     const T *b;
     A5<T> a;
     T wd;
     int rows, cols;
-    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *) const {
-        if (r == 0 || r == rows - 1 || c == 0 || c == cols - 1) return;
-        out[idx] = fx_fma(wd, b[idx] - op5<T>(a, nb), nb.c);
+    __device__ __forceinline__ const T *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int, int, size_t idx, const Nb<T> &nb, const T *av,
+                                               CSum *) const {
+        if (ring) return;
+        out[idx] = fx_fma(wd, av[0] - op5<T>(a, nb), nb.c);
     }
 };
 
 template <typename T>
 struct PtResidual {
+    static constexpr int NA = 1;
     T *out;
     const T *b;
     A5<T> a;
     int rows, cols;
-    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *) const {
-        if (r == 0 || r == rows - 1 || c == 0 || c == cols - 1) return;
-        out[idx] = b[idx] - op5<T>(a, nb);
+    __device__ __forceinline__ const T *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int, int, size_t idx, const Nb<T> &nb, const T *av,
+                                               CSum *) const {
+        if (ring) return;
+        out[idx] = av[0] - op5<T>(a, nb);
     }
 };
 

@@ -67,12 +67,9 @@ struct OpA {
     StencilP P;
     T coeff;
     int rows, cols;
-    __device__ __forceinline__ bool ring(int r, int c) const {
-        return r == 0 || r == rows - 1 || c == 0 || c == cols - 1;
-    }
     // copy_from + stencil_axpy (cg.rs:106-109): interior fma(coeff, S v, v), ring = v
-    __device__ __forceinline__ T apply(int r, int c, const Nb<T> &nb) const {
-        return ring(r, c) ? nb.c : fx_fma(coeff, stencil_eval<T, MODE>(P, nb), nb.c);
+    __device__ __forceinline__ T apply(bool ring, const Nb<T> &nb) const {
+        return ring ? nb.c : fx_fma(coeff, stencil_eval<T, MODE>(P, nb), nb.c);
     }
 };
 
@@ -181,10 +178,12 @@ struct IdentityPc : fx_precond {
 // out = A v (no reduction) or with <v, out> / <out, y> reductions.
 template <typename T, int MODE>
 struct PtApplyOp {
+    static constexpr int NA = 0;
     OpA<T, MODE> A;
     T *out;
-    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *) const {
-        out[idx] = A.apply(r, c, nb);
+    __device__ __forceinline__ const T *aux(int) const { return nullptr; }
+    __device__ __forceinline__ void operator()(bool ring, int r, int c, size_t idx, const Nb<T> &nb, const T *, CSum *) const {
+        out[idx] = A.apply(ring, nb);
     }
 };
 
@@ -266,19 +265,17 @@ void coarse_op(const double *fine, double sigma, double *coarse) {
 template <typename T>
 int sweep(fx_ctx *ctx, const T *in, T *out, const T *b, const double *a5, double omega, size_t rows, size_t cols,
           const int *skip) {
-    constexpr int U = unroll_for<T>();
-    MarchGeom G = march_geom(ctx, rows, cols, U);
-    PtJacobi<T> pt{out, b, make_a5<T>(a5), (T)(omega / a5[0]), G.rows, G.cols};
-    return launch_march<T, U, 0>(ctx, G, LoadArr<T>{in}, pt, NoFin{}, skip, "mg_sweep");
+    const size_t RR = rows, CC = cols;
+    PtJacobi<T> pt{out, b, make_a5<T>(a5), (T)(omega / a5[0]), (int)RR, (int)CC};
+    return launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{in}, pt, NoFin{}, skip, "mg_sweep");
 }
 
 template <typename T>
 int residual(fx_ctx *ctx, const T *x, const T *b, T *r, const double *a5, size_t rows, size_t cols,
              const int *skip) {
-    constexpr int U = unroll_for<T>();
-    MarchGeom G = march_geom(ctx, rows, cols, U);
-    PtResidual<T> pt{r, b, make_a5<T>(a5), G.rows, G.cols};
-    return launch_march<T, U, 0>(ctx, G, LoadArr<T>{x}, pt, NoFin{}, skip, "mg_residual");
+    const size_t RR = rows, CC = cols;
+    PtResidual<T> pt{r, b, make_a5<T>(a5), (int)RR, (int)CC};
+    return launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{x}, pt, NoFin{}, skip, "mg_residual");
 }
 
 template <typename T>
@@ -589,13 +586,15 @@ int prep_op(const fx_grid &g, const fx_stencil *st, const fx_boundaries *bc, Ste
 // r = b - A x (cg.rs:104-111); reduction r.r
 template <typename T, int MODE>
 struct PtInitResid {
+    static constexpr int NA = 1;
     OpA<T, MODE> A;
     const T *b;
     T *r;
     T *r2;  // optional second copy (BiCGSTAB r_hat)
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
-        const T ax = A.apply(rr, c, nb);
-        const T rv = fx_fma((T)-1, ax, b[idx]);
+    __device__ __forceinline__ const T *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T ax = A.apply(ring, nb);
+        const T rv = fx_fma((T)-1, ax, a[0]);
         r[idx] = rv;
         if (r2) r2[idx] = rv;
         csum_add_prod(acc[0], (double)rv, (double)rv);
@@ -618,11 +617,13 @@ struct FinCgInit {  // unpreconditioned: rs_old = r.r; loop-top test of iteratio
 // p_new = (r|z) + beta p_old; ap = A p_new; reduction p.ap
 template <typename T, int MODE>
 struct PtCgDir {
+    static constexpr int NA = 0;
     OpA<T, MODE> A;
     T *p_new;
-    __device__ __forceinline__ void operator()(int r, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+    __device__ __forceinline__ const T *aux(int) const { return nullptr; }
+    __device__ __forceinline__ void operator()(bool ring, int r, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
         p_new[idx] = nb.c;
-        const T ap = A.apply(r, c, nb);
+        const T ap = A.apply(ring, nb);
         csum_add_prod(acc[0], (double)nb.c, (double)ap);
     }
 };
@@ -642,14 +643,16 @@ struct FinCgDir {  // alpha = rs_old / p.ap, breakdown test (cg.rs:133-142)
 // x += alpha p; r -= alpha A p (A p recomputed from p); reduction r.r
 template <typename T, int MODE>
 struct PtCgUpd {
+    static constexpr int NA = 2;
     OpA<T, MODE> A;
     T *x, *r;
     const DevState *S;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+    __device__ __forceinline__ const T *aux(int k) const { return k == 0 ? x : r; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
         const T alpha = (T)S->alpha;
-        const T ap = A.apply(rr, c, nb);
-        x[idx] = fx_fma(alpha, nb.c, x[idx]);
-        const T rv = fx_fma(-alpha, ap, r[idx]);
+        const T ap = A.apply(ring, nb);
+        x[idx] = fx_fma(alpha, nb.c, a[0]);
+        const T rv = fx_fma(-alpha, ap, a[1]);
         r[idx] = rv;
         csum_add_prod(acc[0], (double)rv, (double)rv);
     }
@@ -720,9 +723,8 @@ template <int MODE>
 int cg_solve_impl(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
     using T = double;
     fx_ctx *ctx = s->ctx;
-    constexpr int U = unroll_for<T>();
-    MarchGeom G = march_geom(ctx, s->g.rows, s->g.cols, U);
-    OpA<T, MODE> A{P, (T)coeff, G.rows, G.cols};
+    const size_t RR = s->g.rows, CC = s->g.cols;
+    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
     T *r = (T *)s->bufs[0]->ptr, *z = (T *)s->bufs[1]->ptr;
     T *pb[2] = {(T *)s->bufs[2]->ptr, (T *)s->bufs[3]->ptr};
     T *xp = (T *)x->ptr;
@@ -734,19 +736,19 @@ int cg_solve_impl(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const Sten
     FX_CUDA(cudaMemsetAsync(pb[0], 0, n * sizeof(T), ctx->stream));
     FX_CUDA(cudaMemsetAsync(pb[1], 0, n * sizeof(T), ctx->stream));
     if (!pc) {
-        FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, r, nullptr}, FinCgInit{S},
+        FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, r, nullptr}, FinCgInit{S},
                                       nullptr, "cg_init")));
         auto step = [&](size_t i) -> int {
             T *po = pb[i & 1], *pn = pb[(i + 1) & 1];
-            FX_TRY((launch_march<T, U, 1>(ctx, G, LdAypx<T>{r, po, S}, PtCgDir<T, MODE>{A, pn}, FinCgDir{S}, halt,
+            FX_TRY((launch_march<T, 1>(ctx, RR, CC, LdAypx<T>{r, po, S}, PtCgDir<T, MODE>{A, pn}, FinCgDir{S}, halt,
                                           "cg_dir")));
-            return launch_march<T, U, 1>(ctx, G, Ld1<T>{pn}, PtCgUpd<T, MODE>{A, xp, r, S}, FinCgUpd{S}, halt,
+            return launch_march<T, 1>(ctx, RR, CC, Ld1<T>{pn}, PtCgUpd<T, MODE>{A, xp, r, S}, FinCgUpd{S}, halt,
                                          "cg_update");
         };
         return s->drive(step, s->max_iter + 1, n >= (1u << 20));
     }
     // preconditioned (cg.rs:178-256)
-    FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, r, nullptr}, FinPcgResid{S},
+    FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, r, nullptr}, FinPcgResid{S},
                                   nullptr, "pcg_init")));
     fx_buf rb{ctx, r, n, FX_F64, false}, zb{ctx, z, n, FX_F64, false};
     FX_TRY(zero_fill<T>(ctx, z, n, nullptr));
@@ -754,9 +756,9 @@ int cg_solve_impl(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const Sten
     FX_TRY(launch_flat<1>(ctx, n, FlatDot<T>{r, z}, FinPcgRzInit{S}, halt, "pcg_rz"));
     auto step = [&](size_t i) -> int {
         T *po = pb[i & 1], *pn = pb[(i + 1) & 1];
-        FX_TRY((launch_march<T, U, 1>(ctx, G, LdAypx<T>{z, po, S}, PtCgDir<T, MODE>{A, pn}, FinCgDir{S}, halt,
+        FX_TRY((launch_march<T, 1>(ctx, RR, CC, LdAypx<T>{z, po, S}, PtCgDir<T, MODE>{A, pn}, FinCgDir{S}, halt,
                                       "pcg_dir")));
-        FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{pn}, PtCgUpd<T, MODE>{A, xp, r, S}, FinPcgUpd{S}, halt,
+        FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{pn}, PtCgUpd<T, MODE>{A, xp, r, S}, FinPcgUpd{S}, halt,
                                       "pcg_update")));
         FX_TRY(zero_fill<T>(ctx, z, n, halt));
         FX_TRY(pc->apply(&zb, &rb, halt, true));
@@ -769,20 +771,24 @@ int cg_solve_impl(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const Sten
 
 template <typename T, int MODE>
 struct PtPipeInitQ {  // q = A x; r = b - q
+    static constexpr int NA = 1;
     OpA<T, MODE> A;
     const T *b;
     T *r;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *) const {
-        r[idx] = fx_fma((T)-1, A.apply(rr, c, nb), b[idx]);
+    __device__ __forceinline__ const T *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *) const {
+        r[idx] = fx_fma((T)-1, A.apply(ring, nb), a[0]);
     }
 };
 
 template <typename T, int MODE>
 struct PtPipeInitW {  // w = A r; p = t = z = 0; reductions (r.r, r.w)
+    static constexpr int NA = 0;
     OpA<T, MODE> A;
     T *w, *p, *t, *z;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
-        const T wv = A.apply(rr, c, nb);
+    __device__ __forceinline__ const T *aux(int) const { return nullptr; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T wv = A.apply(ring, nb);
         w[idx] = wv;
         p[idx] = (T)0;
         t[idx] = (T)0;
@@ -818,21 +824,25 @@ struct FinPipeInit {
 // updated vectors for the next iteration's scalars.
 template <typename T, int MODE>
 struct PtPipeIter {
+    static constexpr int NA = 5;
     OpA<T, MODE> A;
     T *z, *t, *p, *x, *r, *w_new;
     const DevState *S;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+    __device__ __forceinline__ const T *aux(int k) const {
+        return k == 0 ? z : (k == 1 ? t : (k == 2 ? p : (k == 3 ? x : r)));
+    }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
         const T alpha = (T)S->alpha, beta = (T)S->beta;
-        const T q = A.apply(rr, c, nb);
+        const T q = A.apply(ring, nb);
         const T w = nb.c;
-        const T zn = q + z[idx] * beta;
-        const T tn = w + t[idx] * beta;
-        const T pn = r[idx] + p[idx] * beta;
+        const T zn = q + a[0] * beta;
+        const T tn = w + a[1] * beta;
+        const T pn = a[4] + a[2] * beta;
         z[idx] = zn;
         t[idx] = tn;
         p[idx] = pn;
-        x[idx] = fx_fma(alpha, pn, x[idx]);
-        const T rn = fx_fma(-alpha, tn, r[idx]);
+        x[idx] = fx_fma(alpha, pn, a[3]);
+        const T rn = fx_fma(-alpha, tn, a[4]);
         const T wn = fx_fma(-alpha, zn, w);
         r[idx] = rn;
         w_new[idx] = wn;
@@ -868,9 +878,8 @@ template <int MODE>
 int pipe_solve_impl(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P) {
     using T = double;
     fx_ctx *ctx = s->ctx;
-    constexpr int U = unroll_for<T>();
-    MarchGeom G = march_geom(ctx, s->g.rows, s->g.cols, U);
-    OpA<T, MODE> A{P, (T)coeff, G.rows, G.cols};
+    const size_t RR = s->g.rows, CC = s->g.cols;
+    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
     T *r = (T *)s->bufs[0]->ptr, *p = (T *)s->bufs[1]->ptr, *t = (T *)s->bufs[2]->ptr, *z = (T *)s->bufs[3]->ptr;
     T *w[2] = {(T *)s->bufs[4]->ptr, (T *)s->bufs[5]->ptr};
     T *xp = (T *)x->ptr;
@@ -878,12 +887,12 @@ int pipe_solve_impl(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff
     DevState *S = s->d_st;
     const int *halt = &S->halt;
     FX_TRY(s->reset_state());
-    FX_TRY((launch_march<T, U, 0>(ctx, G, Ld1<T>{xp}, PtPipeInitQ<T, MODE>{A, bp, r}, NoFin{}, nullptr, "pipe_init_q")));
-    FX_TRY((launch_march<T, U, 2>(ctx, G, Ld1<T>{r}, PtPipeInitW<T, MODE>{A, w[0], p, t, z}, FinPipeInit{S}, nullptr,
+    FX_TRY((launch_march<T, 0>(ctx, RR, CC, Ld1<T>{xp}, PtPipeInitQ<T, MODE>{A, bp, r}, NoFin{}, nullptr, "pipe_init_q")));
+    FX_TRY((launch_march<T, 2>(ctx, RR, CC, Ld1<T>{r}, PtPipeInitW<T, MODE>{A, w[0], p, t, z}, FinPipeInit{S}, nullptr,
                                   "pipe_init_w")));
     auto step = [&](size_t i) -> int {
         T *wo = w[i & 1], *wn = w[(i + 1) & 1];
-        return launch_march<T, U, 2>(ctx, G, Ld1<T>{wo}, PtPipeIter<T, MODE>{A, z, t, p, xp, r, wn, S},
+        return launch_march<T, 2>(ctx, RR, CC, Ld1<T>{wo}, PtPipeIter<T, MODE>{A, z, t, p, xp, r, wn, S},
                                      FinPipeIter{S}, halt, "pipe_iter");
     };
     return s->drive(step, s->max_iter + 1, s->g.rows * s->g.cols >= (1u << 22));
@@ -938,15 +947,17 @@ struct LdBicgP {
 // v = A (p or p_hat); store p_new when marching the fused p; reduction r_hat.v
 template <typename T, int MODE>
 struct PtBicgV {
+    static constexpr int NA = 1;
     OpA<T, MODE> A;
     T *p_store;  // null when the marched field is already stored (p_hat)
     T *v;
     const T *r_hat;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
+    __device__ __forceinline__ const T *aux(int) const { return r_hat; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
         if (p_store) p_store[idx] = nb.c;
-        const T vv = A.apply(rr, c, nb);
+        const T vv = A.apply(ring, nb);
         v[idx] = vv;
-        csum_add_prod(acc[0], (double)r_hat[idx], (double)vv);
+        csum_add_prod(acc[0], (double)a[0], (double)vv);
     }
 };
 
@@ -976,13 +987,15 @@ struct FinBicgS {
 // t = A (s or s_hat); reductions (t.s, t.t)
 template <typename T, int MODE>
 struct PtBicgT {
+    static constexpr int NA = 1;
     OpA<T, MODE> A;
     T *t;
     const T *s;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
-        const T tv = A.apply(rr, c, nb);
+    __device__ __forceinline__ const T *aux(int) const { return s; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T tv = A.apply(ring, nb);
         t[idx] = tv;
-        csum_add_prod(acc[0], (double)tv, (double)s[idx]);
+        csum_add_prod(acc[0], (double)tv, (double)a[0]);
         csum_add_prod(acc[1], (double)tv, (double)tv);
     }
 };
@@ -1063,11 +1076,13 @@ struct FlatBicgP {
 // r = b - A x; r_hat = r; reductions (r.r, r_hat.r)
 template <typename T, int MODE>
 struct PtBicgInit {
+    static constexpr int NA = 1;
     OpA<T, MODE> A;
     const T *b;
     T *r, *rh;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
-        const T rv = fx_fma((T)-1, A.apply(rr, c, nb), b[idx]);
+    __device__ __forceinline__ const T *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T rv = fx_fma((T)-1, A.apply(ring, nb), a[0]);
         r[idx] = rv;
         rh[idx] = rv;
         csum_add_prod(acc[0], (double)rv, (double)rv);
@@ -1087,9 +1102,8 @@ template <int MODE>
 int bicg_solve_impl(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
     using T = double;
     fx_ctx *ctx = s->ctx;
-    constexpr int U = unroll_for<T>();
-    MarchGeom G = march_geom(ctx, s->g.rows, s->g.cols, U);
-    OpA<T, MODE> A{P, (T)coeff, G.rows, G.cols};
+    const size_t RR = s->g.rows, CC = s->g.cols;
+    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
     const size_t n = s->g.rows * s->g.cols;
     T *r = (T *)s->bufs[0]->ptr, *rh = (T *)s->bufs[1]->ptr;
     T *pb[2] = {(T *)s->bufs[2]->ptr, (T *)s->bufs[3]->ptr};
@@ -1106,7 +1120,7 @@ int bicg_solve_impl(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, co
         FX_CUDA(cudaMemsetAsync(vb[k], 0, n * sizeof(T), ctx->stream));
     }
     // r = b - A x; r_hat = r; (r.r, r_hat.r)
-    FX_TRY((launch_march<T, U, 2>(ctx, G, Ld1<T>{xp}, PtBicgInit<T, MODE>{A, bp, r, rh}, FinBicgInit{S}, nullptr,
+    FX_TRY((launch_march<T, 2>(ctx, RR, CC, Ld1<T>{xp}, PtBicgInit<T, MODE>{A, bp, r, rh}, FinBicgInit{S}, nullptr,
                                   "bicg_init")));
     auto s_update = [&](const T *v) -> int {
         return launch_flat<1>(ctx, n, FlatBicgS<T>{r, v, sv, S}, FinBicgS{S}, halt, "bicg_s");
@@ -1118,10 +1132,10 @@ int bicg_solve_impl(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, co
     if (!pc) {
         auto step = [&](size_t i) -> int {
             T *po = pb[i & 1], *pn = pb[(i + 1) & 1], *vo = vb[i & 1], *vn = vb[(i + 1) & 1];
-            FX_TRY((launch_march<T, U, 1>(ctx, G, LdBicgP<T>{r, po, vo, S}, PtBicgV<T, MODE>{A, pn, vn, rh},
+            FX_TRY((launch_march<T, 1>(ctx, RR, CC, LdBicgP<T>{r, po, vo, S}, PtBicgV<T, MODE>{A, pn, vn, rh},
                                           FinBicgRv{S}, halt, "bicg_pv")));
             FX_TRY(s_update(vn));
-            FX_TRY((launch_march<T, U, 2>(ctx, G, Ld1<T>{sv}, PtBicgT<T, MODE>{A, tv, sv}, FinBicgT{S}, halt,
+            FX_TRY((launch_march<T, 2>(ctx, RR, CC, Ld1<T>{sv}, PtBicgT<T, MODE>{A, tv, sv}, FinBicgT{S}, halt,
                                           "bicg_t")));
             return finish(pn, sv);
         };
@@ -1134,12 +1148,12 @@ int bicg_solve_impl(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, co
         FX_TRY(launch_flat<0>(ctx, n, FlatBicgP<T>{p, r, v, S}, NoFin{}, halt, "bicg_p"));
         FX_TRY(zero_fill<T>(ctx, ph, n, halt));
         FX_TRY(pc->apply(&phb, &pbuf, halt, true));
-        FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{ph}, PtBicgV<T, MODE>{A, nullptr, v, rh}, FinBicgRv{S}, halt,
+        FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{ph}, PtBicgV<T, MODE>{A, nullptr, v, rh}, FinBicgRv{S}, halt,
                                       "bicg_v")));
         FX_TRY(s_update(v));
         FX_TRY(zero_fill<T>(ctx, sh, n, halt));
         FX_TRY(pc->apply(&shb, &sbuf, halt, true));
-        FX_TRY((launch_march<T, U, 2>(ctx, G, Ld1<T>{sh}, PtBicgT<T, MODE>{A, tv, sv}, FinBicgT{S}, halt, "bicg_t")));
+        FX_TRY((launch_march<T, 2>(ctx, RR, CC, Ld1<T>{sh}, PtBicgT<T, MODE>{A, tv, sv}, FinBicgT{S}, halt, "bicg_t")));
         return finish(ph, sh);
     };
     return s->drive(step, s->max_iter + 1, true);
@@ -1170,26 +1184,30 @@ struct FinSlot {
 
 template <typename T, int MODE>
 struct PtGmResid {  // out = b - A x (gmres.rs:477-485); reduction out.out
+    static constexpr int NA = 1;
     OpA<T, MODE> A;
     const T *b;
     T *out;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
-        const T ax = A.apply(rr, c, nb);
-        const T v = fx_fma((T)1, b[idx], -ax);
+    __device__ __forceinline__ const T *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T ax = A.apply(ring, nb);
+        const T v = fx_fma((T)1, a[0], -ax);
         out[idx] = v;
         csum_add_prod(acc[0], (double)v, (double)v);
     }
 };
 
-template <typename T, int MODE>
+template <typename T, int MODE, bool HAS_V0>
 struct PtGmAv {  // w = A v; reduction w.v0 (when v0 given)
+    static constexpr int NA = HAS_V0 ? 1 : 0;
     OpA<T, MODE> A;
     T *w;
     const T *v0;
-    __device__ __forceinline__ void operator()(int rr, int c, size_t idx, const Nb<T> &nb, CSum *acc) const {
-        const T wv = A.apply(rr, c, nb);
+    __device__ __forceinline__ const T *aux(int) const { return v0; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T wv = A.apply(ring, nb);
         w[idx] = wv;
-        if (v0) csum_add_prod(acc[0], (double)wv, (double)v0[idx]);
+        if (HAS_V0) csum_add_prod(acc[0], (double)wv, (double)a[0]);
     }
 };
 
@@ -1234,9 +1252,8 @@ template <int MODE>
 int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
     using T = double;
     fx_ctx *ctx = s->ctx;
-    constexpr int U = unroll_for<T>();
-    MarchGeom G = march_geom(ctx, s->g.rows, s->g.cols, U);
-    OpA<T, MODE> A{P, (T)coeff, G.rows, G.cols};
+    const size_t RR = s->g.rows, CC = s->g.cols;
+    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
     const size_t n = s->g.rows * s->g.cols, m = s->restart, mp1 = m + 1;
     std::vector<T *> V(mp1);
     for (size_t i = 0; i < mp1; i++) V[i] = (T *)s->bufs[i]->ptr;
@@ -1284,12 +1301,12 @@ int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, cons
     for (;;) {
         double beta;
         if (!pc) {
-            FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{xp}, PtGmResid<T, MODE>{A, bp, V[0]}, FinSlot{dh}, nullptr,
+            FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{xp}, PtGmResid<T, MODE>{A, bp, V[0]}, FinSlot{dh}, nullptr,
                                           "gmres_resid")));
             FX_TRY(read_h(0));
             beta = std::sqrt(s->h_h[0]);
         } else {
-            FX_TRY((launch_march<T, U, 0>(ctx, G, Ld1<T>{xp}, PtGmResid<T, MODE>{A, bp, w}, NoFin{}, nullptr, "gmres_resid")));
+            FX_TRY((launch_march<T, 0>(ctx, RR, CC, Ld1<T>{xp}, PtGmResid<T, MODE>{A, bp, w}, NoFin{}, nullptr, "gmres_resid")));
             fx_buf v0b{ctx, V[0], n, FX_F64, false};
             FX_TRY(zero_fill<T>(ctx, V[0], n, nullptr));
             FX_TRY(pc->apply(&v0b, &wb, nullptr, true));
@@ -1319,10 +1336,10 @@ int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, cons
             // w = A v_k (+ left preconditioning), then modified Gram-Schmidt with every dot
             // fused into the preceding AXPY
             if (!pc) {
-                FX_TRY((launch_march<T, U, 1>(ctx, G, Ld1<T>{V[k]}, PtGmAv<T, MODE>{A, w, V[0]}, FinSlot{dh + 0}, nullptr,
+                FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{V[k]}, PtGmAv<T, MODE, true>{A, w, V[0]}, FinSlot{dh + 0}, nullptr,
                                               "gmres_av")));
             } else {
-                FX_TRY((launch_march<T, U, 0>(ctx, G, Ld1<T>{V[k]}, PtGmAv<T, MODE>{A, w, nullptr}, NoFin{}, nullptr,
+                FX_TRY((launch_march<T, 0>(ctx, RR, CC, Ld1<T>{V[k]}, PtGmAv<T, MODE, false>{A, w, nullptr}, NoFin{}, nullptr,
                                               "gmres_av")));
                 fx_buf vk1{ctx, V[k + 1], n, FX_F64, false};
                 FX_TRY(zero_fill<T>(ctx, V[k + 1], n, nullptr));

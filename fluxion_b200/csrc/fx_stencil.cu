@@ -8,6 +8,50 @@ using namespace fx;
 
 namespace {
 
+// Boundary ring of apply_stencil / apply_stencil_var (ops.rs:796-843): top and bottom rows
+// (corners included) first, then the left and right columns of rows 1..rows-2; each value
+// from the point itself and its inward neighbour.  The interior is written by the band
+// kernel, so the two writes never overlap.
+template <typename T, bool VAR>
+__global__ void k_ring_values(const T *__restrict__ in, T *__restrict__ out, const T *__restrict__ coeff,
+                              int rows, int cols, BcP B) {
+    const int nring = 2 * cols + 2 * (rows - 2);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nring; i += gridDim.x * blockDim.x) {
+        size_t idx;
+        double v;
+        if (i < cols) {
+            idx = i;
+            v = bc_value(B, 0, (double)in[idx], (double)in[idx + cols], B.dy);
+        } else if (i < 2 * cols) {
+            idx = (size_t)(rows - 1) * cols + (i - cols);
+            v = bc_value(B, 1, (double)in[idx], (double)in[idx - cols], B.dy);
+        } else {
+            const int j = i - 2 * cols;
+            const size_t r = 1 + j / 2;
+            if (j & 1) {
+                idx = r * cols + cols - 1;
+                v = bc_value(B, 3, (double)in[idx], (double)in[idx - 1], B.dx);
+            } else {
+                idx = r * cols;
+                v = bc_value(B, 2, (double)in[idx], (double)in[idx + 1], B.dx);
+            }
+        }
+        T o = (T)v;
+        if (VAR) o = o * coeff[idx];
+        out[idx] = o;
+    }
+}
+
+template <typename T, bool VAR>
+int ring_values(fx_ctx *ctx, const T *in, T *out, const T *coeff, int rows, int cols, const BcP &B) {
+    const int nring = 2 * cols + 2 * (rows - 2);
+    const int blocks = (nring + 255) / 256;
+    timing_pre(ctx, "ring_values");
+    k_ring_values<T, VAR><<<blocks, 256, 0, ctx->stream>>>(in, out, coeff, rows, cols, B);
+    timing_post(ctx, (double)nring);
+    return check_launch(ctx, "ring_values");
+}
+
 // Reference weighted_jacobi (ops.rs:425-473): an in-place lexicographic sweep.  Executed
 // as a wavefront over hyperplanes 2r + c = t: for radius-1 stencils every neighbour that
 // the lexicographic order updates first lies on an earlier hyperplane and every later one
@@ -66,13 +110,13 @@ int fx_apply_stencil(fx_ctx *ctx, const fx_buf *in, fx_buf *out, const fx_grid *
     StencilP P;
     FX_TRY(make_stencil(s, &P));
     FX_DISPATCH(in->dtype, {
-        constexpr int U = unroll_for<T>();
-        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        const size_t RR = g->rows, CC = g->cols;
         FX_MODE_DISPATCH(P.mode, {
-            PtApply<T, MODE, false> pt{(T *)out->ptr, nullptr, P, B, G.rows, G.cols};
-            return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)in->ptr}, pt, NoFin{}, nullptr,
-                                         "apply_stencil");
+            PtApply<T, MODE, false> pt{(T *)out->ptr, nullptr, P, B, (int)RR, (int)CC};
+            FX_TRY(launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)in->ptr}, pt, NoFin{}, nullptr,
+                                      "apply_stencil"));
         });
+        return ring_values<T, false>(ctx, (const T *)in->ptr, (T *)out->ptr, nullptr, (int)RR, (int)CC, B);
     });
 }
 
@@ -85,13 +129,14 @@ int fx_apply_stencil_var(fx_ctx *ctx, const fx_buf *in, fx_buf *out, const fx_bu
     StencilP P;
     FX_TRY(make_stencil(s, &P));
     FX_DISPATCH(in->dtype, {
-        constexpr int U = unroll_for<T>();
-        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        const size_t RR = g->rows, CC = g->cols;
         FX_MODE_DISPATCH(P.mode, {
-            PtApply<T, MODE, true> pt{(T *)out->ptr, (const T *)coeff->ptr, P, B, G.rows, G.cols};
-            return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)in->ptr}, pt, NoFin{}, nullptr,
-                                         "apply_stencil_var");
+            PtApply<T, MODE, true> pt{(T *)out->ptr, (const T *)coeff->ptr, P, B, (int)RR, (int)CC};
+            FX_TRY(launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)in->ptr}, pt, NoFin{}, nullptr,
+                                      "apply_stencil_var"));
         });
+        return ring_values<T, true>(ctx, (const T *)in->ptr, (T *)out->ptr, (const T *)coeff->ptr, (int)RR,
+                                    (int)CC, B);
     });
 }
 
@@ -103,11 +148,10 @@ int fx_stencil_axpy(fx_ctx *ctx, double alpha, const fx_buf *x, fx_buf *y, const
     StencilP P;
     FX_TRY(make_stencil(s, &P));
     FX_DISPATCH(x->dtype, {
-        constexpr int U = unroll_for<T>();
-        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        const size_t RR = g->rows, CC = g->cols;
         FX_MODE_DISPATCH(P.mode, {
-            PtAxpy<T, MODE> pt{(T *)y->ptr, P, (T)alpha, G.rows, G.cols};
-            return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)x->ptr}, pt, NoFin{}, nullptr,
+            PtAxpy<T, MODE> pt{(T *)y->ptr, P, (T)alpha, (int)RR, (int)CC};
+            return launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)x->ptr}, pt, NoFin{}, nullptr,
                                          "stencil_axpy");
         });
     });
@@ -145,11 +189,10 @@ int fx_apply_conv_diff(fx_ctx *ctx, const fx_buf *u, fx_buf *out, const fx_buf *
     FX_TRY(pre_vec(u, vx, "vx"));
     FX_TRY(pre_vec(u, vy, "vy"));
     FX_DISPATCH(u->dtype, {
-        constexpr int U = unroll_for<T>();
-        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        const size_t RR = g->rows, CC = g->cols;
         PtConvDiff<T, false> pt{(T *)out->ptr, (const T *)kappa->ptr, (const T *)vx->ptr, (const T *)vy->ptr,
-                                conv_consts<T>(g->dx, g->dy), (T)0, G.rows, G.cols};
-        return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)u->ptr}, pt, NoFin{}, nullptr,
+                                conv_consts<T>(g->dx, g->dy), (T)0, (int)RR, (int)CC};
+        return launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)u->ptr}, pt, NoFin{}, nullptr,
                                      "apply_conv_diff");
     });
 }
@@ -161,11 +204,10 @@ int fx_conv_diff_axpy(fx_ctx *ctx, double alpha, const fx_buf *u, fx_buf *out, c
     FX_TRY(pre_vec(u, vx, "vx"));
     FX_TRY(pre_vec(u, vy, "vy"));
     FX_DISPATCH(u->dtype, {
-        constexpr int U = unroll_for<T>();
-        MarchGeom G = march_geom(ctx, g->rows, g->cols, U);
+        const size_t RR = g->rows, CC = g->cols;
         PtConvDiff<T, true> pt{(T *)out->ptr, (const T *)kappa->ptr, (const T *)vx->ptr, (const T *)vy->ptr,
-                               conv_consts<T>(g->dx, g->dy), (T)alpha, G.rows, G.cols};
-        return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)u->ptr}, pt, NoFin{}, nullptr,
+                               conv_consts<T>(g->dx, g->dy), (T)alpha, (int)RR, (int)CC};
+        return launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)u->ptr}, pt, NoFin{}, nullptr,
                                      "conv_diff_axpy");
     });
 }
@@ -267,10 +309,9 @@ int fx_jacobi_sweep(fx_ctx *ctx, const fx_buf *x_in, fx_buf *x_out, const fx_buf
     FX_TRY(pre_vec(x_in, b, "b"));
     const double wd = omega / a5[0];
     FX_DISPATCH(x_in->dtype, {
-        constexpr int U = unroll_for<T>();
-        MarchGeom G = march_geom(ctx, rows, cols, U);
-        PtJacobi<T> pt{(T *)x_out->ptr, (const T *)b->ptr, make_a5<T>(a5), (T)wd, G.rows, G.cols};
-        return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)x_in->ptr}, pt, NoFin{}, nullptr,
+        const size_t RR = rows, CC = cols;
+        PtJacobi<T> pt{(T *)x_out->ptr, (const T *)b->ptr, make_a5<T>(a5), (T)wd, (int)RR, (int)CC};
+        return launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)x_in->ptr}, pt, NoFin{}, nullptr,
                                      "jacobi_sweep");
     });
 }
@@ -282,10 +323,9 @@ int fx_residual5(fx_ctx *ctx, const fx_buf *x, const fx_buf *b, fx_buf *r, size_
     FX_TRY(pre_grid2(ctx, x, r, &g));
     FX_TRY(pre_vec(x, b, "b"));
     FX_DISPATCH(x->dtype, {
-        constexpr int U = unroll_for<T>();
-        MarchGeom G = march_geom(ctx, rows, cols, U);
-        PtResidual<T> pt{(T *)r->ptr, (const T *)b->ptr, make_a5<T>(a5), G.rows, G.cols};
-        return launch_march<T, U, 0>(ctx, G, LoadArr<T>{(const T *)x->ptr}, pt, NoFin{}, nullptr, "residual5");
+        const size_t RR = rows, CC = cols;
+        PtResidual<T> pt{(T *)r->ptr, (const T *)b->ptr, make_a5<T>(a5), (int)RR, (int)CC};
+        return launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)x->ptr}, pt, NoFin{}, nullptr, "residual5");
     });
 }
 
