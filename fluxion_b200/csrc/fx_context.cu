@@ -291,6 +291,25 @@ int fx_ctx_timing_begin(fx_ctx *c, const char *kernel) {
     return FX_OK;
 }
 
+int fx_ctx_timing_end_records(fx_ctx *c, double *ms, double *points, size_t max, size_t *count) {
+    if (!c || !ms || !points || !count) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_CUDA(cudaStreamSynchronize(c->stream));
+    size_t k = 0;
+    for (auto &r : c->timing_recs) {
+        if (k >= max) break;
+        float t = 0.f;
+        FX_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+        ms[k] = t;
+        points[k] = r.points;
+        k++;
+    }
+    *count = k;
+    c->timing = false;
+    c->timing_recs.clear();
+    c->pool_next = 0;
+    return FX_OK;
+}
+
 int fx_ctx_timing_end(fx_ctx *c, double *total_ms, unsigned long long *launches, double *total_points) {
     if (!c || !total_ms || !launches || !total_points) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     FX_CUDA(cudaStreamSynchronize(c->stream));

@@ -312,6 +312,19 @@ struct MarchGeom {
 // capacity: CTAs of the kernel resident on the whole GPU at once
 MarchGeom march_geom(size_t rows, size_t cols, int bx, int d, int capacity);
 
+// Functors may define `void prepare()`, called once per thread at kernel start, to read the
+// solver scalars they need from device memory into registers.
+template <typename X>
+__device__ __forceinline__ auto fx_prepare_impl(X &x, int) -> decltype(x.prepare(), void()) {
+    x.prepare();
+}
+template <typename X>
+__device__ __forceinline__ void fx_prepare_impl(X &, long) {}
+template <typename X>
+__device__ __forceinline__ void fx_prepare(X &x) {
+    fx_prepare_impl(x, 0);
+}
+
 template <typename T>
 constexpr int band_cpt() {
     return sizeof(T) == 8 ? 1 : 2;
@@ -319,17 +332,21 @@ constexpr int band_cpt() {
 
 template <int NA>
 constexpr int band_depth() {
-    return NA == 0 ? 8 : (NA == 1 ? 4 : 3);
+    return NA == 0 ? 8 : (NA <= 2 ? 4 : 2);  // even: rows are consumed in pairs
 }
 
 template <typename T, int CPT, int D, int K, typename Loader, typename Point, typename Fin>
-__global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader ld, Point pt, Fin fin,
+__global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader ld_in, Point pt_in, Fin fin,
                                                            RedArgs<K> ra, const int *skip) {
     if (skip && *(volatile const int *)skip) return;
+    Loader ld = ld_in;  // device-resident scalars (alpha, beta, ...) read once per kernel
+    fx_prepare(ld);
+    Point pt = pt_in;
+    fx_prepare(pt);
     constexpr int BX = kBlock * CPT;
     constexpr int W = BX + 2;
     constexpr int NA = Point::NA;
-    __shared__ T ring[4][W];
+    __shared__ T ring[8][W];
     CSum acc[K > 0 ? K : 1];
 #pragma unroll
     for (int k = 0; k < (K > 0 ? K : 1); k++) acc[k] = CSum{0.0, 0.0};
@@ -367,14 +384,22 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader l
     }
     const bool writes_smem = !halo_warp || hl < 2;
 
-    T fv[D][CPT];                      // marched field, row r+1 (D rows ahead)
+    constexpr int NL = Loader::NL;
+    T fv[D][CPT][NL];                  // raw loads of the marched field, row r+1 (D rows ahead)
     T fa[D][CPT][NA > 0 ? NA : 1];     // aux arrays, row r (D rows ahead)
 
-    auto load_field = [&](int r, T (&v)[CPT]) {
+    // raw values only: the loader combines them (e.g. r + beta p) when the row enters the
+    // ring, so no prefetched load is waited on before its row is due
+    auto load_field = [&](int r, T (&v)[CPT][NL]) {
+        const bool rin = r >= 0 && r < rows;
+        const size_t ro = (size_t)(rin ? r : 0) * cols;
 #pragma unroll
         for (int s = 0; s < CPT; s++) {
-            v[s] = (T)0;
-            if (r >= 0 && r < rows && valid[s]) v[s] = ld((size_t)r * cols + col[s]);
+            if (rin && valid[s]) ld.load(ro + col[s], v[s]);
+            else {
+#pragma unroll
+                for (int q = 0; q < NL; q++) v[s][q] = (T)0;
+            }
         }
     };
     auto load_aux = [&](int r, T (&a)[CPT][NA > 0 ? NA : 1]) {
@@ -389,18 +414,44 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader l
             }
         }
     };
-    auto store_row = [&](int r, const T (&v)[CPT]) {
+    auto store_row = [&](int r, const T (&v)[CPT][NL]) {
         if (!writes_smem) return;
-        T *row = ring[r & 3];
+        T *row = ring[r & 7];
+        const bool rin = r >= 0 && r < rows;
 #pragma unroll
         for (int s = 0; s < CPT; s++)
-            if (!halo_warp || s == 0) row[sidx[s]] = v[s];
+            if (!halo_warp || s == 0) row[sidx[s]] = (rin && valid[s]) ? ld.combine(v[s]) : (T)0;
+    };
+    auto compute_row = [&](int r, const T (&a)[CPT][NA > 0 ? NA : 1]) {
+        const T *rn = ring[(r + 7) & 7];
+        const T *rc = ring[r & 7];
+        const T *rs = ring[(r + 1) & 7];
+        const bool ringrow = (r == 0) || (r == rows - 1);
+        const size_t rowoff = (size_t)r * cols;
+#pragma unroll
+        for (int s = 0; s < CPT; s++) {
+            if (point[s]) {
+                const int i = sidx[s];
+                const bool edge = i == 0;  // column 0: no west neighbours
+                Nb<T> nb;
+                nb.c = rc[i];
+                nb.n = rn[i];
+                nb.s = rs[i];
+                nb.w = edge ? (T)0 : rc[i - 1];
+                nb.e = rc[i + 1];
+                nb.nw = edge ? (T)0 : rn[i - 1];
+                nb.ne = rn[i + 1];
+                nb.sw = edge ? (T)0 : rs[i - 1];
+                nb.se = rs[i + 1];
+                pt(ringrow || ringcol[s], r, col[s], rowoff + col[s], nb, a[s], acc);
+            }
+        }
     };
 
     {
-        T v[CPT];
+        T v[CPT][NL];
         load_field(r0 - 1, v);
-        store_row(r0 + 3, v);  // (r0 - 1) & 3 without a negative operand
+        store_row(r0 - 1, v);  // slot (r0 - 1) & 7 (two's complement for r0 = 0)
         load_field(r0, v);
         store_row(r0, v);
     }
@@ -410,40 +461,23 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader l
         load_aux(r0 + u, fa[u]);
     }
 
+    // Two rows per step: rows r+1, r+2 of the field arrive, rows r, r+1 are computed.  The
+    // 8-row ring keeps every row a later step may still read (rows r-1 .. r+2 are needed;
+    // the slots being overwritten were last read three steps, and two barriers, earlier).
     for (int rb = r0; rb < r1; rb += D) {
 #pragma unroll
-        for (int u = 0; u < D; u++) {
+        for (int u = 0; u < D; u += 2) {
             const int r = rb + u;
             store_row(r + 1, fv[u]);
+            store_row(r + 2, fv[u + 1]);
             __syncthreads();
-            if (r < r1) {
-                const T *rn = ring[(r + 3) & 3];
-                const T *rc = ring[r & 3];
-                const T *rs = ring[(r + 1) & 3];
-                const bool ringrow = (r == 0) || (r == rows - 1);
-                const size_t rowoff = (size_t)r * cols;
-#pragma unroll
-                for (int s = 0; s < CPT; s++) {
-                    if (point[s]) {
-                        const int i = sidx[s];
-                        const bool edge = i == 0;  // column 0: no west neighbours
-                        Nb<T> nb;
-                        nb.c = rc[i];
-                        nb.n = rn[i];
-                        nb.s = rs[i];
-                        nb.w = edge ? (T)0 : rc[i - 1];
-                        nb.e = rc[i + 1];
-                        nb.nw = edge ? (T)0 : rn[i - 1];
-                        nb.ne = rn[i + 1];
-                        nb.sw = edge ? (T)0 : rs[i - 1];
-                        nb.se = rs[i + 1];
-                        pt(ringrow || ringcol[s], r, col[s], rowoff + col[s], nb, fa[u][s], acc);
-                    }
-                }
-            }
-            // refill this FIFO stage: field row r+1+D, aux row r+D (only rows the chunk needs)
+            if (r < r1) compute_row(r, fa[u]);
+            if (r + 1 < r1) compute_row(r + 1, fa[u + 1]);
+            // refill these FIFO stages: field rows r+1+D, r+2+D and aux rows r+D, r+1+D
             if (r + 1 + D <= r1) load_field(r + 1 + D, fv[u]);
+            if (r + 2 + D <= r1) load_field(r + 2 + D, fv[u + 1]);
             load_aux(r + D, fa[u]);
+            load_aux(r + 1 + D, fa[u + 1]);
         }
     }
     if constexpr (K > 0) grid_reduce<K>(acc, ra, fin);
@@ -482,9 +516,11 @@ struct FlatGeom {
 FlatGeom flat_geom(fx_ctx *ctx, size_t n);
 
 template <int K, typename F, typename Fin>
-__global__ void __launch_bounds__(kBlock) k_flat(size_t n, F f, Fin fin, RedArgs<K> ra,
+__global__ void __launch_bounds__(kBlock) k_flat(size_t n, F f_in, Fin fin, RedArgs<K> ra,
                                                  const int *skip) {
     if (skip && *(volatile const int *)skip) return;
+    F f = f_in;
+    fx_prepare(f);
     CSum acc[K > 0 ? K : 1];
 #pragma unroll
     for (int k = 0; k < (K > 0 ? K : 1); k++) acc[k] = CSum{0.0, 0.0};

@@ -34,8 +34,10 @@ namespace fx {
 
 template <typename T>
 struct LoadArr {
+    static constexpr int NL = 1;
     const T *p;
-    __device__ __forceinline__ T operator()(size_t i) const { return p[i]; }
+    __device__ __forceinline__ void load(size_t i, T (&v)[1]) const { v[0] = p[i]; }
+    __device__ __forceinline__ T combine(const T (&v)[1]) const { return v[0]; }
 };
 
 template <typename T>

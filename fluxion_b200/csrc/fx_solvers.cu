@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "fx_points.cuh"
+#include "fx_vcycle.cuh"
 
 using namespace fx;
 
@@ -44,6 +45,27 @@ __device__ __forceinline__ void st_finish(DevState *S, int reason, long long ite
     S->resid = resid;
 }
 
+// PCG inner product r.z -> beta (cg.rs:202-212 at the start, :240-247 per iteration)
+struct FinPcgRzInit {  // rz_old = r.z, beta = 0, loop-top test of iteration 0 (cg.rs:202-212)
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->rs_old = v[0];
+        S->beta = 0.0;
+        S->iter = 0;
+        S->r0 = S->resid;
+        if (S->max_iter == 0) st_finish(S, FX_MAX_ITERATIONS, 0, S->resid);
+        else if (S->resid < S->tol) st_finish(S, FX_CONVERGED, 0, S->resid);
+    }
+};
+
+struct FinPcgRz {  // beta = rz_new / rz_old (cg.rs:240-247)
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->beta = v[0] / S->rs_old;
+        S->rs_old = v[0];
+    }
+};
+
 }  // namespace fx
 
 // ---------------------------------------------------------------- preconditioners
@@ -55,6 +77,9 @@ struct fx_precond {
     // z <- M^-1 r.  z_zero: z holds zeros on entry (the solvers zero-fill z first, as the
     // reference does); skip: device word, nonzero means the solve is over.
     virtual int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) = 0;
+    // z <- M^-1 r from a zero z, followed by rz = r.z handed to the PCG state S (first = the
+    // initial product).  Returns FX_ERR_UNSUPPORTED when the preconditioner has no fused form.
+    virtual int apply_pcg(fx_buf *, const fx_buf *, const int *, DevState *, bool) { return FX_ERR_UNSUPPORTED; }
 };
 
 namespace {
@@ -75,19 +100,25 @@ struct OpA {
 
 template <typename T>
 struct Ld1 {
+    static constexpr int NL = 1;
     const T *p;
-    __device__ __forceinline__ T operator()(size_t i) const { return p[i]; }
+    __device__ __forceinline__ void load(size_t i, T (&v)[1]) const { v[0] = p[i]; }
+    __device__ __forceinline__ T combine(const T (&v)[1]) const { return v[0]; }
 };
 
 // r + beta*p, rounded as p.scale(beta); p.axpy(1.0, r) (cg.rs:153-154)
 template <typename T>
 struct LdAypx {
+    static constexpr int NL = 2;
     const T *r, *p;
     const DevState *S;
-    __device__ __forceinline__ T operator()(size_t i) const {
-        const T beta = (T)S->beta;
-        return r[i] + p[i] * beta;
+    T beta;
+    __device__ __forceinline__ void prepare() { beta = (T)S->beta; }
+    __device__ __forceinline__ void load(size_t i, T (&v)[2]) const {
+        v[0] = r[i];
+        v[1] = p[i];
     }
+    __device__ __forceinline__ T combine(const T (&v)[2]) const { return v[0] + v[1] * beta; }
 };
 
 // ------------------------------------------------ flat (pointwise) functors
@@ -223,6 +254,7 @@ struct fx_mg {
     struct View : fx_precond {
         fx_mg *mg = nullptr;
         int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) override;
+        int apply_pcg(fx_buf *z, const fx_buf *r, const int *skip, DevState *S, bool first) override;
     } view;
     ~fx_mg() {
         for (auto &L : lv) {
@@ -298,34 +330,59 @@ int zero_fill(fx_ctx *ctx, T *p, size_t n, const int *skip) {
 // Coarsest level: all sweeps in one block, the grid held in shared memory.  Each point
 // evaluates exactly the expression of the sweep kernel, so the result is bitwise equal
 // to running `nsweeps` separate sweeps.
+// One-block coarsest solve: at most 4 points per thread (4096 points) and two smem copies.
+inline bool coarse_fits(size_t n, size_t esize) { return n <= 4096 && 2 * n * esize <= 48 * 1024; }
+inline int coarse_threads(size_t n) {
+    // one point per thread while the grid fits a block (each sweep is a latency chain), up to
+    // 4 points per thread above that
+    size_t t = ((n + 31) / 32) * 32;
+    if (t < 32) t = 32;
+    if (t > 1024) t = 1024;
+    return (int)t;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(1024) k_coarse_solve(T *u, const T *__restrict__ b, int rows, int cols,
-                                                       A5<T> a, T wd, int nsweeps, const int *skip) {
+                                                       A5<T> a, T wd, int nsweeps, bool zero_init, const int *skip) {
     if (skip && *(volatile const int *)skip) return;
+    // Each thread owns up to kCoarsePts points (fixed for the whole solve): its rhs values and
+    // interior flags stay in registers, the iterate ping-pongs between two smem copies.
+    constexpr int kCoarsePts = 4;
     extern __shared__ unsigned char smem_raw[];
     T *s0 = reinterpret_cast<T *>(smem_raw);
     T *s1 = s0 + rows * cols;
-    T *sb = s1 + rows * cols;
     const int n = rows * cols;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        s0[i] = u[i];
-        s1[i] = u[i];
-        sb[i] = b[i];
+    int idx[kCoarsePts];
+    bool inner[kCoarsePts];
+    T bv[kCoarsePts];
+#pragma unroll
+    for (int k = 0; k < kCoarsePts; k++) {
+        const int i = threadIdx.x + k * blockDim.x;
+        idx[k] = i;
+        const int r = i / cols, c = i % cols;
+        inner[k] = i < n && r > 0 && c > 0 && r < rows - 1 && c < cols - 1;
+        bv[k] = i < n ? b[i] : (T)0;
+        if (i < n) {
+            const T v = zero_init ? (T)0 : u[i];
+            s0[i] = v;
+            s1[i] = v;
+        }
     }
     __syncthreads();
     for (int k = 0; k < nsweeps; k++) {
         const T *src = (k & 1) ? s1 : s0;
         T *dst = (k & 1) ? s0 : s1;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const int r = i / cols, c = i % cols;
-            if (r == 0 || c == 0 || r == rows - 1 || c == cols - 1) continue;
+#pragma unroll
+        for (int q = 0; q < kCoarsePts; q++) {
+            if (!inner[q]) continue;
+            const int i = idx[q];
             Nb<T> nb;
             nb.c = src[i];
             nb.n = src[i - cols];
             nb.s = src[i + cols];
             nb.w = src[i - 1];
             nb.e = src[i + 1];
-            dst[i] = fx_fma(wd, sb[i] - op5<T>(a, nb), nb.c);
+            dst[i] = fx_fma(wd, bv[q] - op5<T>(a, nb), nb.c);
         }
         __syncthreads();
     }
@@ -377,11 +434,11 @@ int vertex_cycle(fx_mg *mg, T *x, const T *b, const int *skip, bool x_zero) {
         const int l = nl - 1;
         MgLevel &L = mg->lv[l];
         const size_t n = L.rows * L.cols;
-        const size_t smem = 3 * n * sizeof(T);
-        if (smem <= 48 * 1024 && mg->coarse_sweeps > 0) {
-            k_coarse_solve<T><<<1, 1024, smem, ctx->stream>>>(cur[l], rhs[l], (int)L.rows, (int)L.cols,
+        const size_t smem = 2 * n * sizeof(T);
+        if (coarse_fits(n, sizeof(T)) && mg->coarse_sweeps > 0) {
+            k_coarse_solve<T><<<1, coarse_threads(n), smem, ctx->stream>>>(cur[l], rhs[l], (int)L.rows, (int)L.cols,
                                                               make_a5<T>(L.a5), (T)(mg->omega / L.a5[0]),
-                                                              (int)mg->coarse_sweeps, skip);
+                                                              (int)mg->coarse_sweeps, false, skip);
             FX_TRY(check_launch(ctx, "mg_coarse_solve"));
             // the kernel writes the final iterate back into cur[l]; cur/oth roles unchanged
         } else {
@@ -443,6 +500,76 @@ int reference_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b, bool x_zero) {
 
 }  // namespace
 
+namespace {
+
+// Fused V(2,2)-cycle from a zero initial guess: per level one down and one up kernel, the
+// coarsest level solved in one block.  b0 / z0 are the finest-level rhs and result (TB / TZ
+// may be double while the cycle runs in T = float); with RZ the finest up kernel also
+// reduces r.z into `fin`.
+template <typename T, typename TB, typename TZ, bool RZ, typename Fin>
+int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
+    fx_ctx *ctx = mg->ctx;
+    const int nl = (int)mg->lv.size();
+    auto vop = [&](int l) {
+        const MgLevel &L = mg->lv[l];
+        return VOp<T>{make_a5<T>(L.a5), (T)(mg->omega / L.a5[0])};
+    };
+    // down: level 0 reads b0 (TB), the others their rhs (T); x2 of level 0 lives in tmp0
+    {
+        const MgLevel &L = mg->lv[0], &C = mg->lv[1];
+        FX_TRY((launch_vdown<T, TB>(ctx, L.rows, L.cols, b0, (T *)mg->tmp0->ptr, (T *)C.rhs->ptr, C.cols,
+                                    vop(0), skip)));
+    }
+    for (int l = 1; l < nl - 1; l++) {
+        const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
+        FX_TRY((launch_vdown<T, T>(ctx, L.rows, L.cols, (const T *)L.rhs->ptr, (T *)L.tmp->ptr, (T *)C.rhs->ptr,
+                                   C.cols, vop(l), skip)));
+    }
+    {
+        const MgLevel &L = mg->lv[nl - 1];
+        const size_t n = L.rows * L.cols;
+        const size_t smem = 2 * n * sizeof(T);
+        if (!coarse_fits(n, sizeof(T)))
+            return fail(FX_ERR_UNSUPPORTED, "coarsest level too large for the one-block solve");
+        timing_pre(ctx, "mg_coarse_solve");
+        k_coarse_solve<T><<<1, coarse_threads(n), smem, ctx->stream>>>((T *)L.u->ptr, (const T *)L.rhs->ptr, (int)L.rows,
+                                                          (int)L.cols, make_a5<T>(L.a5), (T)(mg->omega / L.a5[0]),
+                                                          (int)mg->coarse_sweeps, true, skip);
+        timing_post(ctx, (double)n);
+        FX_TRY(check_launch(ctx, "mg_coarse_solve"));
+    }
+    for (int l = nl - 2; l >= 1; l--) {
+        const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
+        FX_TRY((launch_vup<T, T, T, false>(ctx, L.rows, L.cols, (const T *)L.tmp->ptr, (const T *)C.u->ptr, C.cols,
+                                           (const T *)L.rhs->ptr, (T *)L.u->ptr, vop(l), NoFin{}, skip)));
+    }
+    const MgLevel &L = mg->lv[0], &C = mg->lv[1];
+    return launch_vup<T, TB, TZ, RZ>(ctx, L.rows, L.cols, (const T *)mg->tmp0->ptr, (const T *)C.u->ptr, C.cols, b0,
+                                     z0, vop(0), fin, skip);
+}
+
+bool fusable(const fx_mg *m) {
+    if (m->mode != 1 || m->n_pre != 2 || m->n_post != 2 || m->lv.size() < 2) return false;
+    const MgLevel &L = m->lv.back();
+    return coarse_fits(L.rows * L.cols, m->dtype == FX_F64 ? 8 : 4);
+}
+
+}  // namespace
+
+int fx_mg::View::apply_pcg(fx_buf *z, const fx_buf *r, const int *skip, DevState *S, bool first) {
+    fx_mg *m = mg;
+    if (!fusable(m) || z->dtype != FX_F64 || r->dtype != FX_F64 || z->len != m->lv[0].rows * m->lv[0].cols)
+        return FX_ERR_UNSUPPORTED;
+    const double *b0 = (const double *)r->ptr;
+    double *z0 = (double *)z->ptr;
+    if (m->dtype == FX_F64) {
+        if (first) return fused_cycle<double, double, double, true>(m, b0, z0, FinPcgRzInit{S}, skip);
+        return fused_cycle<double, double, double, true>(m, b0, z0, FinPcgRz{S}, skip);
+    }
+    if (first) return fused_cycle<float, double, double, true>(m, b0, z0, FinPcgRzInit{S}, skip);
+    return fused_cycle<float, double, double, true>(m, b0, z0, FinPcgRz{S}, skip);
+}
+
 int fx_mg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) {
     fx_mg *m = mg;
     const MgLevel &L0 = m->lv[0];
@@ -452,6 +579,14 @@ int fx_mg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero)
                                                    std::to_string(z->len));
     if (z->dtype != r->dtype) return fail(FX_ERR_INVALID_ARGUMENT, "dtype mismatch between buffers");
     if (m->mode == 0) return reference_cycle(m, z, r, z_zero);
+    if (z_zero && fusable(m) && z->dtype == FX_F64) {
+        if (m->dtype == FX_F64)
+            return fused_cycle<double, double, double, false>(m, (const double *)r->ptr, (double *)z->ptr, NoFin{}, skip);
+        return fused_cycle<float, double, double, false>(m, (const double *)r->ptr, (double *)z->ptr, NoFin{}, skip);
+    }
+    if (z_zero) {  // the unfused cycle reads z as its initial guess
+        FX_TRY(launch_flat<0>(m->ctx, z->len, FlatZero<double>{(double *)z->ptr}, NoFin{}, skip, "mg_zero"));
+    }
     if (m->dtype == z->dtype) {
         if (z->dtype == FX_F64) return vertex_cycle<double>(m, (double *)z->ptr, (const double *)r->ptr, skip, z_zero);
         return vertex_cycle<float>(m, (float *)z->ptr, (const float *)r->ptr, skip, z_zero);
@@ -647,9 +782,10 @@ struct PtCgUpd {
     OpA<T, MODE> A;
     T *x, *r;
     const DevState *S;
+    T alpha;
+    __device__ __forceinline__ void prepare() { alpha = (T)S->alpha; }
     __device__ __forceinline__ const T *aux(int k) const { return k == 0 ? x : r; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T alpha = (T)S->alpha;
         const T ap = A.apply(ring, nb);
         x[idx] = fx_fma(alpha, nb.c, a[0]);
         const T rv = fx_fma(-alpha, ap, a[1]);
@@ -688,26 +824,6 @@ struct FinPcgUpd {
         S->resid = sqrt(v[0]);
         if (S->iter >= S->max_iter) st_finish(S, FX_MAX_ITERATIONS, S->max_iter, sqrt(v[0]));
         else if (sqrt(v[0]) < S->tol) st_finish(S, FX_CONVERGED, S->iter, sqrt(v[0]));
-    }
-};
-
-struct FinPcgRzInit {  // rz_old = r.z, beta = 0, loop-top test of iteration 0 (cg.rs:202-212)
-    DevState *S;
-    __device__ void operator()(const double *v) const {
-        S->rs_old = v[0];
-        S->beta = 0.0;
-        S->iter = 0;
-        S->r0 = S->resid;
-        if (S->max_iter == 0) st_finish(S, FX_MAX_ITERATIONS, 0, S->resid);
-        else if (S->resid < S->tol) st_finish(S, FX_CONVERGED, 0, S->resid);
-    }
-};
-
-struct FinPcgRz {  // beta = rz_new / rz_old (cg.rs:240-247)
-    DevState *S;
-    __device__ void operator()(const double *v) const {
-        S->beta = v[0] / S->rs_old;
-        S->rs_old = v[0];
     }
 };
 
@@ -751,18 +867,23 @@ int cg_solve_impl(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const Sten
     FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, r, nullptr}, FinPcgResid{S},
                                   nullptr, "pcg_init")));
     fx_buf rb{ctx, r, n, FX_F64, false}, zb{ctx, z, n, FX_F64, false};
-    FX_TRY(zero_fill<T>(ctx, z, n, nullptr));
-    FX_TRY(pc->apply(&zb, &rb, halt, true));
-    FX_TRY(launch_flat<1>(ctx, n, FlatDot<T>{r, z}, FinPcgRzInit{S}, halt, "pcg_rz"));
+    // z = M^-1 r and rz = r.z, fused into the preconditioner when it has a fused form
+    auto precondition = [&](bool first) -> int {
+        const int st = pc->apply_pcg(&zb, &rb, halt, S, first);
+        if (st != FX_ERR_UNSUPPORTED) return st;
+        FX_TRY(zero_fill<T>(ctx, z, n, halt));
+        FX_TRY(pc->apply(&zb, &rb, halt, true));
+        if (first) return launch_flat<1>(ctx, n, FlatDot<T>{r, z}, FinPcgRzInit{S}, halt, "pcg_rz");
+        return launch_flat<1>(ctx, n, FlatDot<T>{r, z}, FinPcgRz{S}, halt, "pcg_rz");
+    };
+    FX_TRY(precondition(true));
     auto step = [&](size_t i) -> int {
         T *po = pb[i & 1], *pn = pb[(i + 1) & 1];
         FX_TRY((launch_march<T, 1>(ctx, RR, CC, LdAypx<T>{z, po, S}, PtCgDir<T, MODE>{A, pn}, FinCgDir{S}, halt,
                                       "pcg_dir")));
         FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{pn}, PtCgUpd<T, MODE>{A, xp, r, S}, FinPcgUpd{S}, halt,
                                       "pcg_update")));
-        FX_TRY(zero_fill<T>(ctx, z, n, halt));
-        FX_TRY(pc->apply(&zb, &rb, halt, true));
-        return launch_flat<1>(ctx, n, FlatDot<T>{r, z}, FinPcgRz{S}, halt, "pcg_rz");
+        return precondition(false);
     };
     return s->drive(step, s->max_iter + 1, true);
 }
@@ -828,11 +949,15 @@ struct PtPipeIter {
     OpA<T, MODE> A;
     T *z, *t, *p, *x, *r, *w_new;
     const DevState *S;
+    T alpha, beta;
+    __device__ __forceinline__ void prepare() {
+        alpha = (T)S->alpha;
+        beta = (T)S->beta;
+    }
     __device__ __forceinline__ const T *aux(int k) const {
         return k == 0 ? z : (k == 1 ? t : (k == 2 ? p : (k == 3 ? x : r)));
     }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T alpha = (T)S->alpha, beta = (T)S->beta;
         const T q = A.apply(ring, nb);
         const T w = nb.c;
         const T zn = q + a[0] * beta;
@@ -936,12 +1061,20 @@ struct FinBicgInit {
 // p_new = r + beta (p_old - omega v_old), rounded as p.axpy(-omega, v); p.scale(beta); p.axpy(1, r)
 template <typename T>
 struct LdBicgP {
+    static constexpr int NL = 3;
     const T *r, *p, *v;
     const DevState *S;
-    __device__ __forceinline__ T operator()(size_t i) const {
-        const T beta = (T)S->beta, omega = (T)S->omega;
-        return r[i] + fx_fma(-omega, v[i], p[i]) * beta;
+    T beta, omega;
+    __device__ __forceinline__ void prepare() {
+        beta = (T)S->beta;
+        omega = (T)S->omega;
     }
+    __device__ __forceinline__ void load(size_t i, T (&x)[3]) const {
+        x[0] = r[i];
+        x[1] = p[i];
+        x[2] = v[i];
+    }
+    __device__ __forceinline__ T combine(const T (&x)[3]) const { return x[0] + fx_fma(-omega, x[2], x[1]) * beta; }
 };
 
 // v = A (p or p_hat); store p_new when marching the fused p; reduction r_hat.v
@@ -1032,8 +1165,10 @@ struct FlatBicgS {
     const T *r, *v;
     T *s;
     const DevState *S;
+    T alpha;
+    __device__ __forceinline__ void prepare() { alpha = (T)S->alpha; }
     __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
-        const T sv = fx_fma(-(T)S->alpha, v[i], r[i]);
+        const T sv = fx_fma(-alpha, v[i], r[i]);
         s[i] = sv;
         csum_add_prod(acc[0], (double)sv, (double)sv);
     }
@@ -1046,13 +1181,18 @@ struct FlatBicgFinish {
     T *x, *r;
     const T *pp, *ss, *t, *s, *rh;
     const DevState *S;
+    T alpha, omega;
+    int pending;
+    __device__ __forceinline__ void prepare() {
+        alpha = (T)S->alpha;
+        omega = (T)S->omega;
+        pending = S->pending;
+    }
     __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
-        const T alpha = (T)S->alpha;
-        if (S->pending) {
+        if (pending) {
             x[i] = fx_fma(alpha, pp[i], x[i]);
             return;
         }
-        const T omega = (T)S->omega;
         x[i] = fx_fma(omega, ss[i], fx_fma(alpha, pp[i], x[i]));
         const T rv = fx_fma(-omega, t[i], s[i]);
         r[i] = rv;
@@ -1067,8 +1207,12 @@ struct FlatBicgP {
     T *p;
     const T *r, *v;
     const DevState *S;
+    T beta, omega;
+    __device__ __forceinline__ void prepare() {
+        beta = (T)S->beta;
+        omega = (T)S->omega;
+    }
     __device__ __forceinline__ void operator()(size_t i, CSum *) const {
-        const T beta = (T)S->beta, omega = (T)S->omega;
         p[i] = r[i] + fx_fma(-omega, v[i], p[i]) * beta;
     }
 };
@@ -1240,8 +1384,10 @@ struct FlatGmMgs {  // w -= h_j v_j; reduction w.v_{j+1} (or w.w after the last)
     T *w;
     const T *vj, *vn;
     const double *hj;
+    T h;
+    __device__ __forceinline__ void prepare() { h = (T)(*hj); }
     __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
-        const T wv = fx_fma(-(T)(*hj), vj[i], w[i]);
+        const T wv = fx_fma(-h, vj[i], w[i]);
         w[i] = wv;
         if (vn) csum_add_prod(acc[0], (double)wv, (double)vn[i]);
         else csum_add_prod(acc[0], (double)wv, (double)wv);
@@ -1588,6 +1734,13 @@ int fx_mg_v_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b) {
     FX_TRY(check_buf(x, "x"));
     FX_TRY(check_buf(b, "b"));
     return mg->view.apply(x, b, nullptr, false);
+}
+
+int fx_mg_precondition(fx_mg *mg, fx_buf *z, const fx_buf *r) {
+    if (!mg) return fail(FX_ERR_INVALID_ARGUMENT, "null multigrid");
+    FX_TRY(check_buf(z, "z"));
+    FX_TRY(check_buf(r, "r"));
+    return mg->view.apply(z, r, nullptr, true);
 }
 
 fx_precond *fx_mg_as_precond(fx_mg *mg) { return mg ? &mg->view : nullptr; }

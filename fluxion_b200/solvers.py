@@ -152,6 +152,10 @@ class Multigrid(Preconditioner):
     def v_cycle(self, x: Field, b: Field) -> None:
         check(L.lib().fx_mg_v_cycle(self.h, x.storage.handle, b.storage.handle))
 
+    def precondition(self, z: Field, r: Field) -> None:
+        """z = M^-1 r from a zero initial guess (z.fill(0); apply(z, r), cg.rs:196-197)."""
+        check(L.lib().fx_mg_precondition(self.h, z.storage.handle, r.storage.handle))
+
     def _handle(self, device: Device) -> int:
         return L.lib().fx_mg_as_precond(self.h)
 

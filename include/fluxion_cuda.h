@@ -120,6 +120,9 @@ unsigned long long fx_ctx_launch_count(fx_ctx *ctx);
 int fx_ctx_timing_begin(fx_ctx *ctx, const char *kernel);
 int fx_ctx_timing_end(fx_ctx *ctx, double *total_ms, unsigned long long *launches,
                       double *total_points);
+/* Like fx_ctx_timing_end, but also returns up to `max` individual launches (device ms and
+ * grid points each, in launch order) through ms[] / points[]; *count is the number written. */
+int fx_ctx_timing_end_records(fx_ctx *ctx, double *ms, double *points, size_t max, size_t *count);
 
 /* ------------------------------------------------------------------ */
 /* Memory (Backend::allocate / upload_f64 / upload_f32, backend.rs:49-77;
@@ -262,6 +265,9 @@ int fx_mg_depth(const fx_mg *mg, size_t *depth);
 int fx_mg_level_dims(const fx_mg *mg, size_t level, size_t *rows, size_t *cols);
 /* Multigrid::v_cycle (multigrid.rs:188-230): x (initial guess, in/out), b (rhs). */
 int fx_mg_v_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b);
+/* Preconditioner application from a zero initial guess: z = M^-1 r, i.e. the reference's
+ * z.fill(0); pc.apply(z, r) (cg.rs:196-197).  Uses the fused V(2,2) kernels when they apply. */
+int fx_mg_precondition(fx_mg *mg, fx_buf *z, const fx_buf *r);
 /* Borrowed view of the multigrid as a preconditioner (impl Preconditioner, :600-608).
  * Valid until fx_mg_destroy; do not pass it to fx_precond_destroy. */
 fx_precond *fx_mg_as_precond(fx_mg *mg);

@@ -214,6 +214,37 @@ def test_vertex_mg_vcycle_bitwise(dev, n):
     assert np.array_equal(x.to_vec_f64(), xo)
 
 
+@pytest.mark.parametrize("n", [15, 63, 255, 1023])
+def test_fused_vcycle_bitwise(dev, n):
+    """The fused V(2,2) kernels (zero initial guess) equal the oracle's separate sweeps, residual,
+    full weighting and bilinear prolongation bit for bit (F64), and the fused F32 cycle equals
+    the unfused F32 cycle bit for bit."""
+    from fluxion_b200 import DType, Field, Multigrid
+    from fluxion_b200.workloads import poisson_problem
+    P = poisson_problem(n)
+    N = n + 2
+    rng = np.random.default_rng(n + 1)
+    bvec = np.zeros((N, N))
+    bvec[1:-1, 1:-1] = rng.uniform(-1, 1, (n, n))
+    bvec = bvec.ravel()
+    b = Field.from_f64(P.grid, bvec, dev)
+    mg = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200)
+    z = Field.zeros(P.grid, DType.F64, dev)
+    mg.precondition(z, b)
+    omg = O.Multigrid(N, N, P.h, P.h, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=P.stencil.as_triples(),
+                      coarse_max=15, coarse_sweeps=200)
+    zo = np.zeros(N * N)
+    omg.v_cycle(zo, bvec)
+    assert np.array_equal(z.to_vec_f64(), zo)
+    mg32 = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200, DType.F32)
+    zf = Field.zeros(P.grid, DType.F64, dev)
+    mg32.precondition(zf, b)
+    zu = Field.zeros(P.grid, DType.F64, dev)
+    mg32.v_cycle(zu, b)  # unfused path (explicit initial guess)
+    assert np.array_equal(zf.to_vec_f64(), zu.to_vec_f64())
+    assert rel_err(zf.to_vec_f64(), zo) < 1e-5
+
+
 # ---------------------------------------------------------------- solution level
 
 @pytest.mark.parametrize("n,pipelined", [(255, False), (255, True), (511, False)])
