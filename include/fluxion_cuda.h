@@ -170,6 +170,15 @@ int fx_dot(fx_ctx *ctx, const fx_buf *x, const fx_buf *y, double *out);         
 /* dot2 :219-230 -- (a.b, c.d) in one pass. */
 int fx_dot2(fx_ctx *ctx, const fx_buf *a, const fx_buf *b, const fx_buf *c, const fx_buf *d,
             double *ab, double *cd);
+/* No counterpart in the reference.  Dot product of two FP64 device arrays (plain device
+ * pointers) that allocates nothing, for callers that cannot let the library allocate device
+ * memory (an application owning all device memory through its own pool, a loop that must not
+ * reach the allocator).  Its reduction scratch is a fixed static device array (64 KiB per
+ * GPU, held until exit), so n is limited to 8,388,608 elements (FX_ERR_INVALID_ARGUMENT
+ * above that).  Runs on `stream` (a cudaStream_t; NULL = default stream) and synchronises it.
+ * Calls share the scratch: calls that overlap on the GPU race.  The first call on a device
+ * resolves the array's device address; make it before any stream capture. */
+int fx_dot_f64_noalloc(const double *x, const double *y, size_t n, double *out, void *stream);
 /* restrict :240-246 (reference semantics: clamped 2x2 average). */
 int fx_restrict(fx_ctx *ctx, const fx_buf *fine, fx_buf *coarse, const fx_grid *fine_grid,
                 const fx_grid *coarse_grid);
