@@ -44,11 +44,12 @@ void timing_pre(fx_ctx *ctx, const char *what) {
     ctx->timing_open = true;
 }
 
-void timing_post(fx_ctx *ctx, double points) {
+void timing_post(fx_ctx *ctx, double points, double bytes) {
     if (!ctx->timing_open) return;
     fx_timing_rec &r = ctx->timing_recs.back();
     cudaEventRecord(r.b, ctx->stream);
     r.points = points;
+    r.bytes = bytes;
     ctx->timing_open = false;
 }
 
@@ -291,7 +292,7 @@ int fx_ctx_timing_begin(fx_ctx *c, const char *kernel) {
     return FX_OK;
 }
 
-int fx_ctx_timing_end_records(fx_ctx *c, double *ms, double *points, size_t max, size_t *count) {
+int fx_ctx_timing_end_records(fx_ctx *c, double *ms, double *points, double *bytes, size_t max, size_t *count) {
     if (!c || !ms || !points || !count) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     FX_CUDA(cudaStreamSynchronize(c->stream));
     size_t k = 0;
@@ -301,6 +302,7 @@ int fx_ctx_timing_end_records(fx_ctx *c, double *ms, double *points, size_t max,
         FX_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
         ms[k] = t;
         points[k] = r.points;
+        if (bytes) bytes[k] = r.bytes;
         k++;
     }
     *count = k;

@@ -520,25 +520,42 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
         FX_TRY((launch_vdown<T, TB>(ctx, L.rows, L.cols, b0, (T *)mg->tmp0->ptr, (T *)C.rhs->ptr, C.cols,
                                     vop(0), skip)));
     }
-    for (int l = 1; l < nl - 1; l++) {
+    // levels top .. nl-1 run in the one-block tail kernel: top is the finest level >= 1 whose
+    // tail working set fits in shared memory
+    int top = nl - 1;
+    size_t tail_smem = 2 * mg->lv[nl - 1].rows * mg->lv[nl - 1].cols * sizeof(T);
+    for (int t = nl - 2; t >= 1 && nl - t <= kTailMaxLevels; t--) {
+        size_t n[kTailMaxLevels];
+        for (int l = t; l < nl; l++) n[l - t] = mg->lv[l].rows * mg->lv[l].cols;
+        const size_t bytes = tail_smem_bytes(n, nl - t, sizeof(T));
+        if (bytes > kTailSmemMax || n[0] > (size_t)tail_kt<T>() * kTailThreads) break;
+        top = t;
+        tail_smem = bytes;
+    }
+    if (nl - top > kTailMaxLevels || tail_smem > kTailSmemMax ||
+        (top == nl - 1 ? mg->lv[top].rows * mg->lv[top].cols > 4096
+                       : mg->lv[top].rows * mg->lv[top].cols > (size_t)tail_kt<T>() * kTailThreads))
+        return fail(FX_ERR_UNSUPPORTED, "coarsest level too large for the one-block solve");
+    for (int l = 1; l < top; l++) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
         FX_TRY((launch_vdown<T, T>(ctx, L.rows, L.cols, (const T *)L.rhs->ptr, (T *)L.tmp->ptr, (T *)C.rhs->ptr,
                                    C.cols, vop(l), skip)));
     }
     {
-        const MgLevel &L = mg->lv[nl - 1];
-        const size_t n = L.rows * L.cols;
-        const size_t smem = 2 * n * sizeof(T);
-        if (!coarse_fits(n, sizeof(T)))
-            return fail(FX_ERR_UNSUPPORTED, "coarsest level too large for the one-block solve");
-        timing_pre(ctx, "mg_coarse_solve");
-        k_coarse_solve<T><<<1, coarse_threads(n), smem, ctx->stream>>>((T *)L.u->ptr, (const T *)L.rhs->ptr, (int)L.rows,
-                                                          (int)L.cols, make_a5<T>(L.a5), (T)(mg->omega / L.a5[0]),
-                                                          (int)mg->coarse_sweeps, true, skip);
-        timing_post(ctx, (double)n);
-        FX_TRY(check_launch(ctx, "mg_coarse_solve"));
+        TailArgs<T> A{};
+        A.nlev = nl - top;
+        for (int k = 0; k < A.nlev; k++) {
+            A.rows[k] = (int)mg->lv[top + k].rows;
+            A.cols[k] = (int)mg->lv[top + k].cols;
+            A.op[k] = vop(top + k);
+        }
+        const MgLevel &T0 = mg->lv[top];
+        A.b_top = (const T *)T0.rhs->ptr;
+        A.u_top = (T *)T0.u->ptr;
+        A.coarse_sweeps = (int)mg->coarse_sweeps;
+        FX_TRY(launch_vtail<T>(ctx, A, tail_smem, skip));
     }
-    for (int l = nl - 2; l >= 1; l--) {
+    for (int l = top - 1; l >= 1; l--) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
         FX_TRY((launch_vup<T, T, T, false>(ctx, L.rows, L.cols, (const T *)L.tmp->ptr, (const T *)C.u->ptr, C.cols,
                                            (const T *)L.rhs->ptr, (T *)L.u->ptr, vop(l), NoFin{}, skip)));

@@ -120,9 +120,11 @@ unsigned long long fx_ctx_launch_count(fx_ctx *ctx);
 int fx_ctx_timing_begin(fx_ctx *ctx, const char *kernel);
 int fx_ctx_timing_end(fx_ctx *ctx, double *total_ms, unsigned long long *launches,
                       double *total_points);
-/* Like fx_ctx_timing_end, but also returns up to `max` individual launches (device ms and
- * grid points each, in launch order) through ms[] / points[]; *count is the number written. */
-int fx_ctx_timing_end_records(fx_ctx *ctx, double *ms, double *points, size_t max, size_t *count);
+/* Like fx_ctx_timing_end, but also returns up to `max` individual launches in launch order:
+ * device ms, grid points, and the launch's algorithmic DRAM bytes (0 where the launcher does not
+ * state them; `bytes` may be NULL) through ms[] / points[] / bytes[]; *count = number written. */
+int fx_ctx_timing_end_records(fx_ctx *ctx, double *ms, double *points, double *bytes, size_t max,
+                              size_t *count);
 
 /* ------------------------------------------------------------------ */
 /* Memory (Backend::allocate / upload_f64 / upload_f32, backend.rs:49-77;
