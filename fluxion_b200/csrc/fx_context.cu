@@ -152,7 +152,9 @@ MarchGeom march_geom(size_t rows, size_t cols, int bx, int d, int capacity) {
     G.nbands = (int)((cols - 1 + bx - 1) / bx);
     if (G.nbands < 1) G.nbands = 1;
     // Split the rows into chunks so that bands x chunks fills whole waves of resident CTAs
-    // (one work item per CTA, equal work per item); chunks stay at least 4*d rows long.
+    // (one work item per CTA, equal work per item).  A chunk is at least one FIFO depth d
+    // long: on small grids, where a launch is bound by the rows each CTA marches in
+    // sequence, short chunks cut that latency at the cost of a few recomputed halo rows.
     const long R = (long)rows, B = G.nbands;
     long best_chunks = 1;
     double best_eff = -1.0;
@@ -160,7 +162,7 @@ MarchGeom march_geom(size_t rows, size_t cols, int bx, int d, int capacity) {
         long chunks = (long)w * capacity / B;
         if (chunks < 1) chunks = 1;
         long cr = (R + chunks - 1) / chunks;
-        if (cr < 4 * d) cr = 4 * d;
+        if (cr < d) cr = d;
         cr = ((cr + d - 1) / d) * d;
         chunks = (R + cr - 1) / cr;
         const long nb = chunks * B;
@@ -172,7 +174,7 @@ MarchGeom march_geom(size_t rows, size_t cols, int bx, int d, int capacity) {
         }
     }
     long cr = (R + best_chunks - 1) / best_chunks;
-    if (cr < 4 * d) cr = 4 * d;
+    if (cr < d) cr = d;
     cr = ((cr + d - 1) / d) * d;
     G.chunk_rows = (int)cr;
     G.nblocks = (int)(((R + cr - 1) / cr) * B);

@@ -88,11 +88,14 @@ __global__ void __launch_bounds__(kBandThreads, 2)
     S.init(t, c0, cols);
     const int r_need = r1 + 3;  // last rhs row any stage reads
 
+    // zero-initialised predicated loads: nothing consumes the value until put_b
     auto ld_b = [&](int r, TB (&v)[CPT]) {
         const bool rin = r >= 0 && r < rows && r <= r_need;
-        const size_t ro = (size_t)(rin ? r : 0) * cols;
 #pragma unroll
-        for (int s = 0; s < CPT; s++) v[s] = (rin && S.ingrid[s]) ? b[ro + S.col[s]] : (TB)0;
+        for (int s = 0; s < CPT; s++) {
+            v[s] = (TB)0;
+            if (rin && S.ingrid[s]) v[s] = b[(size_t)r * cols + S.col[s]];
+        }
     };
     // b row r (as T) and x1 = w b (0 on the ring) into the rings; slot r & 3 (two's complement)
     auto put_b = [&](int r, const TB (&v)[CPT]) {
@@ -221,48 +224,89 @@ __device__ __forceinline__ T bil_interp(const T *__restrict__ e, int ccols, int 
     return ro ? (co ? v_oo : v_oe) : (co ? v_eo : e00);
 }
 
+// The same interpolation from two coarse rows held in shared memory: e0 = coarse row r >> 1,
+// e1 = the row below it, k = coarse column c >> 1 relative to the rows' first column.
+template <typename T>
+__device__ __forceinline__ T bil_rows(const T *e0, const T *e1, bool ro, bool co, int k) {
+    const T e00 = e0[k];
+    const T e01 = co ? e0[k + 1] : (T)0;
+    const T e10 = ro ? e1[k] : (T)0;
+    const T e11 = (ro && co) ? e1[k + 1] : (T)0;
+    const T v_oe = (T)0.5 * (e00 + e10);
+    const T v_eo = (T)0.5 * (e00 + e01);
+    const T v_oo = (T)0.25 * ((e00 + e10) + (e01 + e11));
+    return ro ? (co ? v_oo : v_oe) : (co ? v_eo : e00);
+}
+
+// Every global load of k_vup is a raw value issued two row pairs ahead (x2 and b of the fine
+// rows, one coarse row of e per pair); nothing waits on them until the rows enter the rings.
+// Coarse rows of e live in a 4-row shared ring: step i (rows i+1 = 2m, i+2 = 2m+1 arrive)
+// interpolates from coarse rows m, m+1 and stores row m+2 for the next step.
 template <typename T, typename TB, typename TZ, int CPT, bool RZ, typename Fin>
 __global__ void __launch_bounds__(kBandThreads, 2)
     k_vup(MarchGeom G, const T *__restrict__ x2g, const T *__restrict__ e, int ccols, const TB *__restrict__ b,
           TZ *__restrict__ z, VOp<T> op, Fin fin, RedArgs<1> ra, const int *skip) {
     if (skip && *(volatile const int *)skip) return;
     constexpr int H = 2, DP = 2, BX = kBlock * CPT, W = BX + 2 * H;
-    __shared__ T sf[8][W], sb[8][W], sx3[4][W];
+    constexpr int WC = BX / 2 + 4;  // coarse columns a band's rows interpolate from (+1 spare)
+    __shared__ T sf[8][W], sb[8][W], sx3[4][W], ec[4][WC];
     const int t = threadIdx.x;
     const int band = blockIdx.x % G.nbands, chunk = blockIdx.x / G.nbands;
     const int c0 = 1 + band * BX;
-    const int r0 = chunk * G.chunk_rows, r1 = min(r0 + G.chunk_rows, G.rows);
-    const int rows = G.rows, cols = G.cols;
+    const int r0 = chunk * G.chunk_rows, r1 = min(r0 + G.chunk_rows, G.rows);  // r0 even
+    const int rows = G.rows, cols = G.cols, crows = (rows - 1) / 2 + 1;
     const bool is_band = t < kBlock;
     const bool is_halo = !is_band && (t - kBlock) < 2 * H;
     VSlots<CPT, H> S;
     S.init(t, c0, cols);
     CSum acc[1] = {CSum{0.0, 0.0}};
     const int r_need = r1 + 2;  // last input row any stage reads
+    // coarse column of ring index 0: (c0 - H) >> 1 (c0 - H is odd); thread t loads index t
+    const int cbase = (c0 - H - 1) / 2;
+    const int ccol = cbase + t;
+    const bool cload = t < WC - 1 && ccol >= 0 && ccol < ccols;
 
-    // F0 = x2 + bilinear(e) at interior points, 0 on the ring; b alongside (kept in its own
-    // precision in registers for the final inner product)
-    auto ld = [&](int r, T (&f)[CPT], TB (&bv)[CPT]) {
+    auto ld = [&](int r, T (&xv)[CPT], TB (&bv)[CPT]) {
         const bool irow = r >= 1 && r <= rows - 2 && r <= r_need;
-        const size_t ro = (size_t)(irow ? r : 0) * cols;
 #pragma unroll
         for (int s = 0; s < CPT; s++) {
-            const bool in = irow && S.inner[s];
-            f[s] = in ? x2g[ro + S.col[s]] + bil_interp(e, ccols, r, S.col[s]) : (T)0;
-            bv[s] = in ? b[ro + S.col[s]] : (TB)0;
+            xv[s] = (T)0;
+            bv[s] = (TB)0;
+            if (irow && S.inner[s]) {
+                const size_t o = (size_t)r * cols + S.col[s];
+                xv[s] = x2g[o];
+                bv[s] = b[o];
+            }
         }
     };
-    auto put = [&](int r, const T (&f)[CPT], const TB (&bv)[CPT]) {
+    auto ld_coarse = [&](int m) -> T {
+        T v = (T)0;
+        if (cload && m >= 0 && m < crows) v = e[(size_t)m * ccols + ccol];
+        return v;
+    };
+    auto put_coarse = [&](int m, T v) {
+        if (t < WC - 1) ec[m & 3][t] = v;
+    };
+    // F0 = x2 + bilinear(e) at interior points, 0 on the ring; b alongside (kept in its own
+    // precision in registers for the final inner product)
+    auto put = [&](int r, const T (&xv)[CPT], const TB (&bv)[CPT]) {
+        const bool irow = r >= 1 && r <= rows - 2;
+        const bool ro = r & 1;
+        const T *e0 = ec[(r >> 1) & 3], *e1 = ec[((r >> 1) + 1) & 3];
         T *rf = sf[r & 7];
         T *rb = sb[r & 7];
         if (is_band) {
 #pragma unroll
             for (int s = 0; s < CPT; s++) {
-                rf[S.j[s]] = f[s];
+                const int c = S.col[s];
+                const T f = xv[s] + bil_rows(e0, e1, ro, c & 1, (c >> 1) - cbase);
+                rf[S.j[s]] = (irow && S.inner[s]) ? f : (T)0;
                 rb[S.j[s]] = (T)bv[s];
             }
         } else if (is_halo) {
-            rf[S.j[0]] = f[0];
+            const int c = S.col[0];
+            const T f = xv[0] + bil_rows(e0, e1, ro, c & 1, (c >> 1) - cbase);
+            rf[S.j[0]] = (irow && S.inner[0]) ? f : (T)0;
             rb[S.j[0]] = (T)bv[0];
         }
     };
@@ -296,41 +340,53 @@ __global__ void __launch_bounds__(kBandThreads, 2)
         }
     };
 
-    // prologue: rows r0-2, r0-1 to the rings; FIFO pairs from (r0, r0+1), the pair the first
-    // step (i = r0-1) consumes; `bp` keeps the rhs of the pair being finished
-    T ff[DP][2][CPT];
+    // prologue: coarse rows m0-1 .. m0+1 (m0 = r0 / 2) to the ring; fine rows r0-2, r0-1 to the
+    // rings; FIFO pairs from (r0, r0+1), the pair the first step (i = r0-1) consumes, with
+    // coarse rows from m0+2; `bp` keeps the rhs of the pair being finished
+    const int m0 = r0 >> 1;
+    T fx[DP][2][CPT];
     TB fb[DP][2][CPT];
+    T fe[DP];
     TB bp[2][CPT];
     {
-        T f[CPT];
-        ld(r0 - 2, f, bp[0]);
-        put(r0 - 2, f, bp[0]);
-        ld(r0 - 1, f, bp[1]);
-        put(r0 - 1, f, bp[1]);
-    }
+        const T c_a = ld_coarse(m0 - 1), c_b = ld_coarse(m0), c_c = ld_coarse(m0 + 1);
+        T xv[2][CPT];
+        ld(r0 - 2, xv[0], bp[0]);
+        ld(r0 - 1, xv[1], bp[1]);
 #pragma unroll
-    for (int p = 0; p < DP; p++) {
-        ld(r0 + 2 * p, ff[p][0], fb[p][0]);
-        ld(r0 + 1 + 2 * p, ff[p][1], fb[p][1]);
+        for (int p = 0; p < DP; p++) {
+            ld(r0 + 2 * p, fx[p][0], fb[p][0]);
+            ld(r0 + 1 + 2 * p, fx[p][1], fb[p][1]);
+            fe[p] = ld_coarse(m0 + 2 + p);
+        }
+        put_coarse(m0 - 1, c_a);
+        put_coarse(m0, c_b);
+        put_coarse(m0 + 1, c_c);
+        __syncthreads();
+        put(r0 - 2, xv[0], bp[0]);
+        put(r0 - 1, xv[1], bp[1]);
     }
 
-    // step i: F0 rows i+1, i+2 arrive; x3 rows i, i+1; x4 rows i-1, i -> z
+    // step i: coarse row m+2 stored; F0 rows i+1, i+2 arrive; x3 rows i, i+1; x4 rows i-1, i -> z
     const int i_first = r0 - 1, i_last = r1;
     for (int ib = i_first; ib <= i_last; ib += 2 * DP) {
 #pragma unroll
         for (int p = 0; p < DP; p++) {
             const int i = ib + 2 * p;
             if (i > i_last) break;
-            put(i + 1, ff[p][0], fb[p][0]);
-            put(i + 2, ff[p][1], fb[p][1]);
+            const int m = (i + 1) >> 1;
+            put_coarse(m + 2, fe[p]);
+            put(i + 1, fx[p][0], fb[p][0]);
+            put(i + 2, fx[p][1], fb[p][1]);
             TB bnew[2][CPT];
 #pragma unroll
             for (int s = 0; s < CPT; s++) {
                 bnew[0][s] = fb[p][0][s];
                 bnew[1][s] = fb[p][1][s];
             }
-            ld(i + 1 + 2 * DP, ff[p][0], fb[p][0]);
-            ld(i + 2 + 2 * DP, ff[p][1], fb[p][1]);
+            ld(i + 1 + 2 * DP, fx[p][0], fb[p][0]);
+            ld(i + 2 + 2 * DP, fx[p][1], fb[p][1]);
+            fe[p] = ld_coarse(m + 2 + DP);
             __syncthreads();
             x3_row(i);
             x3_row(i + 1);
