@@ -12,7 +12,7 @@
 #include <vector>
 
 #include "fx_points.cuh"
-#include "fx_vcycle.cuh"
+#include "fx_wcycle.cuh"
 
 using namespace fx;
 
@@ -517,7 +517,7 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
     // down: level 0 reads b0 (TB), the others their rhs (T); x2 of level 0 lives in tmp0
     {
         const MgLevel &L = mg->lv[0], &C = mg->lv[1];
-        FX_TRY((launch_vdown<T, TB>(ctx, L.rows, L.cols, b0, (T *)mg->tmp0->ptr, (T *)C.rhs->ptr, C.cols,
+        FX_TRY((launch_wdown<T, TB>(ctx, L.rows, L.cols, b0, (T *)mg->tmp0->ptr, (T *)C.rhs->ptr, C.cols,
                                     vop(0), skip)));
     }
     // levels top .. nl-1 run in the one-block tail kernel: top is the finest level >= 1 whose
@@ -538,7 +538,7 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
         return fail(FX_ERR_UNSUPPORTED, "coarsest level too large for the one-block solve");
     for (int l = 1; l < top; l++) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
-        FX_TRY((launch_vdown<T, T>(ctx, L.rows, L.cols, (const T *)L.rhs->ptr, (T *)L.tmp->ptr, (T *)C.rhs->ptr,
+        FX_TRY((launch_wdown<T, T>(ctx, L.rows, L.cols, (const T *)L.rhs->ptr, (T *)L.tmp->ptr, (T *)C.rhs->ptr,
                                    C.cols, vop(l), skip)));
     }
     {
@@ -557,11 +557,11 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
     }
     for (int l = top - 1; l >= 1; l--) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
-        FX_TRY((launch_vup<T, T, T, false>(ctx, L.rows, L.cols, (const T *)L.tmp->ptr, (const T *)C.u->ptr, C.cols,
+        FX_TRY((launch_wup<T, T, T, false>(ctx, L.rows, L.cols, (const T *)L.tmp->ptr, (const T *)C.u->ptr, C.cols,
                                            (const T *)L.rhs->ptr, (T *)L.u->ptr, vop(l), NoFin{}, skip)));
     }
     const MgLevel &L = mg->lv[0], &C = mg->lv[1];
-    return launch_vup<T, TB, TZ, RZ>(ctx, L.rows, L.cols, (const T *)mg->tmp0->ptr, (const T *)C.u->ptr, C.cols, b0,
+    return launch_wup<T, TB, TZ, RZ>(ctx, L.rows, L.cols, (const T *)mg->tmp0->ptr, (const T *)C.u->ptr, C.cols, b0,
                                      z0, vop(0), fin, skip);
 }
 

@@ -726,10 +726,11 @@ int launch_vtail(fx_ctx *ctx, const TailArgs<T> &A, size_t smem, const int *skip
     return check_launch(ctx, "mg_tail");
 }
 
+// blocks of `kernel` (of `threads` threads) resident on the whole GPU at once
 template <typename K>
-int band_capacity(fx_ctx *ctx, K kernel, int &cache) {
+int band_capacity(fx_ctx *ctx, K kernel, int &cache, int threads = kBandThreads) {
     if (!cache) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cache, kernel, kBandThreads, 0) != cudaSuccess || cache < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cache, kernel, threads, 0) != cudaSuccess || cache < 1)
             cache = 1;
     }
     return cache * ctx->num_sms;
