@@ -16,6 +16,8 @@
 // residual / restriction / prolongation kernels), so the cycle stays bitwise equal.
 #pragma once
 
+#include <type_traits>
+
 #include "fx_vcycle.cuh"
 
 namespace fx {
@@ -35,7 +37,7 @@ inline StripGeom strip_geom(size_t rows, size_t cols, int useful, long capacity)
     StripGeom G;
     G.rows = (int)rows;
     G.cols = (int)cols;
-    G.nstrips = (int)((cols - 2 + useful - 1) / useful);
+    G.nstrips = (int)((cols - 1 + useful - 1) / useful);  // own ranges tile [0, cols - 1)
     if (G.nstrips < 1) G.nstrips = 1;
     // one wave of resident warps; chunks of at least 6 rows (an unrolled step)
     const long target = capacity;
@@ -60,80 +62,124 @@ __device__ __forceinline__ T op5v(const A5<T> &a, T c, T n, T s, T w, T e) {
     return fx_fma(a.c, c, fx_fma(a.n, n, fx_fma(a.s, s, fx_fma(a.w, w, a.e * e))));
 }
 
+// Two adjacent columns per lane: lane l of a strip holds columns ca = sb + 2l (even) and
+// cb = ca + 1, so one shuffle per stage gives both points their outer neighbour, the column
+// parity of every register is fixed, and a strip spans 64 columns.  A step whose rows all lie
+// inside the chunk's interior takes a path without row tests (FAST); the first and last few
+// steps of a chunk test every row.
+
+template <bool B>
+using fast_t = std::integral_constant<bool, B>;
+
 // ---------------------------------------------------------------- down
+
+constexpr int kDownOwn = 56;  // own columns per strip: lanes 2..29 (x1 -> x2 -> res -> FW: halo 4)
 
 template <typename T, typename TB>
 __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const TB *__restrict__ b, T *__restrict__ x2g,
                                                              T *__restrict__ coarse, int ccols, VOp<T> op,
                                                              const int *skip) {
     if (skip && *(volatile const int *)skip) return;
-    constexpr int H = 3, U = 32 - 2 * H, D = kStripFifo;
+    constexpr int D = kStripFifo;
     const int lane = threadIdx.x & 31;
     const int item = blockIdx.x * kStripWarps + (threadIdx.x >> 5);
     if (item >= G.nitems) return;  // whole warps
     const int strip = item % G.nstrips, chunk = item / G.nstrips;
     const int rows = G.rows, cols = G.cols;
-    const int c = 1 + strip * U - H + lane;
-    const bool cin = c >= 1 && c <= cols - 2;
-    const bool own = lane >= H && lane < H + U && cin;
-    const bool cpt = own && !(c & 1) && c >= 2 && c <= cols - 3;  // a coarse point's column
+    const int ca = strip * kDownOwn - 4 + 2 * lane, cb = ca + 1;
+    const bool ina = ca >= 1 && ca <= cols - 2, inb = cb >= 1 && cb <= cols - 2;
+    const bool own = lane >= 2 && lane < 30;
+    const bool sta = own && ina, stb = own && inb;
+    const bool cpt = own && ca >= 2 && ca <= cols - 3;  // coarse point (fr, ca) for even fr
     const int r0 = chunk * G.chunk_rows, r1 = min(r0 + G.chunk_rows, rows);  // r0 even
-    // step q: b row q arrives; x1 row q; x2 row q-1; residual row q-2; restriction of fine row
-    // q-3 (even q-3 only)
+    // step q: b row q arrives; x1 row q; x2 row q-1; residual row q-2; full weighting of fine
+    // row q-3 (even q-3 only)
     const int q_first = r0 - 3, q_last = r1 + 2;
+    // steps with every row test true: q-3 >= max(r0, 2), q + D <= min(rows - 2, q_last)
+    const int q_lo = max(r0, 2) + 3, q_hi = min(rows - 2, q_last) - D;
 
-    TB fb[D];
-    auto load = [&](int q, TB &v) {
-        v = (TB)0;
-        if (q >= 1 && q <= rows - 2 && q <= q_last && cin) v = b[(size_t)q * cols + c];
+    TB fa[D], fb[D];
+    auto row_in = [&](int r) { return r >= 1 && r <= rows - 2; };
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+        const int q = q_first + k;
+        fa[k] = (TB)0;
+        fb[k] = (TB)0;
+        if (row_in(q) && q <= q_last) {
+            if (ina) fa[k] = b[(size_t)q * cols + ca];
+            if (inb) fb[k] = b[(size_t)q * cols + cb];
+        }
+    }
+
+    T bwa[3] = {}, bwb[3] = {}, x1a[3] = {}, x1b[3] = {}, x2a[3] = {}, x2b[3] = {};
+    T rsa[3] = {}, rsb[3] = {}, rwa[3] = {};
+    auto step = [&](int k, int q, auto fast) {
+        constexpr bool F = decltype(fast)::value;
+        const int s0 = k % 3, s1 = (k + 2) % 3, s2 = (k + 1) % 3;  // slots of rows q, q-1, q-2
+        const size_t rq = (size_t)q * cols;
+        // row q: rhs and x1 = w b (0 on the ring); refill with row q + D
+        {
+            const T ba = (T)fa[k], bb = (T)fb[k];
+            const bool rin = F || row_in(q);
+            bwa[s0] = ba;
+            bwb[s0] = bb;
+            x1a[s0] = (rin && ina) ? fx_fma(op.wd, ba, (T)0) : (T)0;
+            x1b[s0] = (rin && inb) ? fx_fma(op.wd, bb, (T)0) : (T)0;
+            const int qn = q + D;
+            if (F || (row_in(qn) && qn <= q_last)) {
+                const size_t o = rq + (size_t)D * cols;
+                if (ina) fa[k] = b[o + ca];
+                if (inb) fb[k] = b[o + cb];
+            }
+        }
+        // row q-1: x2
+        {
+            const T xa = x1a[s1], xb = x1b[s1];
+            const T wa = shfl_w(xb), eb = shfl_e(xa);
+            const bool rin = F || row_in(q - 1);
+            T va = (T)0, vb = (T)0;
+            if (rin && ina) va = fx_fma(op.wd, bwa[s1] - op5v(op.a, xa, x1a[s2], x1a[s0], wa, xb), xa);
+            if (rin && inb) vb = fx_fma(op.wd, bwb[s1] - op5v(op.a, xb, x1b[s2], x1b[s0], xa, eb), xb);
+            x2a[s1] = va;
+            x2b[s1] = vb;
+            if (F || (rin && q - 1 >= r0 && q - 1 < r1)) {
+                T *row = x2g + rq - cols;
+                if (sta) row[ca] = va;
+                if (stb) row[cb] = vb;
+            }
+        }
+        // row q-2: residual, and the residual west of ca for the restriction
+        {
+            const T xa = x2a[s2], xb = x2b[s2];
+            const T wa = shfl_w(xb), eb = shfl_e(xa);
+            const bool rin = F || row_in(q - 2);
+            T va = (T)0, vb = (T)0;
+            if (rin && ina) va = bwa[s2] - op5v(op.a, xa, x2a[s0], x2a[s1], wa, xb);
+            if (rin && inb) vb = bwb[s2] - op5v(op.a, xb, x2b[s0], x2b[s1], xa, eb);
+            rsa[s2] = va;
+            rsb[s2] = vb;
+            rwa[s2] = shfl_w(vb);
+        }
+        // fine row q-3 (residual rows q-4 / q-3 / q-2 in slots s1 / s0 / s2): full weighting
+        // onto coarse row (q-3) / 2 at coarse column ca / 2
+        if (!(k & 1)) {  // q - 3 even (r0 even, so q_first odd)
+            const int fr = q - 3;
+            if (cpt && (F || (fr >= r0 && fr < r1 && fr >= 2 && fr <= rows - 3))) {
+                const T e = (rsa[s1] + rsa[s2]) + (rwa[s0] + rsb[s0]);
+                const T d = (rwa[s1] + rsb[s1]) + (rwa[s2] + rsb[s2]);
+                coarse[(size_t)(fr >> 1) * ccols + (ca >> 1)] = ((T)4 * rsa[s0] + ((T)2 * e + d)) * (T)0.0625;
+            }
+        }
     };
-#pragma unroll
-    for (int k = 0; k < D; k++) load(q_first + k, fb[k]);
-
-    T bw[3] = {}, x1[3] = {}, x2[3] = {}, rs[3] = {}, rw[3] = {}, re[3] = {};
     for (int qb = q_first; qb <= q_last; qb += D) {
+        if (qb >= q_lo && qb + D - 1 <= q_hi) {
 #pragma unroll
-        for (int k = 0; k < D; k++) {
-            const int q = qb + k;
-            if (q > q_last) break;  // uniform over the warp
-            const int s0 = k % 3, s1 = (k + 2) % 3, s2 = (k + 1) % 3;  // slots of rows q, q-1, q-2
-            // row q: rhs and x1 = w b (0 on the ring)
-            const T bq = (T)fb[k];
-            load(q + D, fb[k]);
-            const bool in0 = q >= 1 && q <= rows - 2 && cin;
-            bw[s0] = bq;
-            x1[s0] = in0 ? fx_fma(op.wd, bq, (T)0) : (T)0;
-            // row q-1: x2
-            {
-                const int r = q - 1;
-                const T xc = x1[s1];
-                const T xw = shfl_w(xc), xe = shfl_e(xc);
-                T v = (T)0;
-                if (r >= 1 && r <= rows - 2 && cin)
-                    v = fx_fma(op.wd, bw[s1] - op5v(op.a, xc, x1[s2], x1[s0], xw, xe), xc);
-                x2[s1] = v;
-                if (own && r >= r0 && r < r1 && r >= 1 && r <= rows - 2) x2g[(size_t)r * cols + c] = v;
-            }
-            // row q-2: residual (and its west / east neighbours for the restriction)
-            {
-                const int r = q - 2;
-                const T xc = x2[s2];
-                const T xw = shfl_w(xc), xe = shfl_e(xc);
-                T v = (T)0;
-                if (r >= 1 && r <= rows - 2 && cin) v = bw[s2] - op5v(op.a, xc, x2[s0], x2[s1], xw, xe);
-                rs[s2] = v;
-                rw[s2] = shfl_w(v);
-                re[s2] = shfl_e(v);
-            }
-            // fine row q-3 (slot s0 of the residual window, rows q-4 / q-2 in s1 / s2): full
-            // weighting onto coarse row (q-3) / 2
-            if (!(k & 1)) {  // q - 3 even (r0 even, so q_first odd)
-                const int fr = q - 3;
-                if (cpt && fr >= r0 && fr < r1 && fr >= 2 && fr <= rows - 3) {
-                    const T e = (rs[s1] + rs[s2]) + (rw[s0] + re[s0]);
-                    const T d = (rw[s1] + re[s1]) + (rw[s2] + re[s2]);
-                    coarse[(size_t)(fr >> 1) * ccols + (c >> 1)] = ((T)4 * rs[s0] + ((T)2 * e + d)) * (T)0.0625;
-                }
+            for (int k = 0; k < D; k++) step(k, qb + k, fast_t<true>{});
+        } else {
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                if (qb + k > q_last) break;  // uniform over the warp
+                step(k, qb + k, fast_t<false>{});
             }
         }
     }
@@ -141,110 +187,159 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
 
 // ---------------------------------------------------------------- up
 
+constexpr int kUpOwn = 60;  // own columns per strip: lanes 1..30 (f -> x3 -> z: halo 2)
+
 template <typename T, typename TB, typename TZ, bool RZ, typename Fin>
 __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *__restrict__ x2g,
                                                            const T *__restrict__ e, int ccols,
                                                            const TB *__restrict__ b, TZ *__restrict__ z, VOp<T> op,
                                                            Fin fin, RedArgs<1> ra, const int *skip) {
     if (skip && *(volatile const int *)skip) return;
-    constexpr int H = 2, U = 32 - 2 * H, D = kStripFifo;
+    constexpr int D = kStripFifo;
     const int lane = threadIdx.x & 31;
     const int item = blockIdx.x * kStripWarps + (threadIdx.x >> 5);
-    const bool live = item < G.nitems;  // idle warps still join the block reduction
     CSum acc[1] = {CSum{0.0, 0.0}};
-    if (live) {
+    if (item < G.nitems) {  // idle warps still join the block reduction
         const int strip = item % G.nstrips, chunk = item / G.nstrips;
         const int rows = G.rows, cols = G.cols, crows = (rows - 1) / 2 + 1;
-        const int c = 1 + strip * U - H + lane;
-        const bool cin = c >= 1 && c <= cols - 2;
-        const bool own = lane >= H && lane < H + U && cin;
-        const bool co = c & 1;
-        const int kc = c >> 1;  // coarse column (c >= 1 wherever it is used)
+        const int ca = strip * kUpOwn - 2 + 2 * lane, cb = ca + 1;
+        const bool ina = ca >= 1 && ca <= cols - 2, inb = cb >= 1 && cb <= cols - 2;
+        const bool own = lane >= 1 && lane < 31;
+        const bool sta = own && ina, stb = own && inb;
+        const int kc = ca >> 1;  // coarse column of ca; cb interpolates between kc and kc + 1
+        const bool ce0 = kc >= 0 && kc < ccols && (ina || inb), ce1 = kc + 1 < ccols && inb;
         const int r0 = chunk * G.chunk_rows, r1 = min(r0 + G.chunk_rows, rows);  // r0 even
         // step q: F0 row q = x2 + P e; x3 row q-1; z row q-2
         const int q_first = r0 - 2, q_last = r1 + 1;  // q_first even
+        // steps with every row test true: q-2 >= max(r0, 1), q + D <= min(rows - 2, q_last)
+        const int q_lo = max(r0, 1) + 2, q_hi = min(rows - 2, q_last) - D;
+        const int m_last = (q_last >> 1) + 1;  // last coarse row any step reads
+        auto row_in = [&](int r) { return r >= 1 && r <= rows - 2; };
 
-        // FIFO per row: raw x2 and b; for even rows q = 2m also coarse row m+1 at columns kc,
-        // kc+1 (with row m, kept from the previous pair, the two rows rows 2m and 2m+1 need)
-        T fx[D], fe0[D / 2], fe1[D / 2];
-        TB fb[D];
-        auto load = [&](int q, T &xv, TB &bv) {
-            xv = (T)0;
-            bv = (TB)0;
-            if (q >= 1 && q <= rows - 2 && q <= q_last && cin) {
-                const size_t o = (size_t)q * cols + c;
-                xv = x2g[o];
-                bv = b[o];
+        // FIFO per fine row: raw x2 and b of both columns; per fine row pair (2m, 2m+1) the
+        // coarse row m+1 at columns kc, kc+1 (row m is kept from the previous pair)
+        T xa_[D], xb_[D], ea_[D / 2], eb_[D / 2];
+        TB ba_[D], bb_[D];
+        auto load_row = [&](int q, int k) {
+            xa_[k] = (T)0;
+            xb_[k] = (T)0;
+            ba_[k] = (TB)0;
+            bb_[k] = (TB)0;
+            if (row_in(q) && q <= q_last) {
+                const size_t o = (size_t)q * cols;
+                if (ina) {
+                    xa_[k] = x2g[o + ca];
+                    ba_[k] = b[o + ca];
+                }
+                if (inb) {
+                    xb_[k] = x2g[o + cb];
+                    bb_[k] = b[o + cb];
+                }
             }
         };
         auto load_coarse = [&](int m, T &v0, T &v1) {
             v0 = (T)0;
             v1 = (T)0;
-            if (m >= 0 && m < crows && m <= (q_last >> 1) + 1 && cin) {
+            if (m >= 0 && m < crows && m <= m_last) {
                 const size_t o = (size_t)m * ccols + kc;
-                v0 = e[o];
-                if (co) v1 = e[o + 1];
+                if (ce0) v0 = e[o];
+                if (ce1) v1 = e[o + 1];
             }
         };
-        T ec0, ec1;  // coarse row (q >> 1) for the current pair
-        load_coarse(q_first >> 1, ec0, ec1);
+        T c0a, c0b;  // coarse row q >> 1 of the current pair, columns kc, kc+1
+        load_coarse(q_first >> 1, c0a, c0b);
 #pragma unroll
         for (int k = 0; k < D; k++) {
-            load(q_first + k, fx[k], fb[k]);
-            if (!(k & 1)) load_coarse(((q_first + k) >> 1) + 1, fe0[k / 2], fe1[k / 2]);
+            load_row(q_first + k, k);
+            if (!(k & 1)) load_coarse(((q_first + k) >> 1) + 1, ea_[k / 2], eb_[k / 2]);
         }
 
-        T f[3] = {}, x3[3] = {};
-        TB bw[3] = {};
-        for (int qb = q_first; qb <= q_last; qb += D) {
-#pragma unroll
-            for (int k = 0; k < D; k++) {
-                const int q = qb + k;
-                if (q > q_last) break;
-                const int s0 = k % 3, s1 = (k + 2) % 3, s2 = (k + 1) % 3;  // rows q, q-1, q-2
-                // row q: f = x2 + bilinear(e)
-                {
-                    const bool ro = k & 1;  // q_first even
-                    const T n0 = fe0[k / 2], n1 = fe1[k / 2];  // coarse row (q >> 1) + 1
-                    const T e00 = ec0;
-                    const T e01 = co ? ec1 : (T)0;
-                    const T e10 = ro ? n0 : (T)0;
-                    const T e11 = (ro && co) ? n1 : (T)0;
-                    const T v_oe = (T)0.5 * (e00 + e10);
-                    const T v_eo = (T)0.5 * (e00 + e01);
-                    const T v_oo = (T)0.25 * ((e00 + e10) + (e01 + e11));
-                    const T pe = ro ? (co ? v_oo : v_oe) : (co ? v_eo : e00);
-                    const bool in0 = q >= 1 && q <= rows - 2 && cin;
-                    f[s0] = in0 ? fx[k] + pe : (T)0;
-                    bw[s0] = fb[k];
-                    if (ro) {  // the pair is done: its lower coarse row becomes the upper one
-                        ec0 = n0;
-                        ec1 = n1;
-                        load_coarse((q + D + 1) >> 1, fe0[k / 2], fe1[k / 2]);
+        T fa[3] = {}, fb[3] = {}, x3a[3] = {}, x3b[3] = {};
+        TB bwa[3] = {}, bwb[3] = {};
+        auto step = [&](int k, int q, auto fast) {
+            constexpr bool F = decltype(fast)::value;
+            const int s0 = k % 3, s1 = (k + 2) % 3, s2 = (k + 1) % 3;  // rows q, q-1, q-2
+            const size_t rq = (size_t)q * cols;
+            // row q: f = x2 + bilinear(e); the parities are fixed: ca even, cb odd, q odd <=> k odd
+            {
+                const bool ro = k & 1;
+                const T e00 = c0a, e01 = c0b;              // coarse row q >> 1
+                const T e10 = ea_[k / 2], e11 = eb_[k / 2];  // coarse row (q >> 1) + 1
+                T pa, pb;
+                if (ro) {
+                    pa = (T)0.5 * (e00 + e10);                    // v_oe
+                    pb = (T)0.25 * ((e00 + e10) + (e01 + e11));   // v_oo
+                } else {
+                    pa = e00;
+                    pb = (T)0.5 * (e00 + e01);                    // v_eo
+                }
+                const bool rin = F || row_in(q);
+                fa[s0] = (rin && ina) ? xa_[k] + pa : (T)0;
+                fb[s0] = (rin && inb) ? xb_[k] + pb : (T)0;
+                bwa[s0] = ba_[k];
+                bwb[s0] = bb_[k];
+                if (ro) {  // the pair is done: its lower coarse row becomes the upper one
+                    c0a = e10;
+                    c0b = e11;
+                    load_coarse((q + D + 1) >> 1, ea_[k / 2], eb_[k / 2]);
+                }
+                const int qn = q + D;
+                if (F) {
+                    const size_t o = rq + (size_t)D * cols;
+                    if (ina) {
+                        xa_[k] = x2g[o + ca];
+                        ba_[k] = b[o + ca];
                     }
-                    load(q + D, fx[k], fb[k]);
+                    if (inb) {
+                        xb_[k] = x2g[o + cb];
+                        bb_[k] = b[o + cb];
+                    }
+                } else {
+                    load_row(qn, k);
                 }
-                // row q-1: x3
-                {
-                    const int r = q - 1;
-                    const T fc = f[s1];
-                    const T fw = shfl_w(fc), fe = shfl_e(fc);
-                    T v = (T)0;
-                    if (r >= 1 && r <= rows - 2 && cin)
-                        v = fx_fma(op.wd, (T)bw[s1] - op5v(op.a, fc, f[s2], f[s0], fw, fe), fc);
-                    x3[s1] = v;
-                }
-                // row q-2: z
-                {
-                    const int r = q - 2;
-                    const T xc = x3[s2];
-                    const T xw = shfl_w(xc), xe = shfl_e(xc);
-                    if (own && r >= r0 && r < r1 && r >= 1 && r <= rows - 2) {
-                        const TB bv = bw[s2];
-                        const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xc, x3[s0], x3[s1], xw, xe), xc);
-                        z[(size_t)r * cols + c] = (TZ)v;
+            }
+            // row q-1: x3
+            {
+                const T fca = fa[s1], fcb = fb[s1];
+                const T wa = shfl_w(fcb), eb = shfl_e(fca);
+                const bool rin = F || row_in(q - 1);
+                T va = (T)0, vb = (T)0;
+                if (rin && ina) va = fx_fma(op.wd, (T)bwa[s1] - op5v(op.a, fca, fa[s2], fa[s0], wa, fcb), fca);
+                if (rin && inb) vb = fx_fma(op.wd, (T)bwb[s1] - op5v(op.a, fcb, fb[s2], fb[s0], fca, eb), fcb);
+                x3a[s1] = va;
+                x3b[s1] = vb;
+            }
+            // row q-2: z
+            {
+                const T xa = x3a[s2], xb = x3b[s2];
+                const T wa = shfl_w(xb), eb = shfl_e(xa);
+                const int r = q - 2;
+                if (F || (row_in(r) && r >= r0 && r < r1)) {
+                    TZ *row = z + rq - 2 * (size_t)cols;
+                    if (sta) {
+                        const TB bv = bwa[s2];
+                        const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xa, x3a[s0], x3a[s1], wa, xb), xa);
+                        row[ca] = (TZ)v;
                         if (RZ) csum_add_prod(acc[0], (double)bv, (double)(TZ)v);
                     }
+                    if (stb) {
+                        const TB bv = bwb[s2];
+                        const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xb, x3b[s0], x3b[s1], xa, eb), xb);
+                        row[cb] = (TZ)v;
+                        if (RZ) csum_add_prod(acc[0], (double)bv, (double)(TZ)v);
+                    }
+                }
+            }
+        };
+        for (int qb = q_first; qb <= q_last; qb += D) {
+            if (qb >= q_lo && qb + D - 1 <= q_hi) {
+#pragma unroll
+                for (int k = 0; k < D; k++) step(k, qb + k, fast_t<true>{});
+            } else {
+#pragma unroll
+                for (int k = 0; k < D; k++) {
+                    if (qb + k > q_last) break;
+                    step(k, qb + k, fast_t<false>{});
                 }
             }
         }
@@ -257,7 +352,7 @@ int launch_wdown(fx_ctx *ctx, size_t rows, size_t cols, const TB *b, T *x2, T *c
                  const VOp<T> &op, const int *skip) {
     static int occ = 0;
     const long cap = (long)band_capacity(ctx, k_wdown<T, TB>, occ, kStripWarps * 32) * kStripWarps;
-    const StripGeom G = strip_geom(rows, cols, 32 - 6, cap);
+    const StripGeom G = strip_geom(rows, cols, kDownOwn, cap);
     const int blocks = (G.nitems + kStripWarps - 1) / kStripWarps;
     timing_pre(ctx, "mg_down");
     k_wdown<T, TB><<<blocks, kStripWarps * 32, 0, ctx->stream>>>(G, b, x2, coarse, (int)ccols, op, skip);
@@ -272,7 +367,7 @@ int launch_wup(fx_ctx *ctx, size_t rows, size_t cols, const T *x2, const T *e, s
                const VOp<T> &op, Fin fin, const int *skip) {
     static int occ = 0;
     const long cap = (long)band_capacity(ctx, k_wup<T, TB, TZ, RZ, Fin>, occ, kStripWarps * 32) * kStripWarps;
-    const StripGeom G = strip_geom(rows, cols, 32 - 4, cap);
+    const StripGeom G = strip_geom(rows, cols, kUpOwn, cap);
     const int blocks = (G.nitems + kStripWarps - 1) / kStripWarps;
     if (RZ && blocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");
     timing_pre(ctx, "mg_up");
