@@ -37,6 +37,14 @@ sys.path.insert(0, ROOT)
 METRIC = "time to rel-resid 1e-10: learned/mixed vs plain (1 B200); stencil GB/s"
 N_INTERIOR = 4095
 SEED = 2024
+# V(2,2)-cycle parameters: weighted Jacobi 0.8, coarsen while the interior exceeds 7 x 7, 30
+# sweeps on the coarsest grid (the solve takes the same 9 iterations as with a 15 x 15
+# coarsest grid and 200 sweeps)
+OMEGA = 0.8
+COARSE_MAX = 7
+COARSE_SWEEPS = 30
+SOLVER = (f"V(2,2) full weighting / bilinear / weighted Jacobi {OMEGA}, coarsest interior <= "
+          f"{COARSE_MAX}^2 x {COARSE_SWEEPS} sweeps")
 
 # algorithmic bytes per grid point of each kernel (F64 sizes; F32 kernels carry a _f32 tag)
 BYTES_PER_POINT = {
@@ -70,30 +78,82 @@ def measured_peaks():
 # ------------------------------------------------------------------ clocks
 
 class ClockSampler:
-    def __init__(self, gpu_index: int):
-        self.gpu_index = gpu_index
-        self.proc = None
+    """SM clock and clock-event reasons sampled every ~2 ms through NVML while the timed region
+    runs (a solve takes a few ms, far below nvidia-smi's sampling interval); nvidia-smi is the
+    fallback where NVML cannot be loaded.  Reads settings only, changes none."""
+
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
+
+    def __init__(self, gpu_index: int, uuid: str = "", period_s: float = 0.002):
+        self.gpu_index = gpu_index  # CUDA ordinal; the NVML device is found by UUID when given
+        self.uuid = uuid
+        self.period = period_s
+        self.samples = []  # (sm_mhz, reasons bitmask)
+        self.max_mhz = None
         self.lines = []
+        self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            if self.uuid:
+                u = self.uuid if self.uuid.startswith("GPU-") else "GPU-" + self.uuid
+                self.h = pynvml.nvmlDeviceGetHandleByUUID(u)
+            else:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+        except Exception:
+            self.nvml = None
+            self._start_smi()
+        return self
+
+    def _poll(self):
+        nv = self.nvml
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                self.samples.append((mhz, int(get_reasons(self.h))))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def _start_smi(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
+            sel = self.uuid if self.uuid else str(self.gpu_index)
+            if self.uuid and not sel.startswith("GPU-"):
+                sel = "GPU-" + sel
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu_index)],
+                                          "-lms", "200", "-i", sel],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
-        return self
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml is not None:
+            self.t.join(timeout=1)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -102,7 +162,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], 0.0, set()
+        sm, reasons = [], set()
+        mx = self.max_mhz or 0.0
+        for mhz, bits in self.samples:
+            sm.append(mhz)
+            for nm, bit in self.REASONS.items():
+                if bits & bit:
+                    reasons.add(nm)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
@@ -117,36 +183,29 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": mx or None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 # ------------------------------------------------------------------ CPU oracle timing
 
-def cpu_oracle_estimate(n: int, f: np.ndarray, iters_needed: int):
-    """Time the oracle's MG-PCG (same algorithm, FP64) on all host threads on a bounded sample:
-    solves stopped after 1 and 3 iterations; extrapolate to `iters_needed` iterations."""
+def oracle_solve(n: int, f: np.ndarray):
+    """One full MG-PCG solve of the n^2 problem by the oracle (the same algorithm and parameters
+    as the GPU solve, FP64 throughout) on all host threads: (seconds, iterations, threads)."""
     from oracle import oracle as O
     from fluxion_b200.workloads import poisson_problem
 
     O.set_threads(os.cpu_count() or 1)
     P = poisson_problem(n)
     N = n + 2
-    mg = O.Multigrid(N, N, P.h, P.h, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=P.stencil.as_triples(),
-                     coarse_max=15, coarse_sweeps=200)
+    mg = O.Multigrid(N, N, P.h, P.h, 2, 2, OMEGA, mode=1, op_coeff=1.0, entries=P.stencil.as_triples(),
+                     coarse_max=COARSE_MAX, coarse_sweeps=COARSE_SWEEPS)
     tol = 1e-10 * float(np.linalg.norm(f))
-    times = {}
-    for k in (1, 3):
-        x = np.zeros(N * N)
-        t0 = time.perf_counter()
-        O.cg_solve(x, f, N, N, 1.0, P.stencil.as_triples(), tol, k, pc=mg)
-        times[k] = time.perf_counter() - t0
-    per_iter = (times[3] - times[1]) / 2.0
-    est = times[1] + per_iter * max(iters_needed - 1, 0)
-    return est, O.get_threads(), (f"MG-PCG solves of the {n}^2 problem stopped after 1 and 3 iterations "
-                                  f"({times[1]:.2f} s, {times[3]:.2f} s), extrapolated to the {iters_needed} "
-                                  f"iterations the solve needs")
+    x = np.zeros(N * N)
+    t0 = time.perf_counter()
+    iters, _, _ = O.cg_solve(x, f, N, N, 1.0, P.stencil.as_triples(), tol, 200, pc=mg)
+    return time.perf_counter() - t0, int(iters), O.get_threads()
 
 
 def run_reference(args):
@@ -154,49 +213,25 @@ def run_reference(args):
     if rank != 0:
         return 0
     from fluxion_b200.workloads import poisson_modes_rhs
-    from oracle import oracle as O
-    from fluxion_b200.workloads import poisson_problem
 
     n = args.n
-    f = poisson_modes_rhs(n, SEED)
-    O.set_threads(os.cpu_count() or 1)
-    P = poisson_problem(n)
     N = n + 2
-    mg = O.Multigrid(N, N, P.h, P.h, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=P.stencil.as_triples(),
-                     coarse_max=15, coarse_sweeps=200)
-    tol = 1e-10 * float(np.linalg.norm(f))
-    # iterations the CPU solve needs: one full solve on a 1023^2 copy of the problem class (the
-    # V-cycle makes the count grid-independent); each timed step is a bounded 1- and 3-iteration
-    # sample of the full-size solve.
-    nsm = 1023
-    Ps = poisson_problem(nsm)
-    fs = poisson_modes_rhs(nsm, SEED)
-    mgs = O.Multigrid(nsm + 2, nsm + 2, Ps.h, Ps.h, 2, 2, 0.8, mode=1, op_coeff=1.0,
-                      entries=Ps.stencil.as_triples(), coarse_max=15, coarse_sweeps=200)
-    xs = np.zeros((nsm + 2) ** 2)
-    iters, _, _ = O.cg_solve(xs, fs, nsm + 2, nsm + 2, 1.0, Ps.stencil.as_triples(),
-                             1e-10 * float(np.linalg.norm(fs)), 200, pc=mgs)
-    samples = []
+    f = poisson_modes_rhs(n, SEED)
+    samples, iters, threads = [], 0, 1
     for step in range(args.warmup + args.steps):
-        t = {}
-        for k in (1, 3):
-            x = np.zeros(N * N)
-            t0 = time.perf_counter()
-            O.cg_solve(x, f, N, N, 1.0, P.stencil.as_triples(), tol, k, pc=mg)
-            t[k] = time.perf_counter() - t0
-        est = t[1] + (t[3] - t[1]) / 2.0 * max(iters - 1, 0)
+        t, iters, threads = oracle_solve(n, f)
         if step >= args.warmup:
-            samples.append(est)
+            samples.append(t)
     v = float(np.mean(samples))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"poisson_{n}sq_mg_pcg_rel1e-10", "grid": f"{N}x{N} incl. ring",
-                   "solver": "CG + V(2,2) FW/bilinear/weighted-Jacobi 0.8, coarsest 15^2 x 200 (CPU restatement)"},
-        "cpu_baseline": {"value": v, "unit": "s", "cores": O.get_threads(), "kind": "port",
-                         "sample": f"per step: full-size MG-PCG stopped after 1 and 3 iterations, extrapolated "
-                                   f"to the {iters} iterations the solve needs (counted on the 1023^2 problem)"},
+                   "solver": f"CG + {SOLVER} (CPU restatement)"},
+        "iterations": iters,
+        "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": f"per step: one full {n}^2 MG-PCG solve to 1e-10 ({iters} iterations)"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference is Rust (no cargo/rustc here); its CPU backend is timed as the C restatement",
     }
@@ -243,8 +278,8 @@ def main():
     b = Field.from_f64(P.grid, f, dev)
     x = Field.zeros(P.grid, DType.F64, dev)
     cg = CgSolver(P.grid, dev, tol, 100)
-    mg64 = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200, DType.F64)
-    mg32 = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200, DType.F32)
+    mg64 = Multigrid.vertex(P.grid, None, dev, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, DType.F64)
+    mg32 = Multigrid.vertex(P.grid, None, dev, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, DType.F32)
 
     def solve(mg):
         x.fill(0.0)
@@ -284,7 +319,7 @@ def main():
 
     # which kernel dominates the mixed solve? (one untimed solve per candidate)
     import ctypes as C
-    candidates = ["mg_down", "mg_up", "mg_sweep", "pcg_update", "pcg_dir", "mg_residual", "mg_restrict_fw",
+    candidates = ["mg_down", "mg_up", "mg_tail", "mg_sweep", "pcg_update", "pcg_dir", "mg_residual", "mg_restrict_fw",
                   "mg_prolong_bilinear", "pcg_rz", "mg_convert", "mg_zero", "mg_coarse_solve"]
     solve(mg32)
     shares = {}
@@ -299,8 +334,7 @@ def main():
     # plain FP64 and mixed solves
     plain_ms, st64, _, _ = timed(mg64, args.steps, args.warmup)
     u64 = x.to_vec_f64()
-    with ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else
-                      int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])) as clk:
+    with ClockSampler(local, uuid=str(torch.cuda.get_device_properties(local).uuid)) as clk:
         mixed_ms, st32, launches, ktime = timed(mg32, args.steps, args.warmup, kernel=dom)
     u32 = x.to_vec_f64()
 
@@ -377,8 +411,9 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
-            est, cores, sample = cpu_oracle_estimate(n, f, int(st64.iterations))
-            cpu = {"value": est, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+            t, iters, cores = oracle_solve(n, f)
+            cpu = {"value": t, "unit": "s", "cores": cores, "kind": "port",
+                   "sample": f"one full {n}^2 MG-PCG solve to 1e-10 ({iters} iterations)"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
 
@@ -389,7 +424,7 @@ def main():
             "vs_baseline": None, "dtype": "f64 Krylov/residual/update + f32 V-cycle",
             "data": "synthetic (seeded 32-mode sin-sin source + 1e-3 uniform noise)",
             "config": {"workload": f"poisson_{n}sq_mg_pcg_rel1e-10", "grid": f"{N}x{N} incl. Dirichlet ring",
-                       "solver": "CG + V(2,2) full weighting / bilinear / weighted Jacobi 0.8, coarsest 15^2 x 200",
+                       "solver": f"CG + {SOLVER}",
                        "tolerance": "||r||_2 < 1e-10 ||f||_2", "l2": "inputs larger than L2 (134 MB per vector)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "iterations": int(st32.iterations), "rel_residual_fp64": rr32, "err_vs_fp64_direct": err32,

@@ -79,6 +79,33 @@ struct fx_buf {
 namespace fx {
 
 int check_launch(fx_ctx *ctx, const char *what);
+
+// Programmatic dependent launch.  Kernels of the solve path are launched with programmatic
+// stream serialisation, so the next kernel's launch and block scheduling overlap the end of
+// the current one.  Each such kernel first waits for the grid it depends on to complete and
+// flush (griddepcontrol.wait; a no-op when the launch had no programmatic dependency), so no
+// memory access moves ahead of the previous kernel, and then allows its own dependent to be
+// scheduled.  The dependent can start only once every block of this grid has passed that
+// point, i.e. once all of them are resident, so its waiting blocks never hold back ours.
+__device__ __forceinline__ void grid_dep_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(fx_ctx *ctx, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&cfg, kernel, args...);  // errors surface in check_launch
+}
 // Timing hooks around a launch (no-ops unless fx_ctx_timing_begin named this kernel).
 void timing_pre(fx_ctx *ctx, const char *what);
 void timing_post(fx_ctx *ctx, double points, double bytes = 0.0);
@@ -339,6 +366,7 @@ constexpr int band_depth() {
 template <typename T, int CPT, int D, int K, typename Loader, typename Point, typename Fin>
 __global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader ld_in, Point pt_in, Fin fin,
                                                            RedArgs<K> ra, const int *skip) {
+    grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
     Loader ld = ld_in;  // device-resident scalars (alpha, beta, ...) read once per kernel
     fx_prepare(ld);
@@ -499,7 +527,8 @@ int launch_march(fx_ctx *ctx, size_t rows, size_t cols, Loader ld, Point pt, Fin
     const MarchGeom G = march_geom(rows, cols, kBlock * CPT, D, occ * ctx->num_sms);
     if (K > 0 && G.nblocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");
     timing_pre(ctx, what);
-    k_march<T, CPT, D, K><<<G.nblocks, kBandThreads, 0, ctx->stream>>>(G, ld, pt, fin, red_args<K>(ctx), skip);
+    launch_pdl(ctx, k_march<T, CPT, D, K, Loader, Point, Fin>, G.nblocks, kBandThreads, 0, G, ld, pt, fin,
+               red_args<K>(ctx), skip);
     timing_post(ctx, (double)rows * (double)cols);
     return check_launch(ctx, what);
 }
@@ -516,6 +545,7 @@ FlatGeom flat_geom(fx_ctx *ctx, size_t n);
 template <int K, typename F, typename Fin>
 __global__ void __launch_bounds__(kBlock) k_flat(size_t n, F f_in, Fin fin, RedArgs<K> ra,
                                                  const int *skip) {
+    grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
     F f = f_in;
     fx_prepare(f);
@@ -532,7 +562,7 @@ int launch_flat(fx_ctx *ctx, size_t n, F f, Fin fin, const int *skip, const char
     FlatGeom g = flat_geom(ctx, n);
     if (g.blocks == 0) return FX_OK;
     timing_pre(ctx, what);
-    k_flat<K><<<g.blocks, kBlock, 0, ctx->stream>>>(n, f, fin, red_args<K>(ctx), skip);
+    launch_pdl(ctx, k_flat<K, F, Fin>, g.blocks, kBlock, 0, n, f, fin, red_args<K>(ctx), skip);
     timing_post(ctx, (double)n);
     return check_launch(ctx, what);
 }

@@ -1,19 +1,26 @@
 // fx_wcycle.cuh -- fused vertex-centred V(2,2)-cycle level kernels, one warp per strip.
 //
-// The same two passes per level as the band kernels of fx_vcycle.cuh (down: x1 = w b, x2 =
-// x1 + w (b - A x1), res = b - A x2 and its full-weighting restriction; up: f = x2 + P e,
-// x3 = f + w (b - A f), z = x3 + w (b - A x3)), organised for the instruction budget of a
-// memory-bound pass:
+// Two passes per level replace the separate sweep / residual / restriction / prolongation
+// passes of a V(2,2)-cycle with a zero initial guess:
 //
-//  - a warp owns a strip of 32 consecutive columns (32 - 2H of them its own, H halo columns
-//    on each side recomputed by the neighbouring strip) and marches it down a chunk of rows;
-//  - each lane holds its column's last three rows of every stage in registers; the row above
-//    and below are register reads, the west / east neighbours one shuffle each;
+//   k_wdown: from the right-hand side b alone, x1 = w b (first sweep from zero), x2 = x1 +
+//            w (b - A x1) (second sweep), res = b - A x2 and its full-weighting restriction
+//            onto the coarse grid -- one pass that reads b and writes x2 and the coarse rhs;
+//   k_wup:   f = x2 + bilinear(e_coarse), x3 = f + w (b - A f), z = x3 + w (b - A x3), written
+//            out (at the finest level directly as the caller's vector, optionally with the
+//            inner product <b, z> the preconditioned CG needs next).
+//
+// Both are organised for the instruction budget of a memory-bound pass:
+//
+//  - a warp owns a strip of 64 consecutive columns (its own ones plus halo columns on each
+//    side that the neighbouring strips own) and marches it down a chunk of rows;
+//  - each lane holds two adjacent columns' last three rows of every stage in registers; the
+//    row above and below are register reads, the outer west / east neighbours one shuffle;
 //  - every global load is a raw value issued D rows ahead into a register FIFO;
 //  - no shared memory and no block barrier: the warps of a block are independent.
 //
-// Every point value is the expression of the band kernels (and so of the separate sweep /
-// residual / restriction / prolongation kernels), so the cycle stays bitwise equal.
+// Every point value is the expression of the separate kernels, so the fused cycle is
+// bitwise equal to the unfused one.
 #pragma once
 
 #include <type_traits>
@@ -56,7 +63,7 @@ __device__ __forceinline__ float shfl_e(float v) { return __shfl_down_sync(0xfff
 __device__ __forceinline__ double shfl_w(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ double shfl_e(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 
-// a.c c + a.n n + a.s s + a.w w + a.e e in the order of ring_op5
+// a.c c + a.n n + a.s s + a.w w + a.e e, in the order of op5 (fx_points.cuh)
 template <typename T>
 __device__ __forceinline__ T op5v(const A5<T> &a, T c, T n, T s, T w, T e) {
     return fx_fma(a.c, c, fx_fma(a.n, n, fx_fma(a.s, s, fx_fma(a.w, w, a.e * e))));
@@ -79,6 +86,7 @@ template <typename T, typename TB>
 __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const TB *__restrict__ b, T *__restrict__ x2g,
                                                              T *__restrict__ coarse, int ccols, VOp<T> op,
                                                              const int *skip) {
+    grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
     constexpr int D = kStripFifo;
     const int lane = threadIdx.x & 31;
@@ -194,6 +202,7 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
                                                            const T *__restrict__ e, int ccols,
                                                            const TB *__restrict__ b, TZ *__restrict__ z, VOp<T> op,
                                                            Fin fin, RedArgs<1> ra, const int *skip) {
+    grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
     constexpr int D = kStripFifo;
     const int lane = threadIdx.x & 31;
@@ -355,7 +364,7 @@ int launch_wdown(fx_ctx *ctx, size_t rows, size_t cols, const TB *b, T *x2, T *c
     const StripGeom G = strip_geom(rows, cols, kDownOwn, cap);
     const int blocks = (G.nitems + kStripWarps - 1) / kStripWarps;
     timing_pre(ctx, "mg_down");
-    k_wdown<T, TB><<<blocks, kStripWarps * 32, 0, ctx->stream>>>(G, b, x2, coarse, (int)ccols, op, skip);
+    launch_pdl(ctx, k_wdown<T, TB>, blocks, kStripWarps * 32, 0, G, b, x2, coarse, (int)ccols, op, skip);
     // reads b, writes the smoothed x2 and the restricted coarse rhs
     const double pts = (double)rows * (double)cols, cpts = (double)((rows - 1) / 2 + 1) * (double)ccols;
     timing_post(ctx, pts, pts * (sizeof(TB) + sizeof(T)) + cpts * sizeof(T));
@@ -371,8 +380,8 @@ int launch_wup(fx_ctx *ctx, size_t rows, size_t cols, const T *x2, const T *e, s
     const int blocks = (G.nitems + kStripWarps - 1) / kStripWarps;
     if (RZ && blocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");
     timing_pre(ctx, "mg_up");
-    k_wup<T, TB, TZ, RZ, Fin><<<blocks, kStripWarps * 32, 0, ctx->stream>>>(G, x2, e, (int)ccols, b, z, op, fin,
-                                                                             red_args<1>(ctx), skip);
+    launch_pdl(ctx, k_wup<T, TB, TZ, RZ, Fin>, blocks, kStripWarps * 32, 0, G, x2, e, (int)ccols, b, z, op, fin,
+               red_args<1>(ctx), skip);
     // reads x2, the coarse correction e and b, writes z
     const double pts = (double)rows * (double)cols, cpts = (double)((rows - 1) / 2 + 1) * (double)ccols;
     timing_post(ctx, pts, pts * (sizeof(T) + sizeof(TB) + sizeof(TZ)) + cpts * sizeof(T));

@@ -215,7 +215,8 @@ def test_vertex_mg_vcycle_bitwise(dev, n):
 
 
 @pytest.mark.parametrize("n", [15, 63, 255, 1023])
-def test_fused_vcycle_bitwise(dev, n):
+@pytest.mark.parametrize("cm,cs", [(15, 200), (7, 30), (3, 10)])
+def test_fused_vcycle_bitwise(dev, n, cm, cs):
     """The fused V(2,2) kernels (zero initial guess) equal the oracle's separate sweeps, residual,
     full weighting and bilinear prolongation bit for bit (F64), and the fused F32 cycle equals
     the unfused F32 cycle bit for bit."""
@@ -228,15 +229,15 @@ def test_fused_vcycle_bitwise(dev, n):
     bvec[1:-1, 1:-1] = rng.uniform(-1, 1, (n, n))
     bvec = bvec.ravel()
     b = Field.from_f64(P.grid, bvec, dev)
-    mg = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200)
+    mg = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, cm, cs)
     z = Field.zeros(P.grid, DType.F64, dev)
     mg.precondition(z, b)
     omg = O.Multigrid(N, N, P.h, P.h, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=P.stencil.as_triples(),
-                      coarse_max=15, coarse_sweeps=200)
+                      coarse_max=cm, coarse_sweeps=cs)
     zo = np.zeros(N * N)
     omg.v_cycle(zo, bvec)
     assert np.array_equal(z.to_vec_f64(), zo)
-    mg32 = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, 15, 200, DType.F32)
+    mg32 = Multigrid.vertex(P.grid, None, dev, 2, 2, 0.8, cm, cs, DType.F32)
     zf = Field.zeros(P.grid, DType.F64, dev)
     mg32.precondition(zf, b)
     zu = Field.zeros(P.grid, DType.F64, dev)
