@@ -63,6 +63,9 @@ def parse():
     p.add_argument("--n", type=int, default=N_INTERIOR, help="interior nodes per direction")
     p.add_argument("--no-micro", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--mode", default="solve", choices=["solve", "vcycle"],
+                   help="solve: the headline MG-PCG solve; vcycle: preconditioner applications alone "
+                        "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target")
     return p.parse_args()
 
 
@@ -241,10 +244,55 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ our arm
 
+def run_vcycle(args):
+    """Time `steps` applications z = M^-1 r of the F32 V(2,2)-cycle (after `warmup` untimed ones)
+    on the n^2 problem, and report each level kernel's device time from the timing records."""
+    import ctypes as C
+
+    import torch
+    from fluxion_b200 import DType, Device, Field, Multigrid
+    from fluxion_b200 import _lib as L
+    from fluxion_b200.workloads import poisson_modes_rhs, poisson_problem
+
+    n = args.n
+    dev = Device.Cuda(0)
+    be = dev.backend()
+    stream = torch.cuda.Stream()
+    be.set_stream(stream.cuda_stream)
+    P = poisson_problem(n)
+    r = Field.from_f64(P.grid, poisson_modes_rhs(n, SEED), dev)
+    z = Field.zeros(P.grid, DType.F64, dev)
+    mg = Multigrid.vertex(P.grid, None, dev, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, DType.F32)
+    for _ in range(args.warmup):
+        mg.precondition(z, r)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        mg.precondition(z, r)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    per = {}
+    for k in ("mg_down", "mg_up", "mg_tail"):
+        L.lib().fx_ctx_timing_begin(be.ctx, k.encode())
+        mg.precondition(z, r)
+        cap = 64
+        ms, pts, byt, cnt = (C.c_double * cap)(), (C.c_double * cap)(), (C.c_double * cap)(), C.c_size_t()
+        L.lib().fx_ctx_timing_end_records(be.ctx, ms, pts, byt, cap, C.byref(cnt))
+        per[k] = [{"points": pts[i], "us": ms[i] * 1e3, "GBps": byt[i] / (ms[i] * 1e-3) / 1e9 if byt[i] else None}
+                  for i in range(cnt.value)]
+    print(json.dumps({"mode": "vcycle", "workload": f"poisson_{n}sq_f32_vcycle", "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_vcycle": e0.elapsed_time(e1) / args.steps,
+                      "levels": mg.depth(), "per_launch_with_events": per}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "vcycle":
+        return run_vcycle(args)
 
     import torch
 
