@@ -358,9 +358,12 @@ constexpr int band_cpt() {
     return sizeof(T) == 8 ? 1 : 2;
 }
 
-template <int NA>
+// FIFO depth in rows for S streamed arrays besides the marched field (the point's per-point
+// arrays plus the loader's extra ones): deep enough to cover DRAM latency, shallow enough to
+// keep two or three blocks per SM.  Even: rows are consumed in pairs.
+template <int S>
 constexpr int band_depth() {
-    return NA == 0 ? 8 : (NA <= 2 ? 4 : 2);  // even: rows are consumed in pairs
+    return S == 0 ? 8 : (S == 1 ? 6 : (S == 2 ? 4 : 2));
 }
 
 template <typename T, int CPT, int D, int K, typename Loader, typename Point, typename Fin>
@@ -517,7 +520,7 @@ template <typename T, int K, typename Loader, typename Point, typename Fin>
 int launch_march(fx_ctx *ctx, size_t rows, size_t cols, Loader ld, Point pt, Fin fin, const int *skip,
                  const char *what) {
     constexpr int CPT = band_cpt<T>();
-    constexpr int D = band_depth<Point::NA>();
+    constexpr int D = band_depth<Point::NA + Loader::NL - 1>();
     static int occ = 0;  // resident CTAs per SM for this instantiation
     if (!occ) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_march<T, CPT, D, K, Loader, Point, Fin>,

@@ -30,7 +30,10 @@
 namespace fx {
 
 constexpr int kStripWarps = 8;  // warps per block
-constexpr int kStripFifo = 6;   // FIFO depth in rows; the march is unrolled by 6 (= lcm(2, 3))
+constexpr int kStripUnroll = 6;  // the march is unrolled by 6 rows (= lcm(2, 3): row parity x 3-row windows)
+constexpr int kDownFifo = 6;    // rows of raw loads in flight (a divisor of kStripUnroll)
+constexpr int kUpFifo = 6;
+static_assert(kStripUnroll % kDownFifo == 0 && kStripUnroll % kUpFifo == 0, "FIFO depth must divide the unroll");
 
 struct StripGeom {
     int rows, cols;
@@ -51,7 +54,7 @@ inline StripGeom strip_geom(size_t rows, size_t cols, int useful, long capacity)
     long chunks = target / G.nstrips;
     if (chunks < 1) chunks = 1;
     long cr = ((long)rows + chunks - 1) / chunks;
-    if (cr < kStripFifo) cr = kStripFifo;
+    if (cr < kStripUnroll) cr = kStripUnroll;
     cr = (cr + 1) & ~1L;
     G.chunk_rows = (int)cr;
     G.nitems = (int)(G.nstrips * (((long)rows + cr - 1) / cr));
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
                                                              const int *skip) {
     grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
-    constexpr int D = kStripFifo;
+    constexpr int D = kDownFifo, R = kStripUnroll;
     const int lane = threadIdx.x & 31;
     const int item = blockIdx.x * kStripWarps + (threadIdx.x >> 5);
     if (item >= G.nitems) return;  // whole warps
@@ -127,7 +130,7 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
         const size_t rq = (size_t)q * cols;
         // row q: rhs and x1 = w b (0 on the ring); refill with row q + D
         {
-            const T ba = (T)fa[k], bb = (T)fb[k];
+            const T ba = (T)fa[k % D], bb = (T)fb[k % D];
             const bool rin = F || row_in(q);
             bwa[s0] = ba;
             bwb[s0] = bb;
@@ -136,8 +139,8 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
             const int qn = q + D;
             if (F || (row_in(qn) && qn <= q_last)) {
                 const size_t o = rq + (size_t)D * cols;
-                if (ina) fa[k] = b[o + ca];
-                if (inb) fb[k] = b[o + cb];
+                if (ina) fa[k % D] = b[o + ca];
+                if (inb) fb[k % D] = b[o + cb];
             }
         }
         // row q-1: x2
@@ -179,13 +182,13 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
             }
         }
     };
-    for (int qb = q_first; qb <= q_last; qb += D) {
-        if (qb >= q_lo && qb + D - 1 <= q_hi) {
+    for (int qb = q_first; qb <= q_last; qb += R) {
+        if (qb >= q_lo && qb + R - 1 <= q_hi) {
 #pragma unroll
-            for (int k = 0; k < D; k++) step(k, qb + k, fast_t<true>{});
+            for (int k = 0; k < R; k++) step(k, qb + k, fast_t<true>{});
         } else {
 #pragma unroll
-            for (int k = 0; k < D; k++) {
+            for (int k = 0; k < R; k++) {
                 if (qb + k > q_last) break;  // uniform over the warp
                 step(k, qb + k, fast_t<false>{});
             }
@@ -204,7 +207,7 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
                                                            Fin fin, RedArgs<1> ra, const int *skip) {
     grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
-    constexpr int D = kStripFifo;
+    constexpr int D = kUpFifo, R = kStripUnroll;
     const int lane = threadIdx.x & 31;
     const int item = blockIdx.x * kStripWarps + (threadIdx.x >> 5);
     CSum acc[1] = {CSum{0.0, 0.0}};
@@ -225,9 +228,10 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
         const int m_last = (q_last >> 1) + 1;  // last coarse row any step reads
         auto row_in = [&](int r) { return r >= 1 && r <= rows - 2; };
 
-        // FIFO per fine row: raw x2 and b of both columns; per fine row pair (2m, 2m+1) the
-        // coarse row m+1 at columns kc, kc+1 (row m is kept from the previous pair)
-        T xa_[D], xb_[D], ea_[D / 2], eb_[D / 2];
+        // FIFO of D fine rows: raw x2 and b of both columns; per fine row pair (2m, 2m+1) of the
+        // unrolled step the coarse row m+1 at columns kc, kc+1, R rows ahead (row m is kept
+        // from the previous pair)
+        T xa_[D], xb_[D], ea_[R / 2], eb_[R / 2];
         TB ba_[D], bb_[D];
         auto load_row = [&](int q, int k) {
             xa_[k] = (T)0;
@@ -258,10 +262,9 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
         T c0a, c0b;  // coarse row q >> 1 of the current pair, columns kc, kc+1
         load_coarse(q_first >> 1, c0a, c0b);
 #pragma unroll
-        for (int k = 0; k < D; k++) {
-            load_row(q_first + k, k);
-            if (!(k & 1)) load_coarse(((q_first + k) >> 1) + 1, ea_[k / 2], eb_[k / 2]);
-        }
+        for (int k = 0; k < D; k++) load_row(q_first + k, k);
+#pragma unroll
+        for (int k = 0; k < R; k += 2) load_coarse(((q_first + k) >> 1) + 1, ea_[k / 2], eb_[k / 2]);
 
         T fa[3] = {}, fb[3] = {}, x3a[3] = {}, x3b[3] = {};
         TB bwa[3] = {}, bwb[3] = {};
@@ -283,28 +286,28 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
                     pb = (T)0.5 * (e00 + e01);                    // v_eo
                 }
                 const bool rin = F || row_in(q);
-                fa[s0] = (rin && ina) ? xa_[k] + pa : (T)0;
-                fb[s0] = (rin && inb) ? xb_[k] + pb : (T)0;
-                bwa[s0] = ba_[k];
-                bwb[s0] = bb_[k];
+                fa[s0] = (rin && ina) ? xa_[k % D] + pa : (T)0;
+                fb[s0] = (rin && inb) ? xb_[k % D] + pb : (T)0;
+                bwa[s0] = ba_[k % D];
+                bwb[s0] = bb_[k % D];
                 if (ro) {  // the pair is done: its lower coarse row becomes the upper one
                     c0a = e10;
                     c0b = e11;
-                    load_coarse((q + D + 1) >> 1, ea_[k / 2], eb_[k / 2]);
+                    load_coarse((q + R + 1) >> 1, ea_[k / 2], eb_[k / 2]);
                 }
                 const int qn = q + D;
                 if (F) {
                     const size_t o = rq + (size_t)D * cols;
                     if (ina) {
-                        xa_[k] = x2g[o + ca];
-                        ba_[k] = b[o + ca];
+                        xa_[k % D] = x2g[o + ca];
+                        ba_[k % D] = b[o + ca];
                     }
                     if (inb) {
-                        xb_[k] = x2g[o + cb];
-                        bb_[k] = b[o + cb];
+                        xb_[k % D] = x2g[o + cb];
+                        bb_[k % D] = b[o + cb];
                     }
                 } else {
-                    load_row(qn, k);
+                    load_row(qn, k % D);
                 }
             }
             // row q-1: x3
@@ -340,13 +343,13 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
                 }
             }
         };
-        for (int qb = q_first; qb <= q_last; qb += D) {
-            if (qb >= q_lo && qb + D - 1 <= q_hi) {
+        for (int qb = q_first; qb <= q_last; qb += R) {
+            if (qb >= q_lo && qb + R - 1 <= q_hi) {
 #pragma unroll
-                for (int k = 0; k < D; k++) step(k, qb + k, fast_t<true>{});
+                for (int k = 0; k < R; k++) step(k, qb + k, fast_t<true>{});
             } else {
 #pragma unroll
-                for (int k = 0; k < D; k++) {
+                for (int k = 0; k < R; k++) {
                     if (qb + k > q_last) break;
                     step(k, qb + k, fast_t<false>{});
                 }
