@@ -124,10 +124,14 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
 
     T bwa[3] = {}, bwb[3] = {}, x1a[3] = {}, x1b[3] = {}, x2a[3] = {}, x2b[3] = {};
     T rsa[3] = {}, rsb[3] = {}, rwa[3] = {};
+    // element offsets of this lane's column ca, advanced one row per step: the rhs row being
+    // fetched (q + D), the x2 row being stored (q - 1), and the coarse row of fine row q - 3
+    long long ob = (long long)(q_first + D) * cols + ca;
+    long long ox = (long long)(q_first - 1) * cols + ca;
+    long long oc = (long long)((q_first - 3) >> 1) * ccols + (ca >> 1);  // q_first - 3 even
     auto step = [&](int k, int q, auto fast) {
         constexpr bool F = decltype(fast)::value;
         const int s0 = k % 3, s1 = (k + 2) % 3, s2 = (k + 1) % 3;  // slots of rows q, q-1, q-2
-        const size_t rq = (size_t)q * cols;
         // row q: rhs and x1 = w b (0 on the ring); refill with row q + D
         {
             const T ba = (T)fa[k % D], bb = (T)fb[k % D];
@@ -138,10 +142,10 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
             x1b[s0] = (rin && inb) ? fx_fma(op.wd, bb, (T)0) : (T)0;
             const int qn = q + D;
             if (F || (row_in(qn) && qn <= q_last)) {
-                const size_t o = rq + (size_t)D * cols;
-                if (ina) fa[k % D] = b[o + ca];
-                if (inb) fb[k % D] = b[o + cb];
+                if (ina) fa[k % D] = b[ob];
+                if (inb) fb[k % D] = b[ob + 1];
             }
+            ob += cols;
         }
         // row q-1: x2
         {
@@ -154,10 +158,10 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
             x2a[s1] = va;
             x2b[s1] = vb;
             if (F || (rin && q - 1 >= r0 && q - 1 < r1)) {
-                T *row = x2g + rq - cols;
-                if (sta) row[ca] = va;
-                if (stb) row[cb] = vb;
+                if (sta) x2g[ox] = va;
+                if (stb) x2g[ox + 1] = vb;
             }
+            ox += cols;
         }
         // row q-2: residual, and the residual west of ca for the restriction
         {
@@ -178,8 +182,9 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
             if (cpt && (F || (fr >= r0 && fr < r1 && fr >= 2 && fr <= rows - 3))) {
                 const T e = (rsa[s1] + rsa[s2]) + (rwa[s0] + rsb[s0]);
                 const T d = (rwa[s1] + rsb[s1]) + (rwa[s2] + rsb[s2]);
-                coarse[(size_t)(fr >> 1) * ccols + (ca >> 1)] = ((T)4 * rsa[s0] + ((T)2 * e + d)) * (T)0.0625;
+                coarse[oc] = ((T)4 * rsa[s0] + ((T)2 * e + d)) * (T)0.0625;
             }
+            oc += ccols;
         }
     };
     for (int qb = q_first; qb <= q_last; qb += R) {
@@ -233,45 +238,51 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
         // from the previous pair)
         T xa_[D], xb_[D], ea_[R / 2], eb_[R / 2];
         TB ba_[D], bb_[D];
-        auto load_row = [&](int q, int k) {
+        // o: element offset of (q, ca) / (m, kc)
+        auto load_row = [&](int q, int k, long long o) {
             xa_[k] = (T)0;
             xb_[k] = (T)0;
             ba_[k] = (TB)0;
             bb_[k] = (TB)0;
             if (row_in(q) && q <= q_last) {
-                const size_t o = (size_t)q * cols;
                 if (ina) {
-                    xa_[k] = x2g[o + ca];
-                    ba_[k] = b[o + ca];
+                    xa_[k] = x2g[o];
+                    ba_[k] = b[o];
                 }
                 if (inb) {
-                    xb_[k] = x2g[o + cb];
-                    bb_[k] = b[o + cb];
+                    xb_[k] = x2g[o + 1];
+                    bb_[k] = b[o + 1];
                 }
             }
         };
-        auto load_coarse = [&](int m, T &v0, T &v1) {
+        auto load_coarse = [&](int m, T &v0, T &v1, long long o) {
             v0 = (T)0;
             v1 = (T)0;
             if (m >= 0 && m < crows && m <= m_last) {
-                const size_t o = (size_t)m * ccols + kc;
                 if (ce0) v0 = e[o];
                 if (ce1) v1 = e[o + 1];
             }
         };
         T c0a, c0b;  // coarse row q >> 1 of the current pair, columns kc, kc+1
-        load_coarse(q_first >> 1, c0a, c0b);
+        load_coarse(q_first >> 1, c0a, c0b, (long long)(q_first >> 1) * ccols + kc);
 #pragma unroll
-        for (int k = 0; k < D; k++) load_row(q_first + k, k);
+        for (int k = 0; k < D; k++) load_row(q_first + k, k, (long long)(q_first + k) * cols + ca);
 #pragma unroll
-        for (int k = 0; k < R; k += 2) load_coarse(((q_first + k) >> 1) + 1, ea_[k / 2], eb_[k / 2]);
+        for (int k = 0; k < R; k += 2) {
+            const int m = ((q_first + k) >> 1) + 1;
+            load_coarse(m, ea_[k / 2], eb_[k / 2], (long long)m * ccols + kc);
+        }
+        // running element offsets, advanced as the march goes: the fine row being fetched
+        // (q + D), the coarse row fetched at odd steps ((q + R + 1) / 2), the z row (q - 2)
+        long long orow = (long long)(q_first + D) * cols + ca;
+        long long oe = (long long)((q_first + R + 2) >> 1) * ccols + kc;
+        long long oz = (long long)(q_first - 2) * cols + ca;
 
         T fa[3] = {}, fb[3] = {}, x3a[3] = {}, x3b[3] = {};
         TB bwa[3] = {}, bwb[3] = {};
         auto step = [&](int k, int q, auto fast) {
             constexpr bool F = decltype(fast)::value;
             const int s0 = k % 3, s1 = (k + 2) % 3, s2 = (k + 1) % 3;  // rows q, q-1, q-2
-            const size_t rq = (size_t)q * cols;
             // row q: f = x2 + bilinear(e); the parities are fixed: ca even, cb odd, q odd <=> k odd
             {
                 const bool ro = k & 1;
@@ -293,22 +304,23 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
                 if (ro) {  // the pair is done: its lower coarse row becomes the upper one
                     c0a = e10;
                     c0b = e11;
-                    load_coarse((q + R + 1) >> 1, ea_[k / 2], eb_[k / 2]);
+                    load_coarse((q + R + 1) >> 1, ea_[k / 2], eb_[k / 2], oe);
+                    oe += ccols;
                 }
                 const int qn = q + D;
                 if (F) {
-                    const size_t o = rq + (size_t)D * cols;
                     if (ina) {
-                        xa_[k % D] = x2g[o + ca];
-                        ba_[k % D] = b[o + ca];
+                        xa_[k % D] = x2g[orow];
+                        ba_[k % D] = b[orow];
                     }
                     if (inb) {
-                        xb_[k % D] = x2g[o + cb];
-                        bb_[k % D] = b[o + cb];
+                        xb_[k % D] = x2g[orow + 1];
+                        bb_[k % D] = b[orow + 1];
                     }
                 } else {
-                    load_row(qn, k % D);
+                    load_row(qn, k % D, orow);
                 }
+                orow += cols;
             }
             // row q-1: x3
             {
@@ -327,20 +339,21 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
                 const T wa = shfl_w(xb), eb = shfl_e(xa);
                 const int r = q - 2;
                 if (F || (row_in(r) && r >= r0 && r < r1)) {
-                    TZ *row = z + rq - 2 * (size_t)cols;
+                    TZ *row = z + oz;
                     if (sta) {
                         const TB bv = bwa[s2];
                         const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xa, x3a[s0], x3a[s1], wa, xb), xa);
-                        row[ca] = (TZ)v;
+                        row[0] = (TZ)v;
                         if (RZ) csum_add_prod(acc[0], (double)bv, (double)(TZ)v);
                     }
                     if (stb) {
                         const TB bv = bwb[s2];
                         const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xb, x3b[s0], x3b[s1], xa, eb), xb);
-                        row[cb] = (TZ)v;
+                        row[1] = (TZ)v;
                         if (RZ) csum_add_prod(acc[0], (double)bv, (double)(TZ)v);
                     }
                 }
+                oz += cols;
             }
         };
         for (int qb = q_first; qb <= q_last; qb += R) {
