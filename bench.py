@@ -37,12 +37,11 @@ sys.path.insert(0, ROOT)
 METRIC = "time to rel-resid 1e-10: learned/mixed vs plain (1 B200); stencil GB/s"
 N_INTERIOR = 4095
 SEED = 2024
-# V(2,2)-cycle parameters: weighted Jacobi 0.8, coarsen while the interior exceeds 7 x 7, 30
-# sweeps on the coarsest grid (the solve takes the same 9 iterations as with a 15 x 15
-# coarsest grid and 200 sweeps)
+# V(2,2)-cycle parameters of the configuration: weighted Jacobi 0.8, coarsen while the interior
+# exceeds 15 x 15, 200 Jacobi sweeps on the coarsest grid
 OMEGA = 0.8
-COARSE_MAX = 7
-COARSE_SWEEPS = 30
+COARSE_MAX = 15
+COARSE_SWEEPS = 200
 SOLVER = (f"V(2,2) full weighting / bilinear / weighted Jacobi {OMEGA}, coarsest interior <= "
           f"{COARSE_MAX}^2 x {COARSE_SWEEPS} sweeps")
 

@@ -125,8 +125,8 @@ class Multigrid(Preconditioner):
 
     @staticmethod
     def vertex(grid: Grid, boundaries: Optional[Boundaries] = None, device: Optional[Device] = None,
-               n_pre: int = 2, n_post: int = 2, omega: float = 0.8, coarse_max: int = 7,
-               coarse_sweeps: int = 30, dtype: DType = DType.F64, op_coeff: float = 1.0,
+               n_pre: int = 2, n_post: int = 2, omega: float = 0.8, coarse_max: int = 15,
+               coarse_sweeps: int = 200, dtype: DType = DType.F64, op_coeff: float = 1.0,
                op_stencil: Optional[Stencil] = None) -> "Multigrid":
         device = device or Device.best()
         op_stencil = op_stencil or Stencil.poisson_neg_laplacian(grid.dx, grid.dy)

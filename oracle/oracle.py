@@ -285,7 +285,7 @@ class Multigrid:
     full-weighting / bilinear / true weighted Jacobi on the operator being solved."""
 
     def __init__(self, rows, cols, dx, dy, n_pre=2, n_post=2, omega=2.0 / 3.0, mode=0,
-                 op_coeff=1.0, entries=None, bcs=ZERO_DIRICHLET, coarse_max=7, coarse_sweeps=30):
+                 op_coeff=1.0, entries=None, bcs=ZERO_DIRICHLET, coarse_max=15, coarse_sweeps=200):
         entries = entries or laplacian_5pt(dx, dy)
         n, dr, dc, w = _stencil_arrays(entries)
         self._bcs = bcs_array(bcs)
