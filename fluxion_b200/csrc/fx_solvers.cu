@@ -80,6 +80,9 @@ struct fx_precond {
     // z <- M^-1 r from a zero z, followed by rz = r.z handed to the PCG state S (first = the
     // initial product).  Returns FX_ERR_UNSUPPORTED when the preconditioner has no fused form.
     virtual int apply_pcg(fx_buf *, const fx_buf *, const int *, DevState *, bool) { return FX_ERR_UNSUPPORTED; }
+    // true when apply(z, r, skip, true) writes every interior point of z from r alone and leaves
+    // z's ring as it is, so a z whose ring is zero needs no zero-fill before each application
+    virtual bool fills_from_zero(const fx_buf *) const { return false; }
 };
 
 namespace {
@@ -255,6 +258,7 @@ struct fx_mg {
         fx_mg *mg = nullptr;
         int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) override;
         int apply_pcg(fx_buf *z, const fx_buf *r, const int *skip, DevState *S, bool first) override;
+        bool fills_from_zero(const fx_buf *z) const override;
     } view;
     ~fx_mg() {
         for (auto &L : lv) {
@@ -585,6 +589,10 @@ int fx_mg::View::apply_pcg(fx_buf *z, const fx_buf *r, const int *skip, DevState
     }
     if (first) return fused_cycle<float, double, double, true>(m, b0, z0, FinPcgRzInit{S}, skip);
     return fused_cycle<float, double, double, true>(m, b0, z0, FinPcgRz{S}, skip);
+}
+
+bool fx_mg::View::fills_from_zero(const fx_buf *z) const {
+    return fusable(mg) && z->dtype == FX_F64 && z->len == mg->lv[0].rows * mg->lv[0].cols;
 }
 
 int fx_mg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) {
@@ -1038,6 +1046,153 @@ int pipe_solve_impl(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff
                                      FinPipeIter{S}, halt, "pipe_iter");
     };
     return s->drive(step, s->max_iter + 1, s->g.rows * s->g.cols >= (1u << 22));
+}
+
+// ------------------------------------------------ preconditioned pipelined CG
+//
+// Ghysels & Vanroose (2014), Algorithm 4: the reference's PipelinedCgSolver (pipelined_cg.rs)
+// is its unpreconditioned case, and the scalar recurrence (pipe_scalars) and the update forms
+// (z = n + beta z, x += alpha p, ...) are those of its fused update.  With u = M r and m = M w:
+//   init:  r = b - A x;  u = M r;  w = A u;  p = s = z = q = 0
+//   iter:  m = M w;  n = A m;  z = n + b z;  q = m + b q;  s = w + b s;  p = u + b p;
+//          x += a p;  r -= a s;  u -= a q;  w -= a z
+// with gamma = (r, u), delta = (w, u) and the stop test on ||r||_2 reduced in the same pass.
+
+template <typename T, int MODE>
+struct PtPpcgInitW {  // w = A u; p = s = z = q = 0; reductions (r.u, w.u, r.r)
+    static constexpr int NA = 1;
+    OpA<T, MODE> A;
+    const T *r;
+    T *w, *p, *sv, *z, *q;
+    __device__ __forceinline__ const T *aux(int) const { return r; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T u = nb.c;
+        const T wv = A.apply(ring, nb);
+        w[idx] = wv;
+        p[idx] = (T)0;
+        sv[idx] = (T)0;
+        z[idx] = (T)0;
+        q[idx] = (T)0;
+        csum_add_prod(acc[0], (double)a[0], (double)u);
+        csum_add_prod(acc[1], (double)wv, (double)u);
+        csum_add_prod(acc[2], (double)a[0], (double)a[0]);
+    }
+};
+
+struct FinPpcgInit {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->gamma = v[0];
+        S->delta = v[1];
+        S->rr = v[2];
+        S->gamma_prev = INFINITY;
+        S->alpha_prev = INFINITY;
+        S->iter = 0;
+        S->resid = sqrt(v[2]);
+        S->r0 = S->resid;
+        if (S->max_iter == 0) st_finish(S, FX_MAX_ITERATIONS, 0, sqrt(v[2]));
+        else if (sqrt(v[2]) < S->tol) st_finish(S, FX_CONVERGED, 0, sqrt(v[2]));
+        else pipe_scalars(S);
+    }
+};
+
+// One iteration after m = M w: n = A m on the fly, the 8-way update, and (r.u, w.u, r.r) of the
+// updated vectors for the next iteration's scalars and stop test.
+template <typename T, int MODE>
+struct PtPpcgIter {
+    static constexpr int NA = 8;
+    OpA<T, MODE> A;
+    T *z, *q, *sv, *p, *x, *r, *u, *w;
+    const DevState *S;
+    T alpha, beta;
+    __device__ __forceinline__ void prepare() {
+        alpha = (T)S->alpha;
+        beta = (T)S->beta;
+    }
+    __device__ __forceinline__ const T *aux(int k) const {
+        return k == 0 ? z : k == 1 ? q : k == 2 ? sv : k == 3 ? p : k == 4 ? x : k == 5 ? r : k == 6 ? u : w;
+    }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T n = A.apply(ring, nb);
+        const T m = nb.c;
+        const T zn = n + a[0] * beta;
+        const T qn = m + a[1] * beta;
+        const T sn = a[7] + a[2] * beta;
+        const T pn = a[6] + a[3] * beta;
+        const T rn = fx_fma(-alpha, sn, a[5]);
+        const T un = fx_fma(-alpha, qn, a[6]);
+        const T wn = fx_fma(-alpha, zn, a[7]);
+        z[idx] = zn;
+        q[idx] = qn;
+        sv[idx] = sn;
+        p[idx] = pn;
+        x[idx] = fx_fma(alpha, pn, a[4]);
+        r[idx] = rn;
+        u[idx] = un;
+        w[idx] = wn;
+        csum_add_prod(acc[0], (double)rn, (double)un);
+        csum_add_prod(acc[1], (double)wn, (double)un);
+        csum_add_prod(acc[2], (double)rn, (double)rn);
+    }
+};
+
+struct FinPpcgIter {
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->gamma_prev = S->gamma;
+        S->alpha_prev = S->alpha;
+        S->gamma = v[0];
+        S->delta = v[1];
+        S->rr = v[2];
+        S->iter += 1;
+        S->resid = sqrt(v[2]);
+        if (S->iter >= S->max_iter) st_finish(S, FX_MAX_ITERATIONS, S->max_iter, sqrt(v[2]));
+        else if (sqrt(v[2]) < S->tol) st_finish(S, FX_CONVERGED, S->iter, sqrt(v[2]));
+        else pipe_scalars(S);
+    }
+};
+
+template <int MODE>
+int ppcg_solve_impl(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P,
+                    fx_precond *pc) {
+    using T = double;
+    fx_ctx *ctx = s->ctx;
+    const size_t RR = s->g.rows, CC = s->g.cols, n = RR * CC;
+    while (s->bufs.size() < 8) {  // u and q join the unpreconditioned solver's vectors
+        fx_buf *nb = nullptr;
+        FX_TRY(fx_alloc(ctx, n, FX_F64, &nb));
+        s->bufs.push_back(nb);
+    }
+    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
+    T *r = (T *)s->bufs[0]->ptr, *p = (T *)s->bufs[1]->ptr, *sv = (T *)s->bufs[2]->ptr, *z = (T *)s->bufs[3]->ptr;
+    T *w = (T *)s->bufs[4]->ptr, *m = (T *)s->bufs[5]->ptr, *u = (T *)s->bufs[6]->ptr, *q = (T *)s->bufs[7]->ptr;
+    T *xp = (T *)x->ptr;
+    const T *bp = (const T *)b->ptr;
+    DevState *S = s->d_st;
+    const int *halt = &S->halt;
+    fx_buf rb{ctx, r, n, FX_F64, false}, ub{ctx, u, n, FX_F64, false};
+    fx_buf wb{ctx, w, n, FX_F64, false}, mb{ctx, m, n, FX_F64, false};
+    // out = M in from a zero initial guess (z.fill(0); pc.apply(z, r), cg.rs:196-197)
+    const bool reuse = pc->fills_from_zero(&mb);
+    auto precondition = [&](fx_buf *out, const fx_buf *in, const int *skip) -> int {
+        if (!reuse) FX_TRY(zero_fill<T>(ctx, (T *)out->ptr, n, skip));
+        return pc->apply(out, in, skip, true);
+    };
+    FX_TRY(s->reset_state());
+    if (reuse) {  // rings stay zero from here on
+        FX_CUDA(cudaMemsetAsync(u, 0, n * sizeof(T), ctx->stream));
+        FX_CUDA(cudaMemsetAsync(m, 0, n * sizeof(T), ctx->stream));
+    }
+    FX_TRY((launch_march<T, 0>(ctx, RR, CC, Ld1<T>{xp}, PtPipeInitQ<T, MODE>{A, bp, r}, NoFin{}, nullptr, "ppcg_init_r")));
+    FX_TRY(precondition(&ub, &rb, nullptr));
+    FX_TRY((launch_march<T, 3>(ctx, RR, CC, Ld1<T>{u}, PtPpcgInitW<T, MODE>{A, r, w, p, sv, z, q}, FinPpcgInit{S},
+                                  nullptr, "ppcg_init_w")));
+    auto step = [&](size_t) -> int {
+        FX_TRY(precondition(&mb, &wb, halt));
+        return launch_march<T, 3>(ctx, RR, CC, Ld1<T>{m}, PtPpcgIter<T, MODE>{A, z, q, sv, p, xp, r, u, w, S},
+                                     FinPpcgIter{S}, halt, "ppcg_iter");
+    };
+    return s->drive(step, s->max_iter + 1, true);
 }
 
 // ------------------------------------------------ BiCGSTAB (bicgstab.rs:90-346)
@@ -1822,6 +1977,19 @@ int fx_pipelined_cg_solve(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double
     StencilP P;
     FX_TRY(prep_op(s->g, st, bc, &P));
     SOLVER_MODE_DISPATCH(P, FX_TRY(pipe_solve_impl<MODE>(s, x, b, coeff, P)));
+    s->stats(out);
+    return FX_OK;
+}
+
+int fx_pipelined_cg_solve_preconditioned(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff,
+                                         const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
+                                         fx_stats *out) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
+    FX_TRY(s->check_io(x, b));
+    StencilP P;
+    FX_TRY(prep_op(s->g, st, bc, &P));
+    SOLVER_MODE_DISPATCH(P, FX_TRY(ppcg_solve_impl<MODE>(s, x, b, coeff, P, pc)));
     s->stats(out);
     return FX_OK;
 }

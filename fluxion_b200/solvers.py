@@ -253,15 +253,15 @@ class CgSolver(_Native):
 
 
 class PipelinedCgSolver(_Native):
-    """pipelined_cg.rs:25-237 (Ghysels-Vanroose)."""
+    """pipelined_cg.rs:25-237 (Ghysels-Vanroose).  `solve` is the reference's unpreconditioned
+    method; `solve_preconditioned` is new: the preconditioned form of the same method (Ghysels &
+    Vanroose 2014, Algorithm 4), one preconditioner application and one fused pass per iteration,
+    stopping on ||r||_2 < tol as CgSolver does."""
 
     _prefix = "pipelined_cg"
 
     def __init__(self, grid: Grid, device: Optional[Device] = None, tol: float = 1e-8, max_iter: int = 500):
         super().__init__(grid, device, tol, max_iter)
-
-    def solve_preconditioned(self, *a, **k):
-        raise NotImplementedError("PipelinedCgSolver has no preconditioned variant (pipelined_cg.rs)")
 
     def name(self) -> str:
         return "PipelinedCG"

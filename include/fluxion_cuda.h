@@ -306,6 +306,13 @@ int fx_pipelined_cg_destroy(fx_pipelined_cg *s);
 int fx_pipelined_cg_set_params(fx_pipelined_cg *s, double tol, size_t max_iter);
 int fx_pipelined_cg_solve(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff,
                           const fx_stencil *st, const fx_boundaries *bc, fx_stats *out);
+/* Preconditioned pipelined CG (Ghysels & Vanroose 2014, Algorithm 4), new: the reference's
+ * PipelinedCgSolver is its unpreconditioned case (same scalar recurrence, same update forms).
+ * Per iteration one preconditioner application m = M w and one fused pass (n = A m on the fly,
+ * the 8-way vector update, (r.u, w.u, r.r) reduced); stops on ||r||_2 < tol as CgSolver does. */
+int fx_pipelined_cg_solve_preconditioned(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff,
+                                         const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
+                                         fx_stats *out);
 
 /* BiCgStabSolver (bicgstab.rs:19-346) */
 int fx_bicgstab_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter,

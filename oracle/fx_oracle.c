@@ -684,6 +684,55 @@ out:
     return rc;
 }
 
+/* Preconditioned pipelined CG (Ghysels & Vanroose 2014, Algorithm 4).  The reference's
+ * PipelinedCgSolver (pipelined_cg.rs:353-424) is its unpreconditioned case; the scalar
+ * recurrence and the fma forms of the update are kept from it (fxo_pcg_fused_update).  Stop test
+ * on ||r||_2 at the loop top, as cg.rs does. */
+int fxo_pipelined_pcg_solve(const fxo_op *op, double *x, const double *b, double tol, size_t max_iter,
+                            fxo_pc_fn pc, void *pc_ctx, fxo_stats *st) {
+    size_t n = op_len(op);
+    double *r = calloc(n, 8), *u = calloc(n, 8), *w = calloc(n, 8), *m = calloc(n, 8);
+    double *nn = calloc(n, 8), *z = calloc(n, 8), *q = calloc(n, 8), *s = calloc(n, 8);
+    double *p = calloc(n, 8);
+    int rc = apply_op(op, nn, x);
+    if (rc) goto out;
+    fxo_copy(b, r, n);
+    fxo_axpy(-1.0, nn, r, n);
+    fxo_fill(u, n, 0.0);
+    pc(pc_ctx, u, r);
+    apply_op(op, w, u);
+    double gamma_prev = INFINITY, alpha_prev = INFINITY;
+    for (size_t k = 0; k < max_iter; k++) {
+        double gamma = fxo_dot(r, u, n), delta = fxo_dot(w, u, n), rr = fxo_dot(r, r, n);
+        if (sqrt(rr) < tol) {
+            set_stats(st, k, sqrt(rr), 0);
+            goto out;
+        }
+        fxo_fill(m, n, 0.0);
+        pc(pc_ctx, m, w);
+        apply_op(op, nn, m);
+        double beta = gamma / gamma_prev;
+        double alpha = gamma / (delta - beta * gamma / alpha_prev);
+#pragma omp parallel for schedule(static)
+        for (size_t i = 0; i < n; i++) {
+            z[i] = fma(1.0, nn[i], z[i] * beta);
+            q[i] = fma(1.0, m[i], q[i] * beta);
+            s[i] = fma(1.0, w[i], s[i] * beta);
+            p[i] = fma(1.0, u[i], p[i] * beta);
+            x[i] = fma(alpha, p[i], x[i]);
+            r[i] = fma(-alpha, s[i], r[i]);
+            u[i] = fma(-alpha, q[i], u[i]);
+            w[i] = fma(-alpha, z[i], w[i]);
+        }
+        gamma_prev = gamma;
+        alpha_prev = alpha;
+    }
+    set_stats(st, max_iter, sqrt(fxo_dot(r, r, n)), 1);
+out:
+    free(r); free(u); free(w); free(m); free(nn); free(z); free(q); free(s); free(p);
+    return rc;
+}
+
 /* bicgstab.rs:90-210 (pc == NULL) and :218-346 (right-preconditioned). */
 int fxo_bicgstab_solve(const fxo_op *op, double *x, const double *b, double tol, size_t max_iter,
                        fxo_pc_fn pc, void *pc_ctx, fxo_stats *st) {

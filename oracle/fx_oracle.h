@@ -139,6 +139,8 @@ int fxo_cg_solve(const fxo_op *op, double *x, const double *b, double tol, size_
                  fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);
 int fxo_pipelined_cg_solve(const fxo_op *op, double *x, const double *b, double tol,
                            size_t max_iter, fxo_stats *st);
+int fxo_pipelined_pcg_solve(const fxo_op *op, double *x, const double *b, double tol, size_t max_iter,
+                            fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);
 int fxo_bicgstab_solve(const fxo_op *op, double *x, const double *b, double tol, size_t max_iter,
                        fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);
 int fxo_gmres_solve(const fxo_op *op, double *x, const double *b, size_t restart, double tol,

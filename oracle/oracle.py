@@ -101,6 +101,7 @@ def _declare(L):
     stp = C.POINTER(Stats)
     d("fxo_cg_solve", C.c_int, opp, _dp, _dp, C.c_double, _sz, PC_FN, C.c_void_p, stp)
     d("fxo_pipelined_cg_solve", C.c_int, opp, _dp, _dp, C.c_double, _sz, stp)
+    d("fxo_pipelined_pcg_solve", C.c_int, opp, _dp, _dp, C.c_double, _sz, PC_FN, C.c_void_p, stp)
     d("fxo_bicgstab_solve", C.c_int, opp, _dp, _dp, C.c_double, _sz, PC_FN, C.c_void_p, stp)
     d("fxo_gmres_solve", C.c_int, opp, _dp, _dp, _sz, C.c_double, _sz, PC_FN, C.c_void_p, stp)
     d("fxo_mg_create", C.c_void_p, _sz, _sz, C.c_double, C.c_double, bcp, C.c_int, C.c_int,
@@ -340,6 +341,14 @@ def pipelined_cg_solve(x, b, rows, cols, coeff, entries, tol, max_iter, bcs=ZERO
     st = Stats()
     _chk(lib().fxo_pipelined_cg_solve(C.byref(_op(rows, cols, coeff, entries, bcs)), _p(x), _p(b),
                                       tol, max_iter, C.byref(st)), "pipelined_cg")
+    return st.iterations, st.residual, st.reason
+
+
+def pipelined_pcg_solve(x, b, rows, cols, coeff, entries, tol, max_iter, pc, bcs=ZERO_DIRICHLET):
+    st = Stats()
+    fn, ctx = _pc_args(pc)
+    _chk(lib().fxo_pipelined_pcg_solve(C.byref(_op(rows, cols, coeff, entries, bcs)), _p(x), _p(b), tol,
+                                       max_iter, fn, ctx, C.byref(st)), "pipelined_pcg")
     return st.iterations, st.residual, st.reason
 
 

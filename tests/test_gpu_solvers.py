@@ -250,7 +250,7 @@ def test_fused_vcycle_bitwise(dev, n, cm, cs):
 
 @pytest.mark.parametrize("n,pipelined", [(255, False), (255, True), (511, False)])
 def test_mg_pcg_poisson_matches_direct_solve(dev, n, pipelined):
-    from fluxion_b200 import CgSolver, DType, Field, Multigrid
+    from fluxion_b200 import CgSolver, DType, Field, Multigrid, PipelinedCgSolver
     from fluxion_b200.workloads import dst_poisson_solve, neg_laplacian_residual, poisson_problem, \
         poisson_modes_rhs
     P = poisson_problem(n)
@@ -260,7 +260,8 @@ def test_mg_pcg_poisson_matches_direct_solve(dev, n, pipelined):
     x = Field.zeros(P.grid, DType.F64, dev)
     tol = 1e-10 * np.linalg.norm(f)
     mg = Multigrid.vertex(P.grid, None, dev)
-    s = CgSolver(P.grid, dev, tol, 200).solve_preconditioned(x, b, P.coeff, P.stencil, None, mg)
+    solver = (PipelinedCgSolver if pipelined else CgSolver)(P.grid, dev, tol, 200)
+    s = solver.solve_preconditioned(x, b, P.coeff, P.stencil, None, mg)
     assert s.converged() and s.iterations < 30
     u = x.to_vec_f64()
     assert neg_laplacian_residual(u, f, n) < 1.01e-10 * np.linalg.norm(f)
@@ -300,3 +301,46 @@ def test_config1_cg_on_gpu(dev):
     it, res, reason = O.cg_solve(xo, ob, n + 2, n + 2, 1.0, P.stencil.as_triples(), 1e-8 * np.linalg.norm(f), 5000)
     assert reason == 0 and abs(it - s.iterations) <= 2
     assert rel_err(u, xo) < 1e-6
+
+
+# ---------------------------------------------------------------- preconditioned pipelined CG
+
+def test_pipelined_pcg_matches_oracle(dev):
+    """Preconditioned pipelined CG with the FP64 vertex V-cycle against the oracle's restatement:
+    same stop reason, iterations within 1, solutions within 1e-8 (both converge to 1e-10).  (With
+    the FP32 cycle the method stalls near 1e-6: u is carried by recurrence, not recomputed as
+    M r, so the cycle's single-precision rounding accumulates.)"""
+    from fluxion_b200 import DType, Field, Multigrid, PipelinedCgSolver
+    from fluxion_b200.workloads import dst_poisson_solve, poisson_modes_rhs, poisson_problem
+    n = 255
+    P = poisson_problem(n)
+    N = n + 2
+    f = poisson_modes_rhs(n, seed=21)
+    tol = 1e-10 * float(np.linalg.norm(f))
+    b = Field.from_f64(P.grid, f, dev)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    mg = Multigrid.vertex(P.grid, None, dev, dtype=DType.F64)
+    st = PipelinedCgSolver(P.grid, dev, tol, 100).solve_preconditioned(x, b, P.coeff, P.stencil, None, mg)
+    omg = O.Multigrid(N, N, P.h, P.h, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=P.stencil.as_triples())
+    xo = np.zeros(N * N)
+    it, res, reason = O.pipelined_pcg_solve(xo, f, N, N, 1.0, P.stencil.as_triples(), tol, 100, omg)
+    assert st.converged() and reason == 0 and abs(st.iterations - it) <= 1
+    u = x.to_vec_f64()
+    assert rel_err(u, xo) < 1e-8
+    assert rel_err(u, dst_poisson_solve(f, n)) < 1e-8
+
+
+def test_pipelined_pcg_identity_matches_pipelined_cg(dev):
+    """With M = I the preconditioned recurrences reduce to the reference's pipelined CG."""
+    from fluxion_b200 import DType, Field, Identity, PipelinedCgSolver
+    from fluxion_b200.workloads import poisson_modes_rhs, poisson_problem
+    n = 127
+    P = poisson_problem(n)
+    f = poisson_modes_rhs(n, seed=4)
+    tol = 1e-9 * float(np.linalg.norm(f))
+    b = Field.from_f64(P.grid, f, dev)
+    x1, x2 = Field.zeros(P.grid, DType.F64, dev), Field.zeros(P.grid, DType.F64, dev)
+    s1 = PipelinedCgSolver(P.grid, dev, tol, 2000).solve(x1, b, P.coeff, P.stencil, None)
+    s2 = PipelinedCgSolver(P.grid, dev, tol, 2000).solve_preconditioned(x2, b, P.coeff, P.stencil, None, Identity())
+    assert s1.converged() and s2.converged() and abs(s1.iterations - s2.iterations) <= 1
+    assert rel_err(x2.to_vec_f64(), x1.to_vec_f64()) < 1e-8
