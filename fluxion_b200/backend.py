@@ -171,6 +171,27 @@ class CudaBuffer:
 
 # ------------------------------------------------------------------ backend
 
+class CudaGraph:
+    """A recorded and instantiated sequence of this backend's operations (HipGraph,
+    backend-hip/src/graph.rs:14-108): `launch` replays it on the backend's stream; the graph is
+    destroyed with the object, as HipGraph is on Drop."""
+
+    def __init__(self, backend: "CudaBackend", handle: int):
+        self.backend = backend
+        self.h = handle
+
+    def launch(self) -> None:
+        check(L.lib().fx_graph_launch(self.backend.ctx, self.h))
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().fx_graph_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
 class CudaBackend:
     """The B200 backend: one CUDA context and stream per device."""
 
@@ -213,6 +234,18 @@ class CudaBackend:
 
     def stream(self) -> int:
         return L.lib().fx_ctx_get_stream(self.ctx) or 0
+
+    # -------------------------------------------------------------- graphs (HipGraph, graph.rs)
+
+    def graph_begin(self) -> None:
+        """Start recording this backend's stream (HipGraph::begin_capture, graph.rs:35-46)."""
+        check(L.lib().fx_graph_begin(self.ctx))
+
+    def graph_end(self) -> "CudaGraph":
+        """Stop recording and instantiate (HipGraph::end_capture, graph.rs:48-70)."""
+        h = C.c_void_p()
+        check(L.lib().fx_graph_end(self.ctx, C.byref(h)))
+        return CudaGraph(self, h.value)
 
     # -------------------------------------------------------------- memory
 

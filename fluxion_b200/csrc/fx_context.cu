@@ -274,6 +274,56 @@ int fx_ctx_synchronize(fx_ctx *c) {
     return FX_OK;
 }
 
+// ---- graph capture (HipGraph, backend-hip/src/graph.rs:14-108)
+
+struct fx_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+int fx_graph_begin(fx_ctx *c) {
+    if (!c) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    if (!c->stream) return fail(FX_ERR_INVALID_ARGUMENT, "graph capture needs a non-default stream");
+    FX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    return FX_OK;
+}
+
+int fx_graph_end(fx_ctx *c, fx_graph **out) {
+    if (!c || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        return fail(FX_ERR_BACKEND, std::string("graph capture failed: ") +
+                                        (e != cudaSuccess ? cudaGetErrorString(e) : "empty capture"));
+    }
+    cudaGraphExec_t x = nullptr;
+    e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        return fail(FX_ERR_BACKEND, std::string("graph instantiation failed: ") + cudaGetErrorString(e));
+    }
+    *out = new fx_graph{g, x};
+    return FX_OK;
+}
+
+int fx_graph_launch(fx_ctx *c, const fx_graph *g) {
+    if (!c || !g) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_CUDA(cudaGraphLaunch(g->exec, c->stream));
+    return FX_OK;
+}
+
+int fx_graph_destroy(fx_graph *g) {
+    if (!g) return FX_OK;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return FX_OK;
+}
+
 int fx_ctx_set_stream(fx_ctx *c, void *stream) {
     if (!c) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;

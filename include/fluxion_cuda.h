@@ -96,6 +96,7 @@ typedef struct fx_cg fx_cg;
 typedef struct fx_pipelined_cg fx_pipelined_cg;
 typedef struct fx_bicgstab fx_bicgstab;
 typedef struct fx_gmres fx_gmres;
+typedef struct fx_graph fx_graph;
 
 /* ------------------------------------------------------------------ */
 /* Context (HipBackend::new / singleton, backend-hip/src/backend.rs:103-264) */
@@ -125,6 +126,16 @@ int fx_ctx_timing_end(fx_ctx *ctx, double *total_ms, unsigned long long *launche
  * state them; `bytes` may be NULL) through ms[] / points[] / bytes[]; *count = number written. */
 int fx_ctx_timing_end_records(fx_ctx *ctx, double *ms, double *points, double *bytes, size_t max,
                               size_t *count);
+
+/* Graph capture and replay (HipGraph, backend-hip/src/graph.rs:14-108).  Between begin and end,
+ * the operations enqueued on the context's stream are recorded (relaxed capture mode, as the
+ * reference's) instead of run; launch replays them on the context's stream.  Operations that
+ * return a host value (reductions, copies to the host, solves) cannot be recorded: they fail
+ * during capture and end then reports the capture as failed. */
+int fx_graph_begin(fx_ctx *ctx);                          /* HipGraph::begin_capture :35-46 */
+int fx_graph_end(fx_ctx *ctx, fx_graph **out);            /* HipGraph::end_capture :48-70 */
+int fx_graph_launch(fx_ctx *ctx, const fx_graph *graph);  /* HipGraph::launch :72-85 */
+int fx_graph_destroy(fx_graph *graph);                    /* Drop for HipGraph :88-99 */
 
 /* ------------------------------------------------------------------ */
 /* Memory (Backend::allocate / upload_f64 / upload_f32, backend.rs:49-77;
