@@ -272,7 +272,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from fluxion_b200 import CgSolver, DType, Device, Field, Multigrid, PipelinedCgSolver
+    from fluxion_b200 import CgSolver, DType, Device, Field, MixedPrecisionRefinement, Multigrid, PipelinedCgSolver
     from fluxion_b200 import _lib as L
     from fluxion_b200.workloads import dst_poisson_solve, neg_laplacian_residual, poisson_modes_rhs, \
         poisson_problem
@@ -293,6 +293,8 @@ def main():
     x = Field.zeros(P.grid, DType.F64, dev)
     cg = CgSolver(P.grid, dev, tol, 100)
     pcg_pipe = PipelinedCgSolver(P.grid, dev, tol, 100)
+    # FP64 iterative refinement around FP32 V-cycle PCG inner solves (inner tol 1e-4)
+    ir = MixedPrecisionRefinement(P.grid, dev, tol, 20, 1e-4, 100)
     mg64 = Multigrid.vertex(P.grid, None, dev, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, DType.F64)
     mg32 = Multigrid.vertex(P.grid, None, dev, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, DType.F32)
 
@@ -361,6 +363,8 @@ def main():
     # the FP32 cycle's rounding)
     pipe_ms, stp, _, _ = timed(mg64, args.steps, args.warmup, solver=pcg_pipe)
     up = x.to_vec_f64()
+    ir_ms, sti, _, _ = timed(mg32, args.steps, args.warmup, solver=ir)
+    ui = x.to_vec_f64()
 
     # verification in FP64 (plain operator) and against the exact DST-I solve
     u_ref = dst_poisson_solve(f, n)
@@ -369,6 +373,8 @@ def main():
     rr32 = neg_laplacian_residual(u32, f, n) / fnorm
     rr64 = neg_laplacian_residual(u64, f, n) / fnorm
     errp = float(np.linalg.norm(up - u_ref) / np.linalg.norm(u_ref))
+    erri = float(np.linalg.norm(ui - u_ref) / np.linalg.norm(u_ref))
+    rri = neg_laplacian_residual(ui, f, n) / fnorm
     rrp = neg_laplacian_residual(up, f, n) / fnorm
 
     # e2e: host f (pinned) -> solve -> host u (pinned), through the public API
@@ -461,6 +467,10 @@ def main():
             "pipelined_pcg": {"value": pipe_ms / 1e3, "unit": "s", "iterations": int(stp.iterations),
                               "rel_residual_fp64": rrp, "err_vs_fp64_direct": errp,
                               "solver": f"pipelined CG (Ghysels-Vanroose, preconditioned) + F64 {SOLVER}"},
+            "refinement_fp64_fp32_pcg": {"value": ir_ms / 1e3, "unit": "s", "outer_iterations": int(sti.iterations),
+                                         "inner_iterations": ir.last_inner_iterations, "rel_residual_fp64": rri,
+                                         "err_vs_fp64_direct": erri,
+                                         "solver": f"FP64 refinement, FP32 CG + F32 {SOLVER} inner to 1e-4"},
             "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": N * N * 8,
                     "d2h_bytes_per_step": N * N * 8, "result_matches_device_run": e2e_ok},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),

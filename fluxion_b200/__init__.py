@@ -14,19 +14,21 @@ __all__ = [
     "CudaBackend", "CudaBuffer", "BackendUnavailable", "InvalidArgument", "Device", "Field", "DeviceMismatch",
     "CgSolver", "CgStats", "PipelinedCgSolver", "BiCgStabSolver", "GmresSolver", "Multigrid", "SmootherKind",
     "Identity", "Preconditioner", "LinearSolver", "SolveStats", "ConvergenceReason",
+    "MixedPrecisionRefinement", "CudaGraph",
 ]
 
 
 def __getattr__(name):
     # The backend-facing classes load libfluxion_cuda.so; import them lazily so that the
     # core data types stay importable where the library has not been built.
-    if name in ("CudaBackend", "CudaBuffer", "BackendUnavailable", "InvalidArgument"):
+    if name in ("CudaBackend", "CudaBuffer", "BackendUnavailable", "InvalidArgument", "CudaGraph"):
         from . import backend
         return getattr(backend, name)
     if name in ("Device", "Field", "DeviceMismatch"):
         from . import field
         return getattr(field, name)
     if name in ("CgSolver", "CgStats", "PipelinedCgSolver", "BiCgStabSolver", "GmresSolver", "Multigrid",
+                "MixedPrecisionRefinement",
                 "SmootherKind", "Identity", "Preconditioner", "LinearSolver", "SolveStats",
                 "ConvergenceReason"):
         from . import solvers

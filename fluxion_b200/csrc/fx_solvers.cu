@@ -579,8 +579,14 @@ bool fusable(const fx_mg *m) {
 
 int fx_mg::View::apply_pcg(fx_buf *z, const fx_buf *r, const int *skip, DevState *S, bool first) {
     fx_mg *m = mg;
-    if (!fusable(m) || z->dtype != FX_F64 || r->dtype != FX_F64 || z->len != m->lv[0].rows * m->lv[0].cols)
-        return FX_ERR_UNSUPPORTED;
+    if (!fusable(m) || z->len != m->lv[0].rows * m->lv[0].cols || z->dtype != r->dtype) return FX_ERR_UNSUPPORTED;
+    if (z->dtype == FX_F32) {  // single-precision vectors (the inner solves of iterative refinement)
+        if (m->dtype != FX_F32) return FX_ERR_UNSUPPORTED;
+        const float *b0 = (const float *)r->ptr;
+        float *z0 = (float *)z->ptr;
+        if (first) return fused_cycle<float, float, float, true>(m, b0, z0, FinPcgRzInit{S}, skip);
+        return fused_cycle<float, float, float, true>(m, b0, z0, FinPcgRz{S}, skip);
+    }
     const double *b0 = (const double *)r->ptr;
     double *z0 = (double *)z->ptr;
     if (m->dtype == FX_F64) {
@@ -641,17 +647,19 @@ struct SolverBase {
     DevState *d_st = nullptr;
     DevState *h_st = nullptr;
     std::vector<fx_buf *> bufs;
+    int dtype = FX_F64;  // of the solver's vectors (x, b and the work vectors)
 
-    int init_base(fx_ctx *c, const fx_grid *grid, double t, size_t mi, int nvec) {
+    int init_base(fx_ctx *c, const fx_grid *grid, double t, size_t mi, int nvec, int dt = FX_F64) {
         ctx = c;
         g = *grid;
         tol = t;
         max_iter = mi;
+        dtype = dt;
         FX_CUDA(cudaMalloc(&d_st, sizeof(DevState)));
         FX_CUDA(cudaMallocHost(&h_st, sizeof(DevState)));
         for (int i = 0; i < nvec; i++) {
             fx_buf *b = nullptr;
-            FX_TRY(fx_alloc(ctx, g.rows * g.cols, FX_F64, &b));
+            FX_TRY(fx_alloc(ctx, g.rows * g.cols, dt, &b));
             bufs.push_back(b);
         }
         return FX_OK;
@@ -681,8 +689,9 @@ struct SolverBase {
         FX_TRY(check_buf(b, "b"));
         FX_TRY(check_grid_len(&g, x));
         FX_TRY(check_grid_len(&g, b));
-        if (x->dtype != FX_F64 || b->dtype != FX_F64)
-            return fail(FX_ERR_INVALID_ARGUMENT, "solver vectors must be F64");
+        if (x->dtype != dtype || b->dtype != dtype)
+            return fail(FX_ERR_INVALID_ARGUMENT, dtype == FX_F64 ? "solver vectors must be F64"
+                                                                   : "solver vectors must be F32");
         return FX_OK;
     }
     // Run `step(i)` for i = 0, 1, ... until the device says done.  Iterations are enqueued
@@ -860,10 +869,10 @@ struct fx_cg : SolverBase {
 
 namespace {
 
-template <int MODE>
+template <typename T, int MODE>
 int cg_solve_impl(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
-    using T = double;
     fx_ctx *ctx = s->ctx;
+    constexpr int DT = sizeof(T) == 8 ? FX_F64 : FX_F32;
     const size_t RR = s->g.rows, CC = s->g.cols;
     OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
     T *r = (T *)s->bufs[0]->ptr, *z = (T *)s->bufs[1]->ptr;
@@ -891,7 +900,7 @@ int cg_solve_impl(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const Sten
     // preconditioned (cg.rs:178-256)
     FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, r, nullptr}, FinPcgResid{S},
                                   nullptr, "pcg_init")));
-    fx_buf rb{ctx, r, n, FX_F64, false}, zb{ctx, z, n, FX_F64, false};
+    fx_buf rb{ctx, r, n, DT, false}, zb{ctx, z, n, DT, false};
     // z = M^-1 r and rz = r.z, fused into the preconditioner when it has a fused form
     auto precondition = [&](bool first) -> int {
         const int st = pc->apply_pcg(&zb, &rb, halt, S, first);
@@ -1193,6 +1202,91 @@ int ppcg_solve_impl(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff
                                      FinPpcgIter{S}, halt, "ppcg_iter");
     };
     return s->drive(step, s->max_iter + 1, true);
+}
+
+// ------------------------------------------------ mixed-precision iterative refinement
+//
+// New (the reference has no refinement loop): FP64 iterative refinement around FP32
+// preconditioned CG.  FP64 appears only in the outer residual r = b - A x (with its norm) and
+// the update x += d; the inner solve A d = r runs on FP32 vectors with an FP32 V-cycle, its inner
+// products and scalars still compensated FP64.
+
+template <int MODE>
+struct PtIrResid {  // r32 = (float)(b - A x), computed in FP64; reduction ||b - A x||^2
+    static constexpr int NA = 1;
+    OpA<double, MODE> A;
+    const double *b;
+    float *r32;
+    __device__ __forceinline__ const double *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<double> &nb,
+                                               const double *a, CSum *acc) const {
+        const double rv = fx_fma(-1.0, A.apply(ring, nb), a[0]);
+        r32[idx] = (float)rv;
+        csum_add_prod(acc[0], rv, rv);
+    }
+};
+
+struct FlatIrUpdate {  // x += (double)d
+    double *x;
+    const float *d;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const { x[i] = x[i] + (double)d[i]; }
+};
+
+}  // namespace
+
+struct fx_ir : SolverBase {
+    // bufs (F32): 0 r32 (outer residual, the inner right-hand side), 1 d (the correction)
+    double inner_tol = 1e-4;  // inner stop: ||r_inner|| < inner_tol * ||r_outer||
+    size_t inner_max_iter = 100;
+    fx_cg *inner = nullptr;  // FP32 preconditioned CG
+    size_t inner_total = 0;
+    ~fx_ir() override { delete inner; }
+};
+
+namespace {
+
+template <int MODE>
+int ir_solve_impl(fx_ir *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st, const fx_boundaries *bc,
+                  const StencilP &P, fx_precond *pc) {
+    fx_ctx *ctx = s->ctx;
+    const size_t RR = s->g.rows, CC = s->g.cols, n = RR * CC;
+    OpA<double, MODE> A{P, coeff, (int)RR, (int)CC};
+    float *r32 = (float *)s->bufs[0]->ptr, *d = (float *)s->bufs[1]->ptr;
+    double *xp = (double *)x->ptr;
+    const double *bp = (const double *)b->ptr;
+    s->inner_total = 0;
+    DevState &H = *s->h_st;
+    std::memset(&H, 0, sizeof(H));
+    for (size_t k = 0;; k++) {
+        FX_TRY((launch_march<double, 1>(ctx, RR, CC, Ld1<double>{xp}, PtIrResid<MODE>{A, bp, r32},
+                                          StoreFin<1>{ctx->d_result}, nullptr, "ir_residual")));
+        double rr = 0;
+        FX_TRY(read_results(ctx, 1, &rr));
+        const double rnorm = std::sqrt(rr);
+        H.iter = (long long)k;
+        H.resid = rnorm;
+        if (k == 0) H.r0 = rnorm;
+        if (rnorm < s->tol) {
+            H.reason = FX_CONVERGED;
+            return FX_OK;
+        }
+        if (k >= s->max_iter) {
+            H.reason = FX_MAX_ITERATIONS;
+            return FX_OK;
+        }
+        FX_CUDA(cudaMemsetAsync(d, 0, n * sizeof(float), ctx->stream));
+        s->inner->tol = s->inner_tol * rnorm;
+        s->inner->max_iter = s->inner_max_iter;
+        FX_TRY((cg_solve_impl<float, MODE>(s->inner, s->bufs[1], s->bufs[0], coeff, P, pc)));
+        s->inner_total += (size_t)s->inner->h_st->iter;
+        if (s->inner->h_st->reason == FX_BREAKDOWN && s->inner->h_st->iter == 0) {
+            H.reason = FX_BREAKDOWN;
+            return FX_OK;
+        }
+        FX_TRY(launch_flat<0>(ctx, n, FlatIrUpdate{xp, d}, NoFin{}, nullptr, "ir_update"));
+    }
+    (void)st;
+    (void)bc;
 }
 
 // ------------------------------------------------ BiCGSTAB (bicgstab.rs:90-346)
@@ -1721,12 +1815,13 @@ int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, cons
 }
 
 template <typename Solver>
-int create_solver(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, int nvec, Solver **out) {
+int create_solver(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, int nvec, Solver **out,
+                  int dtype = FX_F64) {
     if (!ctx || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     FX_TRY(check_grid(g));
     *out = nullptr;
     Solver *s = new Solver();
-    int st = s->init_base(ctx, g, tol, max_iter, nvec);
+    int st = s->init_base(ctx, g, tol, max_iter, nvec, dtype);
     if (st) {
         delete s;
         return st;
@@ -1939,7 +2034,8 @@ static int cg_entry(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx
     FX_TRY(s->check_io(x, b));
     StencilP P;
     FX_TRY(prep_op(s->g, st, bc, &P));
-    SOLVER_MODE_DISPATCH(P, FX_TRY(cg_solve_impl<MODE>(s, x, b, coeff, P, pc)));
+    if (s->dtype == FX_F32) SOLVER_MODE_DISPATCH(P, FX_TRY((cg_solve_impl<float, MODE>(s, x, b, coeff, P, pc))));
+    else SOLVER_MODE_DISPATCH(P, FX_TRY((cg_solve_impl<double, MODE>(s, x, b, coeff, P, pc))));
     s->stats(out);
     return FX_OK;
 }
@@ -1991,6 +2087,42 @@ int fx_pipelined_cg_solve_preconditioned(fx_pipelined_cg *s, fx_buf *x, const fx
     FX_TRY(prep_op(s->g, st, bc, &P));
     SOLVER_MODE_DISPATCH(P, FX_TRY(ppcg_solve_impl<MODE>(s, x, b, coeff, P, pc)));
     s->stats(out);
+    return FX_OK;
+}
+
+// ---- mixed-precision iterative refinement
+
+int fx_ir_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_outer, double inner_tol,
+                 size_t inner_max_iter, fx_ir **out) {
+    if (!(inner_tol > 0 && inner_tol < 1)) return fail(FX_ERR_INVALID_ARGUMENT, "inner_tol must lie in (0, 1)");
+    FX_TRY(create_solver(ctx, g, tol, max_outer, 2, out, FX_F32));
+    (*out)->inner_tol = inner_tol;
+    (*out)->inner_max_iter = inner_max_iter;
+    const int st = create_solver(ctx, g, 0.0, inner_max_iter, 4, &(*out)->inner, FX_F32);
+    if (st) {
+        delete *out;
+        *out = nullptr;
+    }
+    return st;
+}
+int fx_ir_destroy(fx_ir *s) {
+    delete s;
+    return FX_OK;
+}
+int fx_ir_solve_preconditioned(fx_ir *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                               const fx_boundaries *bc, fx_precond *pc, fx_stats *out, size_t *inner_iterations) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
+    FX_TRY(check_buf(x, "x"));
+    FX_TRY(check_buf(b, "b"));
+    FX_TRY(check_grid_len(&s->g, x));
+    FX_TRY(check_grid_len(&s->g, b));
+    if (x->dtype != FX_F64 || b->dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "x and b must be F64");
+    StencilP P;
+    FX_TRY(prep_op(s->g, st, bc, &P));
+    SOLVER_MODE_DISPATCH(P, FX_TRY(ir_solve_impl<MODE>(s, x, b, coeff, st, bc, P, pc)));
+    s->stats(out);
+    if (inner_iterations) *inner_iterations = s->inner_total;
     return FX_OK;
 }
 

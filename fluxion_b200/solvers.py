@@ -267,6 +267,49 @@ class PipelinedCgSolver(_Native):
         return "PipelinedCG"
 
 
+class MixedPrecisionRefinement:
+    """FP64 iterative refinement around FP32 preconditioned CG (new: the reference has no
+    refinement loop).  Each outer step computes r = b - A x and ||r||_2 in FP64, stops when
+    ||r||_2 < tol or after `max_outer` corrections, and otherwise solves A d = r on FP32 vectors
+    with the preconditioner (an FP32 vertex multigrid) until ||r_inner||_2 < inner_tol ||r||_2,
+    then updates x += d in FP64.  Inner products and CG scalars stay compensated FP64.  x and b
+    are FP64 fields; `last_inner_iterations` holds the inner CG iterations of the last solve."""
+
+    def __init__(self, grid: Grid, device: Optional[Device] = None, tol: float = 1e-8, max_outer: int = 20,
+                 inner_tol: float = 1e-4, inner_max_iter: int = 100):
+        self.device = device or Device.best()
+        self.grid = grid
+        self.tol, self.max_outer = float(tol), int(max_outer)
+        self.inner_tol, self.inner_max_iter = float(inner_tol), int(inner_max_iter)
+        self.last_inner_iterations = 0
+        out = C.c_void_p()
+        g = grid_c(grid)
+        check(L.lib().fx_ir_create(self.device.backend().ctx, C.byref(g), self.tol, self.max_outer,
+                                   self.inner_tol, self.inner_max_iter, C.byref(out)))
+        self.h = out.value
+
+    def solve_preconditioned(self, x, b, coeff, stencil, boundaries, pc: Preconditioner) -> SolveStats:
+        sc = StencilC(stencil)
+        bc = bcs_c(boundaries)
+        st = L.FxStats()
+        inner = C.c_size_t()
+        check(L.lib().fx_ir_solve_preconditioned(self.h, x.storage.handle, b.storage.handle, float(coeff), sc.ptr,
+                                                 C.byref(bc), pc._handle(self.device), C.byref(st), C.byref(inner)))
+        self.last_inner_iterations = int(inner.value)
+        return _stats(st)
+
+    def name(self) -> str:
+        return "FP64 refinement / FP32 PCG"
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().fx_ir_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
 class BiCgStabSolver(_Native):
     """bicgstab.rs:19-346."""
 

@@ -97,6 +97,7 @@ typedef struct fx_pipelined_cg fx_pipelined_cg;
 typedef struct fx_bicgstab fx_bicgstab;
 typedef struct fx_gmres fx_gmres;
 typedef struct fx_graph fx_graph;
+typedef struct fx_ir fx_ir;
 
 /* ------------------------------------------------------------------ */
 /* Context (HipBackend::new / singleton, backend-hip/src/backend.rs:103-264) */
@@ -324,6 +325,21 @@ int fx_pipelined_cg_solve(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double
 int fx_pipelined_cg_solve_preconditioned(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff,
                                          const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
                                          fx_stats *out);
+
+/* Mixed-precision iterative refinement (new: the reference has no refinement loop).  FP64
+ * refinement x += d around FP32 preconditioned CG: each outer step computes r = b - A x and its
+ * norm in FP64 (one pass that also writes r in FP32), stops when ||r||_2 < tol (absolute, as the
+ * solvers' tol) or after max_outer corrections, and otherwise solves A d = r on FP32 vectors
+ * with `pc` (which must accept FP32 vectors, e.g. an FX_F32 vertex multigrid) until
+ * ||r_inner||_2 < inner_tol * ||r||_2 or inner_max_iter iterations.  The inner products and CG
+ * scalars stay compensated FP64.  x and b are F64.  out->iterations counts the corrections;
+ * *inner_iterations (may be NULL) the inner CG iterations over all of them. */
+int fx_ir_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_outer, double inner_tol,
+                 size_t inner_max_iter, fx_ir **out);
+int fx_ir_destroy(fx_ir *s);
+int fx_ir_solve_preconditioned(fx_ir *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                               const fx_boundaries *bc, fx_precond *pc, fx_stats *out,
+                               size_t *inner_iterations);
 
 /* BiCgStabSolver (bicgstab.rs:19-346) */
 int fx_bicgstab_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter,

@@ -344,3 +344,56 @@ def test_pipelined_pcg_identity_matches_pipelined_cg(dev):
     s2 = PipelinedCgSolver(P.grid, dev, tol, 2000).solve_preconditioned(x2, b, P.coeff, P.stencil, None, Identity())
     assert s1.converged() and s2.converged() and abs(s1.iterations - s2.iterations) <= 1
     assert rel_err(x2.to_vec_f64(), x1.to_vec_f64()) < 1e-8
+
+
+# ---------------------------------------------------------------- mixed-precision refinement
+
+@pytest.mark.parametrize("n", [511, 1023])
+def test_iterative_refinement_reaches_fp64_accuracy(dev, n):
+    """FP64 refinement around FP32 V-cycle PCG (inner tol 1e-4) reaches rel. residual 1e-10,
+    recomputed in FP64 with the plain operator, and the FP64 direct solution to 1e-8."""
+    from fluxion_b200 import DType, Field, MixedPrecisionRefinement, Multigrid
+    from fluxion_b200.workloads import dst_poisson_solve, neg_laplacian_residual, poisson_problem, \
+        poisson_modes_rhs
+    P = poisson_problem(n)
+    f = poisson_modes_rhs(n, seed=31)
+    fn = float(np.linalg.norm(f))
+    b = Field.from_f64(P.grid, f, dev)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    mg = Multigrid.vertex(P.grid, None, dev, dtype=DType.F32)
+    ir = MixedPrecisionRefinement(P.grid, dev, 1e-10 * fn, 20, 1e-4, 100)
+    s = ir.solve_preconditioned(x, b, P.coeff, P.stencil, None, mg)
+    assert s.converged() and 1 <= s.iterations <= 6 and ir.last_inner_iterations >= s.iterations
+    u = x.to_vec_f64()
+    assert neg_laplacian_residual(u, f, n) < 1.01e-10 * fn
+    assert rel_err(u, dst_poisson_solve(f, n)) < 1e-8
+
+
+def test_iterative_refinement_matches_fp64_pcg(dev):
+    from fluxion_b200 import CgSolver, DType, Field, MixedPrecisionRefinement, Multigrid
+    from fluxion_b200.workloads import poisson_problem, poisson_uniform_rhs
+    n = 255
+    P = poisson_problem(n)
+    f = poisson_uniform_rhs(n, seed=8)
+    tol = 1e-10 * float(np.linalg.norm(f))
+    b = Field.from_f64(P.grid, f, dev)
+    x1, x2 = Field.zeros(P.grid, DType.F64, dev), Field.zeros(P.grid, DType.F64, dev)
+    assert CgSolver(P.grid, dev, tol, 100).solve_preconditioned(
+        x1, b, P.coeff, P.stencil, None, Multigrid.vertex(P.grid, None, dev)).converged()
+    ir = MixedPrecisionRefinement(P.grid, dev, tol)
+    assert ir.solve_preconditioned(x2, b, P.coeff, P.stencil, None,
+                                   Multigrid.vertex(P.grid, None, dev, dtype=DType.F32)).converged()
+    assert rel_err(x2.to_vec_f64(), x1.to_vec_f64()) < 1e-8
+
+
+def test_iterative_refinement_needs_a_single_precision_preconditioner(dev):
+    from fluxion_b200 import CoreError, DType, Field, MixedPrecisionRefinement, Multigrid
+    from fluxion_b200.workloads import poisson_problem, poisson_uniform_rhs
+    n = 63
+    P = poisson_problem(n)
+    f = poisson_uniform_rhs(n, seed=2)
+    b = Field.from_f64(P.grid, f, dev)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    ir = MixedPrecisionRefinement(P.grid, dev, 1e-8)
+    with pytest.raises(Exception):
+        ir.solve_preconditioned(x, b, P.coeff, P.stencil, None, Multigrid.vertex(P.grid, None, dev))
