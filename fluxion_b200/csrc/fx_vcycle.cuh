@@ -7,6 +7,8 @@
 // bitwise equal to the unfused one.
 #pragma once
 
+#include <type_traits>
+
 #include "fx_points.cuh"
 
 namespace fx {
@@ -16,6 +18,12 @@ struct VOp {
     A5<T> a;
     T wd;  // omega / a_c
 };
+
+// a.c c + a.n n + a.s s + a.w w + a.e e, in the order of op5 (fx_points.cuh)
+template <typename T>
+__device__ __forceinline__ T op5v(const A5<T> &a, T c, T n, T s, T w, T e) {
+    return fx_fma(a.c, c, fx_fma(a.n, n, fx_fma(a.s, s, fx_fma(a.w, w, a.e * e))));
+}
 
 // Bilinear interpolation of the coarse correction at fine point (r, c), the same expression
 // per parity case as the separate prolongation kernel, selected without divergence.
@@ -35,10 +43,12 @@ __device__ __forceinline__ T bil_interp(const T *__restrict__ e, int ccols, int 
 
 // ---------------------------------------------------------------- tail
 //
-// The coarse end of the cycle in one block: from the first level whose working set fits in
-// shared memory down to the coarsest solve and back up.  On these grids a band launch is
-// latency-bound (a few dozen rows marched in sequence, 15-20 us per launch whatever the
-// size), while one 1024-thread block evaluates a whole level phase in a microsecond or two.
+// The coarse end of the cycle in one block: from the first level of at most 9 x 1024 points
+// (65 x 65 on 2^k + 1 grids) whose working set fits in shared memory, down to the coarsest
+// solve and back up.  Below that size a strip launch costs a few microseconds of latency
+// whatever the level's size, while one 1024-thread block evaluates a phase of a 65 x 65 level
+// in about a microsecond.  A 129 x 129 level is past the crossover: one block spends about
+// 20 us on its two legs, more than its two strip launches take.
 //
 // Shared memory, for a first tail level of n0 points:
 //   X [n0]  its pre-smoothed x2, kept for the up leg (and turned into x2 + P e in place);
@@ -59,7 +69,7 @@ constexpr size_t kTailSmemMax = 200 * 1024;  // of the 227 KB a block may opt in
 // most points per thread of the first tail level (its rhs is held in registers once)
 template <typename T>
 __host__ __device__ constexpr int tail_kt() {
-    return sizeof(T) == 4 ? 17 : 9;
+    return 9;
 }
 
 template <typename T>
@@ -98,6 +108,74 @@ __device__ __forceinline__ void jacobi_pts(const T *__restrict__ src, T *__restr
 #pragma unroll
     for (int q = 0; q < NP; q++)
         if (cp[q] >= 0) dst[cp[q]] = v[q];
+}
+
+// Largest coarsest grid, ring included, that one warp solves from registers (F32 only: at
+// the 64 registers a thread of the 1024-thread tail may use, the F64 blocks spill and the
+// shared-memory sweeps are faster).
+constexpr int kWarpCoarseMax = 17;
+
+// `sweeps` weighted-Jacobi sweeps from zero on a coarsest grid of at most 17 x 17 points, by
+// one warp with no barrier.  Lane l holds, in registers, the 4 x 2 block of rows
+// 1 + 4 (l >> 3) + i and columns 1 + 2 (l & 7) + j (i < 4, j < 2): the four block rows and
+// eight block columns cover rows and columns 1 .. 16.  Points that are not interior (the
+// ring, or outside the grid) are held at 0.  A block's outer neighbours come by shuffle from
+// lanes (l - 1), (l + 1), (l - 8) and (l + 8) mod 32.  Where that wraps around the block
+// layout it lands on layout row or column 16, which an interior of at most 15 x 15 leaves
+// empty, so those neighbours are 0, as the ring is.  The update is the expression of
+// jacobi_pts, so the result equals the shared-memory sweeps bit for bit.  out (rows x cols,
+// ring already 0) receives the interior.
+template <typename T>
+__device__ __forceinline__ void coarse_warp(const T *B, T *out, int rows, int cols, const VOp<T> &op, int sweeps) {
+    constexpr unsigned kAll = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int r0 = 1 + 4 * (lane >> 3), c0 = 1 + 2 * (lane & 7);
+    const int lw = (lane + 31) & 31, le = (lane + 1) & 31, ln = (lane + 24) & 31, ls = (lane + 8) & 31;
+    T x[4][2], b[4][2];
+    bool in[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            in[i][j] = r0 + i <= rows - 2 && c0 + j <= cols - 2;
+            b[i][j] = in[i][j] ? B[(r0 + i) * cols + c0 + j] : (T)0;
+            x[i][j] = (T)0;
+        }
+#pragma unroll 2  // two sweeps per pass let the compiler overlap one's shuffles with the other's math
+    for (int k = 0; k < sweeps; k++) {
+        T w[4], e[4], n[2], s[2];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            w[i] = __shfl_sync(kAll, x[i][1], lw);
+            e[i] = __shfl_sync(kAll, x[i][0], le);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            n[j] = __shfl_sync(kAll, x[3][j], ln);
+            s[j] = __shfl_sync(kAll, x[0][j], ls);
+        }
+        T v[4][2];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const T c = x[i][j];
+                const T nn = i == 0 ? n[j] : x[i - 1][j];
+                const T ss = i == 3 ? s[j] : x[i + 1][j];
+                const T ww = j == 0 ? w[i] : x[i][0];
+                const T ee = j == 1 ? e[i] : x[i][1];
+                v[i][j] = in[i][j] ? fx_fma(op.wd, b[i][j] - op5v(op.a, c, nn, ss, ww, ee), c) : (T)0;
+            }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 2; j++) x[i][j] = v[i][j];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+            if (in[i][j]) out[(r0 + i) * cols + c0 + j] = x[i][j];
 }
 
 template <typename T>
@@ -222,8 +300,10 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vtail(TailArgs<T> A, const 
         __syncthreads();
     }
 
-    // ---- coarsest: `coarse_sweeps` weighted-Jacobi sweeps from zero, P <-> Q.  Each of the
-    // first warps owns up to 4 points (rhs in registers); a named barrier joins them.
+    // ---- coarsest: `coarse_sweeps` weighted-Jacobi sweeps from zero.  Up to 17 x 17 points,
+    // warp 0 alone from registers; larger, P <-> Q in shared memory, each of the first warps
+    // owning up to 4 points (rhs in registers) and a named barrier joining them.  Either way
+    // the result lands in P for an even sweep count and in Q for an odd one.
     {
         const int l = nlev - 1, rows = A.rows[l], cols = A.cols[l], n = rows * cols;
         const VOp<T> op = A.op[l];
@@ -233,10 +313,15 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vtail(TailArgs<T> A, const 
             Q[p] = (T)0;
         }
         __syncthreads();
-        {
-            constexpr int kPts = 4;  // n <= 4096
-            const int nthr = min(kTailThreads, ((n + 31) / 32) * 32);
-            if (tid < nthr) {
+        if (sizeof(T) == 4 && rows <= kWarpCoarseMax && cols <= kWarpCoarseMax) {
+            if (tid < 32) coarse_warp<T>(B, (A.coarse_sweeps & 1) ? Q : P, rows, cols, op, A.coarse_sweeps);
+        } else {
+            // kPts points per thread: 1 while n fits the block (a predicated-off point still
+            // costs its instructions every sweep), else 4 (n <= 4096)
+            auto smem_sweeps = [&](auto kp) {
+                constexpr int kPts = decltype(kp)::value;
+                const int nthr = min(kTailThreads, ((n + 31) / 32) * 32);
+                if (tid >= nthr) return;
                 int cp[kPts];
                 T cb[kPts];
 #pragma unroll
@@ -252,7 +337,9 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vtail(TailArgs<T> A, const 
                     else jacobi_pts<T, kPts>(P, Q, cp, cb, op, cols);
                     asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory");
                 }
-            }
+            };
+            if (n <= kTailThreads) smem_sweeps(std::integral_constant<int, 1>{});
+            else smem_sweeps(std::integral_constant<int, 4>{});
         }
         __syncthreads();
         if (nlev == 1) {

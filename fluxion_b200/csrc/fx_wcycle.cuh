@@ -66,12 +66,6 @@ __device__ __forceinline__ float shfl_e(float v) { return __shfl_down_sync(0xfff
 __device__ __forceinline__ double shfl_w(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ double shfl_e(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 
-// a.c c + a.n n + a.s s + a.w w + a.e e, in the order of op5 (fx_points.cuh)
-template <typename T>
-__device__ __forceinline__ T op5v(const A5<T> &a, T c, T n, T s, T w, T e) {
-    return fx_fma(a.c, c, fx_fma(a.n, n, fx_fma(a.s, s, fx_fma(a.w, w, a.e * e))));
-}
-
 // Two adjacent columns per lane: lane l of a strip holds columns ca = sb + 2l (even) and
 // cb = ca + 1, so one shuffle per stage gives both points their outer neighbour, the column
 // parity of every register is fixed, and a strip spans 64 columns.  A step whose rows all lie

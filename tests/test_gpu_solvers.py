@@ -215,11 +215,12 @@ def test_vertex_mg_vcycle_bitwise(dev, n):
 
 
 @pytest.mark.parametrize("n", [15, 63, 255, 1023])
-@pytest.mark.parametrize("cm,cs", [(15, 200), (7, 30), (3, 10)])
+@pytest.mark.parametrize("cm,cs", [(15, 200), (7, 30), (3, 10), (31, 40)])
 def test_fused_vcycle_bitwise(dev, n, cm, cs):
     """The fused V(2,2) kernels (zero initial guess) equal the oracle's separate sweeps, residual,
     full weighting and bilinear prolongation bit for bit (F64), and the fused F32 cycle equals
-    the unfused F32 cycle bit for bit."""
+    the unfused F32 cycle bit for bit.  Coarsest grids of up to 17 x 17 points are solved by one
+    warp from registers, larger ones (coarse_max 31: 33 x 33) in shared memory."""
     from fluxion_b200 import DType, Field, Multigrid
     from fluxion_b200.workloads import poisson_problem
     P = poisson_problem(n)
@@ -242,6 +243,39 @@ def test_fused_vcycle_bitwise(dev, n, cm, cs):
     mg32.precondition(zf, b)
     zu = Field.zeros(P.grid, DType.F64, dev)
     mg32.v_cycle(zu, b)  # unfused path (explicit initial guess)
+    assert np.array_equal(zf.to_vec_f64(), zu.to_vec_f64())
+    assert rel_err(zf.to_vec_f64(), zo) < 1e-5
+
+
+@pytest.mark.parametrize("rows,cols,cm", [(65, 257, 15), (257, 65, 15), (33, 65, 7), (65, 33, 7)])
+def test_fused_vcycle_bitwise_rectangular(dev, rows, cols, cm):
+    """On rectangular grids coarsening stops when either interior side reaches coarse_max, so
+    the coarsest grid is long in one direction (17 x 65, 65 x 17: shared-memory sweeps) or
+    short in both but not square (9 x 17, 17 x 9: one warp).  The fused cycle still equals
+    the oracle's bit for bit (F64), and the fused F32 cycle the unfused F32 one."""
+    from fluxion_b200 import DType, Field, Grid, Multigrid, Stencil
+    dx, dy = 1.0 / (cols - 1), 1.0 / (rows - 1)
+    g = Grid.new(rows, cols, dx, dy)
+    st = Stencil.poisson_neg_laplacian(dx, dy)
+    rng = np.random.default_rng(rows * 1000 + cols)
+    bvec = np.zeros((rows, cols))
+    bvec[1:-1, 1:-1] = rng.uniform(-1, 1, (rows - 2, cols - 2))
+    bvec = bvec.ravel()
+    b = Field.from_f64(g, bvec, dev)
+    mg = Multigrid.vertex(g, None, dev, 2, 2, 0.8, cm, 60)
+    z = Field.zeros(g, DType.F64, dev)
+    mg.precondition(z, b)
+    omg = O.Multigrid(rows, cols, dx, dy, 2, 2, 0.8, mode=1, op_coeff=1.0, entries=st.as_triples(),
+                      coarse_max=cm, coarse_sweeps=60)
+    assert mg.depth() == omg.depth() >= 3
+    zo = np.zeros(rows * cols)
+    omg.v_cycle(zo, bvec)
+    assert np.array_equal(z.to_vec_f64(), zo)
+    mg32 = Multigrid.vertex(g, None, dev, 2, 2, 0.8, cm, 60, DType.F32)
+    zf = Field.zeros(g, DType.F64, dev)
+    mg32.precondition(zf, b)
+    zu = Field.zeros(g, DType.F64, dev)
+    mg32.v_cycle(zu, b)
     assert np.array_equal(zf.to_vec_f64(), zu.to_vec_f64())
     assert rel_err(zf.to_vec_f64(), zo) < 1e-5
 
