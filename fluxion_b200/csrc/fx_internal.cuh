@@ -116,8 +116,10 @@ inline size_t elem_size(int dtype) { return dtype == FX_F32 ? 4 : 8; }
 // Error-free transformations (Knuth TwoSum; TwoProduct via fma, Ogita-Rump-Oishi 2005).
 // Every kernel here is compiled with -fmad=false, so no expression below is contracted.
 
+// s + c: the compensated sum.  p: a plain partial of the products added by csum_fma since the
+// last csum_flush (value-initialised to 0 by CSum{s, c}).
 struct CSum {
-    double s, c;
+    double s, c, p;
 };
 
 __device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
@@ -142,6 +144,35 @@ __device__ __forceinline__ void csum_add_prod(CSum &acc, double a, double b) {
     acc.c += e + pe;
 }
 
+// Partial form for the solvers' quadratic forms (p.Ap, r.r, r.z, ...), whose terms are mostly of
+// one sign: each product goes into the thread's plain partial with one fma, and the partial is
+// folded into the compensated sum once, when the reduction starts (warp_reduce); the sums
+// across threads, blocks and the grid stay compensated.  A thread's partial holds its share
+// of the grid (rows x cols / resident threads: about 150 terms per thread on a 4097 x 4097 F64
+// grid), so the result is within n u sum|terms| for n terms per thread, against u sum|terms|
+// for a Kahan sum of rounded products.  It costs one FP64 operation per term instead of
+// csum_add_prod's ten, which is what keeps the level-0 passes memory-bound rather than
+// FP64-bound.  Flushing every few rows inside the marching loops measured 20 us slower per
+// 4097 x 4097 pass.  Dots whose terms may cancel (the BLAS-1 dot, BiCGSTAB, GMRES) keep
+// csum_add_prod.
+__device__ __forceinline__ void csum_fma(CSum &acc, double a, double b) { acc.p = fma(a, b, acc.p); }
+
+__device__ __forceinline__ void csum_flush(CSum &acc) {
+    double s, e;
+    two_sum(acc.s, acc.p, s, e);
+    acc.s = s;
+    acc.c += e;
+    acc.p = 0.0;
+}
+
+// all accumulators of a thread that hold a partial
+template <int K>
+__device__ __forceinline__ void csum_flush_all(CSum (&acc)[K]) {
+#pragma unroll
+    for (int k = 0; k < K; k++)
+        if (acc[k].p != 0.0) csum_flush(acc[k]);
+}
+
 __device__ __forceinline__ CSum csum_merge(CSum a, CSum b) {
     double s, e;
     two_sum(a.s, b.s, s, e);
@@ -163,6 +194,7 @@ struct RedArgs {
 
 template <int K>
 __device__ __forceinline__ void warp_reduce(CSum (&acc)[K]) {
+    csum_flush_all<K>(acc);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll

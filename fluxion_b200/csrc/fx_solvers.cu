@@ -766,7 +766,7 @@ struct PtInitResid {
         const T rv = fx_fma((T)-1, ax, a[0]);
         r[idx] = rv;
         if (r2) r2[idx] = rv;
-        csum_add_prod(acc[0], (double)rv, (double)rv);
+        csum_fma(acc[0], (double)rv, (double)rv);
     }
 };
 
@@ -793,7 +793,7 @@ struct PtCgDir {
     __device__ __forceinline__ void operator()(bool ring, int r, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
         p_new[idx] = nb.c;
         const T ap = A.apply(ring, nb);
-        csum_add_prod(acc[0], (double)nb.c, (double)ap);
+        csum_fma(acc[0], (double)nb.c, (double)ap);
     }
 };
 
@@ -824,7 +824,7 @@ struct PtCgUpd {
         x[idx] = fx_fma(alpha, nb.c, a[0]);
         const T rv = fx_fma(-alpha, ap, a[1]);
         r[idx] = rv;
-        csum_add_prod(acc[0], (double)rv, (double)rv);
+        csum_fma(acc[0], (double)rv, (double)rv);
     }
 };
 
@@ -948,8 +948,8 @@ struct PtPipeInitW {  // w = A r; p = t = z = 0; reductions (r.r, r.w)
         p[idx] = (T)0;
         t[idx] = (T)0;
         z[idx] = (T)0;
-        csum_add_prod(acc[0], (double)nb.c, (double)nb.c);
-        csum_add_prod(acc[1], (double)nb.c, (double)wv);
+        csum_fma(acc[0], (double)nb.c, (double)nb.c);
+        csum_fma(acc[1], (double)nb.c, (double)wv);
     }
 };
 
@@ -1005,8 +1005,8 @@ struct PtPipeIter {
         const T wn = fx_fma(-alpha, zn, w);
         r[idx] = rn;
         w_new[idx] = wn;
-        csum_add_prod(acc[0], (double)rn, (double)rn);
-        csum_add_prod(acc[1], (double)rn, (double)wn);
+        csum_fma(acc[0], (double)rn, (double)rn);
+        csum_fma(acc[1], (double)rn, (double)wn);
     }
 };
 
@@ -1082,9 +1082,9 @@ struct PtPpcgInitW {  // w = A u; p = s = z = q = 0; reductions (r.u, w.u, r.r)
         sv[idx] = (T)0;
         z[idx] = (T)0;
         q[idx] = (T)0;
-        csum_add_prod(acc[0], (double)a[0], (double)u);
-        csum_add_prod(acc[1], (double)wv, (double)u);
-        csum_add_prod(acc[2], (double)a[0], (double)a[0]);
+        csum_fma(acc[0], (double)a[0], (double)u);
+        csum_fma(acc[1], (double)wv, (double)u);
+        csum_fma(acc[2], (double)a[0], (double)a[0]);
     }
 };
 
@@ -1139,9 +1139,9 @@ struct PtPpcgIter {
         r[idx] = rn;
         u[idx] = un;
         w[idx] = wn;
-        csum_add_prod(acc[0], (double)rn, (double)un);
-        csum_add_prod(acc[1], (double)wn, (double)un);
-        csum_add_prod(acc[2], (double)rn, (double)rn);
+        csum_fma(acc[0], (double)rn, (double)un);
+        csum_fma(acc[1], (double)wn, (double)un);
+        csum_fma(acc[2], (double)rn, (double)rn);
     }
 };
 
@@ -1222,7 +1222,7 @@ struct PtIrResid {  // r32 = (float)(b - A x), computed in FP64; reduction ||b -
                                                const double *a, CSum *acc) const {
         const double rv = fx_fma(-1.0, A.apply(ring, nb), a[0]);
         r32[idx] = (float)rv;
-        csum_add_prod(acc[0], rv, rv);
+        csum_fma(acc[0], rv, rv);
     }
 };
 

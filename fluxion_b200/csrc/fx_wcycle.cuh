@@ -338,13 +338,13 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
                         const TB bv = bwa[s2];
                         const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xa, x3a[s0], x3a[s1], wa, xb), xa);
                         row[0] = (TZ)v;
-                        if (RZ) csum_add_prod(acc[0], (double)bv, (double)(TZ)v);
+                        if (RZ) csum_fma(acc[0], (double)bv, (double)(TZ)v);
                     }
                     if (stb) {
                         const TB bv = bwb[s2];
                         const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xb, x3b[s0], x3b[s1], xa, eb), xb);
                         row[1] = (TZ)v;
-                        if (RZ) csum_add_prod(acc[0], (double)bv, (double)(TZ)v);
+                        if (RZ) csum_fma(acc[0], (double)bv, (double)(TZ)v);
                     }
                 }
                 oz += cols;
