@@ -14,7 +14,7 @@ __all__ = [
     "CudaBackend", "CudaBuffer", "BackendUnavailable", "InvalidArgument", "Device", "Field", "DeviceMismatch",
     "CgSolver", "CgStats", "PipelinedCgSolver", "BiCgStabSolver", "GmresSolver", "Multigrid", "SmootherKind",
     "Identity", "Preconditioner", "LinearSolver", "SolveStats", "ConvergenceReason",
-    "MixedPrecisionRefinement", "CudaGraph",
+    "MixedPrecisionRefinement", "CudaGraph", "FcgSolver", "FgmresSolver", "InnerCg",
 ]
 
 
@@ -28,7 +28,7 @@ def __getattr__(name):
         from . import field
         return getattr(field, name)
     if name in ("CgSolver", "CgStats", "PipelinedCgSolver", "BiCgStabSolver", "GmresSolver", "Multigrid",
-                "MixedPrecisionRefinement",
+                "MixedPrecisionRefinement", "FcgSolver", "FgmresSolver", "InnerCg",
                 "SmootherKind", "Identity", "Preconditioner", "LinearSolver", "SolveStats",
                 "ConvergenceReason"):
         from . import solvers

@@ -696,12 +696,11 @@ struct SolverBase {
     }
     // Run `step(i)` for i = 0, 1, ... until the device says done.  Iterations are enqueued
     // in batches sized from the observed convergence rate; surplus iterations are no-ops.
+    // The first batch follows the setup kernels without a read-back in between (a solve the
+    // setup already finished makes it a no-op), so the device never idles before it.
     template <typename Step>
     int drive(Step step, size_t max_launch, bool expensive) {
-        FX_TRY(read_state());
-        if (h_st->done) return FX_OK;
         size_t launched = 0;
-        const double r0 = h_st->resid > 0 ? h_st->resid : 1.0;
         size_t batch = expensive ? 1 : 4;
         while (launched < max_launch) {
             const size_t nb = std::min(batch, max_launch - launched);
@@ -709,7 +708,9 @@ struct SolverBase {
             launched += nb;
             FX_TRY(read_state());
             if (h_st->done) return FX_OK;
-            // predict the iterations still needed from the mean reduction rate so far
+            // predict the iterations still needed from the mean reduction rate so far (r0: the
+            // initial residual, recorded on the device by every solver's setup finaliser)
+            const double r0 = h_st->r0 > 0 ? h_st->r0 : 1.0;
             const double rk = h_st->resid;
             size_t pred = 1;
             if (rk > 0 && rk < r0 && launched > 0 && h_st->tol > 0) {
@@ -1830,6 +1831,281 @@ int create_solver(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, in
     return FX_OK;
 }
 
+// ------------------------------------------------ flexible CG (new; no reference solver)
+//
+// PCG whose beta is the Polak-Ribiere form z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k) (Golub & Ye 1999;
+// Notay's FCG(1), 2000), evaluated as (r_{k+1}.z_{k+1} - r_k.z_{k+1}) / rz_old, so that a
+// preconditioner that changes between applications (an inner iterative solve) keeps the
+// directions locally A-orthogonal.  Per iteration: pcg_dir and an update pass that writes
+// r_{k+1} beside r_k (the two residual buffers swap roles), z = M^-1 r_{k+1} through the
+// preconditioner's plain apply, and one pass for both inner products.
+
+template <typename T, int MODE>
+struct PtFcgUpd {  // x += alpha p; r_out = r_in - alpha A p, r_in kept; reduction r_out.r_out
+    static constexpr int NA = 2;
+    OpA<T, MODE> A;
+    T *x;
+    const T *r_in;
+    T *r_out;
+    const DevState *S;
+    T alpha;
+    __device__ __forceinline__ void prepare() { alpha = (T)S->alpha; }
+    __device__ __forceinline__ const T *aux(int k) const { return k == 0 ? x : r_in; }
+    __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
+        const T ap = A.apply(ring, nb);
+        x[idx] = fx_fma(alpha, nb.c, a[0]);
+        const T rv = fx_fma(-alpha, ap, a[1]);
+        r_out[idx] = rv;
+        csum_fma(acc[0], (double)rv, (double)rv);
+    }
+};
+
+// (r_new.z, r_prev.z) with exact products: the second is near zero by construction
+template <typename T>
+struct FlatFcgDots {
+    const T *r_new, *r_prev, *z;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        const double zv = (double)z[i];
+        csum_add_prod(acc[0], (double)r_new[i], zv);
+        csum_add_prod(acc[1], (double)r_prev[i], zv);
+    }
+};
+
+struct FinFcgBeta {  // beta = (r_new.z - r_prev.z) / rz_old; rz_old = r_new.z
+    DevState *S;
+    __device__ void operator()(const double *v) const {
+        S->beta = (v[0] - v[1]) / S->rs_old;
+        S->rs_old = v[0];
+    }
+};
+
+}  // namespace
+
+struct fx_fcg : SolverBase {
+    // bufs: 0, 1 residuals (current / previous, swapped every iteration), 2 z, 3, 4 directions
+};
+
+namespace {
+
+template <int MODE>
+int fcg_solve_impl(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
+    using T = double;
+    fx_ctx *ctx = s->ctx;
+    const size_t RR = s->g.rows, CC = s->g.cols, n = RR * CC;
+    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
+    T *rb[2] = {(T *)s->bufs[0]->ptr, (T *)s->bufs[1]->ptr};
+    T *z = (T *)s->bufs[2]->ptr;
+    T *pb[2] = {(T *)s->bufs[3]->ptr, (T *)s->bufs[4]->ptr};
+    T *xp = (T *)x->ptr;
+    const T *bp = (const T *)b->ptr;
+    DevState *S = s->d_st;
+    const int *halt = &S->halt;
+    FX_TRY(s->reset_state());
+    FX_CUDA(cudaMemsetAsync(pb[0], 0, n * sizeof(T), ctx->stream));
+    FX_CUDA(cudaMemsetAsync(pb[1], 0, n * sizeof(T), ctx->stream));
+    FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{xp}, PtInitResid<T, MODE>{A, bp, rb[0], nullptr}, FinPcgResid{S},
+                               nullptr, "fcg_init")));
+    fx_buf zb{ctx, z, n, FX_F64, false};
+    auto precondition = [&](T *r) -> int {  // z = M^-1 r from a zero z
+        fx_buf rbuf{ctx, r, n, FX_F64, false};
+        FX_TRY(zero_fill<T>(ctx, z, n, halt));
+        return pc->apply(&zb, &rbuf, halt, true);
+    };
+    FX_TRY(precondition(rb[0]));
+    FX_TRY(launch_flat<1>(ctx, n, FlatDot<T>{rb[0], z}, FinPcgRzInit{S}, halt, "fcg_rz"));
+    auto step = [&](size_t i) -> int {
+        T *po = pb[i & 1], *pn = pb[(i + 1) & 1];
+        T *rc = rb[i & 1], *rn = rb[(i + 1) & 1];
+        FX_TRY((launch_march<T, 1>(ctx, RR, CC, LdAypx<T>{z, po, S}, PtCgDir<T, MODE>{A, pn}, FinCgDir{S}, halt,
+                                   "fcg_dir")));
+        FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{pn}, PtFcgUpd<T, MODE>{A, xp, rc, rn, S}, FinPcgUpd{S}, halt,
+                                   "fcg_update")));
+        FX_TRY(precondition(rn));
+        return launch_flat<2>(ctx, n, FlatFcgDots<T>{rn, rc, z}, FinFcgBeta{S}, halt, "fcg_beta");
+    };
+    return s->drive(step, s->max_iter + 1, n >= (1u << 20));
+}
+
+// ------------------------------------------------ flexible GMRES(m) (new; Saad 1993)
+//
+// Right preconditioning with the preconditioned directions kept: z_k = M_k^-1 v_k,
+// w = A z_k, then the same fused modified Gram-Schmidt, host Givens rotations and restarts as
+// GMRES; the Givens estimate is the true ||b - A x||, and a cycle ends with x += Z y.  Without
+// a preconditioner z_k is v_k itself, and the method is GMRES step for step.
+
+}  // namespace
+
+struct fx_fgmres : fx_gmres {
+    // bufs: 0..m the basis V, m+1 w, m+2 .. 2m+1 the directions Z
+};
+
+namespace {
+
+template <int MODE>
+int fgmres_solve_impl(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, const StencilP &P, fx_precond *pc) {
+    using T = double;
+    fx_ctx *ctx = s->ctx;
+    const size_t RR = s->g.rows, CC = s->g.cols;
+    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
+    const size_t n = s->g.rows * s->g.cols, m = s->restart, mp1 = m + 1;
+    std::vector<T *> V(mp1), Z(m);
+    for (size_t i = 0; i < mp1; i++) V[i] = (T *)s->bufs[i]->ptr;
+    T *w = (T *)s->bufs[mp1]->ptr;
+    for (size_t i = 0; i < m; i++) Z[i] = pc ? (T *)s->bufs[mp1 + 1 + i]->ptr : V[i];
+    T *xp = (T *)x->ptr;
+    const T *bp = (const T *)b->ptr;
+    double *dh = s->d_h;
+    auto H = [&](size_t i, size_t j) -> double & { return s->hh[j * mp1 + i]; };
+    size_t total_its = 0;
+    fx_stats st{0, 0.0, FX_CONVERGED};
+    auto read_h = [&](size_t k) -> int {
+        FX_CUDA(cudaMemcpyAsync(s->h_h, dh, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        FX_CUDA(cudaStreamSynchronize(ctx->stream));
+        return FX_OK;
+    };
+    auto scale_into = [&](T *dst, const T *src, double f) -> int {
+        return launch_flat<0>(ctx, n, FlatScaleInto<T>{dst, src, (T)f}, NoFin{}, nullptr, "fgmres_scale");
+    };
+    auto build_solution = [&](size_t k) -> int {  // x += Z y (gmres.rs:808-837 with Z for V)
+        if (k == 0) return FX_OK;
+        std::vector<double> y(k, 0.0);
+        for (size_t ii = k; ii-- > 0;) {
+            double sacc = s->grs[ii];
+            for (size_t j = ii + 1; j < k; j++) sacc -= s->hh[j * mp1 + ii] * y[j];
+            const double diag = s->hh[ii * mp1 + ii];
+            if (std::fabs(diag) < 1e-30) break;
+            y[ii] = sacc / diag;
+        }
+        for (size_t i0 = 0; i0 < k; i0 += 8) {
+            const size_t cnt = std::min<size_t>(8, k - i0);
+            FlatGmBuild<T> fb;
+            fb.x = xp;
+            for (size_t j = 0; j < cnt; j++) {
+                fb.v[j] = Z[i0 + j];
+                fb.y[j] = (T)y[i0 + j];
+            }
+            fb.cnt = (int)cnt;
+            FX_TRY(launch_flat<0>(ctx, n, fb, NoFin{}, nullptr, "fgmres_build"));
+        }
+        return FX_OK;
+    };
+    for (;;) {
+        FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{xp}, PtGmResid<T, MODE>{A, bp, V[0]}, FinSlot{dh}, nullptr,
+                                   "fgmres_resid")));
+        FX_TRY(read_h(0));
+        const double beta = std::sqrt(s->h_h[0]);
+        if (beta < s->tol) {
+            st = {total_its, beta, FX_CONVERGED};
+            break;
+        }
+        FX_TRY(scale_into(V[0], V[0], 1.0 / beta));
+        std::fill(s->grs.begin(), s->grs.end(), 0.0);
+        s->grs[0] = beta;
+        std::fill(s->hh.begin(), s->hh.end(), 0.0);
+        double cur_resid = beta;
+        size_t k = 0;
+        bool finished = false;
+        while (k < m) {
+            if (total_its >= s->max_iter) {
+                FX_TRY(build_solution(k));
+                st = {total_its, cur_resid, FX_MAX_ITERATIONS};
+                finished = true;
+                break;
+            }
+            if (pc) {  // z_k = M^-1 v_k from a zero z_k
+                fx_buf zk{ctx, Z[k], n, FX_F64, false}, vk{ctx, V[k], n, FX_F64, false};
+                FX_TRY(zero_fill<T>(ctx, Z[k], n, nullptr));
+                FX_TRY(pc->apply(&zk, &vk, nullptr, true));
+            }
+            // w = A z_k with w.v_0, then modified Gram-Schmidt with each dot fused into the AXPY
+            FX_TRY((launch_march<T, 1>(ctx, RR, CC, Ld1<T>{Z[k]}, PtGmAv<T, MODE, true>{A, w, V[0]}, FinSlot{dh + 0},
+                                       nullptr, "fgmres_av")));
+            for (size_t j = 0; j <= k; j++) {
+                const T *vj = V[j];
+                const T *vn = j < k ? V[j + 1] : nullptr;
+                const double *hj = dh + j;
+                FX_TRY(launch_flat<1>(ctx, n, FlatGmMgs<T>{w, vj, vn, hj}, FinSlot{dh + j + 1}, nullptr, "fgmres_mgs"));
+            }
+            FX_TRY(read_h(k));
+            for (size_t j = 0; j <= k; j++) H(j, k) = s->h_h[j];
+            const double h_kp1_k = std::sqrt(s->h_h[k + 1]);
+            H(k + 1, k) = h_kp1_k;
+            if (h_kp1_k > 1e-30) FX_TRY(scale_into(V[k + 1], w, 1.0 / h_kp1_k));
+            for (size_t j = 0; j < k; j++) {
+                const double h_j = H(j, k), h_jp1 = H(j + 1, k), cj = s->cc[j], sj = s->ss[j];
+                H(j, k) = std::fma(cj, h_j, sj * h_jp1);
+                H(j + 1, k) = std::fma(cj, h_jp1, -sj * h_j);
+            }
+            const double a = H(k, k), bv = H(k + 1, k);
+            const double rr = std::hypot(a, bv);
+            if (std::fabs(rr) < 1e-30) {
+                FX_TRY(build_solution(k));
+                st = {total_its, cur_resid, FX_BREAKDOWN};
+                finished = true;
+                break;
+            }
+            s->cc[k] = a / rr;
+            s->ss[k] = bv / rr;
+            H(k, k) = rr;
+            H(k + 1, k) = 0.0;
+            const double g_k = s->grs[k];
+            s->grs[k] = s->cc[k] * g_k;
+            s->grs[k + 1] = -s->ss[k] * g_k;
+            cur_resid = std::fabs(s->grs[k + 1]);
+            total_its++;
+            k++;
+            if (cur_resid < s->tol) break;
+            if (h_kp1_k <= 1e-30) break;
+        }
+        if (finished) break;
+        FX_TRY(build_solution(k));
+        if (cur_resid < s->tol) {
+            st = {total_its, cur_resid, FX_CONVERGED};
+            break;
+        }
+        if (total_its >= s->max_iter) {
+            st = {total_its, cur_resid, FX_MAX_ITERATIONS};
+            break;
+        }
+    }
+    s->h_st->iter = (long long)st.iterations;
+    s->h_st->resid = st.residual;
+    s->h_st->reason = st.reason;
+    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FX_OK;
+}
+
+// ------------------------------------------------ inner-CG preconditioner (new)
+//
+// z = a fixed number of CG steps (preconditioned by `inner` when set) on A z = r from z = 0,
+// with tolerance 0 so the step count alone ends it (or a breakdown).  The count of the k-th
+// application is steps[k mod nsteps], so a schedule of different counts gives a
+// preconditioner that changes from one application to the next -- the case the flexible
+// solvers exist for; PCG and left-preconditioned GMRES lose their guarantees with it.
+struct InnerCgPc : fx_precond {
+    fx_cg *cg = nullptr;
+    fx_precond *inner = nullptr;
+    double coeff = 0.0;
+    std::vector<int> dr, dc;
+    std::vector<double> wt;
+    fx_boundaries bc{};
+    std::vector<size_t> steps;
+    size_t calls = 0;
+    ~InnerCgPc() override {
+        if (cg) fx_cg_destroy(cg);
+    }
+    int apply(fx_buf *z, const fx_buf *r, const int *, bool z_zero) override {
+        FX_TRY(check_same(z, r));
+        if (z->dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "inner-CG preconditioner vectors must be F64");
+        if (!z_zero) FX_TRY(zero_fill<double>(ctx, (double *)z->ptr, z->len, nullptr));
+        FX_TRY(fx_cg_set_params(cg, 0.0, steps[calls++ % steps.size()]));
+        const fx_stencil st{(int)wt.size(), dr.data(), dc.data(), wt.data()};
+        fx_stats out;
+        if (inner) return fx_cg_solve_preconditioned(cg, z, r, coeff, &st, &bc, inner, &out);
+        return fx_cg_solve(cg, z, r, coeff, &st, &bc, &out);
+    }
+};
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -2208,6 +2484,114 @@ int fx_gmres_solve_preconditioned(fx_gmres *s, fx_buf *x, const fx_buf *b, doubl
                                   const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     return gmres_entry(s, x, b, coeff, st, bc, pc, out);
+}
+
+// ---- flexible CG / flexible GMRES / inner-CG preconditioner (new)
+
+int fx_fcg_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, fx_fcg **out) {
+    return create_solver(ctx, g, tol, max_iter, 5, out);
+}
+int fx_fcg_destroy(fx_fcg *s) {
+    delete s;
+    return FX_OK;
+}
+int fx_fcg_set_params(fx_fcg *s, double tol, size_t max_iter) {
+    if (!s) return fail(FX_ERR_INVALID_ARGUMENT, "null solver");
+    s->tol = tol;
+    s->max_iter = max_iter;
+    return FX_OK;
+}
+static int fcg_entry(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                     const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(s->check_io(x, b));
+    StencilP P;
+    FX_TRY(prep_op(s->g, st, bc, &P));
+    IdentityPc idp;
+    idp.ctx = s->ctx;
+    SOLVER_MODE_DISPATCH(P, FX_TRY(fcg_solve_impl<MODE>(s, x, b, coeff, P, pc ? pc : &idp)));
+    s->stats(out);
+    return FX_OK;
+}
+int fx_fcg_solve(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st, const fx_boundaries *bc,
+                 fx_stats *out) {
+    return fcg_entry(s, x, b, coeff, st, bc, nullptr, out);
+}
+int fx_fcg_solve_preconditioned(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                                const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
+    return fcg_entry(s, x, b, coeff, st, bc, pc, out);
+}
+
+int fx_fgmres_create(fx_ctx *ctx, const fx_grid *g, size_t restart, double tol, size_t max_iter, fx_fgmres **out) {
+    if (restart < 1) return fail(FX_ERR_INVALID_ARGUMENT, "restart must be at least 1");
+    FX_TRY(create_solver(ctx, g, tol, max_iter, 2 * (int)restart + 2, out));
+    fx_fgmres *s = *out;
+    s->restart = restart;
+    s->hh.assign((restart + 1) * restart, 0.0);
+    s->cc.assign(restart, 0.0);
+    s->ss.assign(restart, 0.0);
+    s->grs.assign(restart + 1, 0.0);
+    if (cudaMalloc(&s->d_h, (restart + 2) * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&s->h_h, (restart + 2) * sizeof(double)) != cudaSuccess) {
+        delete s;
+        *out = nullptr;
+        return fail(FX_ERR_BACKEND, "fgmres scratch allocation failed");
+    }
+    return FX_OK;
+}
+int fx_fgmres_destroy(fx_fgmres *s) {
+    delete s;
+    return FX_OK;
+}
+int fx_fgmres_set_params(fx_fgmres *s, double tol, size_t max_iter) {
+    if (!s) return fail(FX_ERR_INVALID_ARGUMENT, "null solver");
+    s->tol = tol;
+    s->max_iter = max_iter;
+    return FX_OK;
+}
+static int fgmres_entry(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                        const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(s->check_io(x, b));
+    StencilP P;
+    FX_TRY(prep_op(s->g, st, bc, &P));
+    SOLVER_MODE_DISPATCH(P, FX_TRY(fgmres_solve_impl<MODE>(s, x, b, coeff, P, pc)));
+    s->stats(out);
+    return FX_OK;
+}
+int fx_fgmres_solve(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                    const fx_boundaries *bc, fx_stats *out) {
+    return fgmres_entry(s, x, b, coeff, st, bc, nullptr, out);
+}
+int fx_fgmres_solve_preconditioned(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                                   const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
+    return fgmres_entry(s, x, b, coeff, st, bc, pc, out);
+}
+
+int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st, const fx_boundaries *bc,
+                        const size_t *steps, size_t nsteps, fx_precond *inner, fx_precond **out) {
+    if (!ctx || !g || !st || !bc || !steps || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (nsteps == 0) return fail(FX_ERR_INVALID_ARGUMENT, "empty step schedule");
+    if (st->n < 1 || !st->dr || !st->dc || !st->w) return fail(FX_ERR_INVALID_ARGUMENT, "empty stencil");
+    *out = nullptr;
+    InnerCgPc *p = new InnerCgPc();
+    p->ctx = ctx;
+    p->inner = inner;
+    p->coeff = coeff;
+    p->dr.assign(st->dr, st->dr + st->n);
+    p->dc.assign(st->dc, st->dc + st->n);
+    p->wt.assign(st->w, st->w + st->n);
+    p->bc = *bc;
+    p->steps.assign(steps, steps + nsteps);
+    const int rc = fx_cg_create(ctx, g, 0.0, steps[0], &p->cg);
+    if (rc) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return FX_OK;
 }
 
 }  // extern "C"

@@ -322,6 +322,68 @@ class BiCgStabSolver(_Native):
         return "BiCGSTAB"
 
 
+class InnerCg(Preconditioner):
+    """Inner-CG preconditioner (new): the k-th application runs ``steps[k % len(steps)]`` CG
+    steps on (I + coeff S) z = r from z = 0 (preconditioned by ``inner`` when given), tolerance
+    0.  With a schedule of different counts it changes from one application to the next, the
+    case `FcgSolver` and `FgmresSolver` are for."""
+
+    def __init__(self, grid: Grid, coeff: float, stencil: Stencil, boundaries: Boundaries, steps,
+                 inner: Optional[Preconditioner] = None, device: Optional[Device] = None):
+        self.device = device or Device.best()
+        self._inner = inner  # kept alive: the native object holds its handle
+        sched = (C.c_size_t * len(steps))(*[int(k) for k in steps])
+        sc = StencilC(stencil)
+        g, bc = grid_c(grid), bcs_c(boundaries)
+        out = C.c_void_p()
+        check(L.lib().fx_precond_inner_cg(self.device.backend().ctx, C.byref(g), float(coeff), sc.ptr, C.byref(bc),
+                                          sched, len(steps), inner._handle(self.device) if inner else None,
+                                          C.byref(out)))
+        self.h = out.value
+
+    def _handle(self, device: Device) -> int:
+        return self.h
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().fx_precond_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class FcgSolver(_Native):
+    """Flexible CG (new; the reference has none): PCG with the Polak-Ribiere beta
+    z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k) (Golub & Ye 1999; Notay 2000), safe with a
+    preconditioner that changes between applications.  Same fields, signatures and stop test as
+    `CgSolver`; with a fixed SPD preconditioner it takes the same iterations."""
+
+    _prefix = "fcg"
+
+    def __init__(self, grid: Grid, device: Optional[Device] = None, tol: float = 1e-8, max_iter: int = 500):
+        super().__init__(grid, device, tol, max_iter)
+
+    def name(self) -> str:
+        return "FCG"
+
+
+class FgmresSolver(_Native):
+    """Flexible GMRES(m) (new; Saad 1993): right preconditioning with the preconditioned
+    directions kept, so the preconditioner may change between applications; it stops on the
+    true ||b - A x||_2 < tol.  Without a preconditioner it is `GmresSolver` step for step."""
+
+    _prefix = "fgmres"
+
+    def __init__(self, grid: Grid, device: Optional[Device] = None, restart: int = 30, tol: float = 1e-8,
+                 max_iter: int = 500):
+        self.restart = int(restart)
+        super().__init__(grid, device, tol, max_iter, C.c_size_t(self.restart))
+
+    def name(self) -> str:
+        return "FGMRES"
+
+
 class GmresSolver(_Native):
     """gmres.rs:24-491: restarted GMRES(m) with modified Gram-Schmidt."""
 

@@ -97,6 +97,8 @@ typedef struct fx_pipelined_cg fx_pipelined_cg;
 typedef struct fx_bicgstab fx_bicgstab;
 typedef struct fx_gmres fx_gmres;
 typedef struct fx_graph fx_graph;
+typedef struct fx_fcg fx_fcg;
+typedef struct fx_fgmres fx_fgmres;
 typedef struct fx_ir fx_ir;
 
 /* ------------------------------------------------------------------ */
@@ -258,6 +260,13 @@ int fx_precond_identity(fx_ctx *ctx, fx_precond **out);
 int fx_precond_destroy(fx_precond *pc);
 /* Preconditioner::apply(z, r) (preconditioner.rs:19-29).  The solvers zero-fill z first. */
 int fx_precond_apply(fx_precond *pc, fx_buf *z, const fx_buf *r);
+/* Inner-CG preconditioner (new): z = steps[k mod nsteps] CG steps on (I + coeff S) z = r from
+ * z = 0 at the k-th application (preconditioned by `inner` when non-null, which must outlive
+ * it), with tolerance 0.  A schedule of different counts makes it vary between applications,
+ * the case fx_fcg_* and fx_fgmres_* are for.  F64 vectors; st and bc are copied. */
+int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st,
+                        const fx_boundaries *bc, const size_t *steps, size_t nsteps, fx_precond *inner,
+                        fx_precond **out);
 
 /* Multigrid::new / ::build (multigrid.rs:61-146): reference hierarchy (rows/2 per level,
  * Laplacian on each level, clamped 2x2 restriction, piecewise-constant prolongation,
@@ -362,6 +371,32 @@ int fx_gmres_solve(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const 
 int fx_gmres_solve_preconditioned(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff,
                                   const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
                                   fx_stats *out);
+
+/* Flexible CG (new; the reference has no flexible solver): PCG with the Polak-Ribiere beta
+ * z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k) (Golub & Ye 1999; Notay's FCG(1), 2000), for
+ * preconditioners that change between applications.  Same stop and breakdown tests as
+ * fx_cg_solve_preconditioned; fx_fcg_solve uses the identity (and is then CG). */
+int fx_fcg_create(fx_ctx *ctx, const fx_grid *g, double tol, size_t max_iter, fx_fcg **out);
+int fx_fcg_destroy(fx_fcg *s);
+int fx_fcg_set_params(fx_fcg *s, double tol, size_t max_iter);
+int fx_fcg_solve(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                 const fx_boundaries *bc, fx_stats *out);
+int fx_fcg_solve_preconditioned(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                                const fx_boundaries *bc, fx_precond *pc, fx_stats *out);
+
+/* Flexible GMRES(m) (new; Saad 1993): right preconditioning with the m preconditioned
+ * directions kept, so the preconditioner may change between applications; the residual it
+ * stops on is the true ||b - A x||.  Gram-Schmidt, Givens rotations and restarts as
+ * fx_gmres_*; without a preconditioner it is GMRES step for step. */
+int fx_fgmres_create(fx_ctx *ctx, const fx_grid *g, size_t restart, double tol, size_t max_iter,
+                     fx_fgmres **out);
+int fx_fgmres_destroy(fx_fgmres *s);
+int fx_fgmres_set_params(fx_fgmres *s, double tol, size_t max_iter);
+int fx_fgmres_solve(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
+                    const fx_boundaries *bc, fx_stats *out);
+int fx_fgmres_solve_preconditioned(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff,
+                                   const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
+                                   fx_stats *out);
 
 #ifdef __cplusplus
 }

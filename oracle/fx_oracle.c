@@ -930,6 +930,165 @@ out:
     return rc;
 }
 
+/* Flexible CG.  New (the reference has no flexible solver): PCG whose beta is the
+ * Polak-Ribiere form z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k) of Golub & Ye (1999, inexact
+ * preconditioned CG) -- equal, in exact arithmetic, to Notay's FCG(1) (2000) -- evaluated as
+ * (r_{k+1}.z_{k+1} - r_k.z_{k+1}) / rz_old.  With a fixed SPD preconditioner r_k.z_{k+1} = 0
+ * in exact arithmetic and the method is PCG; with one that changes between applications
+ * (an inner iterative solve) the directions stay locally A-orthogonal.  Loop, stop test
+ * (||r|| < tol at the loop top) and breakdown test as fxo_cg_solve's preconditioned branch. */
+int fxo_fcg_solve(const fxo_op *op, double *x, const double *b, double tol, size_t max_iter,
+                  fxo_pc_fn pc, void *pc_ctx, fxo_stats *st) {
+    size_t n = op_len(op);
+    double *r = calloc(n, 8), *rp = calloc(n, 8), *z = calloc(n, 8), *p = calloc(n, 8), *ap = calloc(n, 8);
+    int rc = apply_op(op, ap, x);
+    if (rc) goto out;
+    fxo_copy(b, r, n);
+    fxo_axpy(-1.0, ap, r, n);
+    fxo_fill(z, n, 0.0);
+    pc(pc_ctx, z, r);
+    fxo_copy(z, p, n);
+    double rz_old = fxo_dot(r, z, n);
+    for (size_t i = 0; i < max_iter; i++) {
+        double r_norm = sqrt(fxo_dot(r, r, n));
+        if (r_norm < tol) {
+            set_stats(st, i, r_norm, 0);
+            goto out;
+        }
+        apply_op(op, ap, p);
+        double p_ap = fxo_dot(p, ap, n);
+        if (fabs(p_ap) < 1e-30) {
+            set_stats(st, i, r_norm, 2);
+            goto out;
+        }
+        double alpha = rz_old / p_ap;
+        fxo_axpy(alpha, p, x, n);
+        fxo_copy(r, rp, n);
+        fxo_axpy(-alpha, ap, r, n);
+        fxo_fill(z, n, 0.0);
+        pc(pc_ctx, z, r);
+        double rz_new, zr_prev;
+        fxo_dot2(r, z, rp, z, n, &rz_new, &zr_prev);
+        double beta = (rz_new - zr_prev) / rz_old;
+        fxo_scale(p, n, beta);
+        fxo_axpy(1.0, z, p, n);
+        rz_old = rz_new;
+    }
+    set_stats(st, max_iter, sqrt(fxo_dot(r, r, n)), 1);
+out:
+    free(r); free(rp); free(z); free(p); free(ap);
+    return rc;
+}
+
+/* Flexible GMRES(m) (Saad 1993): right preconditioning with the preconditioned directions
+ * z_k = M_k^-1 v_k kept, so M may change from one application to the next; the Arnoldi
+ * relation is A Z_k = V_{k+1} H, the Givens residual estimate is the true ||b - A x||, and
+ * x += Z y at the end of a cycle.  Gram-Schmidt, Givens rotations, breakdown thresholds and
+ * restarts as fxo_gmres_solve. */
+int fxo_fgmres_solve(const fxo_op *op, double *x, const double *b, size_t m, double tol,
+                     size_t max_iter, fxo_pc_fn pc, void *pc_ctx, fxo_stats *st) {
+    size_t n = op_len(op), mp1 = m + 1;
+    double **vv = malloc(mp1 * sizeof(double *)), **zz = malloc(m * sizeof(double *));
+    for (size_t i = 0; i < mp1; i++) vv[i] = calloc(n, 8);
+    for (size_t i = 0; i < m; i++) zz[i] = calloc(n, 8);
+    double *w = calloc(n, 8), *hh = calloc(mp1 * m, 8), *cc = calloc(m, 8), *ss = calloc(m, 8);
+    double *grs = calloc(mp1, 8);
+    size_t total_its = 0;
+    int rc = 0;
+#define H(i, j) hh[(j) * mp1 + (i)]
+    for (;;) {
+        double *v0 = vv[0];
+        rc = apply_op(op, v0, x);
+        if (rc) goto out;
+        fxo_scale(v0, n, -1.0);
+        fxo_axpy(1.0, b, v0, n);
+        double beta = sqrt(fxo_dot(v0, v0, n));
+        if (beta < tol) {
+            set_stats(st, total_its, beta, 0);
+            goto out;
+        }
+        fxo_scale(v0, n, 1.0 / beta);
+        memset(grs, 0, mp1 * 8);
+        grs[0] = beta;
+        memset(hh, 0, mp1 * m * 8);
+        double cur_resid = beta;
+        size_t k = 0;
+        while (k < m) {
+            if (total_its >= max_iter) {
+                gmres_build_solution(x, zz, hh, grs, m, k, n);
+                set_stats(st, total_its, cur_resid, 1);
+                goto out;
+            }
+            fxo_fill(zz[k], n, 0.0);
+            if (pc) pc(pc_ctx, zz[k], vv[k]);
+            else fxo_copy(vv[k], zz[k], n);
+            apply_op(op, w, zz[k]);
+            for (size_t j = 0; j <= k; j++) {
+                double h = fxo_dot(w, vv[j], n);
+                H(j, k) = h;
+                fxo_axpy(-h, vv[j], w, n);
+            }
+            double h_kp1_k = sqrt(fxo_dot(w, w, n));
+            H(k + 1, k) = h_kp1_k;
+            if (h_kp1_k > 1e-30) {
+                fxo_copy(w, vv[k + 1], n);
+                fxo_scale(vv[k + 1], n, 1.0 / h_kp1_k);
+            }
+            for (size_t j = 0; j < k; j++) {
+                double h_j = H(j, k), h_jp1 = H(j + 1, k);
+                double cj = cc[j], sj = ss[j];
+                H(j, k) = fma(cj, h_j, sj * h_jp1);
+                H(j + 1, k) = fma(cj, h_jp1, -sj * h_j);
+            }
+            double a = H(k, k), bv = H(k + 1, k);
+            double rr = hypot(a, bv);
+            if (fabs(rr) < 1e-30) {
+                gmres_build_solution(x, zz, hh, grs, m, k, n);
+                set_stats(st, total_its, cur_resid, 2);
+                goto out;
+            }
+            cc[k] = a / rr;
+            ss[k] = bv / rr;
+            H(k, k) = rr;
+            H(k + 1, k) = 0.0;
+            double g_k = grs[k];
+            grs[k] = cc[k] * g_k;
+            grs[k + 1] = -ss[k] * g_k;
+            cur_resid = fabs(grs[k + 1]);
+            total_its++;
+            k++;
+            if (cur_resid < tol) break;
+            if (h_kp1_k <= 1e-30) break;
+        }
+        gmres_build_solution(x, zz, hh, grs, m, k, n);
+        if (cur_resid < tol) {
+            set_stats(st, total_its, cur_resid, 0);
+            goto out;
+        }
+        if (total_its >= max_iter) {
+            set_stats(st, total_its, cur_resid, 1);
+            goto out;
+        }
+    }
+#undef H
+out:
+    for (size_t i = 0; i < mp1; i++) free(vv[i]);
+    for (size_t i = 0; i < m; i++) free(zz[i]);
+    free(vv); free(zz); free(w); free(hh); free(cc); free(ss); free(grs);
+    return rc;
+}
+
+/* A preconditioner that is itself a number of (optionally preconditioned) CG steps on A z = r
+ * from z = 0 (tolerance 0: the count alone ends it, or a breakdown), the count of the k-th
+ * application being steps[k mod nsteps].  Its action depends on r nonlinearly, and with
+ * different counts it changes between applications: the test case for the flexible solvers. */
+void fxo_inner_cg_pc_apply(void *ctx, double *z, const double *r) {
+    fxo_inner_cg *ic = (fxo_inner_cg *)ctx;
+    fxo_stats st;
+    const size_t k = ic->steps[ic->calls++ % ic->nsteps];
+    fxo_cg_solve(ic->op, z, r, 0.0, k, ic->pc, ic->pc_ctx, &st);
+}
+
 /* ------------------------------------------------------------------ */
 /* Multigrid (multigrid.rs)                                            */
 /* ------------------------------------------------------------------ */

@@ -145,6 +145,21 @@ int fxo_bicgstab_solve(const fxo_op *op, double *x, const double *b, double tol,
                        fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);
 int fxo_gmres_solve(const fxo_op *op, double *x, const double *b, size_t restart, double tol,
                     size_t max_iter, fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);
+/* flexible solvers (new): flexible CG (Polak-Ribiere beta) and flexible GMRES(m) (Saad 1993) */
+int fxo_fcg_solve(const fxo_op *op, double *x, const double *b, double tol, size_t max_iter,
+                  fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);
+int fxo_fgmres_solve(const fxo_op *op, double *x, const double *b, size_t restart, double tol,
+                     size_t max_iter, fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);
+/* nonlinear preconditioner: steps[calls mod nsteps] CG steps (preconditioned by pc when set)
+ * from z = 0; calls counts the applications */
+typedef struct {
+    const fxo_op *op;
+    const size_t *steps;
+    size_t nsteps, calls;
+    fxo_pc_fn pc;
+    void *pc_ctx;
+} fxo_inner_cg;
+void fxo_inner_cg_pc_apply(void *ctx, double *z, const double *r);
 
 /* Multigrid (multigrid.rs).  mode 0 = reference hierarchy and operators
  * (rows/2 coarsening, 2x2 average, piecewise-constant prolongation, lexicographic

@@ -104,6 +104,9 @@ def _declare(L):
     d("fxo_pipelined_pcg_solve", C.c_int, opp, _dp, _dp, C.c_double, _sz, PC_FN, C.c_void_p, stp)
     d("fxo_bicgstab_solve", C.c_int, opp, _dp, _dp, C.c_double, _sz, PC_FN, C.c_void_p, stp)
     d("fxo_gmres_solve", C.c_int, opp, _dp, _dp, _sz, C.c_double, _sz, PC_FN, C.c_void_p, stp)
+    d("fxo_fcg_solve", C.c_int, opp, _dp, _dp, C.c_double, _sz, PC_FN, C.c_void_p, stp)
+    d("fxo_fgmres_solve", C.c_int, opp, _dp, _dp, _sz, C.c_double, _sz, PC_FN, C.c_void_p, stp)
+    d("fxo_inner_cg_pc_apply", None, C.c_void_p, _dp, _dp)
     d("fxo_mg_create", C.c_void_p, _sz, _sz, C.c_double, C.c_double, bcp, C.c_int, C.c_int,
       C.c_double, C.c_int, C.c_double, C.c_int, _ip, _ip, _dp, C.c_int, C.c_int)
     d("fxo_mg_destroy", None, C.c_void_p)
@@ -323,10 +326,34 @@ class IdentityPC:
         self._cb = PC_FN(lambda ctx, z, r: lib().fxo_copy(r, z, n))
 
 
+class InnerCg(C.Structure):
+    _fields_ = [("op", C.c_void_p), ("steps", C.POINTER(C.c_size_t)), ("nsteps", C.c_size_t),
+                ("calls", C.c_size_t), ("pc", PC_FN), ("pc_ctx", C.c_void_p)]
+
+
+class InnerCgPC:
+    """Nonlinear preconditioner (fxo_inner_cg_pc_apply): the k-th application runs
+    steps[k % len(steps)] CG steps (preconditioned by `pc` when given) on A z = r from z = 0
+    with tolerance 0.  A z = r is the operator v + coeff*S v on the same grid and rings."""
+
+    def __init__(self, rows, cols, coeff, entries, steps, pc=None, bcs=ZERO_DIRICHLET):
+        self._op = _op(rows, cols, coeff, entries, bcs)
+        self._steps = (C.c_size_t * len(steps))(*[int(k) for k in steps])
+        self._pc = pc  # kept alive with its callback
+        fn, ctx = _pc_args(pc)
+        self._ic = InnerCg(C.cast(C.pointer(self._op), C.c_void_p), self._steps, len(steps), 0, fn, ctx)
+        self._cb = C.cast(lib().fxo_inner_cg_pc_apply, PC_FN)
+        self._ctx = C.cast(C.pointer(self._ic), C.c_void_p)
+
+    @property
+    def calls(self):
+        return self._ic.calls
+
+
 def _pc_args(pc):
     if pc is None:
         return _NULL_PC, None
-    return pc._cb, None
+    return pc._cb, getattr(pc, "_ctx", None)
 
 
 def cg_solve(x, b, rows, cols, coeff, entries, tol, max_iter, bcs=ZERO_DIRICHLET, pc=None):
@@ -357,6 +384,25 @@ def bicgstab_solve(x, b, rows, cols, coeff, entries, tol, max_iter, bcs=ZERO_DIR
     fn, ctx = _pc_args(pc)
     _chk(lib().fxo_bicgstab_solve(C.byref(_op(rows, cols, coeff, entries, bcs)), _p(x), _p(b), tol,
                                   max_iter, fn, ctx, C.byref(st)), "bicgstab")
+    return st.iterations, st.residual, st.reason
+
+
+def fcg_solve(x, b, rows, cols, coeff, entries, tol, max_iter, pc, bcs=ZERO_DIRICHLET):
+    """Flexible CG (fxo_fcg_solve): PCG with the Polak-Ribiere beta."""
+    st = Stats()
+    fn, ctx = _pc_args(pc)
+    _chk(lib().fxo_fcg_solve(C.byref(_op(rows, cols, coeff, entries, bcs)), _p(x), _p(b), tol,
+                             max_iter, fn, ctx, C.byref(st)), "fcg")
+    return st.iterations, st.residual, st.reason
+
+
+def fgmres_solve(x, b, rows, cols, coeff, entries, restart, tol, max_iter, bcs=ZERO_DIRICHLET,
+                 pc=None):
+    """Flexible GMRES(m) (fxo_fgmres_solve): right preconditioning, z_k kept."""
+    st = Stats()
+    fn, ctx = _pc_args(pc)
+    _chk(lib().fxo_fgmres_solve(C.byref(_op(rows, cols, coeff, entries, bcs)), _p(x), _p(b),
+                                restart, tol, max_iter, fn, ctx, C.byref(st)), "fgmres")
     return st.iterations, st.residual, st.reason
 
 
