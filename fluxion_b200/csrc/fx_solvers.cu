@@ -68,6 +68,17 @@ struct FinPcgRz {  // beta = rz_new / rz_old (cg.rs:240-247)
 
 }  // namespace fx
 
+// ---------------------------------------------------------------- operators
+
+// A conv-diff operator for the solvers' *_solve_op entry points (fx_op_conv_diff).  The field
+// buffers are borrowed: they must outlive the fx_op.
+struct fx_op {
+    fx_ctx *ctx = nullptr;
+    fx_grid g{};
+    double sigma = 1.0, coeff = 1.0, kappa_s = 0.0;
+    const fx_buf *kappa = nullptr, *vx = nullptr, *vy = nullptr;
+};
+
 // ---------------------------------------------------------------- preconditioners
 
 struct fx_precond {
@@ -96,8 +107,48 @@ struct OpA {
     T coeff;
     int rows, cols;
     // copy_from + stencil_axpy (cg.rs:106-109): interior fma(coeff, S v, v), ring = v
-    __device__ __forceinline__ T apply(bool ring, const Nb<T> &nb) const {
+    __device__ __forceinline__ T apply(bool ring, const Nb<T> &nb, size_t) const {
         return ring ? nb.c : fx_fma(coeff, stencil_eval<T, MODE>(P, nb), nb.c);
+    }
+};
+
+// The convection-diffusion operator of an fx_op (new; no reference solver takes it):
+// interior fma(coeff, kappa Lap v + v.grad v, sigma v), upwind as apply_conv_diff
+// (ops.rs:673-791, conv_diff_at), ring = v.  With sigma = 1 it is conv_diff_axpy(coeff, v, v),
+// the implicit-step operator I + coeff CD; with sigma = 0 the steady operator CD.
+constexpr int kModeCD = 100;
+
+template <typename T>
+struct OpA<T, kModeCD> {
+    ConvDiffC<T> K;
+    T sigma, coeff, kap_s;
+    const T *kappa, *vx, *vy;  // kappa null: the scalar kap_s
+    __device__ __forceinline__ T apply(bool ring, const Nb<T> &nb, size_t idx) const {
+        if (ring) return nb.c;
+        const T kap = kappa ? kappa[idx] : kap_s;
+        return fx_fma(coeff, conv_diff_at<T>(K, nb, kap, vx[idx], vy[idx]), sigma * nb.c);
+    }
+};
+
+// The operator a solver applies: the stencil form from (P, coeff), or the solver's fx_op.
+template <typename T, int MODE>
+struct OpMaker {
+    static OpA<T, MODE> make(const StencilP &P, double coeff, size_t rows, size_t cols, const fx_op *) {
+        return OpA<T, MODE>{P, (T)coeff, (int)rows, (int)cols};
+    }
+};
+template <typename T>
+struct OpMaker<T, kModeCD> {
+    static OpA<T, kModeCD> make(const StencilP &, double, size_t, size_t, const fx_op *op) {
+        OpA<T, kModeCD> A;
+        A.K = conv_consts<T>(op->g.dx, op->g.dy);
+        A.sigma = (T)op->sigma;
+        A.coeff = (T)op->coeff;
+        A.kap_s = (T)op->kappa_s;
+        A.kappa = op->kappa ? (const T *)op->kappa->ptr : nullptr;
+        A.vx = (const T *)op->vx->ptr;
+        A.vy = (const T *)op->vy->ptr;
+        return A;
     }
 };
 
@@ -217,7 +268,7 @@ struct PtApplyOp {
     T *out;
     __device__ __forceinline__ const T *aux(int) const { return nullptr; }
     __device__ __forceinline__ void operator()(bool ring, int r, int c, size_t idx, const Nb<T> &nb, const T *, CSum *) const {
-        out[idx] = A.apply(ring, nb);
+        out[idx] = A.apply(ring, nb, idx);
     }
 };
 
@@ -648,6 +699,7 @@ struct SolverBase {
     DevState *h_st = nullptr;
     std::vector<fx_buf *> bufs;
     int dtype = FX_F64;  // of the solver's vectors (x, b and the work vectors)
+    const fx_op *op = nullptr;  // set for the duration of a *_solve_op call
 
     int init_base(fx_ctx *c, const fx_grid *grid, double t, size_t mi, int nvec, int dt = FX_F64) {
         ctx = c;
@@ -763,7 +815,7 @@ struct PtInitResid {
     T *r2;  // optional second copy (BiCGSTAB r_hat)
     __device__ __forceinline__ const T *aux(int) const { return b; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T ax = A.apply(ring, nb);
+        const T ax = A.apply(ring, nb, idx);
         const T rv = fx_fma((T)-1, ax, a[0]);
         r[idx] = rv;
         if (r2) r2[idx] = rv;
@@ -793,7 +845,7 @@ struct PtCgDir {
     __device__ __forceinline__ const T *aux(int) const { return nullptr; }
     __device__ __forceinline__ void operator()(bool ring, int r, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
         p_new[idx] = nb.c;
-        const T ap = A.apply(ring, nb);
+        const T ap = A.apply(ring, nb, idx);
         csum_fma(acc[0], (double)nb.c, (double)ap);
     }
 };
@@ -821,7 +873,7 @@ struct PtCgUpd {
     __device__ __forceinline__ void prepare() { alpha = (T)S->alpha; }
     __device__ __forceinline__ const T *aux(int k) const { return k == 0 ? x : r; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T ap = A.apply(ring, nb);
+        const T ap = A.apply(ring, nb, idx);
         x[idx] = fx_fma(alpha, nb.c, a[0]);
         const T rv = fx_fma(-alpha, ap, a[1]);
         r[idx] = rv;
@@ -933,7 +985,7 @@ struct PtPipeInitQ {  // q = A x; r = b - q
     T *r;
     __device__ __forceinline__ const T *aux(int) const { return b; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *) const {
-        r[idx] = fx_fma((T)-1, A.apply(ring, nb), a[0]);
+        r[idx] = fx_fma((T)-1, A.apply(ring, nb, idx), a[0]);
     }
 };
 
@@ -944,7 +996,7 @@ struct PtPipeInitW {  // w = A r; p = t = z = 0; reductions (r.r, r.w)
     T *w, *p, *t, *z;
     __device__ __forceinline__ const T *aux(int) const { return nullptr; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T wv = A.apply(ring, nb);
+        const T wv = A.apply(ring, nb, idx);
         w[idx] = wv;
         p[idx] = (T)0;
         t[idx] = (T)0;
@@ -993,7 +1045,7 @@ struct PtPipeIter {
         return k == 0 ? z : (k == 1 ? t : (k == 2 ? p : (k == 3 ? x : r)));
     }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T q = A.apply(ring, nb);
+        const T q = A.apply(ring, nb, idx);
         const T w = nb.c;
         const T zn = q + a[0] * beta;
         const T tn = w + a[1] * beta;
@@ -1077,7 +1129,7 @@ struct PtPpcgInitW {  // w = A u; p = s = z = q = 0; reductions (r.u, w.u, r.r)
     __device__ __forceinline__ const T *aux(int) const { return r; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
         const T u = nb.c;
-        const T wv = A.apply(ring, nb);
+        const T wv = A.apply(ring, nb, idx);
         w[idx] = wv;
         p[idx] = (T)0;
         sv[idx] = (T)0;
@@ -1123,7 +1175,7 @@ struct PtPpcgIter {
         return k == 0 ? z : k == 1 ? q : k == 2 ? sv : k == 3 ? p : k == 4 ? x : k == 5 ? r : k == 6 ? u : w;
     }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T n = A.apply(ring, nb);
+        const T n = A.apply(ring, nb, idx);
         const T m = nb.c;
         const T zn = n + a[0] * beta;
         const T qn = m + a[1] * beta;
@@ -1221,7 +1273,7 @@ struct PtIrResid {  // r32 = (float)(b - A x), computed in FP64; reduction ||b -
     __device__ __forceinline__ const double *aux(int) const { return b; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<double> &nb,
                                                const double *a, CSum *acc) const {
-        const double rv = fx_fma(-1.0, A.apply(ring, nb), a[0]);
+        const double rv = fx_fma(-1.0, A.apply(ring, nb, idx), a[0]);
         r32[idx] = (float)rv;
         csum_fma(acc[0], rv, rv);
     }
@@ -1355,7 +1407,7 @@ struct PtBicgV {
     __device__ __forceinline__ const T *aux(int) const { return r_hat; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
         if (p_store) p_store[idx] = nb.c;
-        const T vv = A.apply(ring, nb);
+        const T vv = A.apply(ring, nb, idx);
         v[idx] = vv;
         csum_add_prod(acc[0], (double)a[0], (double)vv);
     }
@@ -1393,7 +1445,7 @@ struct PtBicgT {
     const T *s;
     __device__ __forceinline__ const T *aux(int) const { return s; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T tv = A.apply(ring, nb);
+        const T tv = A.apply(ring, nb, idx);
         t[idx] = tv;
         csum_add_prod(acc[0], (double)tv, (double)a[0]);
         csum_add_prod(acc[1], (double)tv, (double)tv);
@@ -1493,7 +1545,7 @@ struct PtBicgInit {
     T *r, *rh;
     __device__ __forceinline__ const T *aux(int) const { return b; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T rv = fx_fma((T)-1, A.apply(ring, nb), a[0]);
+        const T rv = fx_fma((T)-1, A.apply(ring, nb, idx), a[0]);
         r[idx] = rv;
         rh[idx] = rv;
         csum_add_prod(acc[0], (double)rv, (double)rv);
@@ -1514,7 +1566,7 @@ int bicg_solve_impl(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, co
     using T = double;
     fx_ctx *ctx = s->ctx;
     const size_t RR = s->g.rows, CC = s->g.cols;
-    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
+    const auto A = OpMaker<T, MODE>::make(P, coeff, RR, CC, s->op);
     const size_t n = s->g.rows * s->g.cols;
     T *r = (T *)s->bufs[0]->ptr, *rh = (T *)s->bufs[1]->ptr;
     T *pb[2] = {(T *)s->bufs[2]->ptr, (T *)s->bufs[3]->ptr};
@@ -1601,7 +1653,7 @@ struct PtGmResid {  // out = b - A x (gmres.rs:477-485); reduction out.out
     T *out;
     __device__ __forceinline__ const T *aux(int) const { return b; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T ax = A.apply(ring, nb);
+        const T ax = A.apply(ring, nb, idx);
         const T v = fx_fma((T)1, a[0], -ax);
         out[idx] = v;
         csum_add_prod(acc[0], (double)v, (double)v);
@@ -1616,7 +1668,7 @@ struct PtGmAv {  // w = A v; reduction w.v0 (when v0 given)
     const T *v0;
     __device__ __forceinline__ const T *aux(int) const { return v0; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T wv = A.apply(ring, nb);
+        const T wv = A.apply(ring, nb, idx);
         w[idx] = wv;
         if (HAS_V0) csum_add_prod(acc[0], (double)wv, (double)a[0]);
     }
@@ -1666,7 +1718,7 @@ int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, cons
     using T = double;
     fx_ctx *ctx = s->ctx;
     const size_t RR = s->g.rows, CC = s->g.cols;
-    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
+    const auto A = OpMaker<T, MODE>::make(P, coeff, RR, CC, s->op);
     const size_t n = s->g.rows * s->g.cols, m = s->restart, mp1 = m + 1;
     std::vector<T *> V(mp1);
     for (size_t i = 0; i < mp1; i++) V[i] = (T *)s->bufs[i]->ptr;
@@ -1852,7 +1904,7 @@ struct PtFcgUpd {  // x += alpha p; r_out = r_in - alpha A p, r_in kept; reducti
     __device__ __forceinline__ void prepare() { alpha = (T)S->alpha; }
     __device__ __forceinline__ const T *aux(int k) const { return k == 0 ? x : r_in; }
     __device__ __forceinline__ void operator()(bool ring, int rr, int c, size_t idx, const Nb<T> &nb, const T *a, CSum *acc) const {
-        const T ap = A.apply(ring, nb);
+        const T ap = A.apply(ring, nb, idx);
         x[idx] = fx_fma(alpha, nb.c, a[0]);
         const T rv = fx_fma(-alpha, ap, a[1]);
         r_out[idx] = rv;
@@ -1946,7 +1998,7 @@ int fgmres_solve_impl(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, co
     using T = double;
     fx_ctx *ctx = s->ctx;
     const size_t RR = s->g.rows, CC = s->g.cols;
-    OpA<T, MODE> A{P, (T)coeff, (int)RR, (int)CC};
+    const auto A = OpMaker<T, MODE>::make(P, coeff, RR, CC, s->op);
     const size_t n = s->g.rows * s->g.cols, m = s->restart, mp1 = m + 1;
     std::vector<T *> V(mp1), Z(m);
     for (size_t i = 0; i < mp1; i++) V[i] = (T *)s->bufs[i]->ptr;
@@ -2072,6 +2124,49 @@ int fgmres_solve_impl(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, co
     s->h_st->resid = st.residual;
     s->h_st->reason = st.reason;
     FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FX_OK;
+}
+
+// ------------------------------------------------ Jacobi for the conv-diff operator (new)
+//
+// z = r / diag(A): diag = sigma + coeff (-kappa 2 (1/dx^2 + 1/dy^2) + |vx|/dx + |vy|/dy) inside
+// (the upwind differences put |v|/h on the diagonal), 1 on the ring.
+struct FlatCdJacobi {
+    double *z;
+    const double *r, *kappa, *vx, *vy;
+    double kap_s, sigma, coeff, inv_dx, inv_dy, k2;
+    size_t rows, cols;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const {
+        const size_t row = i / cols, col = i - row * cols;
+        if (row == 0 || col == 0 || row == rows - 1 || col == cols - 1) {
+            z[i] = r[i];
+            return;
+        }
+        const double kap = kappa ? kappa[i] : kap_s;
+        const double dcd = fma(-kap, k2, fma(fabs(vx[i]), inv_dx, fabs(vy[i]) * inv_dy));
+        z[i] = r[i] / fma(coeff, dcd, sigma);
+    }
+};
+
+struct CdJacobiPc : fx_precond {
+    const fx_op *op = nullptr;
+    int apply(fx_buf *z, const fx_buf *r, const int *skip, bool) override {
+        FX_TRY(check_same(z, r));
+        if (z->dtype != FX_F64 || z->len != op->g.rows * op->g.cols)
+            return fail(FX_ERR_DIMENSION_MISMATCH, "Jacobi preconditioner: vectors must be F64 fields of the operator's grid");
+        const ConvDiffC<double> K = conv_consts<double>(op->g.dx, op->g.dy);
+        FlatCdJacobi f{(double *)z->ptr, (const double *)r->ptr,
+                       op->kappa ? (const double *)op->kappa->ptr : nullptr, (const double *)op->vx->ptr,
+                       (const double *)op->vy->ptr, op->kappa_s, op->sigma, op->coeff, K.inv_dx, K.inv_dy, K.k2,
+                       op->g.rows, op->g.cols};
+        return launch_flat<0>(ctx, z->len, f, NoFin{}, skip, "cd_jacobi");
+    }
+};
+
+int check_op(const fx_grid &g, const fx_op *op) {
+    if (!op) return fail(FX_ERR_INVALID_ARGUMENT, "null operator");
+    if (op->g.rows != g.rows || op->g.cols != g.cols)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "operator grid does not match the solver grid");
     return FX_OK;
 }
 
@@ -2568,6 +2663,85 @@ int fx_fgmres_solve_preconditioned(fx_fgmres *s, fx_buf *x, const fx_buf *b, dou
                                    const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     return fgmres_entry(s, x, b, coeff, st, bc, pc, out);
+}
+
+// ---- conv-diff operator in the solvers (new)
+
+int fx_op_conv_diff(fx_ctx *ctx, const fx_grid *g, double sigma, double coeff, const fx_buf *kappa, double kappa_s,
+                    const fx_buf *vx, const fx_buf *vy, fx_op **out) {
+    if (!ctx || !g || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    FX_TRY(check_grid(g));
+    const size_t n = g->rows * g->cols;
+    if (g->rows < 3 || g->cols < 3) return fail(FX_ERR_INVALID_ARGUMENT, "conv-diff operator needs at least 3 x 3 points");
+    for (const fx_buf *f : {vx, vy, kappa}) {
+        if (f == kappa && !kappa) continue;
+        FX_TRY(check_buf(f, "conv-diff field"));
+        if (f->dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "conv-diff fields must be F64");
+        if (f->len != n) return fail(FX_ERR_DIMENSION_MISMATCH, "conv-diff field length does not match the grid");
+    }
+    fx_op *op = new fx_op();
+    op->ctx = ctx;
+    op->g = *g;
+    op->sigma = sigma;
+    op->coeff = coeff;
+    op->kappa = kappa;
+    op->kappa_s = kappa_s;
+    op->vx = vx;
+    op->vy = vy;
+    *out = op;
+    return FX_OK;
+}
+int fx_op_destroy(fx_op *op) {
+    delete op;
+    return FX_OK;
+}
+int fx_op_apply(const fx_op *op, const fx_buf *v, fx_buf *out) {
+    if (!op) return fail(FX_ERR_INVALID_ARGUMENT, "null operator");
+    FX_TRY(check_buf(v, "v"));
+    FX_TRY(check_buf(out, "out"));
+    FX_TRY(check_grid_len(&op->g, v));
+    FX_TRY(check_grid_len(&op->g, out));
+    if (v->dtype != FX_F64 || out->dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "operator vectors must be F64");
+    if (v->ptr == out->ptr) return fail(FX_ERR_INVALID_ARGUMENT, "v and out must be distinct");
+    const auto A = OpMaker<double, kModeCD>::make(StencilP{}, 0.0, op->g.rows, op->g.cols, op);
+    return launch_march<double, 0>(op->ctx, op->g.rows, op->g.cols, Ld1<double>{(const double *)v->ptr},
+                                   PtApplyOp<double, kModeCD>{A, (double *)out->ptr}, NoFin{}, nullptr, "op_apply");
+}
+
+int fx_precond_jacobi_op(const fx_op *op, fx_precond **out) {
+    if (!op || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    CdJacobiPc *p = new CdJacobiPc();
+    p->ctx = op->ctx;
+    p->op = op;
+    *out = p;
+    return FX_OK;
+}
+
+extern "C++" {
+template <typename S, typename Run>
+static int op_entry(S *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_stats *out, Run run) {
+    if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(s->check_io(x, b));
+    FX_TRY(check_op(s->g, op));
+    if (s->dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "the conv-diff operator runs in F64");
+    s->op = op;
+    const int rc = run();
+    s->op = nullptr;
+    FX_TRY(rc);
+    s->stats(out);
+    return FX_OK;
+}
+}  // extern "C++"
+
+int fx_bicgstab_solve_op(fx_bicgstab *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc, fx_stats *out) {
+    return op_entry(s, x, b, op, out, [&] { return bicg_solve_impl<kModeCD>(s, x, b, op->coeff, StencilP{}, pc); });
+}
+int fx_gmres_solve_op(fx_gmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc, fx_stats *out) {
+    return op_entry(s, x, b, op, out, [&] { return gmres_solve_impl<kModeCD>(s, x, b, op->coeff, StencilP{}, pc); });
+}
+int fx_fgmres_solve_op(fx_fgmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc, fx_stats *out) {
+    return op_entry(s, x, b, op, out, [&] { return fgmres_solve_impl<kModeCD>(s, x, b, op->coeff, StencilP{}, pc); });
 }
 
 int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st, const fx_boundaries *bc,

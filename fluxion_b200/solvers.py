@@ -231,6 +231,17 @@ class _Native(LinearSolver):
         fn = getattr(L.lib(), f"fx_{self._prefix}_solve_preconditioned")
         return self._run(fn, x, b, coeff, stencil, boundaries, pc._handle(self.device))
 
+    def solve_op(self, x: Field, b: Field, op: "ConvDiffOperator", pc: Optional[Preconditioner] = None) -> SolveStats:
+        """Solve A x = b for a `ConvDiffOperator` (BiCGSTAB, GMRES and FGMRES only), with an
+        optional preconditioner."""
+        fn = getattr(L.lib(), f"fx_{self._prefix}_solve_op", None)
+        if fn is None:
+            raise NotImplementedError(f"{self.name()} does not take a ConvDiffOperator")
+        st = L.FxStats()
+        check(fn(self.h, x.storage.handle, b.storage.handle, op.h, pc._handle(self.device) if pc else None,
+                 C.byref(st)))
+        return _stats(st)
+
     def __del__(self):
         try:
             if self.h:
@@ -320,6 +331,64 @@ class BiCgStabSolver(_Native):
 
     def name(self) -> str:
         return "BiCGSTAB"
+
+
+class ConvDiffOperator:
+    """Convection-diffusion operator for `BiCgStabSolver`, `GmresSolver` and `FgmresSolver`
+    (``solve_op``; new, the reference's solvers take only v + coeff S v):
+    A v = sigma v + coeff (kappa Lap v + vx dv/dx + vy dv/dy) inside, first-order upwind on the
+    sign of v as ``apply_conv_diff`` (backend.rs:375-384), A v = v on the ring.  sigma = 1 is
+    the implicit-step operator, sigma = 0 the steady one.  ``kappa`` is an F64 `Field` or a
+    float; ``vx``, ``vy`` are F64 fields, kept alive by the operator."""
+
+    def __init__(self, grid: Grid, vx: Field, vy: Field, kappa, sigma: float = 1.0, coeff: float = 1.0):
+        self.device = vx.device()
+        self.grid = grid
+        kf = kappa if isinstance(kappa, Field) else None
+        ks = 0.0 if kf is not None else float(kappa)
+        self._keep = (vx, vy, kf)
+        g = grid_c(grid)
+        out = C.c_void_p()
+        check(L.lib().fx_op_conv_diff(self.device.backend().ctx, C.byref(g), float(sigma), float(coeff),
+                                      kf.storage.handle if kf is not None else None, ks, vx.storage.handle,
+                                      vy.storage.handle, C.byref(out)))
+        self.h = out.value
+
+    def apply(self, v: Field, out: Field) -> None:
+        """out = A v."""
+        check(L.lib().fx_op_apply(self.h, v.storage.handle, out.storage.handle))
+
+    def jacobi(self) -> "OperatorJacobi":
+        return OperatorJacobi(self)
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().fx_op_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class OperatorJacobi(Preconditioner):
+    """z = r / diag(A) for a `ConvDiffOperator` (fx_precond_jacobi_op)."""
+
+    def __init__(self, op: ConvDiffOperator):
+        self._op = op  # the native preconditioner reads the operator
+        out = C.c_void_p()
+        check(L.lib().fx_precond_jacobi_op(op.h, C.byref(out)))
+        self.h = out.value
+
+    def _handle(self, device: Device) -> int:
+        return self.h
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().fx_precond_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 class InnerCg(Preconditioner):

@@ -99,6 +99,7 @@ typedef struct fx_gmres fx_gmres;
 typedef struct fx_graph fx_graph;
 typedef struct fx_fcg fx_fcg;
 typedef struct fx_fgmres fx_fgmres;
+typedef struct fx_op fx_op;
 typedef struct fx_ir fx_ir;
 
 /* ------------------------------------------------------------------ */
@@ -397,6 +398,29 @@ int fx_fgmres_solve(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, cons
 int fx_fgmres_solve_preconditioned(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff,
                                    const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
                                    fx_stats *out);
+
+/* Convection-diffusion operator for the non-symmetric solvers (new; the reference applies
+ * apply_conv_diff / conv_diff_axpy (backend.rs:375-405) but solves only v + coeff S v):
+ * A v = sigma v + coeff (kappa Lap v + vx dv/dx + vy dv/dy) on the interior, first-order
+ * upwind on the sign of v as apply_conv_diff, A v = v on the ring.  sigma = 1 is the
+ * implicit-step operator (conv_diff_axpy(coeff, v, v)); sigma = 0 the steady operator.
+ * kappa: an F64 field, or NULL for the scalar kappa_s; vx, vy: F64 fields.  The fields are
+ * borrowed and must outlive the operator. */
+int fx_op_conv_diff(fx_ctx *ctx, const fx_grid *g, double sigma, double coeff, const fx_buf *kappa,
+                    double kappa_s, const fx_buf *vx, const fx_buf *vy, fx_op **out);
+int fx_op_destroy(fx_op *op);
+/* out = A v (v and out distinct F64 fields of the operator's grid) */
+int fx_op_apply(const fx_op *op, const fx_buf *v, fx_buf *out);
+/* Jacobi preconditioner of the operator: z = r / diag(A); valid while op lives */
+int fx_precond_jacobi_op(const fx_op *op, fx_precond **out);
+/* BiCGSTAB, GMRES(m) and flexible GMRES(m) on the operator (pc may be NULL): the same loops,
+ * recurrences and stop tests as fx_bicgstab_solve*, fx_gmres_solve* and fx_fgmres_solve* */
+int fx_bicgstab_solve_op(fx_bicgstab *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc,
+                         fx_stats *out);
+int fx_gmres_solve_op(fx_gmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc,
+                      fx_stats *out);
+int fx_fgmres_solve_op(fx_fgmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc,
+                       fx_stats *out);
 
 #ifdef __cplusplus
 }

@@ -357,19 +357,25 @@ void fxo_zero_boundaries(double *x, size_t rows, size_t cols) {
 /* Convection-diffusion, ops.rs:673-791                                */
 /* ------------------------------------------------------------------ */
 
-static inline double conv_diff_at(const double *src, const double *k, const double *vxs,
-                                  const double *vys, size_t idx, size_t cols, double inv_dx,
-                                  double inv_dy, double inv_dx2, double inv_dy2) {
+static inline double conv_diff_at_k(const double *src, double kap, const double *vxs,
+                                    const double *vys, size_t idx, size_t cols, double inv_dx,
+                                    double inv_dy, double inv_dx2, double inv_dy2) {
     double c = src[idx];
     double lap = fma(src[idx - 1] + src[idx + 1], inv_dx2,
                      (src[idx - cols] + src[idx + cols]) * inv_dy2) -
                  2.0 * (inv_dx2 + inv_dy2) * c; /* ops.rs:711-713 */
-    double diff = k[idx] * lap;
+    double diff = kap * lap;
     double vx_i = vxs[idx], vy_i = vys[idx];
     double dudx = vx_i >= 0.0 ? (c - src[idx - 1]) * inv_dx : (src[idx + 1] - c) * inv_dx;
     double dudy = vy_i >= 0.0 ? (c - src[idx - cols]) * inv_dy : (src[idx + cols] - c) * inv_dy;
     double conv = fma(vx_i, dudx, vy_i * dudy); /* ops.rs:729-730 */
     return diff + conv;
+}
+
+static inline double conv_diff_at(const double *src, const double *k, const double *vxs,
+                                  const double *vys, size_t idx, size_t cols, double inv_dx,
+                                  double inv_dy, double inv_dx2, double inv_dy2) {
+    return conv_diff_at_k(src, k[idx], vxs, vys, idx, cols, inv_dx, inv_dy, inv_dx2, inv_dy2);
 }
 
 void fxo_apply_conv_diff(const double *u, double *out, const double *kappa, const double *vx,
@@ -563,13 +569,61 @@ int fxo_prolong_bilinear(const double *c, double *fine, size_t crows, size_t cco
 
 static size_t op_len(const fxo_op *op) { return op->rows * op->cols; }
 
+/* conv-diff operator: ring out = inp; interior fma(coeff, CD(inp), sigma * inp) */
+static void apply_cd(const fxo_op *op, double *out, const double *inp) {
+    size_t rows = op->rows, cols = op->cols;
+    double inv_dx = 1.0 / op->dx, inv_dy = 1.0 / op->dy;
+    double inv_dx2 = inv_dx * inv_dx, inv_dy2 = inv_dy * inv_dy;
+    for (size_t col = 0; col < cols; col++) {
+        out[col] = inp[col];
+        out[(rows - 1) * cols + col] = inp[(rows - 1) * cols + col];
+    }
+    for (size_t row = 1; row < rows - 1; row++) {
+        out[row * cols] = inp[row * cols];
+        out[row * cols + cols - 1] = inp[row * cols + cols - 1];
+    }
+#pragma omp parallel for schedule(static)
+    for (size_t row = 1; row < rows - 1; row++)
+        for (size_t col = 1; col < cols - 1; col++) {
+            size_t idx = row * cols + col;
+            double kap = op->kappa ? op->kappa[idx] : op->kappa_s;
+            double v = conv_diff_at_k(inp, kap, op->vx, op->vy, idx, cols, inv_dx, inv_dy, inv_dx2, inv_dy2);
+            out[idx] = fma(op->coeff, v, op->sigma * inp[idx]);
+        }
+}
+
+void fxo_cd_jacobi_apply(void *ctx, double *z, const double *r) {
+    const fxo_op *op = (const fxo_op *)ctx;
+    size_t rows = op->rows, cols = op->cols;
+    double inv_dx = 1.0 / op->dx, inv_dy = 1.0 / op->dy;
+    double k2 = 2.0 * (inv_dx * inv_dx + inv_dy * inv_dy);
+#pragma omp parallel for schedule(static)
+    for (size_t row = 0; row < rows; row++)
+        for (size_t col = 0; col < cols; col++) {
+            size_t idx = row * cols + col;
+            if (row == 0 || col == 0 || row == rows - 1 || col == cols - 1) {
+                z[idx] = r[idx];
+                continue;
+            }
+            double kap = op->kappa ? op->kappa[idx] : op->kappa_s;
+            double dcd = fma(-kap, k2, fma(fabs(op->vx[idx]), inv_dx, fabs(op->vy[idx]) * inv_dy));
+            z[idx] = r[idx] / fma(op->coeff, dcd, op->sigma);
+        }
+}
+
 /* out = inp; out += coeff * S(inp)  (cg.rs:106-109, pipelined_cg.rs:332-343) */
 static int apply_op(const fxo_op *op, double *out, const double *inp) {
+    if (op->cd) {
+        apply_cd(op, out, inp);
+        return 0;
+    }
     if (out != inp) fxo_copy(inp, out, op_len(op));
     /* stencil_axpy reads inp while writing out; out != inp here so a copy suffices */
     return fxo_stencil_axpy(op->coeff, inp, out, op->rows, op->cols, op->ne, op->dr, op->dc,
                             op->w, op->bcs);
 }
+
+int fxo_op_apply(const fxo_op *op, double *out, const double *v) { return apply_op(op, out, v); }
 
 static void set_stats(fxo_stats *st, size_t it, double res, int reason) {
     st->iterations = it;

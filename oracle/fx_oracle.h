@@ -133,7 +133,20 @@ typedef struct {
     const int *dr, *dc;
     const double *w;
     const fxo_bc *bcs;
+    /* cd != 0: the convection-diffusion operator instead of the stencil (new; no reference
+     * solver takes it): A v = sigma v + coeff (kappa Lap v + vx dv/dx + vy dv/dy) on the
+     * interior, first-order upwind as apply_conv_diff (ops.rs:673-791), A v = v on the ring;
+     * kappa from the field when non-null, else kappa_s */
+    int cd;
+    double sigma, kappa_s, dx, dy;
+    const double *kappa, *vx, *vy;
 } fxo_op;
+/* out = A v for either operator kind (out != v) */
+int fxo_op_apply(const fxo_op *op, double *out, const double *v);
+/* pointwise Jacobi for the conv-diff operator, usable as fxo_pc_fn with ctx = the fxo_op:
+ * z = r / diag(A), diag = sigma + coeff (-kappa 2 (1/dx^2 + 1/dy^2) + |vx|/dx + |vy|/dy) inside,
+ * 1 on the ring */
+void fxo_cd_jacobi_apply(void *op, double *z, const double *r);
 
 int fxo_cg_solve(const fxo_op *op, double *x, const double *b, double tol, size_t max_iter,
                  fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);

@@ -38,6 +38,8 @@ class Op(C.Structure):
     _fields_ = [
         ("rows", C.c_size_t), ("cols", C.c_size_t), ("coeff", C.c_double), ("ne", C.c_int),
         ("dr", _ip), ("dc", _ip), ("w", _dp), ("bcs", C.POINTER(Bc)),
+        ("cd", C.c_int), ("sigma", C.c_double), ("kappa_s", C.c_double), ("dx", C.c_double), ("dy", C.c_double),
+        ("kappa", _dp), ("vx", _dp), ("vy", _dp),
     ]
 
 
@@ -107,6 +109,8 @@ def _declare(L):
     d("fxo_fcg_solve", C.c_int, opp, _dp, _dp, C.c_double, _sz, PC_FN, C.c_void_p, stp)
     d("fxo_fgmres_solve", C.c_int, opp, _dp, _dp, _sz, C.c_double, _sz, PC_FN, C.c_void_p, stp)
     d("fxo_inner_cg_pc_apply", None, C.c_void_p, _dp, _dp)
+    d("fxo_op_apply", C.c_int, opp, _dp, _dp)
+    d("fxo_cd_jacobi_apply", None, C.c_void_p, _dp, _dp)
     d("fxo_mg_create", C.c_void_p, _sz, _sz, C.c_double, C.c_double, bcp, C.c_int, C.c_int,
       C.c_double, C.c_int, C.c_double, C.c_int, _ip, _ip, _dp, C.c_int, C.c_int)
     d("fxo_mg_destroy", None, C.c_void_p)
@@ -384,6 +388,59 @@ def bicgstab_solve(x, b, rows, cols, coeff, entries, tol, max_iter, bcs=ZERO_DIR
     fn, ctx = _pc_args(pc)
     _chk(lib().fxo_bicgstab_solve(C.byref(_op(rows, cols, coeff, entries, bcs)), _p(x), _p(b), tol,
                                   max_iter, fn, ctx, C.byref(st)), "bicgstab")
+    return st.iterations, st.residual, st.reason
+
+
+def cd_op(rows, cols, dx, dy, vx, vy, kappa=None, kappa_s=0.0, sigma=1.0, coeff=1.0):
+    """Conv-diff operator A v = sigma v + coeff (kappa Lap v + v.grad v) inside, v on the ring
+    (fxo_op with cd = 1).  kappa: a field, or None for the scalar kappa_s.  The arrays must be
+    contiguous float64 and are kept alive by the returned object."""
+    vx = np.ascontiguousarray(vx, dtype=np.float64)
+    vy = np.ascontiguousarray(vy, dtype=np.float64)
+    k = None if kappa is None else np.ascontiguousarray(kappa, dtype=np.float64)
+    op = Op()
+    op.rows, op.cols, op.coeff = rows, cols, coeff
+    op.cd, op.sigma, op.kappa_s, op.dx, op.dy = 1, sigma, kappa_s, dx, dy
+    op.vx, op.vy = _p(vx), _p(vy)
+    op.kappa = _p(k) if k is not None else C.cast(None, _dp)
+    op._keep = (vx, vy, k)
+    return op
+
+
+def op_apply(op, v):
+    """A v for an Op (stencil or conv-diff)."""
+    out = np.empty_like(v)
+    _chk(lib().fxo_op_apply(C.byref(op), _p(out), _p(np.ascontiguousarray(v))), "op_apply")
+    return out
+
+
+class CdJacobiPC:
+    """z = r / diag(A) for a conv-diff Op (fxo_cd_jacobi_apply)."""
+
+    def __init__(self, op):
+        self._op = op
+        self._cb = C.cast(lib().fxo_cd_jacobi_apply, PC_FN)
+        self._ctx = C.cast(C.pointer(op), C.c_void_p)
+
+
+def bicgstab_solve_op(x, b, op, tol, max_iter, pc=None):
+    st = Stats()
+    fn, ctx = _pc_args(pc)
+    _chk(lib().fxo_bicgstab_solve(C.byref(op), _p(x), _p(b), tol, max_iter, fn, ctx, C.byref(st)), "bicgstab")
+    return st.iterations, st.residual, st.reason
+
+
+def gmres_solve_op(x, b, op, restart, tol, max_iter, pc=None):
+    st = Stats()
+    fn, ctx = _pc_args(pc)
+    _chk(lib().fxo_gmres_solve(C.byref(op), _p(x), _p(b), restart, tol, max_iter, fn, ctx, C.byref(st)), "gmres")
+    return st.iterations, st.residual, st.reason
+
+
+def fgmres_solve_op(x, b, op, restart, tol, max_iter, pc=None):
+    st = Stats()
+    fn, ctx = _pc_args(pc)
+    _chk(lib().fxo_fgmres_solve(C.byref(op), _p(x), _p(b), restart, tol, max_iter, fn, ctx, C.byref(st)), "fgmres")
     return st.iterations, st.residual, st.reason
 
 

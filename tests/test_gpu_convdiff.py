@@ -1,0 +1,97 @@
+"""The convection-diffusion operator in the GPU solvers against the oracle: the operator and its
+Jacobi preconditioner bit for bit, and BiCGSTAB, GMRES and flexible GMRES on the steady
+problem (-nu Lap u + v.grad u = f) and on an implicit step ((I + dt CD) u = b) with the oracle's
+stop reasons, close iteration counts, and the tolerance met on the FP64 residual recomputed by
+the oracle's operator."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    from fluxion_b200 import Device
+    return Device.best()
+
+
+def _problem(n, dev, nu=1e-2, sigma=0.0, coeff=1.0, kappa_field=False, seed=5):
+    from fluxion_b200 import ConvDiffOperator, Field, Grid
+    from fluxion_b200.workloads import poisson_uniform_rhs, stream_velocity
+    N, h = n + 2, 1.0 / (n + 1)
+    g = Grid.square(N, h)
+    vx, vy = stream_velocity(n, seed)
+    kappa = np.full(N * N, -nu) if kappa_field else None
+    f = poisson_uniform_rhs(n, seed + 1)
+    VX, VY = Field.from_f64(g, vx, dev), Field.from_f64(g, vy, dev)
+    K = Field.from_f64(g, kappa, dev) if kappa_field else -nu
+    op = ConvDiffOperator(g, VX, VY, K, sigma=sigma, coeff=coeff)
+    oop = O.cd_op(N, N, h, h, vx, vy, kappa=kappa, kappa_s=-nu, sigma=sigma, coeff=coeff)
+    return g, N, f, op, oop
+
+
+@pytest.mark.parametrize("kappa_field,sigma,coeff", [(False, 0.0, 1.0), (True, 1.0, -2e-3), (True, 0.3, 0.8)])
+def test_operator_and_jacobi_match_oracle_bitwise(dev, kappa_field, sigma, coeff):
+    from fluxion_b200 import DType, Field
+    g, N, f, op, oop = _problem(61, dev, sigma=sigma, coeff=coeff, kappa_field=kappa_field)
+    u = np.random.default_rng(2).uniform(-1, 1, N * N)
+    U, out = Field.from_f64(g, u, dev), Field.zeros(g, DType.F64, dev)
+    op.apply(U, out)
+    assert np.array_equal(out.to_vec_f64(), O.op_apply(oop, u))
+    z = Field.zeros(g, DType.F64, dev)
+    op.jacobi().apply(z, U)
+    zo = np.zeros(N * N)
+    O.lib().fxo_cd_jacobi_apply(O.CdJacobiPC(oop)._ctx, O._p(zo), O._p(u))
+    assert np.array_equal(z.to_vec_f64(), zo)
+
+
+@pytest.mark.parametrize("solver,jacobi", [("bicgstab", False), ("bicgstab", True), ("gmres", True),
+                                           ("fgmres", True), ("fgmres", False)])
+def test_steady_conv_diff_solve_matches_oracle(dev, solver, jacobi):
+    from fluxion_b200 import BiCgStabSolver, DType, FgmresSolver, Field, GmresSolver
+    g, N, f, op, oop = _problem(63, dev)
+    tol = 1e-10 * np.linalg.norm(f)
+    b = Field.from_f64(g, f, dev)
+    x = Field.zeros(g, DType.F64, dev)
+    pc = op.jacobi() if jacobi else None
+    opc = O.CdJacobiPC(oop) if jacobi else None
+    xo = np.zeros(N * N)
+    if solver == "bicgstab":
+        s = BiCgStabSolver(g, dev, tol, 5000).solve_op(x, b, op, pc)
+        it, _, reason = O.bicgstab_solve_op(xo, f, oop, tol, 5000, opc)
+    elif solver == "gmres":
+        s = GmresSolver(g, dev, 30, tol, 5000).solve_op(x, b, op, pc)
+        it, _, reason = O.gmres_solve_op(xo, f, oop, 30, tol, 5000, opc)
+    else:
+        s = FgmresSolver(g, dev, 30, tol, 5000).solve_op(x, b, op, pc)
+        it, _, reason = O.fgmres_solve_op(xo, f, oop, 30, tol, 5000, opc)
+    assert int(s.reason) == reason == 0
+    # hundreds of non-symmetric Krylov steps: roundoff in the inner products (compensated on the
+    # GPU, Kahan in the oracle) moves the stopping step by a few
+    assert abs(s.iterations - it) <= max(3, it // 20), (s.iterations, it)
+    xv = x.to_vec_f64()
+    true = np.linalg.norm(O.op_apply(oop, xv) - f)
+    if solver != "gmres":
+        assert true < 1.01 * tol
+        assert rel_err(xv, xo) < 1e-7  # two solutions within the tolerance differ by ~1e-9
+    else:  # left-preconditioned GMRES stops on ||M^-1 r||, as the reference's
+        assert rel_err(xv, xo) < 1e-5
+
+
+def test_implicit_step_matches_oracle(dev):
+    """(I + dt CD) u = b with kappa = -nu: a backward-Euler step of u_t = nu Lap u - v.grad u,
+    the operator conv_diff_axpy(dt, u, u) of the reference's implicit use."""
+    from fluxion_b200 import BiCgStabSolver, DType, Field
+    g, N, f, op, oop = _problem(127, dev, nu=1e-3, sigma=1.0, coeff=5e-3, kappa_field=True)
+    tol = 1e-10 * np.linalg.norm(f)
+    b = Field.from_f64(g, f, dev)
+    x = Field.zeros(g, DType.F64, dev)
+    s = BiCgStabSolver(g, dev, tol, 500).solve_op(x, b, op, op.jacobi())
+    xo = np.zeros(N * N)
+    it, _, reason = O.bicgstab_solve_op(xo, f, oop, tol, 500, O.CdJacobiPC(oop))
+    assert s.converged() and reason == 0 and abs(s.iterations - it) <= 1
+    assert np.linalg.norm(O.op_apply(oop, x.to_vec_f64()) - f) < 1.01 * tol
+    assert rel_err(x.to_vec_f64(), xo) < 1e-9
