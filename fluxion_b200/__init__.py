@@ -15,7 +15,7 @@ __all__ = [
     "CgSolver", "CgStats", "PipelinedCgSolver", "BiCgStabSolver", "GmresSolver", "Multigrid", "SmootherKind",
     "Identity", "Preconditioner", "LinearSolver", "SolveStats", "ConvergenceReason",
     "MixedPrecisionRefinement", "CudaGraph", "FcgSolver", "FgmresSolver", "InnerCg",
-    "ConvDiffOperator", "OperatorJacobi",
+    "ConvDiffOperator", "OperatorJacobi", "ConvDiffMultigrid",
 ]
 
 
@@ -30,7 +30,7 @@ def __getattr__(name):
         return getattr(field, name)
     if name in ("CgSolver", "CgStats", "PipelinedCgSolver", "BiCgStabSolver", "GmresSolver", "Multigrid",
                 "MixedPrecisionRefinement", "FcgSolver", "FgmresSolver", "InnerCg",
-                "ConvDiffOperator", "OperatorJacobi", "SmootherKind", "Identity", "Preconditioner", "LinearSolver", "SolveStats",
+                "ConvDiffOperator", "OperatorJacobi", "ConvDiffMultigrid", "SmootherKind", "Identity", "Preconditioner", "LinearSolver", "SolveStats",
                 "ConvergenceReason"):
         from . import solvers
         return getattr(solvers, name)

@@ -2170,6 +2170,215 @@ int check_op(const fx_grid &g, const fx_op *op) {
     return FX_OK;
 }
 
+// ------------------------------------------------ multigrid for the conv-diff operator (new)
+//
+// Vertex hierarchy (rows - 1 halves while both interiors exceed coarse_max, as the vertex
+// multigrid).  Each coarse level rediscretises the operator with h doubled and kappa / vx / vy
+// injected from the coincident fine points.  Smoother: x <- x + omega (b - A x) / diag(A)
+// inside; full weighting down, bilinear up; `coarse_sweeps` sweeps on the coarsest level in
+// one block; every cycle from x = 0.  Unfused (a sweep, residual and transfer pass each): the
+// variable coefficients do not fit the constant-stencil level kernels.
+
+__device__ __forceinline__ double cd_diag(const OpA<double, kModeCD> &A, size_t idx) {
+    const double kap = A.kappa ? A.kappa[idx] : A.kap_s;
+    return fma(A.coeff, fma(-kap, A.K.k2, fma(fabs(A.vx[idx]), A.K.inv_dx, fabs(A.vy[idx]) * A.K.inv_dy)), A.sigma);
+}
+
+struct PtCdSweep {  // out = x + omega (b - A x) / diag(A) inside; the ring is not written
+    static constexpr int NA = 1;
+    OpA<double, kModeCD> A;
+    double *out;
+    const double *b;
+    double omega;
+    __device__ __forceinline__ const double *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int, int, size_t idx, const Nb<double> &nb, const double *a,
+                                               CSum *) const {
+        if (ring) return;
+        out[idx] = fma(omega, (a[0] - A.apply(false, nb, idx)) / cd_diag(A, idx), nb.c);
+    }
+};
+
+struct PtCdResid {  // out = b - A x inside
+    static constexpr int NA = 1;
+    OpA<double, kModeCD> A;
+    double *out;
+    const double *b;
+    __device__ __forceinline__ const double *aux(int) const { return b; }
+    __device__ __forceinline__ void operator()(bool ring, int, int, size_t idx, const Nb<double> &nb, const double *a,
+                                               CSum *) const {
+        if (ring) return;
+        out[idx] = a[0] - A.apply(false, nb, idx);
+    }
+};
+
+struct FlatInject {  // coarse field = fine field at the coincident points
+    const double *f;
+    double *c;
+    size_t fcols, ccols;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const {
+        const size_t I = i / ccols, J = i - I * ccols;
+        c[i] = f[(2 * I) * fcols + 2 * J];
+    }
+};
+
+// Coarsest level in one block: the iterate ping-pongs in shared memory, each thread keeps its
+// points' rhs and diagonal in registers; every point value is PtCdSweep's expression.
+__global__ void __launch_bounds__(1024) k_cd_coarse(double *u, const double *__restrict__ b, int rows, int cols,
+                                                    OpA<double, kModeCD> A, double omega, int nsweeps,
+                                                    const int *skip) {
+    if (skip && *(volatile const int *)skip) return;
+    constexpr int kPts = 4;
+    extern __shared__ unsigned char smem_raw[];
+    double *s0 = reinterpret_cast<double *>(smem_raw);
+    double *s1 = s0 + rows * cols;
+    const int n = rows * cols;
+    int idx[kPts];
+    bool inner[kPts];
+    double bv[kPts], dv[kPts];
+#pragma unroll
+    for (int k = 0; k < kPts; k++) {
+        const int i = threadIdx.x + k * blockDim.x;
+        idx[k] = i;
+        const int r = i / cols, c = i % cols;
+        inner[k] = i < n && r > 0 && c > 0 && r < rows - 1 && c < cols - 1;
+        bv[k] = inner[k] ? b[i] : 0.0;
+        dv[k] = inner[k] ? cd_diag(A, (size_t)i) : 1.0;
+        if (i < n) {
+            s0[i] = 0.0;
+            s1[i] = 0.0;
+        }
+    }
+    __syncthreads();
+    for (int k = 0; k < nsweeps; k++) {
+        const double *src = (k & 1) ? s1 : s0;
+        double *dst = (k & 1) ? s0 : s1;
+#pragma unroll
+        for (int q = 0; q < kPts; q++) {
+            if (!inner[q]) continue;
+            const int i = idx[q];
+            Nb<double> nb;
+            nb.c = src[i];
+            nb.n = src[i - cols];
+            nb.s = src[i + cols];
+            nb.w = src[i - 1];
+            nb.e = src[i + 1];
+            dst[i] = fma(omega, (bv[q] - A.apply(false, nb, (size_t)i)) / dv[q], nb.c);
+        }
+        __syncthreads();
+    }
+    const double *fin = (nsweeps & 1) ? s1 : s0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) u[i] = fin[i];
+}
+
+struct CdLevel {
+    size_t rows = 0, cols = 0;
+    double dx = 0, dy = 0;
+    fx_buf *u = nullptr, *rhs = nullptr, *tmp = nullptr;    // levels >= 1
+    fx_buf *vx = nullptr, *vy = nullptr, *kappa = nullptr;  // levels >= 1, injected
+};
+
+}  // namespace
+
+struct fx_cdmg {
+    fx_ctx *ctx = nullptr;
+    const fx_op *op = nullptr;
+    size_t n_pre = 2, n_post = 2, coarse_sweeps = 200;
+    double omega = 0.8;
+    std::vector<CdLevel> lv;
+    fx_buf *tmp0 = nullptr;  // level-0 ping-pong partner
+    struct View : fx_precond {
+        fx_cdmg *mg = nullptr;
+        int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) override;
+    } view;
+    ~fx_cdmg() {
+        for (auto &L : lv)
+            for (fx_buf *f : {L.u, L.rhs, L.tmp, L.vx, L.vy, L.kappa}) fx_free(f);
+        fx_free(tmp0);
+    }
+    OpA<double, kModeCD> level_op(size_t l) const {
+        OpA<double, kModeCD> A = OpMaker<double, kModeCD>::make(StencilP{}, 0.0, 0, 0, op);
+        if (l > 0) {
+            const CdLevel &L = lv[l];
+            A.K = conv_consts<double>(L.dx, L.dy);
+            A.vx = (const double *)L.vx->ptr;
+            A.vy = (const double *)L.vy->ptr;
+            A.kappa = L.kappa ? (const double *)L.kappa->ptr : nullptr;
+        }
+        return A;
+    }
+};
+
+namespace {
+
+int cd_cycle(fx_cdmg *mg, double *x, const double *b, const int *skip) {  // x holds zeros on entry
+    fx_ctx *ctx = mg->ctx;
+    const int nl = (int)mg->lv.size();
+    std::vector<double *> cur(nl), oth(nl);
+    std::vector<const double *> rhs(nl);
+    cur[0] = x;
+    oth[0] = (double *)mg->tmp0->ptr;
+    rhs[0] = b;
+    for (int l = 1; l < nl; l++) {
+        cur[l] = (double *)mg->lv[l].u->ptr;
+        oth[l] = (double *)mg->lv[l].tmp->ptr;
+        rhs[l] = (const double *)mg->lv[l].rhs->ptr;
+    }
+    auto smooth = [&](int l, size_t n) -> int {
+        const CdLevel &L = mg->lv[l];
+        const auto A = mg->level_op(l);
+        for (size_t k = 0; k < n; k++) {
+            FX_TRY((launch_march<double, 0>(ctx, L.rows, L.cols, Ld1<double>{cur[l]},
+                                            PtCdSweep{A, oth[l], rhs[l], mg->omega}, NoFin{}, skip, "cdmg_sweep")));
+            std::swap(cur[l], oth[l]);
+        }
+        return FX_OK;
+    };
+    for (int l = 0; l < nl - 1; l++) {
+        const CdLevel &L = mg->lv[l], &Cl = mg->lv[l + 1];
+        FX_TRY(smooth(l, mg->n_pre));
+        FX_TRY((launch_march<double, 0>(ctx, L.rows, L.cols, Ld1<double>{cur[l]},
+                                        PtCdResid{mg->level_op(l), oth[l], rhs[l]}, NoFin{}, skip, "cdmg_residual")));
+        FX_TRY(restrict_fw<double>(ctx, oth[l], (double *)Cl.rhs->ptr, L.cols, Cl.rows, Cl.cols, skip));
+        FX_TRY(zero_fill<double>(ctx, cur[l + 1], Cl.rows * Cl.cols, skip));
+    }
+    {
+        const int l = nl - 1;
+        const CdLevel &L = mg->lv[l];
+        const size_t n = L.rows * L.cols;
+        if (coarse_fits(n, sizeof(double)) && mg->coarse_sweeps > 0) {
+            k_cd_coarse<<<1, coarse_threads(n), 2 * n * sizeof(double), ctx->stream>>>(
+                cur[l], rhs[l], (int)L.rows, (int)L.cols, mg->level_op(l), mg->omega, (int)mg->coarse_sweeps, skip);
+            FX_TRY(check_launch(ctx, "cdmg_coarse_solve"));
+        } else {
+            FX_TRY(smooth(l, mg->coarse_sweeps));
+        }
+    }
+    for (int l = nl - 2; l >= 0; l--) {
+        const CdLevel &L = mg->lv[l], &Cl = mg->lv[l + 1];
+        FX_TRY(prolong_bilinear<double>(ctx, cur[l + 1], cur[l], Cl.cols, L.rows, L.cols, skip));
+        FX_TRY(smooth(l, mg->n_post));
+    }
+    if (cur[0] != x) {
+        const CdLevel &L0 = mg->lv[0];
+        FX_CUDA(cudaMemcpyAsync(x, cur[0], L0.rows * L0.cols * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return FX_OK;
+}
+
+}  // namespace
+
+int fx_cdmg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) {
+    FX_TRY(check_same(z, r));
+    const CdLevel &L0 = mg->lv[0];
+    if (z->dtype != FX_F64 || z->len != L0.rows * L0.cols)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "conv-diff multigrid: vectors must be F64 fields of the operator's grid");
+    if (z->ptr == r->ptr) return fail(FX_ERR_INVALID_ARGUMENT, "z and r must be distinct");
+    if (!z_zero) FX_TRY(zero_fill<double>(ctx, (double *)z->ptr, z->len, skip));
+    return cd_cycle(mg, (double *)z->ptr, (const double *)r->ptr, skip);
+}
+
+namespace {
+
 // ------------------------------------------------ inner-CG preconditioner (new)
 //
 // z = a fixed number of CG steps (preconditioned by `inner` when set) on A z = r from z = 0,
@@ -2743,6 +2952,74 @@ int fx_gmres_solve_op(fx_gmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, 
 int fx_fgmres_solve_op(fx_fgmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc, fx_stats *out) {
     return op_entry(s, x, b, op, out, [&] { return fgmres_solve_impl<kModeCD>(s, x, b, op->coeff, StencilP{}, pc); });
 }
+
+int fx_cdmg_create(const fx_op *op, size_t n_pre, size_t n_post, double omega, size_t coarse_max,
+                   size_t coarse_sweeps, fx_cdmg **out) {
+    if (!op || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    fx_cdmg *mg = new fx_cdmg();
+    mg->ctx = op->ctx;
+    mg->op = op;
+    mg->n_pre = n_pre;
+    mg->n_post = n_post;
+    mg->omega = omega;
+    mg->coarse_sweeps = coarse_sweeps;
+    mg->view.ctx = op->ctx;
+    mg->view.mg = mg;
+    mg->view.borrowed = true;
+    size_t r = op->g.rows, c = op->g.cols;
+    double hx = op->g.dx, hy = op->g.dy;
+    int rc = FX_OK;
+    for (int l = 0; l < 40 && rc == FX_OK; l++) {
+        CdLevel L;
+        L.rows = r;
+        L.cols = c;
+        L.dx = hx;
+        L.dy = hy;
+        if (l > 0) {
+            const CdLevel &F = mg->lv[l - 1];
+            const double *fvx = l == 1 ? (const double *)op->vx->ptr : (const double *)F.vx->ptr;
+            const double *fvy = l == 1 ? (const double *)op->vy->ptr : (const double *)F.vy->ptr;
+            const double *fk = op->kappa ? (l == 1 ? (const double *)op->kappa->ptr : (const double *)F.kappa->ptr)
+                                         : nullptr;
+            for (fx_buf **bp : {&L.u, &L.rhs, &L.tmp, &L.vx, &L.vy})
+                if (rc == FX_OK) rc = fx_alloc(op->ctx, r * c, FX_F64, bp);
+            if (rc == FX_OK && fk) rc = fx_alloc(op->ctx, r * c, FX_F64, &L.kappa);
+            if (rc == FX_OK)
+                rc = launch_flat<0>(op->ctx, r * c, FlatInject{fvx, (double *)L.vx->ptr, F.cols, c}, NoFin{}, nullptr,
+                                    "cdmg_inject");
+            if (rc == FX_OK)
+                rc = launch_flat<0>(op->ctx, r * c, FlatInject{fvy, (double *)L.vy->ptr, F.cols, c}, NoFin{}, nullptr,
+                                    "cdmg_inject");
+            if (rc == FX_OK && fk)
+                rc = launch_flat<0>(op->ctx, r * c, FlatInject{fk, (double *)L.kappa->ptr, F.cols, c}, NoFin{}, nullptr,
+                                    "cdmg_inject");
+        }
+        mg->lv.push_back(L);
+        if (!(r - 2 > coarse_max && c - 2 > coarse_max && (r - 1) % 2 == 0 && (c - 1) % 2 == 0)) break;
+        r = (r - 1) / 2 + 1;
+        c = (c - 1) / 2 + 1;
+        hx *= 2.0;
+        hy *= 2.0;
+    }
+    if (rc == FX_OK) rc = fx_alloc(op->ctx, op->g.rows * op->g.cols, FX_F64, &mg->tmp0);
+    if (rc != FX_OK) {
+        delete mg;
+        return rc;
+    }
+    *out = mg;
+    return FX_OK;
+}
+int fx_cdmg_destroy(fx_cdmg *mg) {
+    delete mg;
+    return FX_OK;
+}
+int fx_cdmg_depth(const fx_cdmg *mg, size_t *depth) {
+    if (!mg || !depth) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    *depth = mg->lv.size();
+    return FX_OK;
+}
+fx_precond *fx_cdmg_as_precond(fx_cdmg *mg) { return mg ? &mg->view : nullptr; }
 
 int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st, const fx_boundaries *bc,
                         const size_t *steps, size_t nsteps, fx_precond *inner, fx_precond **out) {

@@ -100,6 +100,7 @@ typedef struct fx_graph fx_graph;
 typedef struct fx_fcg fx_fcg;
 typedef struct fx_fgmres fx_fgmres;
 typedef struct fx_op fx_op;
+typedef struct fx_cdmg fx_cdmg;
 typedef struct fx_ir fx_ir;
 
 /* ------------------------------------------------------------------ */
@@ -413,6 +414,18 @@ int fx_op_destroy(fx_op *op);
 int fx_op_apply(const fx_op *op, const fx_buf *v, fx_buf *out);
 /* Jacobi preconditioner of the operator: z = r / diag(A); valid while op lives */
 int fx_precond_jacobi_op(const fx_op *op, fx_precond **out);
+/* Multigrid V-cycle preconditioner for the operator (new): vertex hierarchy as
+ * fx_mg_create_vertex (rows - 1 halves while both interiors exceed coarse_max), each coarse
+ * level the operator rediscretised with h doubled and kappa / vx / vy injected from the
+ * coincident fine points; weighted Jacobi (omega) with the operator's diagonal, full weighting
+ * and bilinear transfers, `coarse_sweeps` sweeps on the coarsest level; one cycle from z = 0
+ * per application.  The operator (and its fields) must outlive it; fx_cdmg_as_precond gives
+ * a borrowed handle valid until fx_cdmg_destroy. */
+int fx_cdmg_create(const fx_op *op, size_t n_pre, size_t n_post, double omega, size_t coarse_max,
+                   size_t coarse_sweeps, fx_cdmg **out);
+int fx_cdmg_destroy(fx_cdmg *mg);
+int fx_cdmg_depth(const fx_cdmg *mg, size_t *depth);
+fx_precond *fx_cdmg_as_precond(fx_cdmg *mg);
 /* BiCGSTAB, GMRES(m) and flexible GMRES(m) on the operator (pc may be NULL): the same loops,
  * recurrences and stop tests as fx_bicgstab_solve*, fx_gmres_solve* and fx_fgmres_solve* */
 int fx_bicgstab_solve_op(fx_bicgstab *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc,

@@ -1144,6 +1144,162 @@ void fxo_inner_cg_pc_apply(void *ctx, double *z, const double *r) {
 }
 
 /* ------------------------------------------------------------------ */
+/* Multigrid for the conv-diff operator (new)                          */
+/* ------------------------------------------------------------------ */
+/* Vertex hierarchy as fxo_mg mode 1 (rows-1 halves while both interiors exceed coarse_max).
+ * Each coarse level rediscretises the operator with h doubled and kappa / vx / vy injected
+ * from the coincident fine points.  Smoother: x <- x + omega (b - A x) / diag(A) inside, the
+ * ring left at 0; full weighting down, bilinear up; `coarse_sweeps` sweeps on the coarsest
+ * level; every cycle from x = 0. */
+
+struct fxo_cdmg {
+    int nlev, n_pre, n_post, coarse_sweeps;
+    double omega;
+    fxo_op op[40];
+    double *vx[40], *vy[40], *kappa[40], *u[40], *rhs[40], *tmp[40];
+};
+
+static double cd_diag(const fxo_op *op, size_t idx, double inv_dx, double inv_dy, double k2) {
+    double kap = op->kappa ? op->kappa[idx] : op->kappa_s;
+    return fma(op->coeff, fma(-kap, k2, fma(fabs(op->vx[idx]), inv_dx, fabs(op->vy[idx]) * inv_dy)), op->sigma);
+}
+
+/* out = x + omega (b - A x) / diag inside (out's ring untouched) */
+static void cd_sweep(const fxo_op *op, const double *x, double *out, const double *b, double omega) {
+    size_t rows = op->rows, cols = op->cols;
+    double inv_dx = 1.0 / op->dx, inv_dy = 1.0 / op->dy;
+    double inv_dx2 = inv_dx * inv_dx, inv_dy2 = inv_dy * inv_dy, k2 = 2.0 * (inv_dx2 + inv_dy2);
+#pragma omp parallel for schedule(static)
+    for (size_t row = 1; row < rows - 1; row++)
+        for (size_t col = 1; col < cols - 1; col++) {
+            size_t idx = row * cols + col;
+            double kap = op->kappa ? op->kappa[idx] : op->kappa_s;
+            double v = conv_diff_at_k(x, kap, op->vx, op->vy, idx, cols, inv_dx, inv_dy, inv_dx2, inv_dy2);
+            double ax = fma(op->coeff, v, op->sigma * x[idx]);
+            out[idx] = fma(omega, (b[idx] - ax) / cd_diag(op, idx, inv_dx, inv_dy, k2), x[idx]);
+        }
+}
+
+static void cd_resid(const fxo_op *op, const double *x, const double *b, double *r) {
+    size_t rows = op->rows, cols = op->cols;
+    double inv_dx = 1.0 / op->dx, inv_dy = 1.0 / op->dy;
+    double inv_dx2 = inv_dx * inv_dx, inv_dy2 = inv_dy * inv_dy;
+#pragma omp parallel for schedule(static)
+    for (size_t row = 1; row < rows - 1; row++)
+        for (size_t col = 1; col < cols - 1; col++) {
+            size_t idx = row * cols + col;
+            double kap = op->kappa ? op->kappa[idx] : op->kappa_s;
+            double v = conv_diff_at_k(x, kap, op->vx, op->vy, idx, cols, inv_dx, inv_dy, inv_dx2, inv_dy2);
+            r[idx] = b[idx] - fma(op->coeff, v, op->sigma * x[idx]);
+        }
+}
+
+static double *inject(const double *f, size_t fcols, size_t crows, size_t ccols) {
+    double *c = malloc(crows * ccols * 8);
+    for (size_t I = 0; I < crows; I++)
+        for (size_t J = 0; J < ccols; J++) c[I * ccols + J] = f[(2 * I) * fcols + 2 * J];
+    return c;
+}
+
+fxo_cdmg *fxo_cdmg_create(const fxo_op *op, int n_pre, int n_post, double omega, int coarse_max,
+                          int coarse_sweeps) {
+    if (!op->cd) return NULL;
+    fxo_cdmg *mg = calloc(1, sizeof(fxo_cdmg));
+    mg->n_pre = n_pre;
+    mg->n_post = n_post;
+    mg->omega = omega;
+    mg->coarse_sweeps = coarse_sweeps;
+    size_t r = op->rows, c = op->cols;
+    for (int l = 0; l < 40; l++) {
+        fxo_op *L = &mg->op[l];
+        if (l == 0) {
+            *L = *op;
+        } else {
+            const fxo_op *F = &mg->op[l - 1];
+            *L = *F;
+            L->rows = r;
+            L->cols = c;
+            L->dx = F->dx * 2.0;
+            L->dy = F->dy * 2.0;
+            mg->vx[l] = inject(F->vx, F->cols, r, c);
+            mg->vy[l] = inject(F->vy, F->cols, r, c);
+            L->vx = mg->vx[l];
+            L->vy = mg->vy[l];
+            if (F->kappa) {
+                mg->kappa[l] = inject(F->kappa, F->cols, r, c);
+                L->kappa = mg->kappa[l];
+            }
+        }
+        mg->u[l] = calloc(r * c, 8);
+        mg->rhs[l] = calloc(r * c, 8);
+        mg->tmp[l] = calloc(r * c, 8);
+        mg->nlev = l + 1;
+        if (!(r - 2 > (size_t)coarse_max && c - 2 > (size_t)coarse_max && (r - 1) % 2 == 0 && (c - 1) % 2 == 0))
+            break;
+        r = (r - 1) / 2 + 1;
+        c = (c - 1) / 2 + 1;
+    }
+    return mg;
+}
+
+void fxo_cdmg_destroy(fxo_cdmg *mg) {
+    if (!mg) return;
+    for (int l = 0; l < mg->nlev; l++) {
+        free(mg->vx[l]); free(mg->vy[l]); free(mg->kappa[l]);
+        free(mg->u[l]); free(mg->rhs[l]); free(mg->tmp[l]);
+    }
+    free(mg);
+}
+
+int fxo_cdmg_depth(const fxo_cdmg *mg) { return mg->nlev; }
+
+/* z = V-cycle(r) from z = 0 (usable as fxo_pc_fn with ctx = the fxo_cdmg) */
+void fxo_cdmg_pc_apply(void *ctx, double *z, const double *r) {
+    fxo_cdmg *mg = (fxo_cdmg *)ctx;
+    int nl = mg->nlev;
+    size_t n0 = mg->op[0].rows * mg->op[0].cols;
+    double *cur[40], *oth[40];
+    const double *rhs[40];
+    cur[0] = mg->u[0];
+    oth[0] = mg->tmp[0];
+    rhs[0] = r;
+    memset(cur[0], 0, n0 * 8);
+    memset(oth[0], 0, n0 * 8);
+    for (int l = 1; l < nl; l++) {
+        cur[l] = mg->u[l];
+        oth[l] = mg->tmp[l];
+        rhs[l] = mg->rhs[l];
+    }
+    for (int l = 0; l < nl - 1; l++) {
+        const fxo_op *L = &mg->op[l], *Cc = &mg->op[l + 1];
+        for (int k = 0; k < mg->n_pre; k++) {
+            cd_sweep(L, cur[l], oth[l], rhs[l], mg->omega);
+            double *t = cur[l]; cur[l] = oth[l]; oth[l] = t;
+        }
+        cd_resid(L, cur[l], rhs[l], oth[l]);
+        fxo_restrict_fw(oth[l], mg->rhs[l + 1], L->rows, L->cols, Cc->rows, Cc->cols);
+        memset(cur[l + 1], 0, Cc->rows * Cc->cols * 8);
+        memset(oth[l + 1], 0, Cc->rows * Cc->cols * 8);
+    }
+    {
+        const fxo_op *L = &mg->op[nl - 1];
+        for (int k = 0; k < mg->coarse_sweeps; k++) {
+            cd_sweep(L, cur[nl - 1], oth[nl - 1], rhs[nl - 1], mg->omega);
+            double *t = cur[nl - 1]; cur[nl - 1] = oth[nl - 1]; oth[nl - 1] = t;
+        }
+    }
+    for (int l = nl - 2; l >= 0; l--) {
+        const fxo_op *L = &mg->op[l], *Cc = &mg->op[l + 1];
+        fxo_prolong_bilinear(cur[l + 1], cur[l], Cc->rows, Cc->cols, L->rows, L->cols);
+        for (int k = 0; k < mg->n_post; k++) {
+            cd_sweep(L, cur[l], oth[l], rhs[l], mg->omega);
+            double *t = cur[l]; cur[l] = oth[l]; oth[l] = t;
+        }
+    }
+    memcpy(z, cur[0], n0 * 8);
+}
+
+/* ------------------------------------------------------------------ */
 /* Multigrid (multigrid.rs)                                            */
 /* ------------------------------------------------------------------ */
 

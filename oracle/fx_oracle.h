@@ -147,6 +147,15 @@ int fxo_op_apply(const fxo_op *op, double *out, const double *v);
  * z = r / diag(A), diag = sigma + coeff (-kappa 2 (1/dx^2 + 1/dy^2) + |vx|/dx + |vy|/dy) inside,
  * 1 on the ring */
 void fxo_cd_jacobi_apply(void *op, double *z, const double *r);
+/* Multigrid for the conv-diff operator: vertex hierarchy, rediscretised coarse operators with
+ * injected fields, weighted Jacobi with the operator's diagonal, full weighting / bilinear,
+ * `coarse_sweeps` sweeps on the coarsest level; fxo_cdmg_pc_apply runs one cycle from z = 0. */
+typedef struct fxo_cdmg fxo_cdmg;
+fxo_cdmg *fxo_cdmg_create(const fxo_op *op, int n_pre, int n_post, double omega, int coarse_max,
+                          int coarse_sweeps);
+void fxo_cdmg_destroy(fxo_cdmg *mg);
+int fxo_cdmg_depth(const fxo_cdmg *mg);
+void fxo_cdmg_pc_apply(void *mg, double *z, const double *r);
 
 int fxo_cg_solve(const fxo_op *op, double *x, const double *b, double tol, size_t max_iter,
                  fxo_pc_fn pc, void *pc_ctx, fxo_stats *st);

@@ -111,6 +111,10 @@ def _declare(L):
     d("fxo_inner_cg_pc_apply", None, C.c_void_p, _dp, _dp)
     d("fxo_op_apply", C.c_int, opp, _dp, _dp)
     d("fxo_cd_jacobi_apply", None, C.c_void_p, _dp, _dp)
+    d("fxo_cdmg_create", C.c_void_p, opp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int)
+    d("fxo_cdmg_destroy", None, C.c_void_p)
+    d("fxo_cdmg_depth", C.c_int, C.c_void_p)
+    d("fxo_cdmg_pc_apply", None, C.c_void_p, _dp, _dp)
     d("fxo_mg_create", C.c_void_p, _sz, _sz, C.c_double, C.c_double, bcp, C.c_int, C.c_int,
       C.c_double, C.c_int, C.c_double, C.c_int, _ip, _ip, _dp, C.c_int, C.c_int)
     d("fxo_mg_destroy", None, C.c_void_p)
@@ -421,6 +425,34 @@ class CdJacobiPC:
         self._op = op
         self._cb = C.cast(lib().fxo_cd_jacobi_apply, PC_FN)
         self._ctx = C.cast(C.pointer(op), C.c_void_p)
+
+
+class CdMultigrid:
+    """V-cycle preconditioner for a conv-diff Op (fxo_cdmg_*): rediscretised coarse operators
+    with injected fields, weighted Jacobi with the operator's diagonal, one cycle from z = 0."""
+
+    def __init__(self, op, n_pre=2, n_post=2, omega=0.8, coarse_max=15, coarse_sweeps=200):
+        self._op = op
+        self.h = lib().fxo_cdmg_create(C.byref(op), n_pre, n_post, omega, coarse_max, coarse_sweeps)
+        if not self.h:
+            raise OracleError(6, "cdmg_create")
+        self._cb = C.cast(lib().fxo_cdmg_pc_apply, PC_FN)
+        self._ctx = C.c_void_p(self.h)
+
+    def depth(self):
+        return lib().fxo_cdmg_depth(self.h)
+
+    def apply(self, r):
+        z = np.zeros_like(r)
+        lib().fxo_cdmg_pc_apply(self.h, _p(z), _p(np.ascontiguousarray(r)))
+        return z
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().fxo_cdmg_destroy(self.h)
+        except Exception:
+            pass
 
 
 def bicgstab_solve_op(x, b, op, tol, max_iter, pc=None):

@@ -95,3 +95,37 @@ def test_implicit_step_matches_oracle(dev):
     assert s.converged() and reason == 0 and abs(s.iterations - it) <= 1
     assert np.linalg.norm(O.op_apply(oop, x.to_vec_f64()) - f) < 1.01 * tol
     assert rel_err(x.to_vec_f64(), xo) < 1e-9
+
+
+@pytest.mark.parametrize("n,nu,sigma,coeff,kappa_field", [(63, 1e-2, 0.0, 1.0, False), (127, 1e-3, 1.0, 5e-3, True)])
+def test_multigrid_cycle_matches_oracle_bitwise(dev, n, nu, sigma, coeff, kappa_field):
+    from fluxion_b200 import ConvDiffMultigrid, DType, Field
+    g, N, f, op, oop = _problem(n, dev, nu=nu, sigma=sigma, coeff=coeff, kappa_field=kappa_field)
+    mg = ConvDiffMultigrid(op)
+    omg = O.CdMultigrid(oop)
+    assert mg.depth() == omg.depth() >= 3
+    r = np.random.default_rng(9).uniform(-1, 1, N * N)
+    for _ in range(2):  # the second application starts from the buffers the first left
+        z = Field.zeros(g, DType.F64, dev)
+        mg.apply(z, Field.from_f64(g, r, dev))
+        assert np.array_equal(z.to_vec_f64(), omg.apply(r))
+
+
+@pytest.mark.parametrize("solver", ["bicgstab", "fgmres"])
+def test_multigrid_preconditioned_solve_matches_oracle(dev, solver):
+    from fluxion_b200 import BiCgStabSolver, ConvDiffMultigrid, DType, FgmresSolver, Field
+    g, N, f, op, oop = _problem(127, dev)
+    tol = 1e-10 * np.linalg.norm(f)
+    b = Field.from_f64(g, f, dev)
+    x = Field.zeros(g, DType.F64, dev)
+    mg, omg = ConvDiffMultigrid(op), O.CdMultigrid(oop)
+    xo = np.zeros(N * N)
+    if solver == "bicgstab":
+        s = BiCgStabSolver(g, dev, tol, 200).solve_op(x, b, op, mg)
+        it, _, reason = O.bicgstab_solve_op(xo, f, oop, tol, 200, omg)
+    else:
+        s = FgmresSolver(g, dev, 30, tol, 200).solve_op(x, b, op, mg)
+        it, _, reason = O.fgmres_solve_op(xo, f, oop, 30, tol, 200, omg)
+    assert s.converged() and reason == 0 and abs(s.iterations - it) <= 1 and s.iterations <= 20
+    assert np.linalg.norm(O.op_apply(oop, x.to_vec_f64()) - f) < 1.01 * tol
+    assert rel_err(x.to_vec_f64(), xo) < 1e-8
