@@ -62,7 +62,8 @@ def parse():
     p.add_argument("--n", type=int, default=N_INTERIOR, help="interior nodes per direction")
     p.add_argument("--no-micro", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--mode", default="solve", choices=["solve", "vcycle"],
+    p.add_argument("--batch", type=int, default=1024, help="problems in --mode batch")
+    p.add_argument("--mode", default="solve", choices=["solve", "vcycle", "batch"],
                    help="solve: the headline MG-PCG solve; vcycle: preconditioner applications alone "
                         "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target")
     return p.parse_args()
@@ -253,12 +254,89 @@ def run_vcycle(args):
     return 0
 
 
+def run_batch(args):
+    """The batched convection-diffusion workload, one problem after another through the public
+    API: `--batch` problems -nu Lap u + v.grad u = f, N x N interior with N = 2^k - 1, k ~ U{6..10},
+    nu = 1e-2, v from a stream function of 8 modes (k, l <= 4, N(0, 1) amplitudes) scaled to
+    max|v| = 1, first-order upwind, Dirichlet 0, f ~ U[-1, 1], all seeded per problem; BiCGSTAB
+    preconditioned by the conv-diff V(2,2)-cycle (omega 0.8, coarsest 15^2 x 200 sweeps) to
+    ||b - A x|| < 1e-10 ||f||, FP64.  Timed per problem (wall clock, after its host arrays are
+    generated): upload of f and the velocity fields, operator and hierarchy set-up, the solve
+    (also timed with CUDA events), the true residual recomputed with the library's operator.
+    One BiCGSTAB object per grid size is reused across the batch.  Reports solves/s over the
+    whole batch, p50 / p99 of that per-problem time and of the device solve time.  The persistent one-launch batched solver is not built: this is the sequential
+    baseline it would replace."""
+    import torch
+    from fluxion_b200 import (BiCgStabSolver, ConvDiffMultigrid, ConvDiffOperator, DType, Device, Field,
+                              Grid)
+    from fluxion_b200.workloads import poisson_uniform_rhs, stream_velocity
+
+    nu = 1e-2
+    dev = Device.Cuda(0)
+    be = dev.backend()
+    stream = torch.cuda.Stream()
+    be.set_stream(stream.cuda_stream)
+    rng = np.random.default_rng(SEED)
+    ks = rng.integers(6, 11, size=args.batch)
+    solvers = {}
+
+    def one(i):
+        n = int(2 ** ks[i] - 1)
+        N, h = n + 2, 1.0 / (n + 1)
+        g = Grid.square(N, h)
+        vx, vy = stream_velocity(n, SEED + 2 * i)
+        f = poisson_uniform_rhs(n, SEED + 2 * i + 1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()  # from here: upload, set-up, solve, check
+        VX, VY, b = Field.from_f64(g, vx, dev), Field.from_f64(g, vy, dev), Field.from_f64(g, f, dev)
+        x = Field.zeros(g, DType.F64, dev)
+        op = ConvDiffOperator(g, VX, VY, -nu, sigma=0.0, coeff=1.0)
+        mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS)
+        tol = 1e-10 * float(np.linalg.norm(f))
+        solver = solvers.get(N)  # one solver (and its work vectors) per grid size, reused
+        if solver is None:
+            solver = solvers[N] = BiCgStabSolver(g, dev, tol, 200)
+        solver.tol = tol
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = solver.solve_op(x, b, op, mg)
+        e1.record(stream)
+        ax = Field.zeros(g, DType.F64, dev)
+        op.apply(x, ax)
+        rel = float(np.linalg.norm(ax.to_vec_f64() - f) / np.linalg.norm(f))
+        torch.cuda.synchronize()
+        return n, st, e0.elapsed_time(e1), rel, time.perf_counter() - t0
+
+    for i in range(min(args.warmup, args.batch)):
+        one(i)
+    res = [one(i) for i in range(args.batch)]
+    wall = sum(r[4] for r in res)  # host data generation excluded
+    ms = np.array([r[2] for r in res])
+    its = np.array([r[1].iterations for r in res])
+    ok = all(r[1].converged() for r in res)
+    print(json.dumps({
+        "mode": "batch", "workload": f"convdiff_batch_{args.batch}_k6-10_nu1e-2_bicgstab_cdmg",
+        "problems": args.batch, "interior_sizes": {str(2 ** k - 1): int((ks == k).sum()) for k in range(6, 11)},
+        "solves_per_s": args.batch / wall, "wall_s_excluding_host_data_generation": wall,
+        "per_problem_ms_p50": float(np.percentile([r[4] * 1e3 for r in res], 50)),
+        "per_problem_ms_p99": float(np.percentile([r[4] * 1e3 for r in res], 99)),
+        "solve_ms_p50": float(np.percentile(ms, 50)), "solve_ms_p99": float(np.percentile(ms, 99)),
+        "iterations_p50": float(np.percentile(its, 50)), "iterations_max": int(its.max()),
+        "all_converged": ok, "max_true_rel_residual": max(r[3] for r in res),
+        "dtype": "f64", "data": "synthetic (seeded per problem)",
+        "note": "sequential solves through the public API; the persistent batched launch is not built"}),
+        flush=True)
+    return 0 if ok else 1
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.mode == "vcycle":
         return run_vcycle(args)
+    if args.mode == "batch":
+        return run_batch(args)
 
     import torch
 

@@ -64,15 +64,15 @@ def stream_velocity(n: int, seed: int, modes: int = 8, kmax: int = 4):
     rng = np.random.default_rng(seed)
     h = 1.0 / (n + 1)
     t = np.arange(0, n + 2) * h
-    X, Y = np.meshgrid(t, t)  # X varies along columns
-    vx = np.zeros_like(X)
-    vy = np.zeros_like(X)
+    x, y = t[None, :], t[:, None]  # x varies along columns; separable, broadcast to the grid
+    vx = np.zeros((n + 2, n + 2))
+    vy = np.zeros((n + 2, n + 2))
     for _ in range(modes):
         k, l = rng.integers(1, kmax + 1, size=2)
         a = rng.normal()
         # psi = a sin(k pi x) sin(l pi y)
-        vx += a * np.sin(k * np.pi * X) * (l * np.pi) * np.cos(l * np.pi * Y)    # d psi / dy
-        vy += -a * (k * np.pi) * np.cos(k * np.pi * X) * np.sin(l * np.pi * Y)   # -d psi / dx
+        vx += a * np.sin(k * np.pi * x) * (l * np.pi) * np.cos(l * np.pi * y)    # d psi / dy
+        vy += -a * (k * np.pi) * np.cos(k * np.pi * x) * np.sin(l * np.pi * y)   # -d psi / dx
     m = np.sqrt(vx * vx + vy * vy).max()
     if m > 0:
         vx /= m
