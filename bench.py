@@ -63,6 +63,7 @@ def parse():
     p.add_argument("--no-micro", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--batch", type=int, default=1024, help="problems in --mode batch")
+    p.add_argument("--autotune", action="store_true", help="--mode vcycle: autotune the cycle's layout first")
     p.add_argument("--mode", default="solve", choices=["solve", "vcycle", "batch"],
                    help="solve: the headline MG-PCG solve; vcycle: preconditioner applications alone "
                         "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target")
@@ -230,6 +231,7 @@ def run_vcycle(args):
     r = Field.from_f64(P.grid, poisson_modes_rhs(n, SEED), dev)
     z = Field.zeros(P.grid, DType.F64, dev)
     mg = Multigrid.vertex(P.grid, None, dev, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, DType.F32)
+    tuned = mg.autotune(z, r, reps=max(3, args.steps)) if args.autotune else None
     for _ in range(args.warmup):
         mg.precondition(z, r)
     torch.cuda.synchronize()
@@ -250,7 +252,7 @@ def run_vcycle(args):
                   for i in range(cnt.value)]
     print(json.dumps({"mode": "vcycle", "workload": f"poisson_{n}sq_f32_vcycle", "steps": args.steps,
                       "warmup": args.warmup, "ms_per_vcycle": e0.elapsed_time(e1) / args.steps,
-                      "levels": mg.depth(), "per_launch_with_events": per}), flush=True)
+                      "levels": mg.depth(), "autotune": tuned, "per_launch_with_events": per}), flush=True)
     return 0
 
 

@@ -49,6 +49,10 @@ class FxStats(C.Structure):
     _fields_ = [("iterations", C.c_size_t), ("residual", C.c_double), ("reason", C.c_int)]
 
 
+class FxMgTuning(C.Structure):
+    _fields_ = [("chunk_pct", C.c_int), ("tail_top_points", C.c_size_t)]
+
+
 class FxMgVertexOpts(C.Structure):
     _fields_ = [("n_pre", C.c_size_t), ("n_post", C.c_size_t), ("omega", C.c_double),
                 ("coarse_max", C.c_size_t), ("coarse_sweeps", C.c_size_t), ("dtype", C.c_int),
@@ -57,7 +61,7 @@ class FxMgVertexOpts(C.Structure):
 
 _STRUCTS = {
     "fx_bc": FxBc, "fx_boundaries": FxBoundaries, "fx_grid": FxGrid, "fx_stencil": FxStencil,
-    "fx_stats": FxStats, "fx_mg_vertex_opts": FxMgVertexOpts,
+    "fx_stats": FxStats, "fx_mg_vertex_opts": FxMgVertexOpts, "fx_mg_tuning": FxMgTuning,
 }
 _OPAQUE = {"fx_ctx", "fx_buf", "fx_precond", "fx_mg", "fx_cg", "fx_pipelined_cg", "fx_bicgstab",
            "fx_gmres", "fx_graph", "fx_ir", "fx_fcg", "fx_fgmres", "fx_op", "fx_cdmg"}

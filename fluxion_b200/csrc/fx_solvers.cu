@@ -305,6 +305,10 @@ struct fx_mg {
     std::vector<MgLevel> lv;
     fx_buf *tmp0 = nullptr;  // level-0 ping-pong partner (vertex mode)
     fx_buf *x32 = nullptr, *b32 = nullptr;  // level-0 single-precision copies (F32 cycle)
+    // layout of the fused cycle (fx_mg_autotune): strip row chunks per launch in percent of one
+    // wave, and the largest level the one-block tail takes (0: as many points as it can hold)
+    int chunk_pct = 100;
+    size_t tail_top_max = 0;
     struct View : fx_precond {
         fx_mg *mg = nullptr;
         int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) override;
@@ -573,28 +577,30 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
     {
         const MgLevel &L = mg->lv[0], &C = mg->lv[1];
         FX_TRY((launch_wdown<T, TB>(ctx, L.rows, L.cols, b0, (T *)mg->tmp0->ptr, (T *)C.rhs->ptr, C.cols,
-                                    vop(0), skip)));
+                                    vop(0), skip, mg->chunk_pct)));
     }
     // levels top .. nl-1 run in the one-block tail kernel: top is the finest level >= 1 whose
     // tail working set fits in shared memory
+    const size_t top_cap = mg->tail_top_max ? std::min(mg->tail_top_max, (size_t)tail_kt<T>() * kTailThreads)
+                                            : (size_t)tail_kt<T>() * kTailThreads;
     int top = nl - 1;
     size_t tail_smem = 2 * mg->lv[nl - 1].rows * mg->lv[nl - 1].cols * sizeof(T);
     for (int t = nl - 2; t >= 1 && nl - t <= kTailMaxLevels; t--) {
         size_t n[kTailMaxLevels];
         for (int l = t; l < nl; l++) n[l - t] = mg->lv[l].rows * mg->lv[l].cols;
         const size_t bytes = tail_smem_bytes(n, nl - t, sizeof(T));
-        if (bytes > kTailSmemMax || n[0] > (size_t)tail_kt<T>() * kTailThreads) break;
+        if (bytes > kTailSmemMax || n[0] > top_cap) break;
         top = t;
         tail_smem = bytes;
     }
     if (nl - top > kTailMaxLevels || tail_smem > kTailSmemMax ||
         (top == nl - 1 ? mg->lv[top].rows * mg->lv[top].cols > 4096
-                       : mg->lv[top].rows * mg->lv[top].cols > (size_t)tail_kt<T>() * kTailThreads))
+                       : mg->lv[top].rows * mg->lv[top].cols > top_cap))
         return fail(FX_ERR_UNSUPPORTED, "coarsest level too large for the one-block solve");
     for (int l = 1; l < top; l++) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
         FX_TRY((launch_wdown<T, T>(ctx, L.rows, L.cols, (const T *)L.rhs->ptr, (T *)L.tmp->ptr, (T *)C.rhs->ptr,
-                                   C.cols, vop(l), skip)));
+                                   C.cols, vop(l), skip, mg->chunk_pct)));
     }
     {
         TailArgs<T> A{};
@@ -613,11 +619,12 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
     for (int l = top - 1; l >= 1; l--) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
         FX_TRY((launch_wup<T, T, T, false>(ctx, L.rows, L.cols, (const T *)L.tmp->ptr, (const T *)C.u->ptr, C.cols,
-                                           (const T *)L.rhs->ptr, (T *)L.u->ptr, vop(l), NoFin{}, skip)));
+                                           (const T *)L.rhs->ptr, (T *)L.u->ptr, vop(l), NoFin{}, skip,
+                                           mg->chunk_pct)));
     }
     const MgLevel &L = mg->lv[0], &C = mg->lv[1];
     return launch_wup<T, TB, TZ, RZ>(ctx, L.rows, L.cols, (const T *)mg->tmp0->ptr, (const T *)C.u->ptr, C.cols, b0,
-                                     z0, vop(0), fin, skip);
+                                     z0, vop(0), fin, skip, mg->chunk_pct);
 }
 
 bool fusable(const fx_mg *m) {
@@ -2591,6 +2598,73 @@ int fx_mg_precondition(fx_mg *mg, fx_buf *z, const fx_buf *r) {
 }
 
 fx_precond *fx_mg_as_precond(fx_mg *mg) { return mg ? &mg->view : nullptr; }
+
+int fx_mg_set_tuning(fx_mg *mg, const fx_mg_tuning *t) {
+    if (!mg || !t) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (t->chunk_pct < 10 || t->chunk_pct > 1000) return fail(FX_ERR_INVALID_ARGUMENT, "chunk_pct must lie in 10..1000");
+    mg->chunk_pct = t->chunk_pct;
+    mg->tail_top_max = t->tail_top_points;
+    return FX_OK;
+}
+
+int fx_mg_get_tuning(const fx_mg *mg, fx_mg_tuning *t) {
+    if (!mg || !t) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    t->chunk_pct = mg->chunk_pct;
+    t->tail_top_points = mg->tail_top_max;
+    return FX_OK;
+}
+
+int fx_mg_autotune(fx_mg *mg, fx_buf *z, const fx_buf *r, int reps, fx_mg_tuning *best, double *best_ms,
+                   double *cand_ms, size_t cand_cap, size_t *ncand) {
+    if (!mg || !z || !r || !best) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (reps < 1) return fail(FX_ERR_INVALID_ARGUMENT, "reps must be at least 1");
+    if (mg->mode != 1 || !fusable(mg) || z->dtype != FX_F64)
+        return fail(FX_ERR_UNSUPPORTED, "autotuning covers the fused vertex V(2,2)-cycle on F64 vectors");
+    static const int kPct[] = {50, 100, 200};
+    static const size_t kTop[] = {9 * 1024, 2 * 1024};  // 65^2 and 33^2 tails on 2^k + 1 grids
+    fx_ctx *ctx = mg->ctx;
+    const int saved_pct = mg->chunk_pct;
+    const size_t saved_top = mg->tail_top_max;
+    cudaEvent_t e0, e1;
+    FX_CUDA(cudaEventCreate(&e0));
+    FX_CUDA(cudaEventCreate(&e1));
+    double best_t = 1e300;
+    size_t k = 0;
+    int rc = FX_OK;
+    for (int ip = 0; ip < 3 && rc == FX_OK; ip++)
+        for (int it = 0; it < 2 && rc == FX_OK; it++, k++) {
+            mg->chunk_pct = kPct[ip];
+            mg->tail_top_max = kTop[it];
+            for (int w = 0; w < 2 && rc == FX_OK; w++) rc = mg->view.apply(z, r, nullptr, true);
+            if (rc != FX_OK) break;
+            cudaEventRecord(e0, ctx->stream);
+            for (int q = 0; q < reps && rc == FX_OK; q++) rc = mg->view.apply(z, r, nullptr, true);
+            cudaEventRecord(e1, ctx->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(FX_ERR_BACKEND, "autotune timing failed");
+            if (rc != FX_OK) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double per = (double)ms / reps;
+            if (cand_ms && k < cand_cap) cand_ms[k] = per;
+            if (per < best_t) {
+                best_t = per;
+                best->chunk_pct = kPct[ip];
+                best->tail_top_points = kTop[it];
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != FX_OK) {
+        mg->chunk_pct = saved_pct;
+        mg->tail_top_max = saved_top;
+        return rc;
+    }
+    mg->chunk_pct = best->chunk_pct;
+    mg->tail_top_max = best->tail_top_points;
+    if (best_ms) *best_ms = best_t;
+    if (ncand) *ncand = k;
+    return FX_OK;
+}
 
 // ---- CG
 

@@ -366,11 +366,19 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *
     if constexpr (RZ) grid_reduce<1>(acc, ra, fin);
 }
 
+// chunk_pct: the row chunks of a launch as a percentage of one wave of resident warps (100: one
+// warp per resident slot; fewer, longer chunks below, more, shorter ones above)
+inline long strip_capacity(long resident_warps, int chunk_pct) {
+    const long cap = resident_warps * chunk_pct / 100;
+    return cap < 1 ? 1 : cap;
+}
+
 template <typename T, typename TB>
 int launch_wdown(fx_ctx *ctx, size_t rows, size_t cols, const TB *b, T *x2, T *coarse, size_t ccols,
-                 const VOp<T> &op, const int *skip) {
+                 const VOp<T> &op, const int *skip, int chunk_pct = 100) {
     static int occ = 0;
-    const long cap = (long)band_capacity(ctx, k_wdown<T, TB>, occ, kStripWarps * 32) * kStripWarps;
+    const long cap = strip_capacity((long)band_capacity(ctx, k_wdown<T, TB>, occ, kStripWarps * 32) * kStripWarps,
+                                    chunk_pct);
     const StripGeom G = strip_geom(rows, cols, kDownOwn, cap);
     const int blocks = (G.nitems + kStripWarps - 1) / kStripWarps;
     timing_pre(ctx, "mg_down");
@@ -383,9 +391,10 @@ int launch_wdown(fx_ctx *ctx, size_t rows, size_t cols, const TB *b, T *x2, T *c
 
 template <typename T, typename TB, typename TZ, bool RZ, typename Fin>
 int launch_wup(fx_ctx *ctx, size_t rows, size_t cols, const T *x2, const T *e, size_t ccols, const TB *b, TZ *z,
-               const VOp<T> &op, Fin fin, const int *skip) {
+               const VOp<T> &op, Fin fin, const int *skip, int chunk_pct = 100) {
     static int occ = 0;
-    const long cap = (long)band_capacity(ctx, k_wup<T, TB, TZ, RZ, Fin>, occ, kStripWarps * 32) * kStripWarps;
+    const long cap = strip_capacity(
+        (long)band_capacity(ctx, k_wup<T, TB, TZ, RZ, Fin>, occ, kStripWarps * 32) * kStripWarps, chunk_pct);
     const StripGeom G = strip_geom(rows, cols, kUpOwn, cap);
     const int blocks = (G.nitems + kStripWarps - 1) / kStripWarps;
     if (RZ && blocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");

@@ -152,6 +152,30 @@ class Multigrid(Preconditioner):
     def v_cycle(self, x: Field, b: Field) -> None:
         check(L.lib().fx_mg_v_cycle(self.h, x.storage.handle, b.storage.handle))
 
+    def set_tuning(self, chunk_pct: int = 100, tail_top_points: int = 0) -> None:
+        """Layout of the fused cycle (no effect on its values): strip row chunks per launch in
+        percent of one wave, and the largest level the one-block tail takes (0: default)."""
+        t = L.FxMgTuning(int(chunk_pct), int(tail_top_points))
+        check(L.lib().fx_mg_set_tuning(self.h, C.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = L.FxMgTuning()
+        check(L.lib().fx_mg_get_tuning(self.h, C.byref(t)))
+        return {"chunk_pct": t.chunk_pct, "tail_top_points": t.tail_top_points}
+
+    def autotune(self, z: Field, r: Field, reps: int = 5) -> dict:
+        """Time the candidate layouts of the fused cycle on (z, r) and keep the fastest
+        (fx_mg_autotune); z is overwritten.  Returns the choice, its time per cycle and every
+        candidate's time."""
+        best = L.FxMgTuning()
+        best_ms = C.c_double()
+        cand = (C.c_double * 8)()
+        ncand = C.c_size_t()
+        check(L.lib().fx_mg_autotune(self.h, z.storage.handle, r.storage.handle, int(reps), C.byref(best),
+                                     C.byref(best_ms), cand, 8, C.byref(ncand)))
+        return {"chunk_pct": best.chunk_pct, "tail_top_points": best.tail_top_points, "ms": best_ms.value,
+                "candidates_ms": [cand[i] for i in range(ncand.value)]}
+
     def precondition(self, z: Field, r: Field) -> None:
         """z = M^-1 r from a zero initial guess (z.fill(0); apply(z, r), cg.rs:196-197)."""
         check(L.lib().fx_mg_precondition(self.h, z.storage.handle, r.storage.handle))

@@ -294,6 +294,23 @@ typedef struct {
 int fx_mg_create_vertex(fx_ctx *ctx, const fx_grid *g, const fx_boundaries *bc,
                         const fx_mg_vertex_opts *opts, fx_mg **out);
 int fx_mg_destroy(fx_mg *mg);
+/* Layout of the fused vertex cycle (new; no reference counterpart): the strip kernels' row
+ * chunks per launch in percent of one wave of resident warps (default 100), and the largest
+ * level, in points, that the one-block tail takes (0 = as large as it can hold: 9216 points).
+ * Neither changes any value the cycle computes. */
+typedef struct {
+    int chunk_pct;
+    size_t tail_top_points;
+} fx_mg_tuning;
+int fx_mg_set_tuning(fx_mg *mg, const fx_mg_tuning *t);
+int fx_mg_get_tuning(const fx_mg *mg, fx_mg_tuning *t);
+/* Autotuner (new): times `reps` cycles z = M^-1 r (after two untimed ones) for each candidate
+ * layout -- chunk_pct in {50, 100, 200} x tail_top_points in {9216, 2048}, in that order --
+ * on the caller's vectors (F64, the fused vertex V(2,2)-cycle of either precision), keeps the
+ * fastest in the multigrid and returns it, its time per cycle, and up to cand_cap candidate
+ * times (ncand of them).  FX_ERR_UNSUPPORTED for other cycles.  z is overwritten. */
+int fx_mg_autotune(fx_mg *mg, fx_buf *z, const fx_buf *r, int reps, fx_mg_tuning *best, double *best_ms,
+                   double *cand_ms, size_t cand_cap, size_t *ncand);
 /* Multigrid::depth (multigrid.rs:174-178) */
 int fx_mg_depth(const fx_mg *mg, size_t *depth);
 int fx_mg_level_dims(const fx_mg *mg, size_t level, size_t *rows, size_t *cols);
