@@ -291,6 +291,7 @@ struct MgLevel {
     double a5[5] = {0, 0, 0, 0, 0};    // vertex: operator on this level
     double lap5[5] = {0, 0, 0, 0, 0};  // reference: Laplacian weights
     fx_buf *u = nullptr, *rhs = nullptr, *tmp = nullptr;
+    fx_buf *w0 = nullptr, *w1 = nullptr;  // reference mode, Chebyshev smoother
 };
 
 }  // namespace
@@ -298,6 +299,7 @@ struct MgLevel {
 struct fx_mg {
     fx_ctx *ctx = nullptr;
     int mode = 0;  // 0 reference, 1 vertex
+    int smoother = 0;  // reference mode: 0 weighted Jacobi, 1 Chebyshev (multigrid.rs:11-20)
     int dtype = FX_F64;
     size_t n_pre = 2, n_post = 2, coarse_sweeps = 200;
     double omega = 2.0 / 3.0;
@@ -320,6 +322,8 @@ struct fx_mg {
             fx_free(L.u);
             fx_free(L.rhs);
             fx_free(L.tmp);
+            fx_free(L.w0);
+            fx_free(L.w1);
         }
         fx_free(tmp0);
         fx_free(x32);
@@ -521,6 +525,52 @@ int convert(fx_ctx *ctx, const S *src, D *dst, size_t n, const int *skip) {
     return launch_flat<0>(ctx, n, FlatConvert<S, D>{src, dst}, NoFin{}, skip, "mg_convert");
 }
 
+// Chebyshev smoother of the reference hierarchy (multigrid.rs:308-473): the first-kind
+// Chebyshev recurrence for D^-1 A with the bounds emax = 2, emin = 0.2 (D the level Laplacian's
+// diagonal) on three rotating vectors u, w0, w1, each step the reference's sequence of backend
+// ops (stencil apply, copy, axpy, scale, zero_boundaries) -- no inner products, no host sync.
+int chebyshev_smooth(fx_ctx *ctx, MgLevel &L, const fx_grid &g, const fx_stencil &s, const fx_boundaries &bc,
+                     size_t n) {
+    if (n == 0) return FX_OK;
+    const double emax = 2.0, emin = 0.1 * emax;
+    const double scale = 2.0 / (emax + emin);
+    const double alpha = 1.0 - scale * emin;
+    const double mu = 1.0 / alpha, omegaprod = 2.0 / alpha;
+    const double inv_dx2 = 1.0 / (L.dx * L.dx), inv_dy2 = 1.0 / (L.dy * L.dy);
+    const double inv_diag = -1.0 / (2.0 * inv_dx2 + 2.0 * inv_dy2);
+    double c_km1 = 1.0, c_k = mu;
+    FX_TRY(fx_apply_stencil(ctx, L.u, L.tmp, &g, &s, &bc));
+    FX_TRY(fx_copy(ctx, L.rhs, L.w0));
+    FX_TRY(fx_axpy(ctx, -1.0, L.tmp, L.w0));
+    FX_TRY(fx_scale(ctx, L.w0, scale * inv_diag));
+    FX_TRY(fx_axpy(ctx, 1.0, L.u, L.w0));
+    FX_TRY(fx_zero_boundaries(ctx, L.w0, L.rows, L.cols));
+    if (n == 1) return fx_copy(ctx, L.w0, L.u);
+    fx_buf *buf[3] = {L.u, L.w0, L.w1};
+    int km1 = 0, k = 1, kp1 = 2;
+    for (size_t i = 1; i < n; i++) {
+        FX_TRY(fx_apply_stencil(ctx, buf[k], L.tmp, &g, &s, &bc));
+        FX_TRY(fx_copy(ctx, L.rhs, buf[kp1]));
+        FX_TRY(fx_axpy(ctx, -1.0, L.tmp, buf[kp1]));
+        FX_TRY(fx_scale(ctx, buf[kp1], inv_diag));
+        const double c_kp1 = 2.0 * mu * c_k - c_km1;
+        const double omega = omegaprod * c_k / c_kp1;
+        FX_TRY(fx_scale(ctx, buf[kp1], omega * scale));
+        FX_TRY(fx_axpy(ctx, omega, buf[k], buf[kp1]));
+        FX_TRY(fx_axpy(ctx, 1.0 - omega, buf[km1], buf[kp1]));
+        FX_TRY(fx_zero_boundaries(ctx, buf[kp1], L.rows, L.cols));
+        c_km1 = c_k;
+        c_k = c_kp1;
+        const int t = km1;
+        km1 = k;
+        k = kp1;
+        kp1 = t;
+    }
+    if (k == 1) return fx_copy(ctx, L.w0, L.u);
+    if (k == 2) return fx_copy(ctx, L.w1, L.u);
+    return FX_OK;
+}
+
 // Reference-semantics cycle (multigrid.rs:188-230), built from the trait ops.
 int reference_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b, bool x_zero) {
     fx_ctx *ctx = mg->ctx;
@@ -533,6 +583,7 @@ int reference_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b, bool x_zero) {
         MgLevel &L = mg->lv[l];
         fx_grid g{L.rows, L.cols, L.dx, L.dy};
         fx_stencil s{5, LAP_DR, LAP_DC, L.lap5};
+        if (mg->smoother == 1) return chebyshev_smooth(ctx, L, g, s, mg->bc, n);
         for (size_t k = 0; k < n; k++) FX_TRY(fx_weighted_jacobi(ctx, L.u, L.rhs, mg->omega, &g, &s, &mg->bc));
         return FX_OK;
     };
@@ -2449,11 +2500,12 @@ int fx_mg_create(fx_ctx *ctx, const fx_grid *g, const fx_boundaries *bc, size_t 
                  int smoother, fx_mg **out) {
     if (!ctx || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     FX_TRY(check_grid(g));
-    if (smoother != 0) return fail(FX_ERR_UNSUPPORTED, "Chebyshev smoother is not implemented");
+    if (smoother != 0 && smoother != 1) return fail(FX_ERR_INVALID_ARGUMENT, "smoother must be 0 (Jacobi) or 1 (Chebyshev)");
     *out = nullptr;
     fx_mg *mg = new fx_mg();
     mg->ctx = ctx;
     mg->mode = 0;
+    mg->smoother = smoother;
     mg->n_pre = n_pre;
     mg->n_post = n_post;
     mg->omega = omega;
@@ -2473,6 +2525,8 @@ int fx_mg_create(fx_ctx *ctx, const fx_grid *g, const fx_boundaries *bc, size_t 
         int st = fx_alloc(ctx, r * c, FX_F64, &L.u);
         if (!st) st = fx_alloc(ctx, r * c, FX_F64, &L.rhs);
         if (!st) st = fx_alloc(ctx, r * c, FX_F64, &L.tmp);
+        if (!st && smoother == 1) st = fx_alloc(ctx, r * c, FX_F64, &L.w0);  // multigrid.rs:113-119
+        if (!st && smoother == 1) st = fx_alloc(ctx, r * c, FX_F64, &L.w1);
         mg->lv.push_back(L);
         if (st) {
             delete mg;

@@ -273,7 +273,8 @@ int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_st
 /* Multigrid::new / ::build (multigrid.rs:61-146): reference hierarchy (rows/2 per level,
  * Laplacian on each level, clamped 2x2 restriction, piecewise-constant prolongation,
  * lexicographic weighted-Jacobi smoother, coarsest level n_pre+n_post+10 sweeps).
- * smoother: 0 = Jacobi (the Chebyshev smoother is not implemented: FX_ERR_UNSUPPORTED). */
+ * smoother: 0 = Jacobi, 1 = Chebyshev (multigrid.rs:308-473: first-kind recurrence for D^-1 A,
+ * emax = 2, emin = 0.2, built from the backend ops, two extra vectors per level). */
 int fx_mg_create(fx_ctx *ctx, const fx_grid *g, const fx_boundaries *bc, size_t n_pre,
                  size_t n_post, double omega, int smoother, fx_mg **out);
 

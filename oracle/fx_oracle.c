@@ -1309,10 +1309,12 @@ typedef struct {
     double a5[5];       /* vertex mode: operator on this level */
     double lap5[5];     /* reference mode: Laplacian (stencil.rs:152-168) c,n,s,w,e */
     double *u, *rhs, *tmp;
+    double *w0, *w1; /* reference mode, Chebyshev smoother: recurrence work vectors */
 } mg_level;
 
 struct fxo_mg {
     int mode, n_pre, n_post, coarse_sweeps, nlev;
+    int smoother; /* reference mode: 0 weighted Jacobi, 1 Chebyshev (multigrid.rs:11-20) */
     double omega;
     fxo_bc bcs[4];
     mg_level lv[40];
@@ -1411,15 +1413,81 @@ void fxo_mg_destroy(fxo_mg *mg) {
         free(mg->lv[l].u);
         free(mg->lv[l].rhs);
         free(mg->lv[l].tmp);
+        free(mg->lv[l].w0);
+        free(mg->lv[l].w1);
     }
     free(mg);
 }
 
+int fxo_mg_set_smoother(fxo_mg *mg, int smoother) {
+    if (mg->mode != 0 || smoother < 0 || smoother > 1) return FXO_ERR_INVALID_ARGUMENT;
+    mg->smoother = smoother;
+    if (smoother == 1)
+        for (int l = 0; l < mg->nlev; l++) {
+            size_t n = mg->lv[l].rows * mg->lv[l].cols;
+            if (!mg->lv[l].w0) mg->lv[l].w0 = calloc(n, 8);
+            if (!mg->lv[l].w1) mg->lv[l].w1 = calloc(n, 8);
+        }
+    return FXO_OK;
+}
+
 static const int LAP_DR[5] = {0, -1, 1, 0, 0}, LAP_DC[5] = {0, 0, 0, -1, 1};
+
+/* Reference-mode Chebyshev smoother (multigrid.rs:308-473): first-kind Chebyshev recurrence for
+ * D^-1 A with the bounds emax = 2, emin = 0.2, D the Laplacian's diagonal, on three rotating
+ * vectors (u, w0, w1), each step built from the backend ops in the reference's order. */
+static void ref_smooth_cheby(fxo_mg *mg, int l, int n) {
+    if (n == 0) return;
+    mg_level *L = &mg->lv[l];
+    size_t len = L->rows * L->cols;
+    double emax = 2.0, emin = 0.1 * emax;
+    double scale = 2.0 / (emax + emin);
+    double alpha = 1.0 - scale * emin;
+    double mu = 1.0 / alpha, omegaprod = 2.0 / alpha;
+    double inv_dx2 = 1.0 / (L->dx * L->dx), inv_dy2 = 1.0 / (L->dy * L->dy);
+    double inv_diag = -1.0 / (2.0 * inv_dx2 + 2.0 * inv_dy2);
+    double c_km1 = 1.0, c_k = mu;
+    fxo_apply_stencil(L->u, L->tmp, L->rows, L->cols, L->dx, L->dy, 5, LAP_DR, LAP_DC, L->lap5, mg->bcs);
+    fxo_copy(L->rhs, L->w0, len);
+    fxo_axpy(-1.0, L->tmp, L->w0, len);
+    fxo_scale(L->w0, len, scale * inv_diag);
+    fxo_axpy(1.0, L->u, L->w0, len);
+    fxo_zero_boundaries(L->w0, L->rows, L->cols);
+    if (n == 1) {
+        fxo_copy(L->w0, L->u, len);
+        return;
+    }
+    double *buf[3] = {L->u, L->w0, L->w1};
+    int km1 = 0, k = 1, kp1 = 2;
+    for (int i = 1; i < n; i++) {
+        fxo_apply_stencil(buf[k], L->tmp, L->rows, L->cols, L->dx, L->dy, 5, LAP_DR, LAP_DC, L->lap5, mg->bcs);
+        fxo_copy(L->rhs, buf[kp1], len);
+        fxo_axpy(-1.0, L->tmp, buf[kp1], len);
+        fxo_scale(buf[kp1], len, inv_diag);
+        double c_kp1 = 2.0 * mu * c_k - c_km1;
+        double omega = omegaprod * c_k / c_kp1;
+        fxo_scale(buf[kp1], len, omega * scale);
+        fxo_axpy(omega, buf[k], buf[kp1], len);
+        fxo_axpy(1.0 - omega, buf[km1], buf[kp1], len);
+        fxo_zero_boundaries(buf[kp1], L->rows, L->cols);
+        c_km1 = c_k;
+        c_k = c_kp1;
+        int t = km1;
+        km1 = k;
+        k = kp1;
+        kp1 = t;
+    }
+    if (k == 1) fxo_copy(L->w0, L->u, len);
+    else if (k == 2) fxo_copy(L->w1, L->u, len);
+}
 
 /* Reference-mode smoother: n lexicographic sweeps (multigrid.rs:245-306). */
 static void ref_smooth(fxo_mg *mg, int l, int n) {
     mg_level *L = &mg->lv[l];
+    if (mg->smoother == 1) {
+        ref_smooth_cheby(mg, l, n);
+        return;
+    }
     for (int k = 0; k < n; k++)
         fxo_weighted_jacobi(L->u, L->rhs, mg->omega, L->rows, L->cols, 5, LAP_DR, LAP_DC, L->lap5);
 }

@@ -194,6 +194,8 @@ fxo_mg *fxo_mg_create(size_t rows, size_t cols, double dx, double dy, const fxo_
                       const int *dr, const int *dc, const double *w, int coarse_max,
                       int coarse_sweeps);
 void fxo_mg_destroy(fxo_mg *mg);
+/* reference mode only: 0 weighted Jacobi (default), 1 Chebyshev (multigrid.rs:308-473) */
+int fxo_mg_set_smoother(fxo_mg *mg, int smoother);
 int fxo_mg_depth(const fxo_mg *mg);
 void fxo_mg_level_dims(const fxo_mg *mg, int lvl, size_t *rows, size_t *cols);
 void fxo_mg_v_cycle(fxo_mg *mg, double *x, const double *b);

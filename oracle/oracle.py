@@ -118,6 +118,7 @@ def _declare(L):
     d("fxo_mg_create", C.c_void_p, _sz, _sz, C.c_double, C.c_double, bcp, C.c_int, C.c_int,
       C.c_double, C.c_int, C.c_double, C.c_int, _ip, _ip, _dp, C.c_int, C.c_int)
     d("fxo_mg_destroy", None, C.c_void_p)
+    d("fxo_mg_set_smoother", C.c_int, C.c_void_p, C.c_int)
     d("fxo_mg_depth", C.c_int, C.c_void_p)
     d("fxo_mg_level_dims", None, C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t))
     d("fxo_mg_v_cycle", None, C.c_void_p, _dp, _dp)
@@ -297,7 +298,8 @@ class Multigrid:
     full-weighting / bilinear / true weighted Jacobi on the operator being solved."""
 
     def __init__(self, rows, cols, dx, dy, n_pre=2, n_post=2, omega=2.0 / 3.0, mode=0,
-                 op_coeff=1.0, entries=None, bcs=ZERO_DIRICHLET, coarse_max=15, coarse_sweeps=200):
+                 op_coeff=1.0, entries=None, bcs=ZERO_DIRICHLET, coarse_max=15, coarse_sweeps=200,
+                 smoother=0):
         entries = entries or laplacian_5pt(dx, dy)
         n, dr, dc, w = _stencil_arrays(entries)
         self._bcs = bcs_array(bcs)
@@ -305,6 +307,8 @@ class Multigrid:
                                      op_coeff, n, dr, dc, w, coarse_max, coarse_sweeps)
         if not self.h:
             raise OracleError(6, "mg_create")
+        if smoother:
+            _chk(lib().fxo_mg_set_smoother(self.h, int(smoother)), "mg_set_smoother")
         self._cb = PC_FN(lambda ctx, z, r: lib().fxo_mg_v_cycle(self.h, z, r))
 
     def depth(self):

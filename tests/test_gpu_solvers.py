@@ -97,17 +97,19 @@ def test_gmres_known_answers(dev):
     assert GmresSolver(g2, dev, 100, 1e-6, 1000).solve(x, b2, -0.5, st2, bc2).converged()
 
 
-def test_multigrid_known_answers(dev):
-    from fluxion_b200 import Boundaries, DType, Field, Grid, Multigrid, Stencil
-    for n, depth in ((64, 5), (32, 4), (8, 2)):  # solvers.rs:813-841
+@pytest.mark.parametrize("smoother", [0, 1])
+def test_multigrid_known_answers(dev, smoother):
+    """solvers.rs:813-841 (depths) and analytical.rs:447-521 with both smoothers."""
+    from fluxion_b200 import Boundaries, DType, Field, Grid, Multigrid, SmootherKind, Stencil
+    for n, depth in ((64, 5), (32, 4), (8, 2)):
         assert Multigrid(Grid.square(n, 1.0 / (n - 1)), Boundaries.zero_dirichlet(), dev, 2, 2,
-                         2.0 / 3.0).depth() == depth
-    n = 64  # analytical.rs:447-521
+                         2.0 / 3.0, SmootherKind(smoother)).depth() == depth
+    n = 64
     h = 1.0 / (n - 1)
     g = Grid.square(n, h)
     bc = Boundaries.zero_dirichlet()
     b = Field.from_f64(g, sin_sin_field(n, h), dev)
-    mg = Multigrid(g, bc, dev, 3, 3, 2.0 / 3.0)
+    mg = Multigrid(g, bc, dev, 3, 3, 2.0 / 3.0, SmootherKind(smoother))
     x = Field.zeros(g, DType.F64, dev)
     st = Stencil.laplacian_2d_5pt(h, h)
     prev = np.inf
@@ -174,16 +176,17 @@ def test_solver_parity_with_oracle(dev, n, coeff, tol):
             assert abs(sg.residual - res) <= 0.1 * res, (name, sg.residual, res)
 
 
-def test_reference_mg_vcycle_bitwise(dev):
-    """multigrid.rs V-cycle (reference semantics) is built from bitwise-exact ops."""
-    from fluxion_b200 import Boundaries, DType, Field, Grid, Multigrid
-    n = 64
+@pytest.mark.parametrize("n,smoother", [(64, 0), (64, 1), (128, 1)])
+def test_reference_mg_vcycle_bitwise(dev, n, smoother):
+    """multigrid.rs V-cycle (reference semantics), with the weighted-Jacobi or the Chebyshev
+    smoother (multigrid.rs:308-473), is built from bitwise-exact ops."""
+    from fluxion_b200 import Boundaries, DType, Field, Grid, Multigrid, SmootherKind
     h = 1.0 / (n - 1)
     g = Grid.square(n, h)
     rng = np.random.default_rng(4)
     bvec = rng.uniform(-1, 1, n * n)
-    mg = Multigrid(g, Boundaries.zero_dirichlet(), dev, 2, 2, 2.0 / 3.0)
-    omg = O.Multigrid(n, n, h, h, 2, 2, 2.0 / 3.0, mode=0)
+    mg = Multigrid(g, Boundaries.zero_dirichlet(), dev, 2, 2, 2.0 / 3.0, SmootherKind(smoother))
+    omg = O.Multigrid(n, n, h, h, 2, 2, 2.0 / 3.0, mode=0, smoother=smoother)
     x = Field.zeros(g, DType.F64, dev)
     b = Field.from_f64(g, bvec, dev)
     xo = np.zeros(n * n)

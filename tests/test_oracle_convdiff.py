@@ -102,3 +102,28 @@ def test_multigrid_preconditions_the_steady_problem():
                 it, _, reason = O.fgmres_solve_op(x, f, op, 30, tol, 200, mg)
             assert reason == 0 and it <= limit and it * 10 < it_j, (n, solver, it, it_j)
             assert np.linalg.norm(O.op_apply(op, x) - f) < 1.01 * tol
+
+
+def test_chebyshev_smoother_reduces_residual_faster_than_jacobi():
+    """analytical.rs:447-521 in the oracle with both smoothers of the reference hierarchy
+    (multigrid.rs:233-473): the residual falls every cycle, and further with Chebyshev."""
+    n = 64
+    h = 1.0 / (n - 1)
+    t = np.arange(n) * h
+    X, Y = np.meshgrid(t, t)
+    b = (np.sin(np.pi * X) * np.sin(np.pi * Y)).ravel()
+    st = O.laplacian_5pt(h, h)
+    final = []
+    for smoother in (0, 1):
+        mg = O.Multigrid(n, n, h, h, 3, 3, 2.0 / 3.0, mode=0, smoother=smoother)
+        x = np.zeros(n * n)
+        prev = np.inf
+        for _ in range(10):
+            mg.v_cycle(x, b)
+            ax = np.zeros(n * n)
+            O.apply_stencil(x, ax, n, n, h, h, st)
+            res = np.linalg.norm(b - ax)
+            assert res < prev
+            prev = res
+        final.append(prev)
+    assert final[1] < final[0] < 10.0
