@@ -16,6 +16,7 @@ __all__ = [
     "Identity", "Preconditioner", "LinearSolver", "SolveStats", "ConvergenceReason",
     "MixedPrecisionRefinement", "CudaGraph", "FcgSolver", "FgmresSolver", "InnerCg",
     "ConvDiffOperator", "OperatorJacobi", "ConvDiffMultigrid",
+    "CrankNicolsonSolver", "BdfSolver", "ImexSolver",
 ]
 
 
@@ -34,4 +35,7 @@ def __getattr__(name):
                 "ConvergenceReason"):
         from . import solvers
         return getattr(solvers, name)
+    if name in ("CrankNicolsonSolver", "BdfSolver", "ImexSolver"):
+        from . import steppers
+        return getattr(steppers, name)
     raise AttributeError(name)
