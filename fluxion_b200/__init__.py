@@ -16,7 +16,7 @@ __all__ = [
     "Identity", "Preconditioner", "LinearSolver", "SolveStats", "ConvergenceReason",
     "MixedPrecisionRefinement", "CudaGraph", "FcgSolver", "FgmresSolver", "InnerCg",
     "ConvDiffOperator", "OperatorJacobi", "ConvDiffMultigrid",
-    "CrankNicolsonSolver", "BdfSolver", "ImexSolver",
+    "CrankNicolsonSolver", "BdfSolver", "ImexSolver", "DiffusionSolver", "TimeScheme",
 ]
 
 
@@ -35,7 +35,7 @@ def __getattr__(name):
                 "ConvergenceReason"):
         from . import solvers
         return getattr(solvers, name)
-    if name in ("CrankNicolsonSolver", "BdfSolver", "ImexSolver"):
+    if name in ("CrankNicolsonSolver", "BdfSolver", "ImexSolver", "DiffusionSolver", "TimeScheme"):
         from . import steppers
         return getattr(steppers, name)
     raise AttributeError(name)

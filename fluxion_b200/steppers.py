@@ -1,13 +1,15 @@
-"""Implicit time steppers of fluxion's runtime over the CUDA solve path.
+"""Time steppers of fluxion's runtime over the CUDA solve path.
 
-``CrankNicolsonSolver`` (crates/runtime/src/implicit.rs:25-237), ``BdfSolver`` (bdf.rs:23-255)
-and ``ImexSolver`` (imex.rs:26-273) restate the reference's steppers: each step assembles its
+``CrankNicolsonSolver`` (crates/runtime/src/implicit.rs:25-237), ``BdfSolver`` (bdf.rs:23-255),
+``ImexSolver`` (imex.rs:26-273) and the explicit ``DiffusionSolver`` (solver.rs:30-642) restate
+the reference's steppers.  The implicit ones: each step assembles its
 right-hand side from the backend's field operations in the reference's order and solves the
 implicit system with `CgSolver` (preconditioned by a reference-hierarchy `Multigrid` when one
 is configured).  Same constructors, fields and step signatures as the reference.
 """
 from __future__ import annotations
 
+import enum
 from typing import List, Optional
 
 from .core import Boundaries, DType, Grid, Stencil
@@ -225,3 +227,143 @@ class ImexSolver:
     def step_n(self, u: Field, n: int) -> None:
         for _ in range(n):
             self.step(u)
+
+
+class TimeScheme(enum.Enum):
+    """solver.rs:16-24"""
+
+    Euler = 0
+    Rk2 = 1
+    Rk4 = 2
+
+
+class DiffusionSolver:
+    """solver.rs:30-642: explicit du/dt = alpha Lap u (+ source) by forward Euler, Heun (RK2) or
+    classical RK4, each stage the reference's sequence of field operations.  The default dt is
+    the reference's stability bound safety * h_min^2 / (4 alpha) (safety 0.4 / 0.8 / 1.4).
+    ``enable_graph()`` is the HipGraph path (solver.rs:182-325) on CUDA graphs: the first
+    ``step_n`` records one step on the backend's stream and later steps replay it."""
+
+    def __init__(self, grid: Grid, alpha: float, dt: Optional[float], boundaries: Boundaries,
+                 scheme: "TimeScheme", device: Optional[Device] = None):
+        self.device = device or Device.best()
+        self.grid = grid
+        h_min = min(grid.dx, grid.dy)
+        safety = {TimeScheme.Euler: 0.4, TimeScheme.Rk2: 0.8, TimeScheme.Rk4: 1.4}[scheme]
+        self._dt = float(dt) if dt is not None else safety * h_min * h_min / (4.0 * alpha)
+        self.alpha = float(alpha)
+        self.stencil = Stencil.laplacian_2d_5pt(grid.dx, grid.dy)
+        self.boundaries = boundaries
+        self._scheme = scheme
+        n_scratch = {TimeScheme.Euler: 1, TimeScheme.Rk2: 2, TimeScheme.Rk4: 5}[scheme]
+        self.scratch = [Field.zeros(grid, DType.F64, self.device) for _ in range(n_scratch)]
+        self._steps_done = 0
+        self._use_graph = False
+        self._graph = None
+        self._graph_u = None
+
+    @staticmethod
+    def new(grid: Grid, alpha: float, dt: Optional[float], device: Optional[Device] = None) -> "DiffusionSolver":
+        return DiffusionSolver(grid, alpha, dt, Boundaries.zero_dirichlet(), TimeScheme.Euler, device)
+
+    @staticmethod
+    def with_boundaries(grid, alpha, dt, boundaries, device=None) -> "DiffusionSolver":
+        return DiffusionSolver(grid, alpha, dt, boundaries, TimeScheme.Euler, device)
+
+    @staticmethod
+    def build(grid, alpha, dt, boundaries, scheme, device=None) -> "DiffusionSolver":
+        return DiffusionSolver(grid, alpha, dt, boundaries, scheme, device)
+
+    def dt(self) -> float:
+        return self._dt
+
+    def steps_done(self) -> int:
+        return self._steps_done
+
+    def sim_time(self) -> float:
+        return self._steps_done * self._dt
+
+    def scheme(self) -> "TimeScheme":
+        return self._scheme
+
+    def enable_graph(self) -> None:
+        """solver.rs:182-186 (enable_hip_graph)."""
+        self._use_graph = True
+
+    def step(self, u: Field, source: Optional[Field] = None) -> None:
+        self._record(u, source)
+        self._steps_done += 1
+
+    def step_n(self, u: Field, n: int) -> None:
+        """solver.rs:231-257; with the graph enabled, the recorded step is replayed n times
+        (one graph per solver, recorded on the first field passed)."""
+        if n == 0:
+            return
+        if self._use_graph:
+            if self._graph is None:
+                be = self.device.backend()
+                be.graph_begin()
+                try:
+                    self._record(u, None)
+                finally:
+                    self._graph = be.graph_end()
+                self._graph_u = u
+            if u is not self._graph_u:
+                raise ValueError("the recorded step belongs to another field")
+            for _ in range(n):
+                self._graph.launch()
+                self._steps_done += 1
+            return
+        for _ in range(n):
+            self.step(u, None)
+
+    def step_n_with_source(self, u: Field, n: int, source: Field) -> None:
+        for _ in range(n):
+            self.step(u, source)
+
+    def _record(self, u: Field, source: Optional[Field]) -> None:
+        {TimeScheme.Euler: self._euler, TimeScheme.Rk2: self._rk2, TimeScheme.Rk4: self._rk4}[self._scheme](u, source)
+
+    def _euler(self, u: Field, source: Optional[Field]) -> None:  # solver.rs:344-369
+        coeff = self.alpha * self._dt
+        self.scratch[0].copy_from(u)
+        u.stencil_axpy(coeff, self.scratch[0], self.stencil, self.boundaries)
+        if source is not None:
+            u.axpy(self._dt, source)
+
+    def _rk2(self, u: Field, source: Optional[Field]) -> None:  # solver.rs:371-419
+        dt = self._dt
+        coeff = dt * self.alpha
+        self.scratch[1].copy_from(u)
+        for _ in range(2):
+            self.scratch[0].copy_from(u)
+            u.stencil_axpy(coeff, self.scratch[0], self.stencil, self.boundaries)
+            if source is not None:
+                u.axpy(dt, source)
+        u.axpy(1.0, self.scratch[1])
+        u.scale(0.5)
+
+    def _rk4(self, u: Field, source: Optional[Field]) -> None:  # solver.rs:421-495
+        dt, alpha = self._dt, self.alpha
+        k, u_old = self.scratch, self.scratch[4]
+        u_old.copy_from(u)
+        u.apply_stencil_into(self.stencil, self.boundaries, k[0])
+        u.copy_from(u_old)
+        u.stencil_axpy(0.5 * dt * alpha, u_old, self.stencil, self.boundaries)
+        u.apply_stencil_into(self.stencil, self.boundaries, k[1])
+        u.copy_from(u_old)
+        u.axpy(0.5 * dt * alpha, k[1])
+        u.zero_boundaries()
+        u.apply_stencil_into(self.stencil, self.boundaries, k[2])
+        u.copy_from(u_old)
+        u.axpy(dt * alpha, k[2])
+        u.zero_boundaries()
+        u.apply_stencil_into(self.stencil, self.boundaries, k[3])
+        u.copy_from(u_old)
+        c = dt * alpha / 6.0
+        u.axpy(c, k[0])
+        u.axpy(2.0 * c, k[1])
+        u.axpy(2.0 * c, k[2])
+        u.axpy(c, k[3])
+        if source is not None:
+            u.axpy(dt, source)

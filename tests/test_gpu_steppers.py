@@ -1,6 +1,7 @@
-"""Implicit time steppers over the CUDA path: the reference's own tests of CrankNicolsonSolver,
-ImexSolver and BdfSolver (crates/runtime/tests/solvers.rs, analytical.rs), restated, and one
-Crank-Nicolson step against the same step assembled from the oracle's operations."""
+"""Time steppers over the CUDA path: the reference's own tests of CrankNicolsonSolver, ImexSolver,
+BdfSolver and the explicit DiffusionSolver (crates/runtime/tests/solvers.rs, analytical.rs,
+src/solver.rs), restated; one Crank-Nicolson step against the same step assembled from the
+oracle's operations; and graph-replayed explicit steps against eager ones."""
 import numpy as np
 import pytest
 
@@ -113,3 +114,56 @@ def test_crank_nicolson_step_matches_oracle(dev):
     it, _, reason = O.cg_solve(x, rhs, n, n, -hda, lap, 1e-10, 100, pc=mg)
     assert st.converged() and reason == 0 and abs(st.iterations - it) <= 1
     assert rel_err(u.to_vec_f64(), x) < 1e-9
+
+
+def test_diffusion_solver_known_answers(dev):
+    """solver.rs:676-800 (unit tests) and solvers.rs rk2/rk4 diffusion tests."""
+    from fluxion_b200 import Boundaries, DType, Field, Grid
+    from fluxion_b200.steppers import DiffusionSolver, TimeScheme
+    g, h, bc, data, u = _setup(64, dev)
+    s = DiffusionSolver.new(g, 0.01, None, dev)
+    s.step_n(u, 100)
+    peak = u.to_vec_f64().max()
+    assert 0.0 < peak < data.max()
+    assert abs(s.dt() - 0.4 * h * h / (4 * 0.01)) < 1e-18
+    n = 32
+    g32 = Grid.square(n, 1.0 / (n - 1))
+    u = Field.from_f64(g32, np.ones(n * n), dev)
+    s = DiffusionSolver.new(g32, 0.01, None, dev)
+    s.step_n(u, 10)
+    assert s.steps_done() == 10
+    s.step_n(u, 5)
+    assert s.steps_done() == 15
+    u = Field.zeros(g32, DType.F64, dev)
+    src = Field.from_f64(g32, np.full(n * n, 100.0), dev)
+    s = DiffusionSolver.new(g32, 0.01, None, dev)
+    s.step_n_with_source(u, 50, src)
+    assert u.max() > 0.0
+    hh = 1.0 / (n - 1)
+    t = np.arange(n) * hh
+    X, Y = np.meshgrid(t, t)
+    sin = (np.sin(np.pi * X) * np.sin(np.pi * Y)).ravel()
+    for scheme in (TimeScheme.Rk2, TimeScheme.Rk4):
+        u = Field.from_f64(g32, sin, dev)
+        s = DiffusionSolver.build(g32, 0.01, None, Boundaries.zero_dirichlet(), scheme, dev)
+        s.step_n(u, 200)
+        nrm = u.norm_l2()
+        assert np.isfinite(nrm) and 0.0 < nrm < np.linalg.norm(sin) and s.scheme() == scheme
+
+
+@pytest.mark.parametrize("scheme", ["Euler", "Rk2", "Rk4"])
+def test_graph_replay_equals_eager_steps(dev, scheme):
+    """The recorded-and-replayed step (solver.rs:259-325 on CUDA graphs) is the same sequence of
+    kernels as the eager step: bitwise equal after 25 steps."""
+    from fluxion_b200 import Boundaries, Field
+    from fluxion_b200.steppers import DiffusionSolver, TimeScheme
+    g, h, bc, data, _ = _setup(64, dev)
+    ue, ug = Field.from_f64(g, data, dev), Field.from_f64(g, data, dev)
+    se = DiffusionSolver.build(g, 0.01, None, Boundaries.zero_dirichlet(), TimeScheme[scheme], dev)
+    sg = DiffusionSolver.build(g, 0.01, None, Boundaries.zero_dirichlet(), TimeScheme[scheme], dev)
+    sg.enable_graph()
+    se.step_n(ue, 25)
+    sg.step_n(ug, 10)
+    sg.step_n(ug, 15)
+    assert sg.steps_done() == se.steps_done() == 25
+    assert np.array_equal(ug.to_vec_f64(), ue.to_vec_f64())
