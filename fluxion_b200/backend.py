@@ -195,23 +195,26 @@ class CudaGraph:
 class CudaBackend:
     """The B200 backend: one CUDA context and stream per device."""
 
-    _instances: Dict[int, "CudaBackend"] = {}
+    _instances: Dict[tuple, "CudaBackend"] = {}
     _lock = threading.Lock()
 
-    def __init__(self, ordinal: int = 0):
+    def __init__(self, ordinal: int = 0, lane: int = 0):
         lib = L.lib()
         h = C.c_void_p()
         check(lib.fx_ctx_create(int(ordinal), C.byref(h)))
         self.ctx = h.value
         self.ordinal = ordinal
+        self.lane = lane
 
     @classmethod
-    def get(cls, ordinal: int = 0) -> "CudaBackend":
+    def get(cls, ordinal: int = 0, lane: int = 0) -> "CudaBackend":
+        """The context of (device, lane): one per pair, created on first use, each with its own
+        non-blocking stream."""
         with cls._lock:
-            b = cls._instances.get(ordinal)
+            b = cls._instances.get((ordinal, lane))
             if b is None:
-                b = cls(ordinal)
-                cls._instances[ordinal] = b
+                b = cls(ordinal, lane)
+                cls._instances[(ordinal, lane)] = b
             return b
 
     @staticmethod

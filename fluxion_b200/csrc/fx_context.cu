@@ -26,6 +26,43 @@ int check_launch(fx_ctx *ctx, const char *what) {
     return FX_OK;
 }
 
+// Buffers come from one stream-ordered memory pool per device, owned by the library and never
+// trimmed (its release threshold is the maximum), so that creating and dropping fields and
+// hierarchies neither synchronises the device nor maps memory again: cudaFree would wait for
+// every stream of the device, which serialises contexts that run independent problems side by
+// side.  An allocation is ordered on the context's stream; fx_ctx_set_stream waits for the old
+// stream before switching, so buffers made earlier are ready on the new one.
+static cudaMemPool_t device_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = p;
+    }
+    return pools[device];
+}
+
+static bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return cs != cudaStreamCaptureStatusNone;
+}
+
 void timing_pre(fx_ctx *ctx, const char *what) {
     if (!ctx->timing || ctx->timing_name != what) return;
     if (ctx->pool_next + 2 > ctx->event_pool.size()) {
@@ -257,6 +294,7 @@ int fx_ctx_create(int device, fx_ctx **out) {
 int fx_ctx_destroy(fx_ctx *c) {
     if (!c) return FX_OK;
     cudaSetDevice(c->device);
+    for (void *p : c->deferred_free) cudaFree(p);  // waits for the device, as it should here
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->d_partials) cudaFree(c->d_partials);
     if (c->d_counter) cudaFree(c->d_counter);
@@ -293,6 +331,8 @@ int fx_graph_end(fx_ctx *c, fx_graph **out) {
     *out = nullptr;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    for (void *p : c->deferred_free) cudaFreeAsync(p, c->stream);
+    c->deferred_free.clear();
     if (e != cudaSuccess || !g) {
         if (g) cudaGraphDestroy(g);
         (void)cudaGetLastError();
@@ -326,7 +366,9 @@ int fx_graph_destroy(fx_graph *g) {
 
 int fx_ctx_set_stream(fx_ctx *c, void *stream) {
     if (!c) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
-    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    cudaStream_t next = stream ? (cudaStream_t)stream : c->own_stream;
+    if (next != c->stream) FX_CUDA(cudaStreamSynchronize(c->stream));
+    c->stream = next;
     return FX_OK;
 }
 
@@ -393,13 +435,21 @@ int fx_alloc(fx_ctx *ctx, size_t len, int dtype, fx_buf **out) {
     b->dtype = dtype;
     const size_t bytes = len * elem_size(dtype);
     if (bytes) {
-        if (cudaMalloc(&b->ptr, bytes) != cudaSuccess) {
+        // While the stream is being captured a pool allocation would become a node of the
+        // graph; a plain allocation is made outside it instead.
+        cudaMemPool_t pool = capturing(ctx->stream) ? nullptr : device_pool(ctx->device);
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&b->ptr, bytes, pool, ctx->stream) : cudaMalloc(&b->ptr, bytes);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
             delete b;
-            return fail(FX_ERR_BACKEND, std::string("backend error: allocation failed: ") +
-                                            cudaGetErrorString(cudaGetLastError()));
+            return fail(FX_ERR_BACKEND, std::string("backend error: allocation failed: ") + cudaGetErrorString(e));
         }
+        b->pooled = pool != nullptr;
         if (cudaMemsetAsync(b->ptr, 0, bytes, ctx->stream) != cudaSuccess) {
-            cudaFree(b->ptr);
+            if (b->pooled)
+                cudaFreeAsync(b->ptr, ctx->stream);
+            else
+                cudaFree(b->ptr);
             delete b;
             return fail(FX_ERR_BACKEND, "backend error: memset failed");
         }
@@ -424,8 +474,14 @@ int fx_wrap(fx_ctx *ctx, void *ptr, size_t len, int dtype, fx_buf **out) {
 int fx_free(fx_buf *b) {
     if (!b) return FX_OK;
     if (b->owned && b->ptr) {
-        cudaStreamSynchronize(b->ctx->stream);
-        cudaFree(b->ptr);
+        if (!b->pooled) {
+            cudaStreamSynchronize(b->ctx->stream);
+            cudaFree(b->ptr);
+        } else if (capturing(b->ctx->stream)) {
+            b->ctx->deferred_free.push_back(b->ptr);
+        } else {
+            cudaFreeAsync(b->ptr, b->ctx->stream);  // after the work queued on it so far
+        }
     }
     delete b;
     return FX_OK;
@@ -460,7 +516,9 @@ int write_host(fx_ctx *ctx, fx_buf *b, const void *src, int src_dtype, size_t le
         return FX_OK;
     }
     void *tmp = nullptr;
-    FX_CUDA(cudaMallocAsync(&tmp, len * elem_size(src_dtype), ctx->stream));
+    cudaMemPool_t pool = device_pool(ctx->device);
+    FX_CUDA(pool ? cudaMallocFromPoolAsync(&tmp, len * elem_size(src_dtype), pool, ctx->stream)
+                 : cudaMallocAsync(&tmp, len * elem_size(src_dtype), ctx->stream));
     FX_CUDA(cudaMemcpyAsync(tmp, src, len * elem_size(src_dtype), cudaMemcpyHostToDevice, ctx->stream));
     FlatGeom g = flat_geom(ctx, len);
     if (src_dtype == FX_F64)
@@ -485,7 +543,9 @@ int read_host(fx_ctx *ctx, const fx_buf *b, void *dst, int dst_dtype, size_t len
         return FX_OK;
     }
     void *tmp = nullptr;
-    FX_CUDA(cudaMallocAsync(&tmp, len * elem_size(dst_dtype), ctx->stream));
+    cudaMemPool_t pool = device_pool(ctx->device);
+    FX_CUDA(pool ? cudaMallocFromPoolAsync(&tmp, len * elem_size(dst_dtype), pool, ctx->stream)
+                 : cudaMallocAsync(&tmp, len * elem_size(dst_dtype), ctx->stream));
     FlatGeom g = flat_geom(ctx, len);
     if (dst_dtype == FX_F32)
         k_f64_to_f32<<<g.blocks, kBlock, 0, ctx->stream>>>((const double *)b->ptr, (float *)tmp, len);

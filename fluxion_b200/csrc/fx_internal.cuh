@@ -3,6 +3,7 @@
 // row-marching stencil framework every grid kernel is built on.
 #pragma once
 
+#include <atomic>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -66,6 +67,9 @@ struct fx_ctx {
     std::vector<cudaEvent_t> event_pool;
     size_t pool_next = 0;
     bool timing_open = false;
+    // pool memory whose buffer was freed while the stream was being captured; returned to the
+    // pool, in stream order, once the capture ends (or the context is destroyed)
+    std::vector<void *> deferred_free;
 };
 
 struct fx_buf {
@@ -74,6 +78,7 @@ struct fx_buf {
     size_t len = 0;
     int dtype = FX_F64;
     bool owned = true;
+    bool pooled = false;  // from the device's stream-ordered pool (else plain cudaMalloc)
 };
 
 namespace fx {
@@ -553,11 +558,15 @@ int launch_march(fx_ctx *ctx, size_t rows, size_t cols, Loader ld, Point pt, Fin
                  const char *what) {
     constexpr int CPT = band_cpt<T>();
     constexpr int D = band_depth<Point::NA + Loader::NL - 1>();
-    static int occ = 0;  // resident CTAs per SM for this instantiation
+    // resident CTAs per SM for this instantiation, cached (contexts may launch from several
+    // host threads: every thread computes the same value)
+    static std::atomic<int> occ_cache{0};
+    int occ = occ_cache.load(std::memory_order_relaxed);
     if (!occ) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_march<T, CPT, D, K, Loader, Point, Fin>,
                                                           kBandThreads, 0) != cudaSuccess || occ < 1)
             occ = 1;
+        occ_cache.store(occ, std::memory_order_relaxed);
     }
     const MarchGeom G = march_geom(rows, cols, kBlock * CPT, D, occ * ctx->num_sms);
     if (K > 0 && G.nblocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");

@@ -7,6 +7,7 @@
 // bitwise equal to the unfused one.
 #pragma once
 
+#include <atomic>
 #include <type_traits>
 
 #include "fx_points.cuh"
@@ -433,10 +434,12 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vtail(TailArgs<T> A, const 
 
 template <typename T>
 int launch_vtail(fx_ctx *ctx, const TailArgs<T> &A, size_t smem, const int *skip) {
-    static size_t attr = 0;  // dynamic shared memory opted in for this instantiation so far
-    if (smem > 48 * 1024 && smem > attr) {
+    static std::atomic<size_t> attr{0};  // dynamic shared memory opted in for this instantiation so far
+    if (smem > 48 * 1024 && smem > attr.load()) {
         FX_CUDA(cudaFuncSetAttribute(k_vtail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = smem;
+        size_t cur = attr.load();
+        while (smem > cur && !attr.compare_exchange_weak(cur, smem)) {
+        }
     }
     timing_pre(ctx, "mg_tail");
     launch_pdl(ctx, k_vtail<T>, 1, kTailThreads, smem, A, skip);
@@ -446,12 +449,14 @@ int launch_vtail(fx_ctx *ctx, const TailArgs<T> &A, size_t smem, const int *skip
 
 // blocks of `kernel` (of `threads` threads) resident on the whole GPU at once
 template <typename K>
-int band_capacity(fx_ctx *ctx, K kernel, int &cache, int threads = kBandThreads) {
-    if (!cache) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cache, kernel, threads, 0) != cudaSuccess || cache < 1)
-            cache = 1;
+int band_capacity(fx_ctx *ctx, K kernel, std::atomic<int> &cache, int threads = kBandThreads) {
+    int occ = cache.load(std::memory_order_relaxed);
+    if (!occ) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, 0) != cudaSuccess || occ < 1)
+            occ = 1;
+        cache.store(occ, std::memory_order_relaxed);
     }
-    return cache * ctx->num_sms;
+    return occ * ctx->num_sms;
 }
 
 }  // namespace fx

@@ -376,7 +376,7 @@ inline long strip_capacity(long resident_warps, int chunk_pct) {
 template <typename T, typename TB>
 int launch_wdown(fx_ctx *ctx, size_t rows, size_t cols, const TB *b, T *x2, T *coarse, size_t ccols,
                  const VOp<T> &op, const int *skip, int chunk_pct = 100) {
-    static int occ = 0;
+    static std::atomic<int> occ{0};
     const long cap = strip_capacity((long)band_capacity(ctx, k_wdown<T, TB>, occ, kStripWarps * 32) * kStripWarps,
                                     chunk_pct);
     const StripGeom G = strip_geom(rows, cols, kDownOwn, cap);
@@ -392,7 +392,7 @@ int launch_wdown(fx_ctx *ctx, size_t rows, size_t cols, const TB *b, T *x2, T *c
 template <typename T, typename TB, typename TZ, bool RZ, typename Fin>
 int launch_wup(fx_ctx *ctx, size_t rows, size_t cols, const T *x2, const T *e, size_t ccols, const TB *b, TZ *z,
                const VOp<T> &op, Fin fin, const int *skip, int chunk_pct = 100) {
-    static int occ = 0;
+    static std::atomic<int> occ{0};
     const long cap = strip_capacity(
         (long)band_capacity(ctx, k_wup<T, TB, TZ, RZ, Fin>, occ, kStripWarps * 32) * kStripWarps, chunk_pct);
     const StripGeom G = strip_geom(rows, cols, kUpOwn, cap);

@@ -24,13 +24,19 @@ class DeviceMismatch(Exception):
 
 @dataclass(frozen=True)
 class Device:
-    """crates/runtime/src/device.rs:3-11 (only the CUDA variant exists here)."""
+    """crates/runtime/src/device.rs:3-11 (only the CUDA variant exists here).
+
+    ``lane`` selects one of several independent contexts on the same GPU, each with its own
+    stream (new; the reference has one stream per device): work on different lanes may run
+    concurrently, so independent problems can share the GPU from several host threads.  A field
+    belongs to its lane; operations never mix lanes."""
 
     ordinal: int = 0
+    lane: int = 0
 
     @staticmethod
-    def Cuda(ordinal: int = 0) -> "Device":  # noqa: N802 - reference variant name
-        return Device(int(ordinal))
+    def Cuda(ordinal: int = 0, lane: int = 0) -> "Device":  # noqa: N802 - reference variant name
+        return Device(int(ordinal), int(lane))
 
     @staticmethod
     def best() -> "Device":
@@ -40,10 +46,10 @@ class Device:
         raise BackendUnavailable("no CUDA device")
 
     def backend(self) -> CudaBackend:
-        return CudaBackend.get(self.ordinal)
+        return CudaBackend.get(self.ordinal, self.lane)
 
     def __str__(self):
-        return f"cuda:{self.ordinal}"
+        return f"cuda:{self.ordinal}" + (f"/lane{self.lane}" if self.lane else "")
 
 
 class Field:

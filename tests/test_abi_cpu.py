@@ -69,3 +69,11 @@ def test_null_handles_are_rejected():
     assert lib.fx_ctx_synchronize(None) == L.FX_ERR_INVALID_ARGUMENT
     out = C.c_double()
     assert lib.fx_dot(None, None, None, C.byref(out)) == L.FX_ERR_INVALID_ARGUMENT
+
+
+def test_device_lanes_are_distinct_values():
+    from fluxion_b200 import Device
+    assert Device.Cuda(0) == Device(0, 0) and str(Device.Cuda(0)) == "cuda:0"
+    d = Device.Cuda(0, lane=3)
+    assert d.lane == 3 and d != Device.Cuda(0) and str(d) == "cuda:0/lane3"
+    assert len({Device.Cuda(0, k) for k in range(4)}) == 4
