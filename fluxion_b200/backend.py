@@ -235,6 +235,10 @@ class CudaBackend:
     def set_stream(self, stream_ptr: Optional[int]) -> None:
         check(L.lib().fx_ctx_set_stream(self.ctx, stream_ptr or None))
 
+    def set_pdl(self, enabled: bool) -> None:
+        """Programmatic dependent launch for this context's kernels (on by default)."""
+        check(L.lib().fx_ctx_set_pdl(self.ctx, 1 if enabled else 0))
+
     def stream(self) -> int:
         return L.lib().fx_ctx_get_stream(self.ctx) or 0
 

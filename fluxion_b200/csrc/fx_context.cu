@@ -372,6 +372,12 @@ int fx_ctx_set_stream(fx_ctx *c, void *stream) {
     return FX_OK;
 }
 
+int fx_ctx_set_pdl(fx_ctx *c, int enabled) {
+    if (!c) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    c->pdl = enabled != 0;
+    return FX_OK;
+}
+
 void *fx_ctx_get_stream(fx_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 unsigned long long fx_ctx_launch_count(fx_ctx *c) { return c ? c->launches : 0ull; }

@@ -55,6 +55,7 @@ struct fx_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     int num_sms = 148;
+    bool pdl = true;  // programmatic dependent launch (fx_ctx_set_pdl)
     double *d_partials = nullptr;  // [kMaxRedBlocks][2*kMaxSums]
     unsigned *d_counter = nullptr; // last-block ticket
     double *d_result = nullptr;    // results of standalone reductions [kMaxSums]
@@ -108,7 +109,7 @@ inline void launch_pdl(fx_ctx *ctx, void (*kernel)(KArgs...), dim3 grid, dim3 bl
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = ctx->pdl ? 1 : 0;
     (void)cudaLaunchKernelEx(&cfg, kernel, args...);  // errors surface in check_launch
 }
 // Timing hooks around a launch (no-ops unless fx_ctx_timing_begin named this kernel).

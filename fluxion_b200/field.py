@@ -101,6 +101,18 @@ class Field:
         self.storage.copy_to_host_f64(out)
         return out
 
+    def copy_to_host(self, out: np.ndarray) -> None:
+        """This field into an existing contiguous host array of its length (f64 or f32,
+        converted on the device); with page-locked memory the copy is a direct DMA."""
+        if out.size != self.storage.len() or not out.flags.c_contiguous:
+            raise DimensionMismatch(self.storage.len(), out.size)
+        if out.dtype == np.float64:
+            self.storage.copy_to_host_f64(out)
+        elif out.dtype == np.float32:
+            self.storage.copy_to_host_f32(out)
+        else:
+            raise TypeError(f"host array must be float64 or float32, not {out.dtype}")
+
     def to_vec_f32(self) -> np.ndarray:
         out = np.empty(self.storage.len(), dtype=np.float32)
         self.storage.copy_to_host_f32(out)

@@ -118,6 +118,12 @@ int fx_ctx_synchronize(fx_ctx *ctx);
 /* Use an external cudaStream_t (e.g. the caller's); NULL restores the context's own. */
 int fx_ctx_set_stream(fx_ctx *ctx, void *stream);
 void *fx_ctx_get_stream(fx_ctx *ctx);
+/* Programmatic dependent launch for this context's kernels: 1 (the default) lets each kernel's
+ * blocks be scheduled while the previous kernel drains and wait on the SM for its results; 0
+ * launches them plainly.  A context that shares the GPU with other busy contexts may do better
+ * with 0, since the waiting blocks hold SM slots that the others' kernels could use.  Results
+ * are the same either way. */
+int fx_ctx_set_pdl(fx_ctx *ctx, int enabled);
 /* Number of kernels this context has launched (for launch accounting). */
 unsigned long long fx_ctx_launch_count(fx_ctx *ctx);
 /* Per-kernel timing: from fx_ctx_timing_begin until fx_ctx_timing_end, every launch of the

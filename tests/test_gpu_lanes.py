@@ -81,3 +81,12 @@ def test_pool_buffers_are_zeroed_and_follow_a_stream_switch():
     finally:
         be.set_stream(None)
     assert np.array_equal(v.to_vec_f64(), data)
+    out = torch.empty(data.size, dtype=torch.float64, pin_memory=True).numpy()
+    v.copy_to_host(out)
+    assert np.array_equal(out, data)
+    out32 = np.empty(data.size, dtype=np.float32)
+    v.copy_to_host(out32)
+    assert np.array_equal(out32, data.astype(np.float32))
+    from fluxion_b200 import DimensionMismatch
+    with pytest.raises(DimensionMismatch):
+        v.copy_to_host(np.empty(data.size - 1))
