@@ -578,6 +578,51 @@ int launch_march(fx_ctx *ctx, size_t rows, size_t cols, Loader ld, Point pt, Fin
     return check_launch(ctx, what);
 }
 
+// The point functor of a march, one point per thread: the field's neighbours are loaded
+// straight from memory (zeros outside the grid, as the march's ring holds), the aux arrays at
+// the point, and the point is called with the same arguments the march passes.  For point
+// functors that read further arrays of their own at every point (the convection-diffusion
+// operator's velocity and kappa fields), whose loads the march's FIFO does not run ahead of,
+// full occupancy hides the latency instead.  Diagonal neighbours are not loaded: the functors
+// launched this way use the 5-point neighbourhood only.
+template <typename T, int K, typename Loader, typename Point, typename Fin>
+__global__ void __launch_bounds__(kBlock) k_point(size_t rows, size_t cols, Loader ld_in, Point pt_in, Fin fin,
+                                                  RedArgs<K> ra, const int *skip) {
+    grid_dep_enter();
+    if (skip && *(volatile const int *)skip) return;
+    Loader ld = ld_in;
+    fx_prepare(ld);
+    Point pt = pt_in;
+    fx_prepare(pt);
+    constexpr int NA = Point::NA;
+    constexpr int NL = Loader::NL;
+    CSum acc[K > 0 ? K : 1];
+#pragma unroll
+    for (int k = 0; k < (K > 0 ? K : 1); k++) acc[k] = CSum{0.0, 0.0};
+    auto val = [&](size_t j) -> T {
+        T v[NL];
+        ld.load(j, v);
+        return ld.combine(v);
+    };
+    const size_t n = rows * cols, stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const size_t r = i / cols, c = i - r * cols;
+        Nb<T> nb;
+        nb.c = val(i);
+        nb.n = r > 0 ? val(i - cols) : (T)0;
+        nb.s = r + 1 < rows ? val(i + cols) : (T)0;
+        nb.w = c > 0 ? val(i - 1) : (T)0;
+        nb.e = c + 1 < cols ? val(i + 1) : (T)0;
+        nb.nw = nb.ne = nb.sw = nb.se = (T)0;
+        T a[NA > 0 ? NA : 1];
+#pragma unroll
+        for (int k = 0; k < NA; k++) a[k] = pt.aux(k)[i];
+        const bool ring = r == 0 || c == 0 || r + 1 == rows || c + 1 == cols;
+        pt(ring, (int)r, (int)c, i, nb, a, acc);
+    }
+    if constexpr (K > 0) grid_reduce<K>(acc, ra, fin);
+}
+
 // ------------------------------------------------------------------ flat (1-D) kernels
 
 struct FlatGeom {
@@ -609,6 +654,18 @@ int launch_flat(fx_ctx *ctx, size_t n, F f, Fin fin, const int *skip, const char
     timing_pre(ctx, what);
     launch_pdl(ctx, k_flat<K, F, Fin>, g.blocks, kBlock, 0, n, f, fin, red_args<K>(ctx), skip);
     timing_post(ctx, (double)n);
+    return check_launch(ctx, what);
+}
+
+template <typename T, int K, typename Loader, typename Point, typename Fin>
+int launch_point(fx_ctx *ctx, size_t rows, size_t cols, Loader ld, Point pt, Fin fin, const int *skip,
+                 const char *what) {
+    FlatGeom g = flat_geom(ctx, rows * cols);
+    if (g.blocks == 0) return FX_OK;
+    timing_pre(ctx, what);
+    launch_pdl(ctx, k_point<T, K, Loader, Point, Fin>, g.blocks, kBlock, 0, rows, cols, ld, pt, fin, red_args<K>(ctx),
+               skip);
+    timing_post(ctx, (double)rows * (double)cols);
     return check_launch(ctx, what);
 }
 
