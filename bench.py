@@ -72,6 +72,8 @@ def parse():
                         "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target; batch: "
                         "1024 conv-diff problems; convdiff: convection-dominated conv-diff at --n")
     p.add_argument("--nu", default="1e-3,1e-4", help="--mode convdiff: viscosities, comma-separated")
+    p.add_argument("--mg-dtype", default="f64", choices=["f64", "f32"],
+                   help="--mode batch: arithmetic of the conv-diff V-cycle (the Krylov solver stays FP64)")
     return p.parse_args()
 
 
@@ -287,6 +289,7 @@ def run_batch(args):
 
     nu = 1e-2
     lanes = max(1, int(args.lanes))
+    mg_dtype = DType.F32 if args.mg_dtype == "f32" else DType.F64
     rng = np.random.default_rng(SEED)
     ks = rng.integers(6, 11, size=args.batch)
     sizes = [int(2 ** k + 1) ** 2 for k in ks]
@@ -322,7 +325,7 @@ def run_batch(args):
         VX, VY, b = Field.from_f64(g, vx, dev), Field.from_f64(g, vy, dev), Field.from_f64(g, f, dev)
         x = Field.zeros(g, DType.F64, dev)
         op = ConvDiffOperator(g, VX, VY, -nu, sigma=0.0, coeff=1.0)
-        mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS)
+        mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, mg_dtype)
         solver = solvers.get(N)  # one solver (and its work vectors) per grid size, reused
         if solver is None:
             solver = solvers[N] = BiCgStabSolver(g, dev, 1.0, 200)
@@ -378,7 +381,7 @@ def run_batch(args):
     ok = all(r[1].converged() for r in res)
     print(json.dumps({
         "mode": "batch", "workload": f"convdiff_batch_{args.batch}_k6-10_nu1e-2_bicgstab_cdmg",
-        "problems": args.batch, "lanes": lanes, "pdl": bool(args.pdl),
+        "problems": args.batch, "lanes": lanes, "pdl": bool(args.pdl), "vcycle_dtype": args.mg_dtype,
         "interior_sizes": {str(2 ** k - 1): int((ks == k).sum()) for k in range(6, 11)},
         "solves_per_s": args.batch / wall, "wall_s_excluding_host_data_generation": wall,
         "per_problem_ms_p50": float(np.percentile([r[4] * 1e3 for r in res], 50)),
@@ -386,7 +389,8 @@ def run_batch(args):
         "solve_ms_p50": float(np.percentile(ms, 50)), "solve_ms_p99": float(np.percentile(ms, 99)),
         "iterations_p50": float(np.percentile(its, 50)), "iterations_max": int(its.max()),
         "all_converged": ok, "max_true_rel_residual": max(r[3] for r in res),
-        "dtype": "f64", "data": "synthetic (seeded per problem), page-locked host arrays",
+        "dtype": "f64" if args.mg_dtype == "f64" else "f64 (Krylov) / f32 (V-cycle)",
+        "data": "synthetic (seeded per problem), page-locked host arrays",
         "note": f"{lanes} host thread(s), one context and stream each, through the public API; "
                 "the persistent batched launch is not built"}),
         flush=True)
@@ -400,7 +404,8 @@ def run_convdiff(args):
     seeded.  Each solver to ||b - A x|| < 1e-10 ||f|| (FP64) from x = 0, preconditioned by the
     conv-diff V(2,2)-cycle (weighted Jacobi 0.8, full weighting / bilinear, coarsest 15^2 x 200
     sweeps): flexible GMRES(30), GMRES(30) (left-preconditioned: it stops on the preconditioned
-    residual, so its true residual is reported beside it) and BiCGSTAB.  Device time with CUDA
+    residual, so its true residual is reported beside it) and BiCGSTAB; FGMRES and BiCGSTAB
+    again with the cycle in FP32 (the Krylov solver, its vectors and the residual stay FP64).  Device time with CUDA
     events around each solve; the true residual recomputed on the device.  These are the plain
     Jacobi-multigrid arms; the learned smoother is not built."""
     import torch
@@ -422,10 +427,13 @@ def run_convdiff(args):
     ok = True
     for nu in [float(v) for v in args.nu.split(",")]:
         op = ConvDiffOperator(g, VX, VY, -nu, sigma=0.0, coeff=1.0)
-        mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS)
-        for name, make in (("fgmres30", lambda: FgmresSolver(g, dev, 30, 1e-10 * fnorm, 2000)),
-                           ("gmres30", lambda: GmresSolver(g, dev, 30, 1e-10 * fnorm, 2000)),
-                           ("bicgstab", lambda: BiCgStabSolver(g, dev, 1e-10 * fnorm, 2000))):
+        arms = [(mdt, name, make) for mdt in (DType.F64, DType.F32) for name, make in (
+            ("fgmres30", lambda: FgmresSolver(g, dev, 30, 1e-10 * fnorm, 2000)),
+            ("gmres30", lambda: GmresSolver(g, dev, 30, 1e-10 * fnorm, 2000)),
+            ("bicgstab", lambda: BiCgStabSolver(g, dev, 1e-10 * fnorm, 2000)))
+            if mdt == DType.F64 or name != "gmres30"]
+        for mdt, name, make in arms:
+            mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, mdt)
             solver = make()
             x = Field.zeros(g, DType.F64, dev)
             solver.solve_op(x, b, op, mg)  # warm-up solve (same problem)
@@ -442,7 +450,8 @@ def run_convdiff(args):
             true_rel = ax.norm_l2() / fnorm
             ok = ok and st.converged() and (name == "gmres30" or true_rel < 1e-10)
             cell_peclet = h / (2.0 * nu)  # max|v| h / (2 nu)
-            runs.append({"nu": nu, "solver": name + " + conv-diff V(2,2)-cycle", "iterations": st.iterations,
+            cyc = " + conv-diff V(2,2)-cycle" + (" in FP32" if mdt == DType.F32 else "")
+            runs.append({"nu": nu, "solver": name + cyc, "iterations": st.iterations,
                          "converged": st.converged(), "ms": e0.elapsed_time(e1), "true_rel_residual": true_rel,
                          "ms_per_iteration": e0.elapsed_time(e1) / max(1, st.iterations),
                          "max_cell_peclet": cell_peclet})

@@ -2258,9 +2258,11 @@ int check_op(const fx_grid &g, const fx_op *op) {
 // one block; every cycle from x = 0.  Unfused (a sweep, residual and transfer pass each): the
 // variable coefficients do not fit the constant-stencil level kernels.
 
-__device__ __forceinline__ double cd_diag(const OpA<double, kModeCD> &A, size_t idx) {
-    const double kap = A.kappa ? A.kappa[idx] : A.kap_s;
-    return fma(A.coeff, fma(-kap, A.K.k2, fma(fabs(A.vx[idx]), A.K.inv_dx, fabs(A.vy[idx]) * A.K.inv_dy)), A.sigma);
+template <typename T>
+__device__ __forceinline__ T cd_diag(const OpA<T, kModeCD> &A, size_t idx) {
+    const T kap = A.kappa ? A.kappa[idx] : A.kap_s;
+    return fx_fma(A.coeff, fx_fma(-kap, A.K.k2, fx_fma(fabs(A.vx[idx]), A.K.inv_dx, fabs(A.vy[idx]) * A.K.inv_dy)),
+                  A.sigma);
 }
 
 // Smoothing sweep (out = x + omega (b - A x) / diag(A)) and residual (out = b - A x), inside
@@ -2268,36 +2270,38 @@ __device__ __forceinline__ double cd_diag(const OpA<double, kModeCD> &A, size_t 
 // memory (west / east from the same cache lines, north / south from L2): with four input arrays
 // a row march holds too few loads in flight per SM (it measured 2.8 TB/s on the finest 4097^2
 // sweep), these run at full occupancy.
+template <typename T>
 struct FlatCdSweep {
-    OpA<double, kModeCD> A;
-    const double *x;
-    double *out;
-    const double *b;
-    double omega;
+    OpA<T, kModeCD> A;
+    const T *x;
+    T *out;
+    const T *b;
+    T omega;
     size_t rows, cols;
     __device__ __forceinline__ void operator()(size_t i, CSum *) const {
         const size_t row = i / cols, col = i - row * cols;
         if (row == 0 || col == 0 || row == rows - 1 || col == cols - 1) return;
-        Nb<double> nb;
+        Nb<T> nb;
         nb.c = x[i];
         nb.n = x[i - cols];
         nb.s = x[i + cols];
         nb.w = x[i - 1];
         nb.e = x[i + 1];
-        out[i] = fma(omega, (b[i] - A.apply(false, nb, i)) / cd_diag(A, i), nb.c);
+        out[i] = fx_fma(omega, (b[i] - A.apply(false, nb, i)) / cd_diag(A, i), nb.c);
     }
 };
 
+template <typename T>
 struct FlatCdResid {
-    OpA<double, kModeCD> A;
-    const double *x;
-    double *out;
-    const double *b;
+    OpA<T, kModeCD> A;
+    const T *x;
+    T *out;
+    const T *b;
     size_t rows, cols;
     __device__ __forceinline__ void operator()(size_t i, CSum *) const {
         const size_t row = i / cols, col = i - row * cols;
         if (row == 0 || col == 0 || row == rows - 1 || col == cols - 1) return;
-        Nb<double> nb;
+        Nb<T> nb;
         nb.c = x[i];
         nb.n = x[i - cols];
         nb.s = x[i + cols];
@@ -2307,70 +2311,80 @@ struct FlatCdResid {
     }
 };
 
-struct FlatInject {  // coarse field = fine field at the coincident points
-    const double *f;
-    double *c;
+template <typename S, typename D>
+struct FlatInject {  // coarse field = fine field at the coincident points (S -> D)
+    const S *f;
+    D *c;
     size_t fcols, ccols;
     __device__ __forceinline__ void operator()(size_t i, CSum *) const {
         const size_t I = i / ccols, J = i - I * ccols;
-        c[i] = f[(2 * I) * fcols + 2 * J];
+        c[i] = (D)f[(2 * I) * fcols + 2 * J];
     }
+};
+
+template <typename S, typename D>
+struct FlatCast {  // d = (D) s
+    const S *s;
+    D *d;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const { d[i] = (D)s[i]; }
 };
 
 // Coarsest level in one block: the iterate ping-pongs in shared memory, each thread keeps its
 // points' rhs and diagonal in registers; every point value is FlatCdSweep's expression.
-__global__ void __launch_bounds__(1024) k_cd_coarse(double *u, const double *__restrict__ b, int rows, int cols,
-                                                    OpA<double, kModeCD> A, double omega, int nsweeps,
-                                                    const int *skip) {
+template <typename T>
+__global__ void __launch_bounds__(1024) k_cd_coarse(T *u, const T *__restrict__ b, int rows, int cols,
+                                                    OpA<T, kModeCD> A, T omega, int nsweeps, const int *skip) {
     if (skip && *(volatile const int *)skip) return;
     constexpr int kPts = 4;
     extern __shared__ unsigned char smem_raw[];
-    double *s0 = reinterpret_cast<double *>(smem_raw);
-    double *s1 = s0 + rows * cols;
+    T *s0 = reinterpret_cast<T *>(smem_raw);
+    T *s1 = s0 + rows * cols;
     const int n = rows * cols;
     int idx[kPts];
     bool inner[kPts];
-    double bv[kPts], dv[kPts];
+    T bv[kPts], dv[kPts];
 #pragma unroll
     for (int k = 0; k < kPts; k++) {
         const int i = threadIdx.x + k * blockDim.x;
         idx[k] = i;
         const int r = i / cols, c = i % cols;
         inner[k] = i < n && r > 0 && c > 0 && r < rows - 1 && c < cols - 1;
-        bv[k] = inner[k] ? b[i] : 0.0;
-        dv[k] = inner[k] ? cd_diag(A, (size_t)i) : 1.0;
+        bv[k] = inner[k] ? b[i] : (T)0;
+        dv[k] = inner[k] ? cd_diag(A, (size_t)i) : (T)1;
         if (i < n) {
-            s0[i] = 0.0;
-            s1[i] = 0.0;
+            s0[i] = (T)0;
+            s1[i] = (T)0;
         }
     }
     __syncthreads();
     for (int k = 0; k < nsweeps; k++) {
-        const double *src = (k & 1) ? s1 : s0;
-        double *dst = (k & 1) ? s0 : s1;
+        const T *src = (k & 1) ? s1 : s0;
+        T *dst = (k & 1) ? s0 : s1;
 #pragma unroll
         for (int q = 0; q < kPts; q++) {
             if (!inner[q]) continue;
             const int i = idx[q];
-            Nb<double> nb;
+            Nb<T> nb;
             nb.c = src[i];
             nb.n = src[i - cols];
             nb.s = src[i + cols];
             nb.w = src[i - 1];
             nb.e = src[i + 1];
-            dst[i] = fma(omega, (bv[q] - A.apply(false, nb, (size_t)i)) / dv[q], nb.c);
+            dst[i] = fx_fma(omega, (bv[q] - A.apply(false, nb, (size_t)i)) / dv[q], nb.c);
         }
         __syncthreads();
     }
-    const double *fin = (nsweeps & 1) ? s1 : s0;
+    const T *fin = (nsweeps & 1) ? s1 : s0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) u[i] = fin[i];
 }
 
 struct CdLevel {
     size_t rows = 0, cols = 0;
     double dx = 0, dy = 0;
-    fx_buf *u = nullptr, *rhs = nullptr, *tmp = nullptr;    // levels >= 1
-    fx_buf *vx = nullptr, *vy = nullptr, *kappa = nullptr;  // levels >= 1, injected
+    // levels >= 1, and level 0 of an F32 cycle: iterate, right-hand side, ping-pong partner
+    fx_buf *u = nullptr, *rhs = nullptr, *tmp = nullptr;
+    // levels >= 1 (injected), and level 0 of an F32 cycle (the operator's fields in F32)
+    fx_buf *vx = nullptr, *vy = nullptr, *kappa = nullptr;
 };
 
 }  // namespace
@@ -2380,8 +2394,9 @@ struct fx_cdmg {
     const fx_op *op = nullptr;
     size_t n_pre = 2, n_post = 2, coarse_sweeps = 200;
     double omega = 0.8;
+    int dtype = FX_F64;  // arithmetic and storage of the cycle; the vectors z, r stay F64
     std::vector<CdLevel> lv;
-    fx_buf *tmp0 = nullptr;  // level-0 ping-pong partner
+    fx_buf *tmp0 = nullptr;  // level-0 ping-pong partner of an F64 cycle
     struct View : fx_precond {
         fx_cdmg *mg = nullptr;
         int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) override;
@@ -2391,40 +2406,48 @@ struct fx_cdmg {
             for (fx_buf *f : {L.u, L.rhs, L.tmp, L.vx, L.vy, L.kappa}) fx_free(f);
         fx_free(tmp0);
     }
-    OpA<double, kModeCD> level_op(size_t l) const {
-        OpA<double, kModeCD> A = OpMaker<double, kModeCD>::make(StencilP{}, 0.0, 0, 0, op);
-        if (l > 0) {
-            const CdLevel &L = lv[l];
-            A.K = conv_consts<double>(L.dx, L.dy);
-            A.vx = (const double *)L.vx->ptr;
-            A.vy = (const double *)L.vy->ptr;
-            A.kappa = L.kappa ? (const double *)L.kappa->ptr : nullptr;
-        }
+    // The operator on level l: h doubled per level, the injected fields; level 0 of an F64
+    // cycle reads the operator's own fields.
+    template <typename T>
+    OpA<T, kModeCD> level_op(size_t l) const {
+        const CdLevel &L = lv[l];
+        OpA<T, kModeCD> A;
+        A.K = conv_consts<T>(L.dx, L.dy);
+        A.sigma = (T)op->sigma;
+        A.coeff = (T)op->coeff;
+        A.kap_s = (T)op->kappa_s;
+        const bool own = l == 0 && dtype == FX_F64;
+        A.vx = (const T *)(own ? op->vx->ptr : L.vx->ptr);
+        A.vy = (const T *)(own ? op->vy->ptr : L.vy->ptr);
+        const fx_buf *k = own ? op->kappa : L.kappa;
+        A.kappa = k ? (const T *)k->ptr : nullptr;
         return A;
     }
 };
 
 namespace {
 
-int cd_cycle(fx_cdmg *mg, double *x, const double *b, const int *skip) {  // x holds zeros on entry
+template <typename T>
+int cd_cycle(fx_cdmg *mg, T *x, const T *b, T *x_other, const int *skip) {  // x holds zeros on entry
     fx_ctx *ctx = mg->ctx;
     const int nl = (int)mg->lv.size();
-    std::vector<double *> cur(nl), oth(nl);
-    std::vector<const double *> rhs(nl);
+    std::vector<T *> cur(nl), oth(nl);
+    std::vector<const T *> rhs(nl);
     cur[0] = x;
-    oth[0] = (double *)mg->tmp0->ptr;
+    oth[0] = x_other;
     rhs[0] = b;
     for (int l = 1; l < nl; l++) {
-        cur[l] = (double *)mg->lv[l].u->ptr;
-        oth[l] = (double *)mg->lv[l].tmp->ptr;
-        rhs[l] = (const double *)mg->lv[l].rhs->ptr;
+        cur[l] = (T *)mg->lv[l].u->ptr;
+        oth[l] = (T *)mg->lv[l].tmp->ptr;
+        rhs[l] = (const T *)mg->lv[l].rhs->ptr;
     }
+    const T omega = (T)mg->omega;
     auto smooth = [&](int l, size_t n) -> int {
         const CdLevel &L = mg->lv[l];
-        const auto A = mg->level_op(l);
+        const auto A = mg->level_op<T>(l);
         for (size_t k = 0; k < n; k++) {
             FX_TRY((launch_flat<0>(ctx, L.rows * L.cols,
-                                   FlatCdSweep{A, cur[l], oth[l], rhs[l], mg->omega, L.rows, L.cols}, NoFin{}, skip,
+                                   FlatCdSweep<T>{A, cur[l], oth[l], rhs[l], omega, L.rows, L.cols}, NoFin{}, skip,
                                    "cdmg_sweep")));
             std::swap(cur[l], oth[l]);
         }
@@ -2433,18 +2456,19 @@ int cd_cycle(fx_cdmg *mg, double *x, const double *b, const int *skip) {  // x h
     for (int l = 0; l < nl - 1; l++) {
         const CdLevel &L = mg->lv[l], &Cl = mg->lv[l + 1];
         FX_TRY(smooth(l, mg->n_pre));
-        FX_TRY((launch_flat<0>(ctx, L.rows * L.cols, FlatCdResid{mg->level_op(l), cur[l], oth[l], rhs[l], L.rows, L.cols},
-                               NoFin{}, skip, "cdmg_residual")));
-        FX_TRY(restrict_fw<double>(ctx, oth[l], (double *)Cl.rhs->ptr, L.cols, Cl.rows, Cl.cols, skip));
-        FX_TRY(zero_fill<double>(ctx, cur[l + 1], Cl.rows * Cl.cols, skip));
+        FX_TRY((launch_flat<0>(ctx, L.rows * L.cols,
+                               FlatCdResid<T>{mg->level_op<T>(l), cur[l], oth[l], rhs[l], L.rows, L.cols}, NoFin{},
+                               skip, "cdmg_residual")));
+        FX_TRY(restrict_fw<T>(ctx, oth[l], (T *)Cl.rhs->ptr, L.cols, Cl.rows, Cl.cols, skip));
+        FX_TRY(zero_fill<T>(ctx, cur[l + 1], Cl.rows * Cl.cols, skip));
     }
     {
         const int l = nl - 1;
         const CdLevel &L = mg->lv[l];
         const size_t n = L.rows * L.cols;
-        if (coarse_fits(n, sizeof(double)) && mg->coarse_sweeps > 0) {
-            k_cd_coarse<<<1, coarse_threads(n), 2 * n * sizeof(double), ctx->stream>>>(
-                cur[l], rhs[l], (int)L.rows, (int)L.cols, mg->level_op(l), mg->omega, (int)mg->coarse_sweeps, skip);
+        if (coarse_fits(n, sizeof(T)) && mg->coarse_sweeps > 0) {
+            k_cd_coarse<T><<<1, coarse_threads(n), 2 * n * sizeof(T), ctx->stream>>>(
+                cur[l], rhs[l], (int)L.rows, (int)L.cols, mg->level_op<T>(l), omega, (int)mg->coarse_sweeps, skip);
             FX_TRY(check_launch(ctx, "cdmg_coarse_solve"));
         } else {
             FX_TRY(smooth(l, mg->coarse_sweeps));
@@ -2452,12 +2476,12 @@ int cd_cycle(fx_cdmg *mg, double *x, const double *b, const int *skip) {  // x h
     }
     for (int l = nl - 2; l >= 0; l--) {
         const CdLevel &L = mg->lv[l], &Cl = mg->lv[l + 1];
-        FX_TRY(prolong_bilinear<double>(ctx, cur[l + 1], cur[l], Cl.cols, L.rows, L.cols, skip));
+        FX_TRY(prolong_bilinear<T>(ctx, cur[l + 1], cur[l], Cl.cols, L.rows, L.cols, skip));
         FX_TRY(smooth(l, mg->n_post));
     }
     if (cur[0] != x) {
         const CdLevel &L0 = mg->lv[0];
-        FX_CUDA(cudaMemcpyAsync(x, cur[0], L0.rows * L0.cols * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        FX_CUDA(cudaMemcpyAsync(x, cur[0], L0.rows * L0.cols * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
     }
     return FX_OK;
 }
@@ -2466,12 +2490,20 @@ int cd_cycle(fx_cdmg *mg, double *x, const double *b, const int *skip) {  // x h
 
 int fx_cdmg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) {
     FX_TRY(check_same(z, r));
-    const CdLevel &L0 = mg->lv[0];
-    if (z->dtype != FX_F64 || z->len != L0.rows * L0.cols)
+    CdLevel &L0 = mg->lv[0];
+    const size_t n = L0.rows * L0.cols;
+    if (z->dtype != FX_F64 || z->len != n)
         return fail(FX_ERR_DIMENSION_MISMATCH, "conv-diff multigrid: vectors must be F64 fields of the operator's grid");
     if (z->ptr == r->ptr) return fail(FX_ERR_INVALID_ARGUMENT, "z and r must be distinct");
+    if (mg->dtype == FX_F32) {  // r -> F32, the cycle in F32, z = its F64 image
+        float *x = (float *)L0.u->ptr, *b = (float *)L0.rhs->ptr;
+        FX_TRY((launch_flat<0>(ctx, n, FlatCast<double, float>{(const double *)r->ptr, b}, NoFin{}, skip, "cdmg_convert")));
+        FX_TRY(zero_fill<float>(ctx, x, n, skip));
+        FX_TRY(cd_cycle<float>(mg, x, b, (float *)L0.tmp->ptr, skip));
+        return launch_flat<0>(ctx, n, FlatCast<float, double>{x, (double *)z->ptr}, NoFin{}, skip, "cdmg_convert");
+    }
     if (!z_zero) FX_TRY(zero_fill<double>(ctx, (double *)z->ptr, z->len, skip));
-    return cd_cycle(mg, (double *)z->ptr, (const double *)r->ptr, skip);
+    return cd_cycle<double>(mg, (double *)z->ptr, (const double *)r->ptr, (double *)mg->tmp0->ptr, skip);
 }
 
 namespace {
@@ -3122,7 +3154,13 @@ int fx_fgmres_solve_op(fx_fgmres *s, fx_buf *x, const fx_buf *b, const fx_op *op
 
 int fx_cdmg_create(const fx_op *op, size_t n_pre, size_t n_post, double omega, size_t coarse_max,
                    size_t coarse_sweeps, fx_cdmg **out) {
+    return fx_cdmg_create_typed(op, n_pre, n_post, omega, coarse_max, coarse_sweeps, FX_F64, out);
+}
+
+int fx_cdmg_create_typed(const fx_op *op, size_t n_pre, size_t n_post, double omega, size_t coarse_max,
+                         size_t coarse_sweeps, int dtype, fx_cdmg **out) {
     if (!op || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (dtype != FX_F32 && dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "unknown dtype");
     *out = nullptr;
     fx_cdmg *mg = new fx_cdmg();
     mg->ctx = op->ctx;
@@ -3131,45 +3169,63 @@ int fx_cdmg_create(const fx_op *op, size_t n_pre, size_t n_post, double omega, s
     mg->n_post = n_post;
     mg->omega = omega;
     mg->coarse_sweeps = coarse_sweeps;
+    mg->dtype = dtype;
     mg->view.ctx = op->ctx;
     mg->view.mg = mg;
     mg->view.borrowed = true;
+    const bool f32 = dtype == FX_F32;
     size_t r = op->g.rows, c = op->g.cols;
     double hx = op->g.dx, hy = op->g.dy;
     int rc = FX_OK;
-    for (int l = 0; l < 40 && rc == FX_OK; l++) {
+    // the level fields in the cycle's type: level 0 casts the operator's own (F32 cycle only),
+    // coarser levels inject from the level above
+    auto fields = [&](CdLevel &L, size_t l) -> int {
+        const fx_buf *src[3] = {op->vx, op->vy, op->kappa};
+        fx_buf **dst[3] = {&L.vx, &L.vy, &L.kappa};
+        for (int k = 0; k < 3 && rc == FX_OK; k++) {
+            if (!src[k]) continue;
+            FX_TRY(fx_alloc(op->ctx, r * c, dtype, dst[k]));
+            const double *own = (const double *)src[k]->ptr;
+            if (l == 0) {
+                FX_TRY((launch_flat<0>(op->ctx, r * c, FlatCast<double, float>{own, (float *)(*dst[k])->ptr}, NoFin{},
+                                       nullptr, "cdmg_inject")));
+                continue;
+            }
+            const CdLevel &F = mg->lv[l - 1];
+            const fx_buf *fine = l == 1 && !f32 ? src[k] : (k == 0 ? F.vx : (k == 1 ? F.vy : F.kappa));
+            if (f32)
+                FX_TRY((launch_flat<0>(op->ctx, r * c,
+                                       FlatInject<float, float>{(const float *)fine->ptr, (float *)(*dst[k])->ptr,
+                                                                F.cols, c},
+                                       NoFin{}, nullptr, "cdmg_inject")));
+            else
+                FX_TRY((launch_flat<0>(op->ctx, r * c,
+                                       FlatInject<double, double>{(const double *)fine->ptr,
+                                                                  (double *)(*dst[k])->ptr, F.cols, c},
+                                       NoFin{}, nullptr, "cdmg_inject")));
+        }
+        return FX_OK;
+    };
+    for (size_t l = 0; l < 40 && rc == FX_OK; l++) {
         CdLevel L;
         L.rows = r;
         L.cols = c;
         L.dx = hx;
         L.dy = hy;
-        if (l > 0) {
-            const CdLevel &F = mg->lv[l - 1];
-            const double *fvx = l == 1 ? (const double *)op->vx->ptr : (const double *)F.vx->ptr;
-            const double *fvy = l == 1 ? (const double *)op->vy->ptr : (const double *)F.vy->ptr;
-            const double *fk = op->kappa ? (l == 1 ? (const double *)op->kappa->ptr : (const double *)F.kappa->ptr)
-                                         : nullptr;
-            for (fx_buf **bp : {&L.u, &L.rhs, &L.tmp, &L.vx, &L.vy})
-                if (rc == FX_OK) rc = fx_alloc(op->ctx, r * c, FX_F64, bp);
-            if (rc == FX_OK && fk) rc = fx_alloc(op->ctx, r * c, FX_F64, &L.kappa);
-            if (rc == FX_OK)
-                rc = launch_flat<0>(op->ctx, r * c, FlatInject{fvx, (double *)L.vx->ptr, F.cols, c}, NoFin{}, nullptr,
-                                    "cdmg_inject");
-            if (rc == FX_OK)
-                rc = launch_flat<0>(op->ctx, r * c, FlatInject{fvy, (double *)L.vy->ptr, F.cols, c}, NoFin{}, nullptr,
-                                    "cdmg_inject");
-            if (rc == FX_OK && fk)
-                rc = launch_flat<0>(op->ctx, r * c, FlatInject{fk, (double *)L.kappa->ptr, F.cols, c}, NoFin{}, nullptr,
-                                    "cdmg_inject");
+        if (l > 0 || f32) {
+            for (fx_buf **bp : {&L.u, &L.rhs, &L.tmp})
+                if (rc == FX_OK) rc = fx_alloc(op->ctx, r * c, dtype, bp);
+            if (rc == FX_OK) rc = fields(L, l);
         }
         mg->lv.push_back(L);
+        if (rc != FX_OK) break;
         if (!(r - 2 > coarse_max && c - 2 > coarse_max && (r - 1) % 2 == 0 && (c - 1) % 2 == 0)) break;
         r = (r - 1) / 2 + 1;
         c = (c - 1) / 2 + 1;
         hx *= 2.0;
         hy *= 2.0;
     }
-    if (rc == FX_OK) rc = fx_alloc(op->ctx, op->g.rows * op->g.cols, FX_F64, &mg->tmp0);
+    if (rc == FX_OK && !f32) rc = fx_alloc(op->ctx, op->g.rows * op->g.cols, FX_F64, &mg->tmp0);
     if (rc != FX_OK) {
         delete mg;
         return rc;

@@ -402,12 +402,15 @@ class ConvDiffMultigrid(Preconditioner):
     cycle from z = 0 per application."""
 
     def __init__(self, op: "ConvDiffOperator", n_pre: int = 2, n_post: int = 2, omega: float = 0.8,
-                 coarse_max: int = 15, coarse_sweeps: int = 200):
+                 coarse_max: int = 15, coarse_sweeps: int = 200, dtype: DType = DType.F64):
+        """``dtype=DType.F32`` runs the cycle in single precision (fx_cdmg_create_typed); the
+        vectors it is applied to stay F64."""
         self._op = op  # the cycle reads the operator's fields
         out = C.c_void_p()
-        check(L.lib().fx_cdmg_create(op.h, int(n_pre), int(n_post), float(omega), int(coarse_max),
-                                     int(coarse_sweeps), C.byref(out)))
+        check(L.lib().fx_cdmg_create_typed(op.h, int(n_pre), int(n_post), float(omega), int(coarse_max),
+                                           int(coarse_sweeps), int(dtype), C.byref(out)))
         self.h = out.value
+        self.dtype = DType(dtype)
 
     def depth(self) -> int:
         d = C.c_size_t()

@@ -447,6 +447,12 @@ int fx_precond_jacobi_op(const fx_op *op, fx_precond **out);
  * a borrowed handle valid until fx_cdmg_destroy. */
 int fx_cdmg_create(const fx_op *op, size_t n_pre, size_t n_post, double omega, size_t coarse_max,
                    size_t coarse_sweeps, fx_cdmg **out);
+/* The same cycle computed and stored in `dtype` (FX_F64: fx_cdmg_create; FX_F32: every level,
+ * including F32 copies of the operator's fields on level 0, in single precision).  The vectors
+ * z and r of an application stay F64: r is rounded to F32 on entry, z is the F64 image of the
+ * F32 cycle.  An FP32 preconditioner inside an FP64 Krylov solver. */
+int fx_cdmg_create_typed(const fx_op *op, size_t n_pre, size_t n_post, double omega, size_t coarse_max,
+                         size_t coarse_sweeps, int dtype, fx_cdmg **out);
 int fx_cdmg_destroy(fx_cdmg *mg);
 int fx_cdmg_depth(const fx_cdmg *mg, size_t *depth);
 fx_precond *fx_cdmg_as_precond(fx_cdmg *mg);

@@ -129,3 +129,46 @@ def test_multigrid_preconditioned_solve_matches_oracle(dev, solver):
     assert s.converged() and reason == 0 and abs(s.iterations - it) <= 1 and s.iterations <= 20
     assert np.linalg.norm(O.op_apply(oop, x.to_vec_f64()) - f) < 1.01 * tol
     assert rel_err(x.to_vec_f64(), xo) < 1e-8
+
+
+@pytest.mark.parametrize("n,nu,sigma,coeff,kappa_field", [(63, 1e-2, 0.0, 1.0, False), (127, 1e-3, 1.0, 5e-3, True)])
+def test_f32_multigrid_cycle_close_to_oracle(dev, n, nu, sigma, coeff, kappa_field):
+    """The cycle in single precision (fx_cdmg_create_typed, FX_F32): the same hierarchy and the
+    same cycle as the F64 one, rounded to F32 -- within 1e-4 of the oracle's F64 cycle, and not
+    equal to it (it does compute in F32)."""
+    from fluxion_b200 import ConvDiffMultigrid, DType, Field
+    g, N, f, op, oop = _problem(n, dev, nu=nu, sigma=sigma, coeff=coeff, kappa_field=kappa_field)
+    mg = ConvDiffMultigrid(op, dtype=DType.F32)
+    omg = O.CdMultigrid(oop)
+    assert mg.depth() == omg.depth() >= 3 and mg.dtype == DType.F32
+    r = np.random.default_rng(9).uniform(-1, 1, N * N)
+    zo = omg.apply(r)
+    for _ in range(2):
+        z = Field.zeros(g, DType.F64, dev)
+        z.fill(7.0)  # every point is written
+        mg.apply(z, Field.from_f64(g, r, dev))
+        e = rel_err(z.to_vec_f64(), zo)
+        assert 0.0 < e < 1e-4, e
+
+
+@pytest.mark.parametrize("solver,nu", [("bicgstab", 1e-2), ("fgmres", 1e-2), ("bicgstab", 1e-3), ("fgmres", 1e-3)])
+def test_f32_multigrid_inside_fp64_solvers(dev, solver, nu):
+    """BiCGSTAB and FGMRES in FP64 with the F32 cycle as preconditioner reach the FP64 tolerance
+    on the true residual (recomputed by the oracle's operator) in at most two iterations more
+    than with the F64 cycle."""
+    from fluxion_b200 import BiCgStabSolver, ConvDiffMultigrid, DType, FgmresSolver, Field
+    g, N, f, op, oop = _problem(127, dev, nu=nu)
+    tol = 1e-10 * np.linalg.norm(f)
+    b = Field.from_f64(g, f, dev)
+    its = {}
+    for dt in (DType.F64, DType.F32):
+        mg = ConvDiffMultigrid(op, dtype=dt)
+        x = Field.zeros(g, DType.F64, dev)
+        if solver == "bicgstab":
+            s = BiCgStabSolver(g, dev, tol, 200).solve_op(x, b, op, mg)
+        else:
+            s = FgmresSolver(g, dev, 30, tol, 200).solve_op(x, b, op, mg)
+        assert s.converged(), (dt, s)
+        assert np.linalg.norm(O.op_apply(oop, x.to_vec_f64()) - f) < 1.01 * tol
+        its[dt] = s.iterations
+    assert its[DType.F32] <= its[DType.F64] + 2, its
