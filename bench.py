@@ -72,6 +72,8 @@ def parse():
                         "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target; batch: "
                         "1024 conv-diff problems; convdiff: convection-dominated conv-diff at --n")
     p.add_argument("--nu", default="1e-3,1e-4", help="--mode convdiff: viscosities, comma-separated")
+    p.add_argument("--replay", type=int, default=0, choices=[0, 1],
+                   help="--mode batch: record each hierarchy's cycle into a CUDA graph and replay it")
     p.add_argument("--mg-dtype", default="f64", choices=["f64", "f32"],
                    help="--mode batch: arithmetic of the conv-diff V-cycle (the Krylov solver stays FP64)")
     return p.parse_args()
@@ -326,6 +328,8 @@ def run_batch(args):
         x = Field.zeros(g, DType.F64, dev)
         op = ConvDiffOperator(g, VX, VY, -nu, sigma=0.0, coeff=1.0)
         mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, mg_dtype)
+        if args.replay:
+            mg.set_replay(True)
         solver = solvers.get(N)  # one solver (and its work vectors) per grid size, reused
         if solver is None:
             solver = solvers[N] = BiCgStabSolver(g, dev, 1.0, 200)
@@ -381,7 +385,7 @@ def run_batch(args):
     ok = all(r[1].converged() for r in res)
     print(json.dumps({
         "mode": "batch", "workload": f"convdiff_batch_{args.batch}_k6-10_nu1e-2_bicgstab_cdmg",
-        "problems": args.batch, "lanes": lanes, "pdl": bool(args.pdl), "vcycle_dtype": args.mg_dtype,
+        "problems": args.batch, "lanes": lanes, "pdl": bool(args.pdl), "vcycle_dtype": args.mg_dtype, "vcycle_replay": bool(args.replay),
         "interior_sizes": {str(2 ** k - 1): int((ks == k).sum()) for k in range(6, 11)},
         "solves_per_s": args.batch / wall, "wall_s_excluding_host_data_generation": wall,
         "per_problem_ms_p50": float(np.percentile([r[4] * 1e3 for r in res], 50)),

@@ -54,7 +54,7 @@ static cudaMemPool_t device_pool(int device) {
     return pools[device];
 }
 
-static bool capturing(cudaStream_t s) {
+bool capturing(cudaStream_t s) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
         (void)cudaGetLastError();

@@ -85,6 +85,7 @@ struct fx_buf {
 namespace fx {
 
 int check_launch(fx_ctx *ctx, const char *what);
+bool capturing(cudaStream_t s);  // the stream is being captured into a graph
 
 // Programmatic dependent launch.  Kernels of the solve path are launched with programmatic
 // stream serialisation, so the next kernel's launch and block scheduling overlap the end of

@@ -2473,8 +2473,25 @@ struct fx_cdmg {
     struct View : fx_precond {
         fx_cdmg *mg = nullptr;
         int apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) override;
+        int record(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero);
     } view;
+    // One application is a fixed sequence of launches for given (z, r, halt flag, stream).  With
+    // replay on (fx_cdmg_set_replay), it is recorded into a CUDA graph the first time and
+    // replayed after that: one launch instead of 20-50.  Off by default: recording and
+    // instantiating costs more than a short-lived hierarchy's replays save (the batched
+    // workload, one new hierarchy per problem, same box: -5 % on one lane, -4 to -9 % on 8).
+    struct Replay {
+        const void *z, *r;
+        const int *skip;
+        bool z_zero;
+        cudaStream_t stream;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Replay> replays;
+    bool replay = false;      // fx_cdmg_set_replay
+    bool replay_off = false;  // a recording failed: launch directly from then on
     ~fx_cdmg() {
+        for (auto &g : replays) cudaGraphExecDestroy(g.exec);
         for (auto &L : lv)
             for (fx_buf *f : {L.u, L.rhs, L.tmp, L.vx, L.vy, L.kappa}) fx_free(f);
         fx_free(tmp0);
@@ -2573,6 +2590,40 @@ int cd_cycle(fx_cdmg *mg, T *x, const T *b, T *x_other, const int *skip) {  // x
 
 int fx_cdmg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) {
     FX_TRY(check_same(z, r));
+    // the checks of record(), before a replay: a recycled address must carry the same extent
+    const CdLevel &L0 = mg->lv[0];
+    if (z->dtype != FX_F64 || z->len != L0.rows * L0.cols)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "conv-diff multigrid: vectors must be F64 fields of the operator's grid");
+    if (z->ptr == r->ptr) return fail(FX_ERR_INVALID_ARGUMENT, "z and r must be distinct");
+    if (!mg->replay || mg->replay_off || capturing(ctx->stream)) return record(z, r, skip, z_zero);
+    for (auto &g : mg->replays)
+        if (g.z == z->ptr && g.r == r->ptr && g.skip == skip && g.z_zero == z_zero && g.stream == ctx->stream) {
+            FX_CUDA(cudaGraphLaunch(g.exec, ctx->stream));
+            ctx->launches++;
+            return FX_OK;
+        }
+    if (mg->replays.size() >= 16) return record(z, r, skip, z_zero);  // many distinct pairs: no cache
+    FX_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+    const int st = record(z, r, skip, z_zero);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (st == FX_OK && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        mg->replays.push_back({z->ptr, r->ptr, skip, z_zero, ctx->stream, exec});
+        FX_CUDA(cudaGraphLaunch(exec, ctx->stream));
+        ctx->launches++;
+        return FX_OK;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    (void)cudaGetLastError();
+    if (st != FX_OK) return st;
+    mg->replay_off = true;  // not recordable here: run it directly, now and from now on
+    return record(z, r, skip, z_zero);
+}
+
+// The launches of one application (recorded by apply, or run directly).
+int fx_cdmg::View::record(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero) {
     CdLevel &L0 = mg->lv[0];
     const size_t n = L0.rows * L0.cols;
     if (z->dtype != FX_F64 || z->len != n)
@@ -3326,6 +3377,11 @@ int fx_cdmg_depth(const fx_cdmg *mg, size_t *depth) {
     return FX_OK;
 }
 fx_precond *fx_cdmg_as_precond(fx_cdmg *mg) { return mg ? &mg->view : nullptr; }
+int fx_cdmg_set_replay(fx_cdmg *mg, int enabled) {
+    if (!mg) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    mg->replay = enabled != 0;
+    return FX_OK;
+}
 
 int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st, const fx_boundaries *bc,
                         const size_t *steps, size_t nsteps, fx_precond *inner, fx_precond **out) {

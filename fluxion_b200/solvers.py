@@ -417,6 +417,11 @@ class ConvDiffMultigrid(Preconditioner):
         check(L.lib().fx_cdmg_depth(self.h, C.byref(d)))
         return d.value
 
+    def set_replay(self, enabled: bool) -> None:
+        """Record each (z, r) pair's cycle into a CUDA graph once and replay it
+        (fx_cdmg_set_replay; off by default)."""
+        check(L.lib().fx_cdmg_set_replay(self.h, 1 if enabled else 0))
+
     def _handle(self, device: Device) -> int:
         return L.lib().fx_cdmg_as_precond(self.h)
 

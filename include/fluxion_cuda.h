@@ -453,6 +453,11 @@ int fx_cdmg_create(const fx_op *op, size_t n_pre, size_t n_post, double omega, s
  * F32 cycle.  An FP32 preconditioner inside an FP64 Krylov solver. */
 int fx_cdmg_create_typed(const fx_op *op, size_t n_pre, size_t n_post, double omega, size_t coarse_max,
                          size_t coarse_sweeps, int dtype, fx_cdmg **out);
+/* Replay (new; off by default): the first application to a given (z, r) pair on a stream is
+ * recorded into a CUDA graph, later ones launch that graph.  The results are the same.  It
+ * pays for a hierarchy applied many times; recording costs more host time than a short-lived
+ * hierarchy saves.  Applications inside a caller's own capture are never recorded. */
+int fx_cdmg_set_replay(fx_cdmg *mg, int enabled);
 int fx_cdmg_destroy(fx_cdmg *mg);
 int fx_cdmg_depth(const fx_cdmg *mg, size_t *depth);
 fx_precond *fx_cdmg_as_precond(fx_cdmg *mg);

@@ -172,3 +172,31 @@ def test_f32_multigrid_inside_fp64_solvers(dev, solver, nu):
         assert np.linalg.norm(O.op_apply(oop, x.to_vec_f64()) - f) < 1.01 * tol
         its[dt] = s.iterations
     assert its[DType.F32] <= its[DType.F64] + 2, its
+
+
+def test_multigrid_replays_its_recorded_cycle(dev):
+    """With replay on, the first application to a (z, r) pair records the cycle into a CUDA graph
+    (its kernels counted once as launched), later ones replay it as one launch; every
+    application gives the same z, equal to the oracle's cycle in F64."""
+    from fluxion_b200 import ConvDiffMultigrid, DimensionMismatch, DType, Field, Grid
+    g, N, f, op, oop = _problem(127, dev)
+    be = dev.backend()
+    rv = np.random.default_rng(3).uniform(-1, 1, N * N)
+    zo = O.CdMultigrid(oop).apply(rv)
+    for dt in (DType.F64, DType.F32):
+        mg = ConvDiffMultigrid(op, dtype=dt)
+        mg.set_replay(True)
+        r, z = Field.from_f64(g, rv, dev), Field.zeros(g, DType.F64, dev)
+        outs, counts = [], []
+        for _ in range(3):
+            c0 = be.launch_count()
+            mg.apply(z, r)
+            counts.append(be.launch_count() - c0)
+            outs.append(z.to_vec_f64())
+        assert counts[0] > 10 and counts[1] == counts[2] == 1, counts
+        assert all(np.array_equal(o, outs[0]) for o in outs)
+        if dt == DType.F64:
+            assert np.array_equal(outs[0], zo)
+        small = Grid.square(N - 2, 1.0)  # vectors of another extent are refused before any replay
+        with pytest.raises(DimensionMismatch):
+            mg.apply(Field.zeros(small, DType.F64, dev), Field.zeros(small, DType.F64, dev))
