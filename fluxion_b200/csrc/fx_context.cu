@@ -367,7 +367,7 @@ int fx_graph_destroy(fx_graph *g) {
 int fx_ctx_set_stream(fx_ctx *c, void *stream) {
     if (!c) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
     cudaStream_t next = stream ? (cudaStream_t)stream : c->own_stream;
-    if (next != c->stream) FX_CUDA(cudaStreamSynchronize(c->stream));
+    if (next != c->stream && !capturing(c->stream)) FX_CUDA(cudaStreamSynchronize(c->stream));
     c->stream = next;
     return FX_OK;
 }
