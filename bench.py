@@ -72,6 +72,8 @@ def parse():
                         "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target; batch: "
                         "1024 conv-diff problems; convdiff: convection-dominated conv-diff at --n")
     p.add_argument("--nu", default="1e-3,1e-4", help="--mode convdiff: viscosities, comma-separated")
+    p.add_argument("--k-range", default="6,10",
+                   help="--mode batch: interior sizes 2^k - 1 for k uniform in this inclusive range")
     p.add_argument("--replay", type=int, default=0, choices=[0, 1],
                    help="--mode batch: record each hierarchy's cycle into a CUDA graph and replay it")
     p.add_argument("--mg-dtype", default="f64", choices=["f64", "f32"],
@@ -293,7 +295,8 @@ def run_batch(args):
     lanes = max(1, int(args.lanes))
     mg_dtype = DType.F32 if args.mg_dtype == "f32" else DType.F64
     rng = np.random.default_rng(SEED)
-    ks = rng.integers(6, 11, size=args.batch)
+    k_lo, k_hi = (int(v) for v in args.k_range.split(","))
+    ks = rng.integers(k_lo, k_hi + 1, size=args.batch)
     sizes = [int(2 ** k + 1) ** 2 for k in ks]
     pinned = torch.empty(3 * sum(sizes), dtype=torch.float64, pin_memory=True).numpy()
     host, off = [], 0
@@ -384,9 +387,9 @@ def run_batch(args):
     its = np.array([r[1].iterations for r in res])
     ok = all(r[1].converged() for r in res)
     print(json.dumps({
-        "mode": "batch", "workload": f"convdiff_batch_{args.batch}_k6-10_nu1e-2_bicgstab_cdmg",
+        "mode": "batch", "workload": f"convdiff_batch_{args.batch}_k{k_lo}-{k_hi}_nu1e-2_bicgstab_cdmg",
         "problems": args.batch, "lanes": lanes, "pdl": bool(args.pdl), "vcycle_dtype": args.mg_dtype, "vcycle_replay": bool(args.replay),
-        "interior_sizes": {str(2 ** k - 1): int((ks == k).sum()) for k in range(6, 11)},
+        "interior_sizes": {str(2 ** k - 1): int((ks == k).sum()) for k in range(k_lo, k_hi + 1)},
         "solves_per_s": args.batch / wall, "wall_s_excluding_host_data_generation": wall,
         "per_problem_ms_p50": float(np.percentile([r[4] * 1e3 for r in res], 50)),
         "per_problem_ms_p99": float(np.percentile([r[4] * 1e3 for r in res], 99)),
