@@ -2265,7 +2265,8 @@ __device__ __forceinline__ T cd_diag(const OpA<T, kModeCD> &A, size_t idx) {
                   A.sigma);
 }
 
-// Smoothing sweep (out = x + omega (b - A x) / diag(A)) and residual (out = b - A x), inside
+// Smoothing sweep (out = x + omega (b - A x) (1 / diag(A)), one division per point) and
+// residual (out = b - A x), inside
 // only: the ring of `out` is not written.  One point per thread, neighbours read straight from
 // memory (west / east from the same cache lines, north / south from L2): with four input arrays
 // a row march holds too few loads in flight per SM (it measured 2.8 TB/s on the finest 4097^2
@@ -2287,7 +2288,8 @@ struct FlatCdSweep {
         nb.s = x[i + cols];
         nb.w = x[i - 1];
         nb.e = x[i + 1];
-        out[i] = fx_fma(omega, (b[i] - A.apply(false, nb, i)) / cd_diag(A, i), nb.c);
+        const T inv_d = (T)1 / cd_diag(A, i);
+        out[i] = fx_fma(omega, (b[i] - A.apply(false, nb, i)) * inv_d, nb.c);
     }
 };
 
@@ -2330,6 +2332,7 @@ __global__ void __launch_bounds__(256) k_cd_sweep2(OpA<T, kModeCD> A, const T *_
     if (skip && *(volatile const int *)skip) return;
     __shared__ T xs[kSw2X * kSw2X];
     __shared__ T ys[kSw2Y * kSw2Y];
+    __shared__ T ds[kSw2Y * kSw2Y];  // 1 / diag(A) over the first sweep's tile
     const int tid = threadIdx.x;
     const int r0 = blockIdx.y * kSw2T, c0 = blockIdx.x * kSw2T;
     // fixed trip counts (256 threads), unrolled so that each thread's loads issue together
@@ -2347,12 +2350,13 @@ __global__ void __launch_bounds__(256) k_cd_sweep2(OpA<T, kModeCD> A, const T *_
         if (k >= kSw2Y * kSw2Y) break;
         const int lr = k / kSw2Y, lc = k % kSw2Y;
         const int gr = r0 - 1 + lr, gc = c0 - 1 + lc;
-        T y = (T)0;
+        T y = (T)0, inv_d = (T)0;
         if (gr >= 0 && gr < rows && gc >= 0 && gc < cols) {
             const size_t g = (size_t)gr * cols + gc;
             if (gr == 0 || gc == 0 || gr == rows - 1 || gc == cols - 1) {
                 y = out[g];
             } else {
+                inv_d = (T)1 / cd_diag(A, g);
                 const int q = (lr + 1) * kSw2X + (lc + 1);
                 Nb<T> nb;
                 nb.c = xs[q];
@@ -2360,10 +2364,11 @@ __global__ void __launch_bounds__(256) k_cd_sweep2(OpA<T, kModeCD> A, const T *_
                 nb.s = xs[q + kSw2X];
                 nb.w = xs[q - 1];
                 nb.e = xs[q + 1];
-                y = fx_fma(omega, (b[g] - A.apply(false, nb, g)) / cd_diag(A, g), nb.c);
+                y = fx_fma(omega, (b[g] - A.apply(false, nb, g)) * inv_d, nb.c);
             }
         }
         ys[k] = y;
+        ds[k] = inv_d;
     }
     __syncthreads();
 #pragma unroll
@@ -2380,7 +2385,7 @@ __global__ void __launch_bounds__(256) k_cd_sweep2(OpA<T, kModeCD> A, const T *_
         nb.s = ys[q + kSw2Y];
         nb.w = ys[q - 1];
         nb.e = ys[q + 1];
-        out[g] = fx_fma(omega, (b[g] - A.apply(false, nb, g)) / cd_diag(A, g), nb.c);
+        out[g] = fx_fma(omega, (b[g] - A.apply(false, nb, g)) * ds[q], nb.c);
     }
 }
 
@@ -2403,7 +2408,8 @@ struct FlatCast {  // d = (D) s
 };
 
 // Coarsest level in one block: the iterate ping-pongs in shared memory, each thread keeps its
-// points' rhs and diagonal in registers; every point value is FlatCdSweep's expression.
+// points' rhs and reciprocal diagonal in registers; every point value is FlatCdSweep's
+// expression.
 template <typename T>
 __global__ void __launch_bounds__(1024) k_cd_coarse(T *u, const T *__restrict__ b, int rows, int cols,
                                                     OpA<T, kModeCD> A, T omega, int nsweeps, const int *skip) {
@@ -2423,7 +2429,7 @@ __global__ void __launch_bounds__(1024) k_cd_coarse(T *u, const T *__restrict__ 
         const int r = i / cols, c = i % cols;
         inner[k] = i < n && r > 0 && c > 0 && r < rows - 1 && c < cols - 1;
         bv[k] = inner[k] ? b[i] : (T)0;
-        dv[k] = inner[k] ? cd_diag(A, (size_t)i) : (T)1;
+        dv[k] = inner[k] ? (T)1 / cd_diag(A, (size_t)i) : (T)1;  // 1 / diag
         if (i < n) {
             s0[i] = (T)0;
             s1[i] = (T)0;
@@ -2443,7 +2449,7 @@ __global__ void __launch_bounds__(1024) k_cd_coarse(T *u, const T *__restrict__ 
             nb.s = src[i + cols];
             nb.w = src[i - 1];
             nb.e = src[i + 1];
-            dst[i] = fx_fma(omega, (bv[q] - A.apply(false, nb, (size_t)i)) / dv[q], nb.c);
+            dst[i] = fx_fma(omega, (bv[q] - A.apply(false, nb, (size_t)i)) * dv[q], nb.c);
         }
         __syncthreads();
     }

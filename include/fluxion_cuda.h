@@ -441,7 +441,8 @@ int fx_precond_jacobi_op(const fx_op *op, fx_precond **out);
 /* Multigrid V-cycle preconditioner for the operator (new): vertex hierarchy as
  * fx_mg_create_vertex (rows - 1 halves while both interiors exceed coarse_max), each coarse
  * level the operator rediscretised with h doubled and kappa / vx / vy injected from the
- * coincident fine points; weighted Jacobi (omega) with the operator's diagonal, full weighting
+ * coincident fine points; weighted Jacobi (omega) with the operator's diagonal
+ * (x += omega (b - A x) (1 / diag)), full weighting
  * and bilinear transfers, `coarse_sweeps` sweeps on the coarsest level; one cycle from z = 0
  * per application.  The operator (and its fields) must outlive it; fx_cdmg_as_precond gives
  * a borrowed handle valid until fx_cdmg_destroy. */

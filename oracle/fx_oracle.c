@@ -1148,7 +1148,7 @@ void fxo_inner_cg_pc_apply(void *ctx, double *z, const double *r) {
 /* ------------------------------------------------------------------ */
 /* Vertex hierarchy as fxo_mg mode 1 (rows-1 halves while both interiors exceed coarse_max).
  * Each coarse level rediscretises the operator with h doubled and kappa / vx / vy injected
- * from the coincident fine points.  Smoother: x <- x + omega (b - A x) / diag(A) inside, the
+ * from the coincident fine points.  Smoother: x <- x + omega (b - A x) (1 / diag(A)) inside, the
  * ring left at 0; full weighting down, bilinear up; `coarse_sweeps` sweeps on the coarsest
  * level; every cycle from x = 0. */
 
@@ -1164,7 +1164,8 @@ static double cd_diag(const fxo_op *op, size_t idx, double inv_dx, double inv_dy
     return fma(op->coeff, fma(-kap, k2, fma(fabs(op->vx[idx]), inv_dx, fabs(op->vy[idx]) * inv_dy)), op->sigma);
 }
 
-/* out = x + omega (b - A x) / diag inside (out's ring untouched) */
+/* out = x + omega (b - A x) (1 / diag) inside (out's ring untouched): one division per point,
+ * as the GPU sweeps do */
 static void cd_sweep(const fxo_op *op, const double *x, double *out, const double *b, double omega) {
     size_t rows = op->rows, cols = op->cols;
     double inv_dx = 1.0 / op->dx, inv_dy = 1.0 / op->dy;
@@ -1176,7 +1177,8 @@ static void cd_sweep(const fxo_op *op, const double *x, double *out, const doubl
             double kap = op->kappa ? op->kappa[idx] : op->kappa_s;
             double v = conv_diff_at_k(x, kap, op->vx, op->vy, idx, cols, inv_dx, inv_dy, inv_dx2, inv_dy2);
             double ax = fma(op->coeff, v, op->sigma * x[idx]);
-            out[idx] = fma(omega, (b[idx] - ax) / cd_diag(op, idx, inv_dx, inv_dy, k2), x[idx]);
+            double inv_d = 1.0 / cd_diag(op, idx, inv_dx, inv_dy, k2);
+            out[idx] = fma(omega, (b[idx] - ax) * inv_d, x[idx]);
         }
 }
 
