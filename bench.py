@@ -6,8 +6,9 @@ with the Dirichlet ring), f = 32 seeded sin-sin modes (k, l in 1..64, N(0,1) amp
 1e-3 * U[-1,1] noise, u0 = 0, CG preconditioned by one V(2,2)-cycle per iteration (full
 weighting, bilinear prolongation, weighted Jacobi omega = 0.8, coarsest 15^2 with 200 sweeps)
 to ||r|| < 1e-10 ||f|| (verified in FP64 against the plain operator and against the exact
-DST-I solve).  Two variants are timed: the plain FP64 solve and the mixed one (FP64 CG,
-residual, update and inner products; FP32 V-cycle); `value` is the mixed one.
+DST-I solve).  `value` and `e2e` are the plain FP64 solve, the same arithmetic as the reference
+arm; the mixed solve (FP64 CG, residual, update and inner products; FP32 V-cycle) and the other
+variants are reported beside it under their own keys.
 
 Also reported: e2e time through the public API with the source and the solution in pinned host
 memory; the live roofline of the dominant kernel (CUDA events on its launching stream over the
@@ -77,7 +78,7 @@ def parse():
     p.add_argument("--replay", type=int, default=0, choices=[0, 1],
                    help="--mode batch: record each hierarchy's cycle into a CUDA graph and replay it")
     p.add_argument("--mg-dtype", default="f64", choices=["f64", "f32"],
-                   help="--mode batch: arithmetic of the conv-diff V-cycle (the Krylov solver stays FP64)")
+                   help="--mode batch / vcycle: arithmetic of the V-cycle (the Krylov solver stays FP64)")
     return p.parse_args()
 
 
@@ -190,6 +191,17 @@ def oracle_solve(n: int, f: np.ndarray):
     return time.perf_counter() - t0, int(iters), O.get_threads()
 
 
+def headline_config(n: int, world: int) -> dict:
+    """The `config` both arms print for the headline solve: identical keys and strings."""
+    N = n + 2
+    return {"workload": f"poisson_{n}sq_mg_pcg_rel1e-10", "grid": f"{N}x{N} incl. Dirichlet ring",
+            "solver": f"CG + {SOLVER}", "precision": "fp64 throughout",
+            "tolerance": "||r||_2 < 1e-10 ||f||_2", "coarse": f"{COARSE_MAX}^2 interior x {COARSE_SWEEPS} sweeps",
+            "rhs": "32 sin-sin modes, k,l in 1..64, N(0,1) amplitudes, + 1e-3 U[-1,1] noise", "seed": SEED,
+            "l2": "inputs larger than L2 (134 MB per vector)",
+            "parallelism": "replicas" if world > 1 else "single device"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -209,8 +221,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"poisson_{n}sq_mg_pcg_rel1e-10", "grid": f"{N}x{N} incl. ring",
-                   "solver": f"CG + {SOLVER} (CPU restatement)"},
+        "config": headline_config(n, int(os.environ.get("WORLD_SIZE", "1"))),
         "iterations": iters,
         "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
                          "sample": f"per step: one full {n}^2 MG-PCG solve to 1e-10 ({iters} iterations)"},
@@ -224,7 +235,7 @@ def run_reference(args):
 # ------------------------------------------------------------------ our arm
 
 def run_vcycle(args):
-    """Time `steps` applications z = M^-1 r of the F32 V(2,2)-cycle (after `warmup` untimed ones)
+    """Time `steps` applications z = M^-1 r of the V(2,2)-cycle in `--mg-dtype` (after `warmup` untimed ones)
     on the n^2 problem, and report each level kernel's device time from the timing records."""
     import ctypes as C
 
@@ -241,7 +252,8 @@ def run_vcycle(args):
     P = poisson_problem(n)
     r = Field.from_f64(P.grid, poisson_modes_rhs(n, SEED), dev)
     z = Field.zeros(P.grid, DType.F64, dev)
-    mg = Multigrid.vertex(P.grid, None, dev, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS, DType.F32)
+    mg = Multigrid.vertex(P.grid, None, dev, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS,
+                          DType.F32 if args.mg_dtype == "f32" else DType.F64)
     tuned = mg.autotune(z, r, reps=max(3, args.steps)) if args.autotune else None
     for _ in range(args.warmup):
         mg.precondition(z, r)
@@ -261,7 +273,7 @@ def run_vcycle(args):
         L.lib().fx_ctx_timing_end_records(be.ctx, ms, pts, byt, cap, C.byref(cnt))
         per[k] = [{"points": pts[i], "us": ms[i] * 1e3, "GBps": byt[i] / (ms[i] * 1e-3) / 1e9 if byt[i] else None}
                   for i in range(cnt.value)]
-    print(json.dumps({"mode": "vcycle", "workload": f"poisson_{n}sq_f32_vcycle", "steps": args.steps,
+    print(json.dumps({"mode": "vcycle", "workload": f"poisson_{n}sq_{args.mg_dtype}_vcycle", "steps": args.steps,
                       "warmup": args.warmup, "ms_per_vcycle": e0.elapsed_time(e1) / args.steps,
                       "levels": mg.depth(), "autotune": tuned, "per_launch_with_events": per}), flush=True)
     return 0
@@ -554,30 +566,31 @@ def main():
             ms_total = float(t.item())
         return ms_total / k, st, launches, ktime
 
-    # which kernel dominates the mixed solve? (one untimed solve per candidate)
+    # which kernel dominates the plain FP64 solve? (one untimed solve per candidate)
     import ctypes as C
     candidates = ["mg_down", "mg_up", "mg_tail", "mg_sweep", "pcg_update", "pcg_dir", "mg_residual", "mg_restrict_fw",
                   "mg_prolong_bilinear", "pcg_rz", "mg_convert", "mg_zero", "mg_coarse_solve"]
-    solve(mg32)
+    solve(mg64)
     shares = {}
     for kname in candidates:
         L.lib().fx_ctx_timing_begin(be.ctx, kname.encode())
-        solve(mg32)
+        solve(mg64)
         ms, cnt, pts = C.c_double(), C.c_ulonglong(), C.c_double()
         L.lib().fx_ctx_timing_end(be.ctx, C.byref(ms), C.byref(cnt), C.byref(pts))
         shares[kname] = ms.value
     dom = max(shares, key=shares.get)
 
-    # plain FP64 and mixed solves
-    plain_ms, st64, _, _ = timed(mg64, args.steps, args.warmup)
-    u64 = x.to_vec_f64()
+    # the headline: the plain FP64 solve (clocks sampled over its timed region)
     with ClockSampler(local, uuid=str(torch.cuda.get_device_properties(local).uuid)) as clk:
-        mixed_ms, st32, launches, _ = timed(mg32, args.steps, args.warmup)
-    u32 = x.to_vec_f64()
+        plain_ms, st64, launches, _ = timed(mg64, args.steps, args.warmup)
+    u64 = x.to_vec_f64()
     # the dominant kernel's launches, bracketed by CUDA events on the launch stream, over a second
     # timed pass of the same K solves: the events split the programmatic-launch overlap, so they
     # stay out of the pass that gives `value`
-    hooked_ms, _, _, ktime = timed(mg32, args.steps, 0, kernel=dom)
+    hooked_ms, _, _, ktime = timed(mg64, args.steps, 0, kernel=dom)
+    # the mixed solve: FP64 CG, residual, update and inner products around the FP32 V-cycle
+    mixed_ms, st32, mixed_launches, _ = timed(mg32, args.steps, args.warmup)
+    u32 = x.to_vec_f64()
     # the configuration's second solver: pipelined CG preconditioned by the V-cycle (FP64 cycle:
     # the pipelined recurrences carry u = M r instead of recomputing it, and stall near 1e-6 with
     # the FP32 cycle's rounding)
@@ -602,39 +615,44 @@ def main():
     f_host[:] = f
     u_host = torch.empty(N * N, dtype=torch.float64, pin_memory=True).numpy()
 
-    def e2e_step():
-        b.write(f_host)
-        x.fill(0.0)
-        cg.solve_preconditioned(x, b, P.coeff, P.stencil, None, mg32)
-        x.storage.copy_to_host_f64(u_host)
+    def e2e(mg, want):
+        def step():
+            b.write(f_host)
+            x.fill(0.0)
+            cg.solve_preconditioned(x, b, P.coeff, P.stencil, None, mg)
+            x.storage.copy_to_host_f64(u_host)
 
-    for _ in range(args.warmup):
-        e2e_step()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    w0 = time.perf_counter()
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - w0) * 1e3) / args.steps
-    if dist:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_ok = bool(np.array_equal(u_host, u32))
+        for _ in range(args.warmup):
+            step()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - w0) * 1e3) / args.steps
+        if dist:
+            t = torch.tensor([e_ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        return {"value": e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": N * N * 8,
+                "d2h_bytes_per_step": N * N * 8, "result_matches_device_run": bool(np.array_equal(u_host, want))}
 
-    # roofline of the dominant kernel, live over the timed mixed solves
+    e2e_plain = e2e(mg64, u64)
+    e2e_mixed = e2e(mg32, u32)
+
+    # roofline of the dominant kernel, live over the timed plain solves
     roof = None
     if ktime:
         # The roofline is taken over the dominant kernel's finest-grid launches (the multigrid
         # kernels also run on every coarser level, where they are latency-bound); the
-        # all-launch average is reported beside it.
-        esize = 4 if dom.startswith("mg_") and dom not in ("mg_convert",) else 8
-        bpp_table = 12 if dom == "mg_convert" else BYTES_PER_POINT.get(dom, 3) * esize
+        # all-launch average is reported beside it.  Kernels that do not state their bytes
+        # get the table's F64 figure.
+        bpp_table = BYTES_PER_POINT.get(dom, 3) * 8
         nbytes = [b if b > 0 else p * bpp_table for (_, p, b) in ktime]
         top = max(p for (_, p, _) in ktime)
         fine = [i for i, (_, p, _) in enumerate(ktime) if p == top]
@@ -643,12 +661,12 @@ def main():
         achieved = f_bytes / (f_ms * 1e-3) / 1e9
         all_ms = sum(t for (t, _, _) in ktime)
         traffic = None
-        tp = os.path.join(ROOT, "profiles", f"{dom}_traffic.txt")
+        tp = os.path.join(ROOT, "profiles", f"{dom}_f64_traffic.txt")
         if os.path.exists(tp):
             for ln in open(tp):
                 if ln.startswith("dram_bytes_per_point:"):
                     traffic = float(ln.split(":")[1]) * top
-        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        roof = {"kernel": dom + " (F64 cycle)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": f_bytes, "bytes_per_point": f_bytes / top,
                 "grid_points_per_launch": top, "launches": len(fine), "avg_launch_ms": f_ms,
@@ -666,23 +684,23 @@ def main():
         try:
             t, iters, cores = oracle_solve(n, f)
             cpu = {"value": t, "unit": "s", "cores": cores, "kind": "port",
-                   "sample": f"one full {n}^2 MG-PCG solve to 1e-10 ({iters} iterations)"}
+                   "sample": f"one full {n}^2 MG-PCG solve to 1e-10 ({iters} iterations), FP64"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": mixed_ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": mixed_ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 Krylov/residual/update + f32 V-cycle",
+            "metric": METRIC, "value": plain_ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": plain_ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded 32-mode sin-sin source + 1e-3 uniform noise)",
-            "config": {"workload": f"poisson_{n}sq_mg_pcg_rel1e-10", "grid": f"{N}x{N} incl. Dirichlet ring",
-                       "solver": f"CG + {SOLVER}",
-                       "tolerance": "||r||_2 < 1e-10 ||f||_2", "l2": "inputs larger than L2 (134 MB per vector)",
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
-            "iterations": int(st32.iterations), "rel_residual_fp64": rr32, "err_vs_fp64_direct": err32,
-            "plain_fp64": {"value": plain_ms / 1e3, "unit": "s", "iterations": int(st64.iterations),
-                           "rel_residual_fp64": rr64, "err_vs_fp64_direct": err64},
+            "config": headline_config(n, world),
+            "iterations": int(st64.iterations), "rel_residual_fp64": rr64, "err_vs_fp64_direct": err64,
+            "e2e": e2e_plain,
+            "mixed_fp32_cycle": {"value": mixed_ms / 1e3, "unit": "s", "iterations": int(st32.iterations),
+                                 "rel_residual_fp64": rr32, "err_vs_fp64_direct": err32, "e2e": e2e_mixed,
+                                 "gpu_launches": int(mixed_launches),
+                                 "solver": f"FP64 CG, residual, update and dots + F32 {SOLVER}"},
             "speedup_mixed_vs_plain": plain_ms / mixed_ms,
             "pipelined_pcg": {"value": pipe_ms / 1e3, "unit": "s", "iterations": int(stp.iterations),
                               "rel_residual_fp64": rrp, "err_vs_fp64_direct": errp,
@@ -691,8 +709,6 @@ def main():
                                          "inner_iterations": ir.last_inner_iterations, "rel_residual_fp64": rri,
                                          "err_vs_fp64_direct": erri,
                                          "solver": f"FP64 refinement, FP32 CG + F32 {SOLVER} inner to 1e-4"},
-            "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": N * N * 8,
-                    "d2h_bytes_per_step": N * N * 8, "result_matches_device_run": e2e_ok},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
             "gpu_launches": int(launches), "kernel_time_shares_ms": shares, "microbench": micro,
         }

@@ -231,8 +231,7 @@ int fx_norm_l2(fx_ctx *ctx, const fx_buf *buf, double *out) {
         const T *p = (const T *)buf->ptr;
         FX_TRY(launch_flat<1>(ctx, buf->len,
                               [=] __device__(size_t i, CSum *acc) {
-                                  const double v = (double)p[i];
-                                  csum_add_prod(acc[0], v, v);
+                                  csum_add_prod_t<T>(acc[0], p[i], p[i]);
                               },
                               StoreFin<1>{ctx->d_result}, nullptr, "norm_l2"));
     });
@@ -270,7 +269,7 @@ int fx_dot(fx_ctx *ctx, const fx_buf *x, const fx_buf *y, double *out) {
         const T *xp = (const T *)x->ptr;
         const T *yp = (const T *)y->ptr;
         FX_TRY(launch_flat<1>(ctx, x->len,
-                              [=] __device__(size_t i, CSum *acc) { csum_add_prod(acc[0], (double)xp[i], (double)yp[i]); },
+                              [=] __device__(size_t i, CSum *acc) { csum_add_prod_t<T>(acc[0], xp[i], yp[i]); },
                               StoreFin<1>{ctx->d_result}, nullptr, "dot"));
     });
     return read_results(ctx, 1, out);
@@ -293,8 +292,8 @@ int fx_dot2(fx_ctx *ctx, const fx_buf *a, const fx_buf *b, const fx_buf *c, cons
         const T *dp = (const T *)d->ptr;
         FX_TRY(launch_flat<2>(ctx, a->len,
                               [=] __device__(size_t i, CSum *acc) {
-                                  csum_add_prod(acc[0], (double)ap[i], (double)bp[i]);
-                                  csum_add_prod(acc[1], (double)cp[i], (double)dp[i]);
+                                  csum_add_prod_t<T>(acc[0], ap[i], bp[i]);
+                                  csum_add_prod_t<T>(acc[1], cp[i], dp[i]);
                               },
                               StoreFin<2>{ctx->d_result}, nullptr, "dot2"));
     });

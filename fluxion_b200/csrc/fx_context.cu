@@ -31,7 +31,8 @@ int check_launch(fx_ctx *ctx, const char *what) {
 // hierarchies neither synchronises the device nor maps memory again: cudaFree would wait for
 // every stream of the device, which serialises contexts that run independent problems side by
 // side.  An allocation is ordered on the context's stream; fx_ctx_set_stream waits for the old
-// stream before switching, so buffers made earlier are ready on the new one.
+// stream before switching, so buffers made earlier are ready on the new one (and refuses to switch
+// while the old stream is being captured, when that wait cannot be made).
 static cudaMemPool_t device_pool(int device) {
     static std::mutex mu;
     static cudaMemPool_t pools[64] = {};
@@ -317,6 +318,10 @@ int fx_ctx_synchronize(fx_ctx *c) {
 struct fx_graph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int device = 0;
+    // pool memory of buffers freed while this graph was being recorded: the graph's kernels
+    // still address it, so it returns to the pool only when the graph is destroyed
+    std::vector<void *> frees;
 };
 
 int fx_graph_begin(fx_ctx *c) {
@@ -331,11 +336,15 @@ int fx_graph_end(fx_ctx *c, fx_graph **out) {
     *out = nullptr;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-    for (void *p : c->deferred_free) cudaFreeAsync(p, c->stream);
-    c->deferred_free.clear();
+    std::vector<void *> frees;
+    frees.swap(c->deferred_free);
+    auto release_now = [&] {  // no graph refers to the memory: back to the pool in stream order
+        for (void *p : frees) cudaFreeAsync(p, c->stream);
+    };
     if (e != cudaSuccess || !g) {
         if (g) cudaGraphDestroy(g);
         (void)cudaGetLastError();
+        release_now();
         return fail(FX_ERR_BACKEND, std::string("graph capture failed: ") +
                                         (e != cudaSuccess ? cudaGetErrorString(e) : "empty capture"));
     }
@@ -344,9 +353,15 @@ int fx_graph_end(fx_ctx *c, fx_graph **out) {
     if (e != cudaSuccess) {
         cudaGraphDestroy(g);
         (void)cudaGetLastError();
+        release_now();
         return fail(FX_ERR_BACKEND, std::string("graph instantiation failed: ") + cudaGetErrorString(e));
     }
-    *out = new fx_graph{g, x};
+    fx_graph *G = new fx_graph();
+    G->graph = g;
+    G->exec = x;
+    G->device = c->device;
+    G->frees.swap(frees);
+    *out = G;
     return FX_OK;
 }
 
@@ -360,6 +375,11 @@ int fx_graph_destroy(fx_graph *g) {
     if (!g) return FX_OK;
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
+    if (!g->frees.empty()) {
+        // a launch of the graph may still be running on some stream: cudaFree waits for the device
+        cudaSetDevice(g->device);
+        for (void *p : g->frees) cudaFree(p);
+    }
     delete g;
     return FX_OK;
 }
@@ -367,7 +387,15 @@ int fx_graph_destroy(fx_graph *g) {
 int fx_ctx_set_stream(fx_ctx *c, void *stream) {
     if (!c) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
     cudaStream_t next = stream ? (cudaStream_t)stream : c->own_stream;
-    if (next != c->stream && !capturing(c->stream)) FX_CUDA(cudaStreamSynchronize(c->stream));
+    if (next != c->stream) {
+        // Work on the old stream (pool allocations and their zero fill included) must be complete
+        // before the new stream may touch it.  A stream being captured cannot be waited for, and
+        // moving away from it would also end the capture on the wrong stream: refused.
+        if (capturing(c->stream))
+            return fail(FX_ERR_INVALID_ARGUMENT,
+                        "cannot switch the context's stream while it is being captured into a graph");
+        FX_CUDA(cudaStreamSynchronize(c->stream));
+    }
     c->stream = next;
     return FX_OK;
 }

@@ -68,8 +68,11 @@ struct fx_ctx {
     std::vector<cudaEvent_t> event_pool;
     size_t pool_next = 0;
     bool timing_open = false;
-    // pool memory whose buffer was freed while the stream was being captured; returned to the
-    // pool, in stream order, once the capture ends (or the context is destroyed)
+    // pool memory whose buffer was freed while the stream was being captured.  The graph made
+    // from that capture may still address it, so the capture's owner takes the list when the
+    // capture ends and frees the memory only once the graph is destroyed (fx_graph_end /
+    // fx_graph_destroy, the conv-diff cycle's replay); a failed capture frees it at once, and
+    // the context frees what is left when it is destroyed.
     std::vector<void *> deferred_free;
 };
 
@@ -163,6 +166,19 @@ __device__ __forceinline__ void csum_add_prod(CSum &acc, double a, double b) {
 // 4097 x 4097 pass.  Dots whose terms may cancel (the BLAS-1 dot, BiCGSTAB, GMRES) keep
 // csum_add_prod.
 __device__ __forceinline__ void csum_fma(CSum &acc, double a, double b) { acc.p = fma(a, b, acc.p); }
+
+// A product of two FP32 values is exact in FP64 (24 + 24 significant bits), so it needs no
+// TwoProduct: it goes straight into the thread's FP64 partial (one FP64 operation per term,
+// against ten for csum_add_prod), which keeps the FP32 dots memory-bound.  The partial is folded
+// into the compensated sum when the reduction starts, as csum_fma's.  FP64 values keep the exact
+// TwoProduct form.
+template <typename T>
+__device__ __forceinline__ void csum_add_prod_t(CSum &acc, T a, T b) {
+    if constexpr (sizeof(T) == 4)
+        acc.p = fma((double)a, (double)b, acc.p);
+    else
+        csum_add_prod(acc, (double)a, (double)b);
+}
 
 __device__ __forceinline__ void csum_flush(CSum &acc) {
     double s, e;

@@ -15,7 +15,9 @@
 //  - all calls share the array: calls whose kernels overlap on the GPU (different streams,
 //    or different host threads on one device) race and must be serialised by the caller;
 //  - the first call on a device looks up the array's device address (cudaGetSymbolAddress)
-//    with that device current; make that first call before any stream capture begins.
+//    with that device current; make that first call before any stream capture begins;
+//  - that address is kept for the life of the process: calls after a reset of the device's
+//    primary context (cudaDeviceReset, by this process or a library in it) are not supported.
 #include <mutex>
 
 #include "fx_internal.cuh"

@@ -2492,12 +2492,16 @@ struct fx_cdmg {
         bool z_zero;
         cudaStream_t stream;
         cudaGraphExec_t exec;
+        std::vector<void *> frees;  // pool memory freed during the recording, still addressed by exec
     };
     std::vector<Replay> replays;
     bool replay = false;      // fx_cdmg_set_replay
     bool replay_off = false;  // a recording failed: launch directly from then on
     ~fx_cdmg() {
-        for (auto &g : replays) cudaGraphExecDestroy(g.exec);
+        for (auto &g : replays) {
+            cudaGraphExecDestroy(g.exec);
+            for (void *p : g.frees) cudaFree(p);  // waits for the device: a replay may still run
+        }
         for (auto &L : lv)
             for (fx_buf *f : {L.u, L.rhs, L.tmp, L.vx, L.vy, L.kappa}) fx_free(f);
         fx_free(tmp0);
@@ -2601,7 +2605,9 @@ int fx_cdmg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zer
     if (z->dtype != FX_F64 || z->len != L0.rows * L0.cols)
         return fail(FX_ERR_DIMENSION_MISMATCH, "conv-diff multigrid: vectors must be F64 fields of the operator's grid");
     if (z->ptr == r->ptr) return fail(FX_ERR_INVALID_ARGUMENT, "z and r must be distinct");
-    if (!mg->replay || mg->replay_off || capturing(ctx->stream)) return record(z, r, skip, z_zero);
+    // Per-launch timing records events on the stream, which a recording would capture: while
+    // timing is on, the application runs directly.
+    if (!mg->replay || mg->replay_off || ctx->timing || capturing(ctx->stream)) return record(z, r, skip, z_zero);
     for (auto &g : mg->replays)
         if (g.z == z->ptr && g.r == r->ptr && g.skip == skip && g.z_zero == z_zero && g.stream == ctx->stream) {
             FX_CUDA(cudaGraphLaunch(g.exec, ctx->stream));
@@ -2609,22 +2615,29 @@ int fx_cdmg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zer
             return FX_OK;
         }
     if (mg->replays.size() >= 16) return record(z, r, skip, z_zero);  // many distinct pairs: no cache
+    const size_t nf0 = ctx->deferred_free.size();
     FX_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
     const int st = record(z, r, skip, z_zero);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    // buffers freed while recording: they belong to this graph (or, if it failed, to no graph)
+    std::vector<void *> frees(ctx->deferred_free.begin() + (std::ptrdiff_t)std::min(nf0, ctx->deferred_free.size()),
+                              ctx->deferred_free.end());
+    ctx->deferred_free.resize(std::min(nf0, ctx->deferred_free.size()));
     cudaGraphExec_t exec = nullptr;
     if (st == FX_OK && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
         cudaGraphDestroy(graph);
-        mg->replays.push_back({z->ptr, r->ptr, skip, z_zero, ctx->stream, exec});
+        mg->replays.push_back({z->ptr, r->ptr, skip, z_zero, ctx->stream, exec, std::move(frees)});
         FX_CUDA(cudaGraphLaunch(exec, ctx->stream));
         ctx->launches++;
         return FX_OK;
     }
     if (graph) cudaGraphDestroy(graph);
     (void)cudaGetLastError();
-    if (st != FX_OK) return st;
-    mg->replay_off = true;  // not recordable here: run it directly, now and from now on
+    for (void *p : frees) cudaFreeAsync(p, ctx->stream);
+    // Not recordable here (a capture-illegal call inside, or the capture was invalidated): run
+    // the application directly, now and from now on.  A genuine error shows again in that run.
+    mg->replay_off = true;
     return record(z, r, skip, z_zero);
 }
 

@@ -115,7 +115,9 @@ const char *fx_backend_name(void);
 int fx_ctx_create(int device, fx_ctx **out);
 int fx_ctx_destroy(fx_ctx *ctx);
 int fx_ctx_synchronize(fx_ctx *ctx);
-/* Use an external cudaStream_t (e.g. the caller's); NULL restores the context's own. */
+/* Use an external cudaStream_t (e.g. the caller's); NULL restores the context's own.  Waits for
+ * the old stream first.  FX_ERR_INVALID_ARGUMENT while the current stream is being captured
+ * (between fx_graph_begin and fx_graph_end, or in a caller's capture) and `stream` differs. */
 int fx_ctx_set_stream(fx_ctx *ctx, void *stream);
 void *fx_ctx_get_stream(fx_ctx *ctx);
 /* Programmatic dependent launch for this context's kernels: 1 (the default) lets each kernel's
@@ -201,7 +203,9 @@ int fx_dot2(fx_ctx *ctx, const fx_buf *a, const fx_buf *b, const fx_buf *c, cons
  * GPU, held until exit), so n is limited to 8,388,608 elements (FX_ERR_INVALID_ARGUMENT
  * above that).  Runs on `stream` (a cudaStream_t; NULL = default stream) and synchronises it.
  * Calls share the scratch: calls that overlap on the GPU race.  The first call on a device
- * resolves the array's device address; make it before any stream capture. */
+ * resolves the array's device address; make it before any stream capture.  The address is kept
+ * for the process's life, so calls after a reset of the device (cudaDeviceReset) are not
+ * supported. */
 int fx_dot_f64_noalloc(const double *x, const double *y, size_t n, double *out, void *stream);
 /* restrict :240-246 (reference semantics: clamped 2x2 average). */
 int fx_restrict(fx_ctx *ctx, const fx_buf *fine, fx_buf *coarse, const fx_grid *fine_grid,

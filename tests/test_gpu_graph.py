@@ -83,3 +83,48 @@ def test_host_value_op_fails_capture_and_context_recovers(be):
         be.graph_end()
     be.fill(a, 3.0)
     assert abs(be.dot(a, a) - 900.0) < 1e-12
+
+
+def test_stream_switch_refused_while_capturing(be):
+    """Switching the context's stream in the middle of a capture is refused (the old stream cannot
+    be waited for, and the capture must end on the stream it began on); the capture itself is
+    unharmed and replays correctly."""
+    import torch
+    from fluxion_b200.backend import InvalidArgument
+    buf = be.allocate(512, DType.F64)
+    s = torch.cuda.Stream()
+    be.graph_begin()
+    be.fill(buf, 4.0)
+    with pytest.raises(InvalidArgument):
+        be.set_stream(s.cuda_stream)
+    be.scale(buf, 0.25)
+    graph = be.graph_end()
+    be.fill(buf, 0.0)
+    graph.launch()
+    be.synchronize()
+    assert np.all(buf.to_numpy().astype(np.float64) == 1.0)
+    be.set_stream(s.cuda_stream)  # outside a capture the switch is allowed
+    be.set_stream(None)
+
+
+def test_buffer_freed_during_capture_stays_owned_by_the_graph(be):
+    """A pool buffer freed while its operations are being recorded is still addressed by the graph:
+    its memory must not return to the pool (and reach a new buffer) before the graph is destroyed."""
+    n = 1 << 16
+    y = be.allocate(n, DType.F64)
+    t = be.allocate(n, DType.F64)
+    be.graph_begin()
+    be.fill(t, 1.0)
+    be.axpy(2.0, t, y)
+    t.free()
+    graph = be.graph_end()
+    others = [be.allocate(n, DType.F64) for _ in range(4)]  # would reuse t's block if it were free
+    for o in others:
+        be.fill(o, 7.0)
+    for _ in range(3):
+        graph.launch()
+    be.synchronize()
+    assert np.all(y.to_numpy().astype(np.float64) == 6.0)
+    for o in others:
+        assert np.all(o.to_numpy().astype(np.float64) == 7.0)
+    del graph  # fx_graph_destroy: the held memory returns to the pool only now

@@ -125,6 +125,23 @@ def test_reductions(be, n):
     assert be.dot(X, Y) == be.dot(X, Y)
 
 
+@pytest.mark.parametrize("n", [1, 4097, 1 << 20, 3_000_017])
+def test_reductions_f32(be, n):
+    """F32 dots: each product of two floats is exact in FP64; the sum is within 1e-13 sum|x_i y_i|
+    of the exact FP64 sum of the same float32 data (math.fsum)."""
+    import math
+    rng = np.random.default_rng(29 + n)
+    x, y = rand(rng, n).astype(np.float32), rand(rng, n).astype(np.float32)
+    X, Y = be.upload_f32(x), be.upload_f32(y)
+    xd, yd = x.astype(np.float64), y.astype(np.float64)
+    exact_xy, exact_xx = math.fsum(xd * yd), math.fsum(xd * xd)
+    assert abs(be.dot(X, Y) - exact_xy) <= RED_TOL * np.sum(np.abs(xd * yd))
+    a, b = be.dot2(X, Y, X, X)
+    assert abs(a - exact_xy) <= RED_TOL * np.sum(np.abs(xd * yd)) and abs(b - exact_xx) <= RED_TOL * exact_xx
+    assert abs(be.norm_l2(X) ** 2 - exact_xx) <= 2 * RED_TOL * exact_xx
+    assert be.dot(X, Y) == be.dot(X, Y)
+
+
 def test_compensated_dot_recovers_cancelled_terms(be):
     # +B and -B pairs cancel exactly; only the small terms survive.  A plain double sum
     # loses them, the compensated (twice-working-precision) sum must not.
