@@ -1559,3 +1559,109 @@ void fxo_mg_v_cycle(fxo_mg *mg, double *x, const double *b) {
 void fxo_mg_pc_apply(void *ctx, double *z, const double *r) {
     fxo_mg_v_cycle((fxo_mg *)ctx, z, r);
 }
+
+/* ------------------------------------------------------------------ */
+/* FP32 vertex cycle: the cycle above evaluated in single precision, as the CUDA library runs a
+ * vertex multigrid created with dtype F32 on FP64 vectors.  Per level the operator weights are
+ * the FP64 weights rounded to float and the Jacobi factor is (float)(omega / a_c); every sweep,
+ * residual, restriction and prolongation is the FP64 expression above in float arithmetic
+ * (explicit fmaf where the FP64 code has fma, no other contraction).  The FP64 rhs is rounded to
+ * float on entry, the cycle starts from zero, and z is the float result widened to FP64.      */
+/* ------------------------------------------------------------------ */
+
+static inline float op5f(const float *a5, const float *x, size_t i, size_t cols) {
+    return fmaf(a5[0], x[i],
+                fmaf(a5[1], x[i - cols], fmaf(a5[2], x[i + cols], fmaf(a5[3], x[i - 1], a5[4] * x[i + 1]))));
+}
+
+static void jacobi_f(const float *x_in, float *x_out, const float *b, float wd, size_t rows, size_t cols,
+                     const float *a5) {
+#pragma omp parallel for schedule(static)
+    for (size_t row = 1; row < rows - 1; row++)
+        for (size_t col = 1; col < cols - 1; col++) {
+            size_t i = row * cols + col;
+            float r = b[i] - op5f(a5, x_in, i, cols);
+            x_out[i] = fmaf(wd, r, x_in[i]);
+        }
+}
+
+static void residual_f(const float *x, const float *b, float *r, size_t rows, size_t cols, const float *a5) {
+#pragma omp parallel for schedule(static)
+    for (size_t row = 1; row < rows - 1; row++)
+        for (size_t col = 1; col < cols - 1; col++) {
+            size_t i = row * cols + col;
+            r[i] = b[i] - op5f(a5, x, i, cols);
+        }
+}
+
+static void restrict_fw_f(const float *f, float *c, size_t frows, size_t fcols, size_t crows, size_t ccols) {
+    (void)frows;
+    memset(c, 0, crows * ccols * sizeof(float));
+#pragma omp parallel for schedule(static)
+    for (size_t I = 1; I < crows - 1; I++)
+        for (size_t J = 1; J < ccols - 1; J++) {
+            size_t i = (2 * I) * fcols + 2 * J, fc = fcols;
+            float e = (f[i - fc] + f[i + fc]) + (f[i - 1] + f[i + 1]);
+            float d = (f[i - fc - 1] + f[i - fc + 1]) + (f[i + fc - 1] + f[i + fc + 1]);
+            c[I * ccols + J] = (4.0f * f[i] + (2.0f * e + d)) * 0.0625f;
+        }
+}
+
+static void prolong_bilinear_f(const float *c, float *fine, size_t ccols, size_t frows, size_t fcols) {
+#pragma omp parallel for schedule(static)
+    for (size_t i = 1; i < frows - 1; i++)
+        for (size_t j = 1; j < fcols - 1; j++) {
+            size_t I = i / 2, J = j / 2, k = I * ccols + J;
+            float e;
+            if (!(i & 1) && !(j & 1)) e = c[k];
+            else if ((i & 1) && !(j & 1)) e = 0.5f * (c[k] + c[k + ccols]);
+            else if (!(i & 1) && (j & 1)) e = 0.5f * (c[k] + c[k + 1]);
+            else e = 0.25f * ((c[k] + c[k + ccols]) + (c[k + 1] + c[k + ccols + 1]));
+            fine[i * fcols + j] += e;
+        }
+}
+
+int fxo_mg_v_cycle_f32(fxo_mg *mg, double *z, const double *r) {
+    if (mg->mode != 1) return FXO_ERR_INVALID_ARGUMENT;
+    int nl = mg->nlev;
+    float *u[40], *t[40], *b[40], a5[40][5], wd[40];
+    for (int l = 0; l < nl; l++) {
+        size_t n = mg->lv[l].rows * mg->lv[l].cols;
+        u[l] = calloc(n, sizeof(float));
+        t[l] = calloc(n, sizeof(float));
+        b[l] = calloc(n, sizeof(float));
+        for (int k = 0; k < 5; k++) a5[l][k] = (float)mg->lv[l].a5[k];
+        wd[l] = (float)(mg->omega / mg->lv[l].a5[0]);
+    }
+    size_t n0 = mg->lv[0].rows * mg->lv[0].cols;
+    for (size_t i = 0; i < n0; i++) b[0][i] = (float)r[i];
+#define FXO_SMOOTH(l, cnt)                                                                            \
+    for (int k_ = 0; k_ < (cnt); k_++) {                                                              \
+        jacobi_f(u[l], t[l], b[l], wd[l], mg->lv[l].rows, mg->lv[l].cols, a5[l]);                    \
+        float *s_ = u[l];                                                                             \
+        u[l] = t[l];                                                                                  \
+        t[l] = s_;                                                                                    \
+    }
+    for (int l = 0; l < nl - 1; l++) {
+        mg_level *L = &mg->lv[l], *Cl = &mg->lv[l + 1];
+        FXO_SMOOTH(l, mg->n_pre);
+        residual_f(u[l], b[l], t[l], L->rows, L->cols, a5[l]);
+        restrict_fw_f(t[l], b[l + 1], L->rows, L->cols, Cl->rows, Cl->cols);
+    }
+    FXO_SMOOTH(nl - 1, mg->coarse_sweeps);
+    for (int l = nl - 2; l >= 0; l--) {
+        mg_level *L = &mg->lv[l], *Cl = &mg->lv[l + 1];
+        prolong_bilinear_f(u[l + 1], u[l], Cl->cols, L->rows, L->cols);
+        FXO_SMOOTH(l, mg->n_post);
+    }
+#undef FXO_SMOOTH
+    for (size_t i = 0; i < n0; i++) z[i] = (double)u[0][i];
+    for (int l = 0; l < nl; l++) {
+        free(u[l]);
+        free(t[l]);
+        free(b[l]);
+    }
+    return FXO_OK;
+}
+
+void fxo_mg_pc_apply_f32(void *ctx, double *z, const double *r) { fxo_mg_v_cycle_f32((fxo_mg *)ctx, z, r); }

@@ -201,6 +201,10 @@ void fxo_mg_level_dims(const fxo_mg *mg, int lvl, size_t *rows, size_t *cols);
 void fxo_mg_v_cycle(fxo_mg *mg, double *x, const double *b);
 /* usable as fxo_pc_fn with ctx = the fxo_mg */
 void fxo_mg_pc_apply(void *mg, double *z, const double *r);
+/* FP32 vertex cycle (the CUDA library's dtype-F32 multigrid on FP64 vectors): z = (double) of
+ * the float cycle of (float) r from zero.  FXO_ERR_INVALID_ARGUMENT for a reference-mode mg. */
+int fxo_mg_v_cycle_f32(fxo_mg *mg, double *z, const double *r);
+void fxo_mg_pc_apply_f32(void *mg, double *z, const double *r);
 /* coarse-level operator weights of the vertex hierarchy */
 void fxo_mg_coarse_op(const double *fine, double sigma, double *coarse);
 

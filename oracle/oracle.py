@@ -122,6 +122,7 @@ def _declare(L):
     d("fxo_mg_depth", C.c_int, C.c_void_p)
     d("fxo_mg_level_dims", None, C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t))
     d("fxo_mg_v_cycle", None, C.c_void_p, _dp, _dp)
+    d("fxo_mg_v_cycle_f32", C.c_int, C.c_void_p, _dp, _dp)
     d("fxo_mg_coarse_op", None, _dp, C.c_double, _dp)
 
 
@@ -299,7 +300,7 @@ class Multigrid:
 
     def __init__(self, rows, cols, dx, dy, n_pre=2, n_post=2, omega=2.0 / 3.0, mode=0,
                  op_coeff=1.0, entries=None, bcs=ZERO_DIRICHLET, coarse_max=15, coarse_sweeps=200,
-                 smoother=0):
+                 smoother=0, f32=False):
         entries = entries or laplacian_5pt(dx, dy)
         n, dr, dc, w = _stencil_arrays(entries)
         self._bcs = bcs_array(bcs)
@@ -309,7 +310,12 @@ class Multigrid:
             raise OracleError(6, "mg_create")
         if smoother:
             _chk(lib().fxo_mg_set_smoother(self.h, int(smoother)), "mg_set_smoother")
-        self._cb = PC_FN(lambda ctx, z, r: lib().fxo_mg_v_cycle(self.h, z, r))
+        if f32:  # the single-precision cycle on FP64 vectors (vertex mode only), from zero
+            if mode != 1:
+                raise OracleError(5, "the FP32 cycle exists for the vertex hierarchy only")
+            self._cb = PC_FN(lambda ctx, z, r: lib().fxo_mg_v_cycle_f32(self.h, z, r))
+        else:
+            self._cb = PC_FN(lambda ctx, z, r: lib().fxo_mg_v_cycle(self.h, z, r))
 
     def depth(self):
         return lib().fxo_mg_depth(self.h)
@@ -321,6 +327,10 @@ class Multigrid:
 
     def v_cycle(self, x, b):
         lib().fxo_mg_v_cycle(self.h, _p(x), _p(b))
+
+    def v_cycle_f32(self, z, r):
+        """z = the FP32 cycle of r from zero (vertex mode), widened to FP64."""
+        _chk(lib().fxo_mg_v_cycle_f32(self.h, _p(z), _p(r)), "mg_v_cycle_f32")
 
     def __del__(self):
         try:

@@ -221,9 +221,10 @@ def test_vertex_mg_vcycle_bitwise(dev, n):
 @pytest.mark.parametrize("cm,cs", [(15, 200), (7, 30), (3, 10), (31, 40)])
 def test_fused_vcycle_bitwise(dev, n, cm, cs):
     """The fused V(2,2) kernels (zero initial guess) equal the oracle's separate sweeps, residual,
-    full weighting and bilinear prolongation bit for bit (F64), and the fused F32 cycle equals
-    the unfused F32 cycle bit for bit.  Coarsest grids of up to 17 x 17 points are solved by one
-    warp from registers, larger ones (coarse_max 31: 33 x 33) in shared memory."""
+    full weighting and bilinear prolongation bit for bit (F64); the fused F32 cycle equals the
+    oracle's FP32 restatement of the cycle bit for bit, and the unfused F32 cycle.  Coarsest grids
+    of up to 17 x 17 points are solved by one warp from registers, larger ones (coarse_max 31:
+    33 x 33) in shared memory."""
     from fluxion_b200 import DType, Field, Multigrid
     from fluxion_b200.workloads import poisson_problem
     P = poisson_problem(n)
@@ -246,6 +247,9 @@ def test_fused_vcycle_bitwise(dev, n, cm, cs):
     mg32.precondition(zf, b)
     zu = Field.zeros(P.grid, DType.F64, dev)
     mg32.v_cycle(zu, b)  # unfused path (explicit initial guess)
+    zo32 = np.zeros(N * N)
+    omg.v_cycle_f32(zo32, bvec)
+    assert np.array_equal(zf.to_vec_f64(), zo32)
     assert np.array_equal(zf.to_vec_f64(), zu.to_vec_f64())
     assert rel_err(zf.to_vec_f64(), zo) < 1e-5
 
@@ -255,7 +259,8 @@ def test_fused_vcycle_bitwise_rectangular(dev, rows, cols, cm):
     """On rectangular grids coarsening stops when either interior side reaches coarse_max, so
     the coarsest grid is long in one direction (17 x 65, 65 x 17: shared-memory sweeps) or
     short in both but not square (9 x 17, 17 x 9: one warp).  The fused cycle still equals
-    the oracle's bit for bit (F64), and the fused F32 cycle the unfused F32 one."""
+    the oracle's bit for bit (F64), and the fused F32 cycle the oracle's FP32 restatement and the
+    unfused F32 one."""
     from fluxion_b200 import DType, Field, Grid, Multigrid, Stencil
     dx, dy = 1.0 / (cols - 1), 1.0 / (rows - 1)
     g = Grid.new(rows, cols, dx, dy)
@@ -279,6 +284,9 @@ def test_fused_vcycle_bitwise_rectangular(dev, rows, cols, cm):
     mg32.precondition(zf, b)
     zu = Field.zeros(g, DType.F64, dev)
     mg32.v_cycle(zu, b)
+    zo32 = np.zeros(rows * cols)
+    omg.v_cycle_f32(zo32, bvec)
+    assert np.array_equal(zf.to_vec_f64(), zo32)
     assert np.array_equal(zf.to_vec_f64(), zu.to_vec_f64())
     assert rel_err(zf.to_vec_f64(), zo) < 1e-5
 
