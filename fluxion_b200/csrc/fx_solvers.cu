@@ -9,10 +9,12 @@
 // `done` word in device memory turns the surplus launches into no-ops once the stop
 // test (evaluated on the device, exactly as the reference evaluates it) has fired.
 #include <cmath>
+#include <random>
 #include <type_traits>
 #include <utility>
 #include <vector>
 
+#include "fx_learned.cuh"
 #include "fx_points.cuh"
 #include "fx_wcycle.cuh"
 
@@ -2313,6 +2315,200 @@ struct FlatCdResid {
     }
 };
 
+// ---- learned smoother (fx_learned.cuh): the level operator as the network kernels see it, the
+// residual pass that feeds the network, the training-sample extractor and the per-cycle check
+
+template <typename T>
+struct LsmOp {
+    OpA<T, kModeCD> A;
+    __device__ __forceinline__ T diag(size_t i) const { return cd_diag(A, i); }
+    __device__ __forceinline__ T vxv(size_t i) const { return A.vx[i]; }
+    __device__ __forceinline__ T vyv(size_t i) const { return A.vy[i]; }
+};
+
+// q = (b - A x) (1 / diag(A)) on the interior (the increment of FlatCdSweep divided by omega),
+// 0 on the ring; sum of q^2 over the interior reduced for the scale
+template <typename T>
+struct FlatLsmResid {
+    OpA<T, kModeCD> A;
+    const T *x;
+    T *q;
+    const T *b;
+    size_t rows, cols;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        const size_t row = i / cols, col = i - row * cols;
+        if (row == 0 || col == 0 || row == rows - 1 || col == cols - 1) {
+            q[i] = (T)0;
+            return;
+        }
+        Nb<T> nb;
+        nb.c = x[i];
+        nb.n = x[i - cols];
+        nb.s = x[i + cols];
+        nb.w = x[i - 1];
+        nb.e = x[i + 1];
+        const T inv_d = (T)1 / cd_diag(A, i);
+        const T v = (b[i] - A.apply(false, nb, i)) * inv_d;
+        q[i] = v;
+        csum_fma(acc[0], (double)v, (double)v);
+    }
+};
+
+// scale[0] = s = sqrt(sum q^2 / interior points), scale[1] = 1 / s (0 when s = 0)
+struct FinLsmScale {
+    double *scale;
+    double inv_n;
+    __device__ void operator()(const double *v) const {
+        const double s = sqrt(v[0] * inv_n);
+        scale[0] = s;
+        scale[1] = s > 0.0 ? 1.0 / s : 0.0;
+    }
+};
+
+// One training sample per block from the fields of one iterate (see fx_learned.cuh): the network
+// inputs over the 25 x 25 input region and, over the 16 x 16 loss patch, t = (H e - omega H q) / s
+// and n = ||H e||^2 / s^2.  origins: (row, col) of each patch's first loss point.
+template <typename Op>
+__global__ void __launch_bounds__(256) k_lsm_extract(Op A, const double *__restrict__ q, const double *__restrict__ e,
+                                                     const double *__restrict__ scale, double omega,
+                                                     const int *__restrict__ origins, __nv_bfloat16 *d_in,
+                                                     float *d_tgt, float *d_norm, int rows, int cols, double inv_dx,
+                                                     double inv_dy) {
+    using namespace lsm;
+    __shared__ double se[kP3 * kP3], sq[kP3 * kP3], re[kNCo * kNCo], rq[kNCo * kNCo], red[8];
+    const int tid = threadIdx.x;
+    const int y0 = origins[2 * blockIdx.x], x0 = origins[2 * blockIdx.x + 1];
+    const double inv_s = scale[1];
+    __nv_bfloat16 *in = d_in + (size_t)blockIdx.x * kInLen;
+    for (int k = tid; k < kPin * kPin; k += 256) {
+        const int iy = k / kPin, ix = k - iy * kPin;
+        const size_t i = (size_t)(y0 - 4 + iy) * cols + (x0 - 4 + ix);
+        float c0, c1, c2;
+        input_channels<double>(q[i], A.vxv(i), A.vyv(i), A.diag(i), inv_s, inv_dx, inv_dy, c0, c1, c2);
+        in[k] = __float2bfloat16_rn(c0);
+        in[kPin * kPin + k] = __float2bfloat16_rn(c1);
+        in[2 * kPin * kPin + k] = __float2bfloat16_rn(c2);
+    }
+    for (int k = tid; k < kP3 * kP3; k += 256) {
+        const int y = k / kP3, x = k - y * kP3;
+        const size_t i = (size_t)(y0 - 1 + y) * cols + (x0 - 1 + x);
+        se[k] = e[i];
+        sq[k] = q[i];
+    }
+    __syncthreads();
+    for (int k = tid; k < kNCo * kNCo; k += 256) {  // full weighting at the coarse points
+        const int I = k / kNCo, J = k - I * kNCo;
+        const int c = (2 * I + 1) * kP3 + 2 * J + 1;
+        const double *f[2] = {se, sq};
+        double *o[2] = {re, rq};
+        for (int t = 0; t < 2; t++) {
+            const double *v = f[t];
+            const double ee = (v[c - kP3] + v[c + kP3]) + (v[c - 1] + v[c + 1]);
+            const double dd = (v[c - kP3 - 1] + v[c - kP3 + 1]) + (v[c + kP3 - 1] + v[c + kP3 + 1]);
+            o[t][k] = (4.0 * v[c] + (2.0 * ee + dd)) * 0.0625;
+        }
+    }
+    __syncthreads();
+    double nsum = 0.0;
+    for (int k = tid; k < kT * kT; k += 256) {
+        const int py = k / kT, px = k - py * kT;
+        const int I = py >> 1, J = px >> 1;
+        const bool oy = py & 1, ox = px & 1;
+        double pe, pq;
+        const int b = I * kNCo + J;
+        if (!oy && !ox) {
+            pe = re[b];
+            pq = rq[b];
+        } else if (oy && !ox) {
+            pe = 0.5 * (re[b] + re[b + kNCo]);
+            pq = 0.5 * (rq[b] + rq[b + kNCo]);
+        } else if (!oy && ox) {
+            pe = 0.5 * (re[b] + re[b + 1]);
+            pq = 0.5 * (rq[b] + rq[b + 1]);
+        } else {
+            pe = 0.25 * ((re[b] + re[b + kNCo]) + (re[b + 1] + re[b + kNCo + 1]));
+            pq = 0.25 * ((rq[b] + rq[b + kNCo]) + (rq[b + 1] + rq[b + kNCo + 1]));
+        }
+        const int c = (py + 1) * kP3 + px + 1;
+        const double he = se[c] - pe, hq = sq[c] - pq;
+        d_tgt[(size_t)blockIdx.x * kTgtLen + k] = (float)((he - omega * hq) * inv_s);
+        nsum += he * he;
+    }
+    for (int off = 16; off > 0; off >>= 1) nsum += __shfl_down_sync(0xffffffffu, nsum, off);
+    if ((tid & 31) == 0) red[tid >> 5] = nsum;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += red[w];
+        d_norm[blockIdx.x] = (float)(t * inv_s * inv_s);
+    }
+}
+
+// Per-cycle check of the learned cycle (on the F64 vectors of the application): ||r||^2 and
+// ||r - A z||^2 over the interior.
+struct FlatLsmCheck {
+    OpA<double, kModeCD> A;
+    const double *z, *r;
+    size_t rows, cols;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        const size_t row = i / cols, col = i - row * cols;
+        if (row == 0 || col == 0 || row == rows - 1 || col == cols - 1) return;
+        Nb<double> nb;
+        nb.c = z[i];
+        nb.n = z[i - cols];
+        nb.s = z[i + cols];
+        nb.w = z[i - 1];
+        nb.e = z[i + 1];
+        const double rv = r[i], d = rv - A.apply(false, nb, i);
+        csum_fma(acc[0], rv, rv);
+        csum_fma(acc[1], d, d);
+    }
+};
+
+// plain_skip = (the learned cycle reduced ||r|| by at least `ratio`, or the solve is over);
+// counts applications and fallbacks while the solve runs
+struct FinLsmCheck {
+    double ratio2;
+    const int *skip;
+    int *plain_skip;
+    unsigned long long *counts;  // [0] applications, [1] fallbacks
+    __device__ void operator()(const double *v) const {
+        const bool done = skip && *(volatile const int *)skip;
+        const bool ok = v[1] <= ratio2 * v[0];
+        *plain_skip = (ok || done) ? 1 : 0;
+        if (!done) {
+            counts[0] += 1;
+            if (!ok) counts[1] += 1;
+        }
+    }
+};
+
+// One learned smoothing step on a level (fx_learned.cuh): q and the scale s in one pass, then the
+// network and the update x <- x + omega q + s c in place.  q may be any scratch vector of the level.
+template <typename T>
+int lsm_step(fx_ctx *ctx, const fx_lsm *m, const OpA<T, kModeCD> &A, T *x, T *q, const T *b, T omega, size_t rows,
+             size_t cols, double dx, double dy, double *scale, const int *skip) {
+    using namespace lsm;
+    if (rows < 3 || cols < 3) return fail(FX_ERR_INVALID_GRID, "learned smoother: grid too small");
+    const double n_int = (double)(rows - 2) * (double)(cols - 2);
+    FX_TRY((launch_flat<1>(ctx, rows * cols, FlatLsmResid<T>{A, x, q, b, rows, cols}, FinLsmScale{scale, 1.0 / n_int},
+                           skip, "lsm_resid")));
+    static std::atomic<unsigned long long> attr_done{0};  // one bit per device
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_done.load() & bit)) {
+        FX_CUDA(cudaFuncSetAttribute(k_lsm_apply<T, LsmOp<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kSmemApply));
+        attr_done.fetch_or(bit);
+    }
+    const dim3 grid((unsigned)((cols + kTile - 1) / kTile), (unsigned)((rows + kTile - 1) / kTile));
+    timing_pre(ctx, "lsm_apply");
+    launch_pdl(ctx, k_lsm_apply<T, LsmOp<T>>, grid, dim3(256), (size_t)kSmemApply, LsmOp<T>{A},
+               (const uint32_t *)m->d_frag, (const float *)m->d_wq, (const T *)q, x, (const double *)scale, omega,
+               (int)rows, (int)cols, 1.0 / dx, 1.0 / dy, skip);
+    timing_post(ctx, (double)rows * (double)cols);
+    return check_launch(ctx, "lsm_apply");
+}
+
 // Two sweeps in one pass (temporal blocking): a 32 x 32 tile of the second sweep's points,
 // with x over the tile plus a two-point halo and the first sweep's values over the tile plus
 // a one-point halo in shared memory.  x is read once and only the second sweep's values are
@@ -2497,11 +2693,27 @@ struct fx_cdmg {
     std::vector<Replay> replays;
     bool replay = false;      // fx_cdmg_set_replay
     bool replay_off = false;  // a recording failed: launch directly from then on
-    ~fx_cdmg() {
+    // learned smoothing (fx_cdmg_set_learned): levels of at least lsm_min_points points smooth
+    // with the network; each application is checked and, when the learned cycle reduced
+    // ||r|| by less than lsm_ratio, recomputed with the plain cycle
+    const fx_lsm *lsm = nullptr;
+    size_t lsm_min_points = 0;
+    double lsm_ratio = 0.9;
+    double *d_lsm_scale = nullptr;          // [2]: s, 1 / s of the current learned step
+    int *d_plain_skip = nullptr;            // 1: the plain recomputation is not needed
+    unsigned long long *d_lsm_counts = nullptr;  // [2]: checked applications, fallbacks
+    void drop_replays() {
         for (auto &g : replays) {
             cudaGraphExecDestroy(g.exec);
             for (void *p : g.frees) cudaFree(p);  // waits for the device: a replay may still run
         }
+        replays.clear();
+    }
+    ~fx_cdmg() {
+        drop_replays();
+        if (d_lsm_scale) cudaFree(d_lsm_scale);
+        if (d_plain_skip) cudaFree(d_plain_skip);
+        if (d_lsm_counts) cudaFree(d_lsm_counts);
         for (auto &L : lv)
             for (fx_buf *f : {L.u, L.rhs, L.tmp, L.vx, L.vy, L.kappa}) fx_free(f);
         fx_free(tmp0);
@@ -2528,7 +2740,7 @@ struct fx_cdmg {
 namespace {
 
 template <typename T>
-int cd_cycle(fx_cdmg *mg, T *x, const T *b, T *x_other, const int *skip) {  // x holds zeros on entry
+int cd_cycle(fx_cdmg *mg, T *x, const T *b, T *x_other, const int *skip, bool learned) {  // x holds zeros on entry
     fx_ctx *ctx = mg->ctx;
     const int nl = (int)mg->lv.size();
     std::vector<T *> cur(nl), oth(nl);
@@ -2545,6 +2757,12 @@ int cd_cycle(fx_cdmg *mg, T *x, const T *b, T *x_other, const int *skip) {  // x
     auto smooth = [&](int l, size_t n) -> int {
         const CdLevel &L = mg->lv[l];
         const auto A = mg->level_op<T>(l);
+        if (learned && l < nl - 1 && L.rows * L.cols >= mg->lsm_min_points) {  // in place; oth[l] holds q
+            for (size_t k = 0; k < n; k++)
+                FX_TRY(lsm_step<T>(ctx, mg->lsm, A, cur[l], oth[l], rhs[l], omega, L.rows, L.cols, L.dx, L.dy,
+                                   mg->d_lsm_scale, skip));
+            return FX_OK;
+        }
         size_t k = 0;
         for (; k + 2 <= n; k += 2) {  // pairs in one pass; the result lands in the partner buffer
             const dim3 grid((unsigned)((L.cols + kSw2T - 1) / kSw2T), (unsigned)((L.rows + kSw2T - 1) / kSw2T));
@@ -2648,15 +2866,28 @@ int fx_cdmg::View::record(fx_buf *z, const fx_buf *r, const int *skip, bool z_ze
     if (z->dtype != FX_F64 || z->len != n)
         return fail(FX_ERR_DIMENSION_MISMATCH, "conv-diff multigrid: vectors must be F64 fields of the operator's grid");
     if (z->ptr == r->ptr) return fail(FX_ERR_INVALID_ARGUMENT, "z and r must be distinct");
-    if (mg->dtype == FX_F32) {  // r -> F32, the cycle in F32, z = its F64 image
-        float *x = (float *)L0.u->ptr, *b = (float *)L0.rhs->ptr;
-        FX_TRY((launch_flat<0>(ctx, n, FlatCast<double, float>{(const double *)r->ptr, b}, NoFin{}, skip, "cdmg_convert")));
-        FX_TRY(zero_fill<float>(ctx, x, n, skip));
-        FX_TRY(cd_cycle<float>(mg, x, b, (float *)L0.tmp->ptr, skip));
-        return launch_flat<0>(ctx, n, FlatCast<float, double>{x, (double *)z->ptr}, NoFin{}, skip, "cdmg_convert");
-    }
-    if (!z_zero) FX_TRY(zero_fill<double>(ctx, (double *)z->ptr, z->len, skip));
-    return cd_cycle<double>(mg, (double *)z->ptr, (const double *)r->ptr, (double *)mg->tmp0->ptr, skip);
+    auto run = [&](bool learned, const int *sk, bool zz) -> int {
+        if (mg->dtype == FX_F32) {  // r -> F32, the cycle in F32, z = its F64 image
+            float *x = (float *)L0.u->ptr, *b = (float *)L0.rhs->ptr;
+            FX_TRY((launch_flat<0>(ctx, n, FlatCast<double, float>{(const double *)r->ptr, b}, NoFin{}, sk,
+                                   "cdmg_convert")));
+            FX_TRY(zero_fill<float>(ctx, x, n, sk));
+            FX_TRY(cd_cycle<float>(mg, x, b, (float *)L0.tmp->ptr, sk, learned));
+            return launch_flat<0>(ctx, n, FlatCast<float, double>{x, (double *)z->ptr}, NoFin{}, sk, "cdmg_convert");
+        }
+        if (!zz) FX_TRY(zero_fill<double>(ctx, (double *)z->ptr, z->len, sk));
+        return cd_cycle<double>(mg, (double *)z->ptr, (const double *)r->ptr, (double *)mg->tmp0->ptr, sk, learned);
+    };
+    if (!mg->lsm) return run(false, skip, z_zero);
+    // the learned cycle, its check, and the plain cycle where the check failed (all on the device)
+    FX_TRY(run(true, skip, z_zero));
+    const double ratio2 = mg->lsm_ratio * mg->lsm_ratio;
+    FX_TRY((launch_flat<2>(ctx, n,
+                           FlatLsmCheck{mg->level_op<double>(0), (const double *)z->ptr, (const double *)r->ptr,
+                                        L0.rows, L0.cols},
+                           FinLsmCheck{ratio2, skip, mg->d_plain_skip, mg->d_lsm_counts}, nullptr,
+                           "cdmg_learned_check")));
+    return run(false, mg->d_plain_skip, false);
 }
 
 namespace {
@@ -3400,6 +3631,195 @@ int fx_cdmg_set_replay(fx_cdmg *mg, int enabled) {
     if (!mg) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     mg->replay = enabled != 0;
     return FX_OK;
+}
+
+int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, double fallback_ratio) {
+    if (!mg) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (lsm && lsm->ctx->device != mg->ctx->device)
+        return fail(FX_ERR_INVALID_ARGUMENT, "learned smoother lives on another device");
+    if (lsm && !(fallback_ratio > 0.0)) return fail(FX_ERR_INVALID_ARGUMENT, "fallback ratio must be positive");
+    if (lsm && mg->lv[0].rows * mg->lv[0].cols < min_points)
+        return fail(FX_ERR_INVALID_ARGUMENT, "no level reaches min_points: the cycle would not use the network");
+    FX_CUDA(cudaStreamSynchronize(mg->ctx->stream));
+    mg->drop_replays();  // the recorded launch sequence changes
+    if (lsm && !mg->d_lsm_scale) {
+        FX_CUDA(cudaMalloc(&mg->d_lsm_scale, 2 * sizeof(double)));
+        FX_CUDA(cudaMalloc(&mg->d_plain_skip, sizeof(int)));
+        FX_CUDA(cudaMalloc(&mg->d_lsm_counts, 2 * sizeof(unsigned long long)));
+        FX_CUDA(cudaMemset(mg->d_lsm_counts, 0, 2 * sizeof(unsigned long long)));
+    }
+    mg->lsm = lsm;
+    mg->lsm_min_points = min_points;
+    mg->lsm_ratio = fallback_ratio;
+    return FX_OK;
+}
+
+int fx_cdmg_learned_stats(fx_cdmg *mg, unsigned long long *applications, unsigned long long *fallbacks) {
+    if (!mg || !applications || !fallbacks) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    unsigned long long c[2] = {0, 0};
+    if (mg->d_lsm_counts) {
+        FX_CUDA(cudaStreamSynchronize(mg->ctx->stream));
+        FX_CUDA(cudaMemcpy(c, mg->d_lsm_counts, sizeof(c), cudaMemcpyDeviceToHost));
+    }
+    *applications = c[0];
+    *fallbacks = c[1];
+    return FX_OK;
+}
+
+// ------------------------------------------------ learned smoother: operator-side entry points
+
+namespace {
+
+int lsm_check_op(const fx_op *op) {
+    if (!op) return fail(FX_ERR_INVALID_ARGUMENT, "null operator");
+    if (op->vx->dtype != FX_F64 || op->vy->dtype != FX_F64 || (op->kappa && op->kappa->dtype != FX_F64))
+        return fail(FX_ERR_INVALID_ARGUMENT, "learned smoother: operator fields must be F64");
+    return FX_OK;
+}
+
+int lsm_check_field(const fx_op *op, const fx_buf *v, const char *name) {
+    FX_TRY(check_buf(v, name));
+    if (v->dtype != FX_F64 || v->len != op->g.rows * op->g.cols)
+        return fail(FX_ERR_DIMENSION_MISMATCH, std::string("learned smoother: ") + name +
+                                                   " must be an F64 field of the operator's grid");
+    return FX_OK;
+}
+
+}  // namespace
+
+int fx_lsm_smooth(fx_lsm *m, const fx_op *op, fx_buf *x, const fx_buf *b, double omega, size_t steps) {
+    if (!m) return fail(FX_ERR_INVALID_ARGUMENT, "null learned smoother");
+    FX_TRY(lsm_check_op(op));
+    FX_TRY(lsm_check_field(op, x, "x"));
+    FX_TRY(lsm_check_field(op, b, "b"));
+    if (x->ptr == b->ptr) return fail(FX_ERR_INVALID_ARGUMENT, "x and b must be distinct");
+    fx_ctx *ctx = op->ctx;
+    if (m->ctx->device != ctx->device) return fail(FX_ERR_INVALID_ARGUMENT, "learned smoother lives on another device");
+    if (!steps) return FX_OK;
+    fx_buf *q = nullptr;
+    FX_TRY(fx_alloc(ctx, x->len, FX_F64, &q));
+    double *scale = nullptr;
+    int st = cudaMallocAsync(&scale, 2 * sizeof(double), ctx->stream) == cudaSuccess
+                 ? FX_OK
+                 : fail(FX_ERR_BACKEND, "learned smoother: scratch allocation failed");
+    const OpA<double, kModeCD> A = OpMaker<double, kModeCD>::make(StencilP{}, 0.0, 0, 0, op);
+    for (size_t k = 0; k < steps && st == FX_OK; k++)
+        st = lsm_step<double>(ctx, m, A, (double *)x->ptr, (double *)q->ptr, (const double *)b->ptr, omega,
+                              op->g.rows, op->g.cols, op->g.dx, op->g.dy, scale, nullptr);
+    if (scale) cudaFreeAsync(scale, ctx->stream);
+    fx_free(q);
+    if (st == FX_OK) FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return st;
+}
+
+int fx_lsm_data_add_patches(fx_lsm_data *d, const fx_op *op, const fx_buf *x, const fx_buf *e, const fx_buf *b,
+                            double omega, const int *origins, size_t count) {
+    using namespace lsm;
+    if (!d || !origins) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(lsm_check_op(op));
+    FX_TRY(lsm_check_field(op, x, "x"));
+    FX_TRY(lsm_check_field(op, e, "e"));
+    FX_TRY(lsm_check_field(op, b, "b"));
+    if (d->ctx->device != op->ctx->device) return fail(FX_ERR_INVALID_ARGUMENT, "samples live on another device");
+    if (count == 0) return FX_OK;
+    if (count > d->cap - d->count) return fail(FX_ERR_INVALID_ARGUMENT, "sample capacity exceeded");
+    const long rows = (long)op->g.rows, cols = (long)op->g.cols;
+    for (size_t k = 0; k < count; k++) {  // input region inside the grid, output region inside the interior
+        const long y0 = origins[2 * k], x0 = origins[2 * k + 1];
+        if ((y0 & 1) || (x0 & 1) || y0 < 4 || x0 < 4 || y0 + kT + 4 >= rows || x0 + kT + 4 >= cols)
+            return fail(FX_ERR_INVALID_ARGUMENT,
+                        "patch origin " + std::to_string(y0) + "," + std::to_string(x0) +
+                            " must be even and leave the 25 x 25 input region inside the grid");
+    }
+    fx_ctx *ctx = op->ctx;
+    fx_buf *q = nullptr;
+    FX_TRY(fx_alloc(ctx, x->len, FX_F64, &q));
+    void *scratch = nullptr;  // scale [2 doubles] + origins
+    const size_t obytes = count * 2 * sizeof(int);
+    int st = cudaMallocAsync(&scratch, 16 + obytes, ctx->stream) == cudaSuccess
+                 ? FX_OK
+                 : fail(FX_ERR_BACKEND, "learned smoother: scratch allocation failed");
+    double *scale = (double *)scratch;
+    int *d_orig = (int *)((char *)scratch + 16);
+    const OpA<double, kModeCD> A = OpMaker<double, kModeCD>::make(StencilP{}, 0.0, 0, 0, op);
+    const size_t n = x->len;
+    if (st == FX_OK && cudaMemcpyAsync(d_orig, origins, obytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        st = fail(FX_ERR_BACKEND, "learned smoother: origin upload failed");
+    if (st == FX_OK)
+        st = launch_flat<1>(ctx, n,
+                            FlatLsmResid<double>{A, (const double *)x->ptr, (double *)q->ptr, (const double *)b->ptr,
+                                                 op->g.rows, op->g.cols},
+                            FinLsmScale{scale, 1.0 / ((double)(rows - 2) * (double)(cols - 2))}, nullptr, "lsm_resid");
+    if (st == FX_OK) {
+        k_lsm_extract<LsmOp<double>><<<(unsigned)count, 256, 0, ctx->stream>>>(
+            LsmOp<double>{A}, (const double *)q->ptr, (const double *)e->ptr, scale, omega, d_orig,
+            d->d_in + d->count * kInLen, d->d_tgt + d->count * kTgtLen, d->d_norm + d->count, (int)rows, (int)cols,
+            1.0 / op->g.dx, 1.0 / op->g.dy);
+        st = check_launch(ctx, "lsm_extract");
+    }
+    if (scratch) cudaFreeAsync(scratch, ctx->stream);
+    fx_free(q);
+    if (st == FX_OK) {
+        FX_CUDA(cudaStreamSynchronize(ctx->stream));
+        d->count += count;
+    }
+    return st;
+}
+
+int fx_lsm_data_add_problem(fx_lsm_data *d, const fx_op *op, const fx_buf *b, size_t iterates,
+                            size_t patches_per_iterate, double omega, unsigned long long seed, size_t *added) {
+    using namespace lsm;
+    if (!d || !added) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    *added = 0;
+    FX_TRY(lsm_check_op(op));
+    FX_TRY(lsm_check_field(op, b, "b"));
+    const long rows = (long)op->g.rows, cols = (long)op->g.cols;
+    if (rows < 2 * kT + 10 || cols < 2 * kT + 10)
+        return fail(FX_ERR_INVALID_GRID, "learned smoother samples need a grid of at least 42 x 42 points");
+    fx_ctx *ctx = op->ctx;
+    const size_t n = b->len;
+    double bnorm = 0.0;
+    FX_TRY(fx_norm_l2(ctx, b, &bnorm));
+    // the exact solution u of A u = b: FGMRES(30) with the plain cycle, to 1e-12 relative
+    fx_cdmg *mg = nullptr;
+    FX_TRY(fx_cdmg_create(op, 2, 2, omega, 15, 200, &mg));
+    fx_fgmres *solver = nullptr;
+    std::vector<fx_buf *> bufs(5, nullptr);  // u, x, e, r, z
+    int st = fx_fgmres_create(ctx, &op->g, 30, 1e-12 * bnorm, 600, &solver);
+    for (auto &p : bufs)
+        if (st == FX_OK) st = fx_alloc(ctx, n, FX_F64, &p);
+    fx_stats stats{};
+    if (st == FX_OK) st = fx_fgmres_solve_op(solver, bufs[0], b, op, fx_cdmg_as_precond(mg), &stats);
+    if (st == FX_OK && stats.residual > 1e-9 * bnorm)
+        st = fail(FX_ERR_BACKEND, "learned smoother samples: reference solve did not converge");
+    std::mt19937_64 rng(seed);
+    std::uniform_int_distribution<long> ry(2, (rows - kT - 5) / 2), rx(2, (cols - kT - 5) / 2);
+    std::vector<int> org;
+    fx_buf *u = bufs[0], *x = bufs[1], *e = bufs[2], *r = bufs[3], *z = bufs[4];
+    for (size_t it = 0; it < iterates && st == FX_OK; it++) {
+        // e = u - x; samples from (x, e); then one plain cycle: x += M (b - A x)
+        st = fx_waxpy(ctx, 1.0, u, -1.0, x, e);
+        const size_t room = d->cap - d->count;
+        const size_t k = std::min(room, patches_per_iterate);
+        if (st == FX_OK && k) {
+            org.resize(2 * k);
+            for (size_t j = 0; j < k; j++) {
+                org[2 * j] = (int)(2 * ry(rng));
+                org[2 * j + 1] = (int)(2 * rx(rng));
+            }
+            st = fx_lsm_data_add_patches(d, op, x, e, b, omega, org.data(), k);
+            if (st == FX_OK) *added += k;
+        }
+        if (st == FX_OK) st = fx_op_apply(op, x, r);
+        if (st == FX_OK) st = fx_waxpy(ctx, 1.0, b, -1.0, r, r);
+        if (st == FX_OK) st = fx_fill(ctx, z, 0.0);
+        if (st == FX_OK) st = fx_precond_apply(fx_cdmg_as_precond(mg), z, r);
+        if (st == FX_OK) st = fx_axpy(ctx, 1.0, z, x);
+    }
+    for (auto *p : bufs) fx_free(p);
+    if (solver) fx_fgmres_destroy(solver);
+    fx_cdmg_destroy(mg);
+    return st;
 }
 
 int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st, const fx_boundaries *bc,

@@ -422,6 +422,21 @@ class ConvDiffMultigrid(Preconditioner):
         (fx_cdmg_set_replay; off by default)."""
         check(L.lib().fx_cdmg_set_replay(self.h, 1 if enabled else 0))
 
+    def set_learned(self, smoother, min_points: int = 4096, fallback_ratio: float = 0.9) -> None:
+        """Smooth every level of at least `min_points` points (the coarsest excepted) with the
+        learned smoother (`fluxion_b200.learned.LearnedSmoother`) in place of the Jacobi sweeps;
+        each application whose ||r - A z|| exceeds fallback_ratio ||r|| is recomputed by the plain
+        cycle on the device (fx_cdmg_set_learned).  None switches it off."""
+        self._lsm = smoother
+        check(L.lib().fx_cdmg_set_learned(self.h, smoother.h if smoother is not None else None, int(min_points),
+                                          float(fallback_ratio)))
+
+    def learned_stats(self):
+        """(checked applications, fallbacks to the plain cycle) so far."""
+        a, f = C.c_ulonglong(), C.c_ulonglong()
+        check(L.lib().fx_cdmg_learned_stats(self.h, C.byref(a), C.byref(f)))
+        return a.value, f.value
+
     def _handle(self, device: Device) -> int:
         return L.lib().fx_cdmg_as_precond(self.h)
 

@@ -102,6 +102,8 @@ typedef struct fx_fgmres fx_fgmres;
 typedef struct fx_op fx_op;
 typedef struct fx_cdmg fx_cdmg;
 typedef struct fx_ir fx_ir;
+typedef struct fx_lsm fx_lsm;
+typedef struct fx_lsm_data fx_lsm_data;
 
 /* ------------------------------------------------------------------ */
 /* Context (HipBackend::new / singleton, backend-hip/src/backend.rs:103-264) */
@@ -466,6 +468,64 @@ int fx_cdmg_set_replay(fx_cdmg *mg, int enabled);
 int fx_cdmg_destroy(fx_cdmg *mg);
 int fx_cdmg_depth(const fx_cdmg *mg, size_t *depth);
 fx_precond *fx_cdmg_as_precond(fx_cdmg *mg);
+/* ------------------------------------------------------------------ */
+/* Learned smoother (new; the reference smooths with weighted Jacobi only, multigrid.rs:245-306).
+ * A 3 -> 16 -> 16 -> 1 network of 3 x 3 convolutions (ReLU after the first two; BF16 weights and
+ * activations, FP32 accumulation and biases; 2913 parameters) corrects the weighted-Jacobi step
+ * of the conv-diff multigrid: with q = (b - A x) / diag(A) (0 on the ring) and s the RMS of q
+ * over the interior, one learned step is x <- x + omega q + s N(q / s, vx / (dx diag), vy / (dy diag))
+ * on the interior, evaluated on the tensor cores.  With the last layer zero (as created) the
+ * step is the Jacobi sweep.  The network is trained on the GPU by the library's own forward,
+ * backward and Adam kernels on samples cut from plain V-cycle iterates: the loss of a sample is
+ * ||H e'||^2 / ||H e||^2, e' the error after the step and H = I - P R the part of an error that
+ * the coarse grid cannot represent (full weighting R, bilinear P).
+ * ------------------------------------------------------------------ */
+int fx_lsm_param_count(size_t *n);  /* 2913 */
+/* Parameters W1[16][3][9], b1[16], W2[16][16][9], b2[16], W3[16][9], b3: He-normal W1, W2 from
+ * `seed`, zero biases, zero last layer. */
+int fx_lsm_create(fx_ctx *ctx, unsigned long long seed, fx_lsm **out);
+int fx_lsm_destroy(fx_lsm *m);
+/* FP32 master parameters in the order above (set also resets the optimiser state). */
+int fx_lsm_get_params(fx_lsm *m, float *dst, size_t n);
+int fx_lsm_set_params(fx_lsm *m, const float *src, size_t n);
+/* `steps` learned smoothing steps on op's grid: x (in/out) and b are F64 fields of the grid;
+ * the operator's fields must be F64.  Synchronises. */
+int fx_lsm_smooth(fx_lsm *m, const fx_op *op, fx_buf *x, const fx_buf *b, double omega, size_t steps);
+/* Training samples on the device, up to `capacity` of them.  A sample is a 16 x 16 loss patch
+ * whose first point (row, col) is even: the network inputs over the 25 x 25 region from
+ * (row - 4, col - 4) (BF16, channel-major), the target t = (H e - omega H q) / s over the patch
+ * and n = ||H e||^2 / s^2 (FP32). */
+int fx_lsm_data_create(fx_ctx *ctx, size_t capacity, fx_lsm_data **out);
+int fx_lsm_data_destroy(fx_lsm_data *d);
+int fx_lsm_data_size(const fx_lsm_data *d, size_t *n);
+/* Samples from an iterate x with error e for A u = b: one per (row, col) pair in origins[2 count]
+ * (even, with 4 <= row <= rows - 21 and 4 <= col <= cols - 21); s is the RMS of q over the grid. */
+int fx_lsm_data_add_patches(fx_lsm_data *d, const fx_op *op, const fx_buf *x, const fx_buf *e, const fx_buf *b,
+                            double omega, const int *origins, size_t count);
+/* Samples from the plain V-cycle on A u = b: u is solved to 1e-12 (FGMRES(30) with the conv-diff
+ * V(2,2)-cycle), then from x = 0 `iterates` iterates x <- x + M (b - A x) each give
+ * patches_per_iterate samples at seeded random origins.  *added = samples stored. */
+int fx_lsm_data_add_problem(fx_lsm_data *d, const fx_op *op, const fx_buf *b, size_t iterates,
+                            size_t patches_per_iterate, double omega, unsigned long long seed, size_t *added);
+/* Sample `index` back on the host: inputs[3 * 25 * 25] (the BF16 values, exactly), target[256], norm. */
+int fx_lsm_data_get(const fx_lsm_data *d, size_t index, float *inputs, float *target, float *norm);
+/* Mean loss of the samples indices[0..count) and, when grad is not NULL, its gradient
+ * grad[2913] with respect to the parameters (bitwise reproducible). */
+int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, size_t count, double *loss,
+                     float *grad);
+/* Adam (lr; beta 0.9 / 0.999, eps 1e-8) over `epochs` seeded shuffles of the samples in batches
+ * of `batch`; epoch_loss[e] (may be NULL) = mean sample loss of epoch e, each batch's loss taken
+ * before its step. */
+int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, double lr,
+                 unsigned long long seed, double *epoch_loss);
+/* Learned smoothing in a conv-diff multigrid: every level of at least min_points points except the
+ * coarsest smooths with learned steps in place of the Jacobi sweeps (n_pre and n_post of them).
+ * Each application is checked on the device: when ||r - A z|| > fallback_ratio ||r|| the plain
+ * cycle recomputes z (the flexible solvers accept either).  lsm NULL switches it off; lsm must
+ * outlive the multigrid's use of it.  stats: checked applications and fallbacks so far. */
+int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, double fallback_ratio);
+int fx_cdmg_learned_stats(fx_cdmg *mg, unsigned long long *applications, unsigned long long *fallbacks);
+
 /* BiCGSTAB, GMRES(m) and flexible GMRES(m) on the operator (pc may be NULL): the same loops,
  * recurrences and stop tests as fx_bicgstab_solve*, fx_gmres_solve* and fx_fgmres_solve* */
 int fx_bicgstab_solve_op(fx_bicgstab *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc,
