@@ -303,6 +303,8 @@ def run_batch(args):
                               Grid)
     from fluxion_b200.workloads import poisson_uniform_rhs, stream_velocity
 
+    from fluxion_b200.batch import gather_results, partition_by_points
+
     nu = 1e-2
     lanes = max(1, int(args.lanes))
     mg_dtype = DType.F32 if args.mg_dtype == "f32" else DType.F64
@@ -310,9 +312,21 @@ def run_batch(args):
     k_lo, k_hi = (int(v) for v in args.k_range.split(","))
     ks = rng.integers(k_lo, k_hi + 1, size=args.batch)
     sizes = [int(2 ** k + 1) ** 2 for k in ks]
-    pinned = torch.empty(3 * sum(sizes), dtype=torch.float64, pin_memory=True).numpy()
-    host, off = [], 0
-    for i in range(args.batch):
+    # one process per GPU: each rank solves its share of the problems (split by points), no
+    # data-path exchange; one gather of the per-problem results at the end
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    mine = partition_by_points(sizes, world)[rank]
+    pinned = torch.empty(3 * sum(sizes[i] for i in mine), dtype=torch.float64, pin_memory=True).numpy()
+    host, off = {}, 0
+    for i in mine:
         n = int(2 ** ks[i] - 1)
         vx, vy = stream_velocity(n, SEED + 2 * i)
         arrs = []
@@ -321,11 +335,11 @@ def run_batch(args):
             dst[:] = a.ravel()
             arrs.append(dst)
             off += a.size
-        host.append((n, *arrs, float(np.linalg.norm(arrs[2]))))
-    first_of_size = sorted({int(ks[i]): i for i in reversed(range(args.batch))}.values())
+        host[i] = (n, *arrs, float(np.linalg.norm(arrs[2])))
+    first_of_size = sorted({int(ks[i]): i for i in reversed(mine)}.values())
 
     def make_lane(k):
-        dev = Device.Cuda(0, lane=k)
+        dev = Device.Cuda(local_rank, lane=k)
         stream = torch.cuda.Stream()
         dev.backend().set_stream(stream.cuda_stream)
         dev.backend().set_pdl(args.pdl)
@@ -366,7 +380,7 @@ def run_batch(args):
         for i in first_of_size:
             one(lane, i)
     torch.cuda.synchronize()
-    res = [None] * args.batch
+    res = {}
     nxt = [0]
     mu = threading.Lock()
     errors = []
@@ -377,15 +391,19 @@ def run_batch(args):
             start.wait()
             while True:
                 with mu:
-                    i = nxt[0]
+                    j = nxt[0]
                     nxt[0] += 1
-                if i >= args.batch:
+                if j >= len(mine):
                     return
-                res[i] = one(lane, i)
+                i = mine[j]
+                r = one(lane, i)
+                res[i] = (r[0], int(r[1].iterations), bool(r[1].converged()), r[2], r[3], r[4])
         except Exception as e:  # reported after the join
             errors.append(e)
 
     threads = [threading.Thread(target=work, args=(lane,)) for lane in lane_state]
+    if dist:
+        dist.barrier()
     for t in threads:
         t.start()
     start.wait()
@@ -395,19 +413,32 @@ def run_batch(args):
     wall = time.perf_counter() - t_begin
     if errors:
         raise errors[0]
-    ms = np.array([r[2] for r in res])
-    its = np.array([r[1].iterations for r in res])
-    ok = all(r[1].converged() for r in res)
+    if dist:  # the job's wall time is the slowest rank's; then one gather of the results
+        t = torch.tensor([wall], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall = float(t.item())
+        allres = gather_results(res, args.batch)
+        dist.barrier()
+        dist.destroy_process_group()
+    else:
+        allres = [res[i] for i in range(args.batch)]
+    if rank != 0:
+        return 0
+    res = allres
+    ms = np.array([r[3] for r in res])
+    its = np.array([r[1] for r in res])
+    ok = all(r[2] for r in res)
     print(json.dumps({
         "mode": "batch", "workload": f"convdiff_batch_{args.batch}_k{k_lo}-{k_hi}_nu1e-2_bicgstab_cdmg",
-        "problems": args.batch, "lanes": lanes, "pdl": bool(args.pdl), "vcycle_dtype": args.mg_dtype, "vcycle_replay": bool(args.replay),
+        "problems": args.batch, "n_gpus": world, "scaling": "strong", "lanes": lanes, "pdl": bool(args.pdl),
+        "vcycle_dtype": args.mg_dtype, "vcycle_replay": bool(args.replay),
         "interior_sizes": {str(2 ** k - 1): int((ks == k).sum()) for k in range(k_lo, k_hi + 1)},
         "solves_per_s": args.batch / wall, "wall_s_excluding_host_data_generation": wall,
-        "per_problem_ms_p50": float(np.percentile([r[4] * 1e3 for r in res], 50)),
-        "per_problem_ms_p99": float(np.percentile([r[4] * 1e3 for r in res], 99)),
+        "per_problem_ms_p50": float(np.percentile([r[5] * 1e3 for r in res], 50)),
+        "per_problem_ms_p99": float(np.percentile([r[5] * 1e3 for r in res], 99)),
         "solve_ms_p50": float(np.percentile(ms, 50)), "solve_ms_p99": float(np.percentile(ms, 99)),
         "iterations_p50": float(np.percentile(its, 50)), "iterations_max": int(its.max()),
-        "all_converged": ok, "max_true_rel_residual": max(r[3] for r in res),
+        "all_converged": ok, "max_true_rel_residual": max(r[4] for r in res),
         "dtype": "f64" if args.mg_dtype == "f64" else "f64 (Krylov) / f32 (V-cycle)",
         "data": "synthetic (seeded per problem), page-locked host arrays",
         "note": f"{lanes} host thread(s), one context and stream each, through the public API; "
