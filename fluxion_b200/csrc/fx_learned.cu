@@ -30,10 +30,10 @@ constexpr int kSmIn = kIn * kPin * kPin;   // 1875
 constexpr int kSmA1 = kC * kP1 * kP1;      // 8464: a1, later the gradient at a1's pre-activation
 constexpr int kSmA2 = kC * kP2 * kP2;      // 7056: a2, later the gradient at a2's pre-activation
 constexpr int kSmC = kP3 * kP3;            // 361: network output c, later dL/dc
-constexpr int kSmG = kT * kT;              // 256: dL/d(Hc)
+constexpr int kSmG = kT * kT;              // 256: dL/d(Hc), then 256: the whole-error part of dL/dc
 constexpr int kSmR = kNCo * kNCo;          // 81: R c, later P^T dL/d(Hc)
 constexpr int kSmW = kNParams;             // parameters (weights BF16-rounded)
-constexpr int kSmTrain = (kSmIn + kSmA1 + kSmA2 + 2 * kSmC + kSmG + kSmR + kSmW + 32) * 4;
+constexpr int kSmTrain = (kSmIn + kSmA1 + kSmA2 + 2 * kSmC + 2 * kSmG + kSmR + kSmW + 32) * 4;
 
 // R at coarse point (I, J) of a field over the output region [-1, 17]^2 (index offset 1)
 __device__ __forceinline__ float fw19(const float *f, int I, int J) {
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(kTrThreads) k_lsm_train(const float *__restric
                                                           const __nv_bfloat16 *__restrict__ in_all,
                                                           const float *__restrict__ tgt_all,
                                                           const float *__restrict__ norm_all,
-                                                          const int *__restrict__ idx, int count,
+                                                          const int *__restrict__ idx, int count, float lambda,
                                                           float *__restrict__ part) {
     extern __shared__ __align__(16) float tsm[];
     float *S_in = tsm;
@@ -70,7 +70,8 @@ __global__ void __launch_bounds__(kTrThreads) k_lsm_train(const float *__restric
     float *S_c = S_a2 + kSmA2;
     float *S_gc = S_c + kSmC;
     float *S_gh = S_gc + kSmC;
-    float *S_r = S_gh + kSmG;
+    float *S_ge = S_gh + kSmG;
+    float *S_r = S_ge + kSmG;
     float *S_w = S_r + kSmR;
     float *S_red = S_w + kSmW;
     const int tid = threadIdx.x;
@@ -84,8 +85,9 @@ __global__ void __launch_bounds__(kTrThreads) k_lsm_train(const float *__restric
     for (int sidx = blockIdx.x; sidx < count; sidx += gridDim.x) {
         const int s = idx[sidx];
         const __nv_bfloat16 *in = in_all + (size_t)s * kInLen;
-        const float *tgt = tgt_all + (size_t)s * kTgtLen;
-        const float inv_n = norm_all[s] > 0.f ? 1.f / norm_all[s] : 0.f;
+        const float *tgt = tgt_all + (size_t)s * kTgtLen;  // tH [256], tE [256]
+        const float nrm = norm_all[2 * s] + lambda * norm_all[2 * s + 1];
+        const float inv_n = nrm > 0.f ? 1.f / nrm : 0.f;
         for (int k = tid; k < kSmIn; k += kTrThreads) S_in[k] = __bfloat162float(in[k]);
         __syncthreads();
         // ---- forward
@@ -126,14 +128,17 @@ __global__ void __launch_bounds__(kTrThreads) k_lsm_train(const float *__restric
         __syncthreads();
         for (int o = tid; o < kSmR; o += kTrThreads) S_r[o] = fw19(S_c, o / kNCo, o % kNCo);
         __syncthreads();
-        // ---- loss and dL/d(Hc) = -2 (t - Hc) / n
+        // ---- loss; dL/d(Hc) = -2 (tH - Hc) / n and the whole-error part -2 lambda (tE - c) / n
         float lsum = 0.f;
         for (int o = tid; o < kT * kT; o += kTrThreads) {
             const int py = o / kT, px = o - py * kT;
-            const float hc = S_c[(py + 1) * kP3 + px + 1] - bil9(S_r, py, px);
-            const float u = tgt[o] - hc;
+            const float cv = S_c[(py + 1) * kP3 + px + 1];
+            const float u = tgt[o] - (cv - bil9(S_r, py, px));
+            const float w = tgt[kT * kT + o] - cv;
             lsum = fmaf(u, u, lsum);
+            lsum = fmaf(lambda * w, w, lsum);
             S_gh[o] = -2.f * u * inv_n;
+            S_ge[o] = -2.f * lambda * w * inv_n;
         }
         // block sum of lsum: warp shuffles, then the 8 warp partials (the barrier also publishes
         // S_gh and ends the previous sample's reads of S_red)
@@ -163,7 +168,7 @@ __global__ void __launch_bounds__(kTrThreads) k_lsm_train(const float *__restric
         for (int o = tid; o < kP3 * kP3; o += kTrThreads) {  // dL/dc over [-1, 17]^2
             const int y = o / kP3, x = o - y * kP3;
             const int ly = y - 1, lx = x - 1;  // loss coordinates
-            float g = (ly >= 0 && lx >= 0 && ly < kT && lx < kT) ? S_gh[ly * kT + lx] : 0.f;
+            float g = (ly >= 0 && lx >= 0 && ly < kT && lx < kT) ? S_gh[ly * kT + lx] + S_ge[ly * kT + lx] : 0.f;
             for (int I = (ly - 1 + 1) >> 1; I <= (ly + 1) >> 1; I++) {
                 if (I < 0 || I >= kNCo || 2 * I < ly - 1 || 2 * I > ly + 1) continue;
                 for (int J = (lx - 1 + 1) >> 1; J <= (lx + 1) >> 1; J++) {
@@ -348,7 +353,7 @@ int fx_lsm::pack() {
 namespace fx {
 
 // The summed gradient and loss of the samples h_idx[0..count) -> m->d_grad (asynchronous).
-int lsm_batch_grad(fx_lsm *m, const fx_lsm_data *d, const int *h_idx, size_t count) {
+int lsm_batch_grad(fx_lsm *m, const fx_lsm_data *d, const int *h_idx, size_t count, float lambda) {
     fx_ctx *ctx = m->ctx;
     if (count == 0) return fail(FX_ERR_INVALID_ARGUMENT, "empty batch");
     for (size_t i = 0; i < count; i++)
@@ -364,7 +369,7 @@ int lsm_batch_grad(fx_lsm *m, const fx_lsm_data *d, const int *h_idx, size_t cou
     const int blocks = (int)std::min<size_t>(count, (size_t)m->part_blocks);
     timing_pre(ctx, "lsm_train");
     k_lsm_train<<<blocks, kTrThreads, kSmTrain, ctx->stream>>>(m->d_wq, d->d_in, d->d_tgt, d->d_norm, m->d_idx,
-                                                               (int)count, m->d_part);
+                                                               (int)count, lambda, m->d_part);
     timing_post(ctx, (double)count);
     FX_TRY(check_launch(ctx, "lsm_train"));
     k_lsm_reduce<<<(kNParams + 1 + 255) / 256, 256, 0, ctx->stream>>>(m->d_part, blocks, m->d_grad);
@@ -467,7 +472,7 @@ int fx_lsm_data_create(fx_ctx *ctx, size_t capacity, fx_lsm_data **out) {
     d->cap = capacity;
     if (cudaMalloc(&d->d_in, capacity * kInLen * sizeof(__nv_bfloat16)) != cudaSuccess ||
         cudaMalloc(&d->d_tgt, capacity * kTgtLen * 4) != cudaSuccess ||
-        cudaMalloc(&d->d_norm, capacity * 4) != cudaSuccess) {
+        cudaMalloc(&d->d_norm, capacity * 2 * 4) != cudaSuccess) {
         (void)cudaGetLastError();
         if (d->d_in) cudaFree(d->d_in);
         if (d->d_tgt) cudaFree(d->d_tgt);
@@ -503,7 +508,7 @@ int fx_lsm_data_get(const fx_lsm_data *d, size_t index, float *inputs, float *ta
     cudaStream_t s = d->ctx->stream;
     FX_CUDA(cudaMemcpyAsync(b.data(), d->d_in + index * kInLen, kInLen * 2, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaMemcpyAsync(target, d->d_tgt + index * kTgtLen, kTgtLen * 4, cudaMemcpyDeviceToHost, s));
-    FX_CUDA(cudaMemcpyAsync(norm, d->d_norm + index, 4, cudaMemcpyDeviceToHost, s));
+    FX_CUDA(cudaMemcpyAsync(norm, d->d_norm + 2 * index, 8, cudaMemcpyDeviceToHost, s));
     FX_CUDA(cudaStreamSynchronize(s));
     for (int k = 0; k < kInLen; k++) {  // BF16 -> FP32 is exact: the high half of the word
         uint16_t u;
@@ -514,8 +519,8 @@ int fx_lsm_data_get(const fx_lsm_data *d, size_t index, float *inputs, float *ta
     return FX_OK;
 }
 
-int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, size_t count, double *loss,
-                     float *grad) {
+int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, size_t count, double lambda,
+                     double *loss, float *grad) {
     if (!m || !d || !indices || !loss) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     if (d->ctx->device != m->ctx->device) return fail(FX_ERR_INVALID_ARGUMENT, "samples on another device");
     std::vector<int> idx(count);
@@ -523,7 +528,8 @@ int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, siz
         if (indices[i] >= d->count) return fail(FX_ERR_INVALID_ARGUMENT, "sample index out of range");
         idx[i] = (int)indices[i];
     }
-    FX_TRY(lsm_batch_grad(m, d, idx.data(), count));
+    if (!(lambda >= 0.0)) return fail(FX_ERR_INVALID_ARGUMENT, "lambda must be non-negative");
+    FX_TRY(lsm_batch_grad(m, d, idx.data(), count, (float)lambda));
     std::vector<float> g(kNParams + 1);
     FX_CUDA(cudaMemcpyAsync(g.data(), m->d_grad, (kNParams + 1) * 4, cudaMemcpyDeviceToHost, m->ctx->stream));
     FX_CUDA(cudaStreamSynchronize(m->ctx->stream));
@@ -533,9 +539,10 @@ int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, siz
     return FX_OK;
 }
 
-int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, double lr,
+int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, double lr, double lambda,
                  unsigned long long seed, double *epoch_loss) {
     if (!m || !d) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (!(lambda >= 0.0)) return fail(FX_ERR_INVALID_ARGUMENT, "lambda must be non-negative");
     if (d->count == 0 || batch == 0) return fail(FX_ERR_INVALID_ARGUMENT, "no samples or zero batch");
     if (!(lr > 0.0)) return fail(FX_ERR_INVALID_ARGUMENT, "learning rate must be positive");
     fx_ctx *ctx = m->ctx;
@@ -553,7 +560,7 @@ int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, d
     for (size_t e = 0; e < epochs && st == FX_OK; e++) {
         std::shuffle(order.begin(), order.end(), rng);
         for (size_t k = 0; k < steps && st == FX_OK; k++) {
-            st = lsm_batch_grad(m, d, order.data() + k * batch, batch);
+            st = lsm_batch_grad(m, d, order.data() + k * batch, batch, (float)lambda);
             if (st != FX_OK) break;
             m->adam_t++;
             const float c1 = 1.f - (float)std::pow((double)b1, (double)m->adam_t);

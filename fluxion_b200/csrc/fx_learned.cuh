@@ -17,9 +17,12 @@
 // Training target (one sample = a 16 x 16 patch of a plain V-cycle iterate's residual and
 // error, with the network's input halo): the error after the step, e' = e - omega q - s c,
 // measured by its part that the coarse grid cannot represent, H e' with H = I - P R (R full
-// weighting onto the even points, P bilinear interpolation back).  Per sample
-//   loss = || H e' ||^2 / || H e ||^2 = || t - H c ||^2 / n,
-//   t = (H e - omega H q) / s on the patch, n = || H e ||^2 / s^2,
+// weighting onto the even points, P bilinear interpolation back), plus lambda times the whole
+// error (a smoother must not add error that is smooth, which H alone would not see).  Per sample
+//   loss = (|| H e' ||^2 + lambda || e' ||^2) / (|| H e ||^2 + lambda || e ||^2)
+//        = (|| tH - H c ||^2 + lambda || tE - c ||^2) / (nH + lambda nE),
+//   tH = (H e - omega H q) / s, tE = (e - omega q) / s on the patch, nH = ||H e||^2 / s^2,
+//   nE = ||e||^2 / s^2,
 // so the untrained network (c = 0) scores the Jacobi step's loss.
 #pragma once
 
@@ -50,7 +53,7 @@ constexpr int kP2 = kT + 5;    // 21: second hidden layer on [-2, 18]^2
 constexpr int kP3 = kT + 3;    // 19: network output on [-1, 17]^2 (what H needs)
 constexpr int kNCo = kT / 2 + 1;  // 9 coarse points per side, at loss coordinates 0, 2, .., 16
 constexpr int kInLen = kIn * kPin * kPin;  // 1875 BF16 values per sample
-constexpr int kTgtLen = kT * kT;           // 256
+constexpr int kTgtLen = 2 * kT * kT;       // tH then tE, 256 each
 
 // packed BF16 operand fragments of the three convolutions for mma.m16n8k16 (32-bit words):
 // conv1 [kstep 3][n-half 2][lane 32][2], conv2 [tap 9][n-half 2][lane 32][2], conv3 [tap 9][lane 32][2]
@@ -319,11 +322,11 @@ struct fx_lsm_data {
     fx_ctx *ctx = nullptr;
     size_t cap = 0, count = 0;
     __nv_bfloat16 *d_in = nullptr;  // [cap][3][25][25]
-    float *d_tgt = nullptr;         // [cap][16][16]
-    float *d_norm = nullptr;        // [cap]
+    float *d_tgt = nullptr;         // [cap][2][16][16]: tH, tE
+    float *d_norm = nullptr;        // [cap][2]: nH, nE
 };
 
 namespace fx {
 // training-side entry points of fx_learned.cu used by the operator code in fx_solvers.cu
-int lsm_batch_grad(fx_lsm *m, const fx_lsm_data *d, const int *h_idx, size_t count);  // -> m->d_grad
+int lsm_batch_grad(fx_lsm *m, const fx_lsm_data *d, const int *h_idx, size_t count, float lambda);  // -> m->d_grad
 }  // namespace fx

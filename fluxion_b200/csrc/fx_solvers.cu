@@ -2375,7 +2375,7 @@ __global__ void __launch_bounds__(256) k_lsm_extract(Op A, const double *__restr
                                                      float *d_tgt, float *d_norm, int rows, int cols, double inv_dx,
                                                      double inv_dy) {
     using namespace lsm;
-    __shared__ double se[kP3 * kP3], sq[kP3 * kP3], re[kNCo * kNCo], rq[kNCo * kNCo], red[8];
+    __shared__ double se[kP3 * kP3], sq[kP3 * kP3], re[kNCo * kNCo], rq[kNCo * kNCo], red[16];
     const int tid = threadIdx.x;
     const int y0 = origins[2 * blockIdx.x], x0 = origins[2 * blockIdx.x + 1];
     const double inv_s = scale[1];
@@ -2409,7 +2409,7 @@ __global__ void __launch_bounds__(256) k_lsm_extract(Op A, const double *__restr
         }
     }
     __syncthreads();
-    double nsum = 0.0;
+    double nsum = 0.0, esum = 0.0;
     for (int k = tid; k < kT * kT; k += 256) {
         const int py = k / kT, px = k - py * kT;
         const int I = py >> 1, J = px >> 1;
@@ -2432,15 +2432,27 @@ __global__ void __launch_bounds__(256) k_lsm_extract(Op A, const double *__restr
         const int c = (py + 1) * kP3 + px + 1;
         const double he = se[c] - pe, hq = sq[c] - pq;
         d_tgt[(size_t)blockIdx.x * kTgtLen + k] = (float)((he - omega * hq) * inv_s);
+        d_tgt[(size_t)blockIdx.x * kTgtLen + kT * kT + k] = (float)((se[c] - omega * sq[c]) * inv_s);
         nsum += he * he;
+        esum += se[c] * se[c];
     }
-    for (int off = 16; off > 0; off >>= 1) nsum += __shfl_down_sync(0xffffffffu, nsum, off);
-    if ((tid & 31) == 0) red[tid >> 5] = nsum;
+    for (int off = 16; off > 0; off >>= 1) {
+        nsum += __shfl_down_sync(0xffffffffu, nsum, off);
+        esum += __shfl_down_sync(0xffffffffu, esum, off);
+    }
+    if ((tid & 31) == 0) {
+        red[tid >> 5] = nsum;
+        red[8 + (tid >> 5)] = esum;
+    }
     __syncthreads();
     if (tid == 0) {
-        double t = 0.0;
-        for (int w = 0; w < 8; w++) t += red[w];
-        d_norm[blockIdx.x] = (float)(t * inv_s * inv_s);
+        double t = 0.0, te = 0.0;
+        for (int w = 0; w < 8; w++) {
+            t += red[w];
+            te += red[8 + w];
+        }
+        d_norm[2 * blockIdx.x] = (float)(t * inv_s * inv_s);
+        d_norm[2 * blockIdx.x + 1] = (float)(te * inv_s * inv_s);
     }
 }
 
@@ -3753,7 +3765,7 @@ int fx_lsm_data_add_patches(fx_lsm_data *d, const fx_op *op, const fx_buf *x, co
     if (st == FX_OK) {
         k_lsm_extract<LsmOp<double>><<<(unsigned)count, 256, 0, ctx->stream>>>(
             LsmOp<double>{A}, (const double *)q->ptr, (const double *)e->ptr, scale, omega, d_orig,
-            d->d_in + d->count * kInLen, d->d_tgt + d->count * kTgtLen, d->d_norm + d->count, (int)rows, (int)cols,
+            d->d_in + d->count * kInLen, d->d_tgt + d->count * kTgtLen, d->d_norm + 2 * d->count, (int)rows, (int)cols,
             1.0 / op->g.dx, 1.0 / op->g.dy);
         st = check_launch(ctx, "lsm_extract");
     }

@@ -7,7 +7,7 @@ q = (b - A x) / diag(A) and s the RMS of q over the interior, one learned step i
 x <- x + omega q + s N(q / s, vx / (dx diag), vy / (dy diag)).  Its network runs on the tensor
 cores; it is trained on the GPU by the library's forward, backward and Adam kernels on samples
 cut from plain V-cycle iterates (`SmootherSamples.add_problem`), with the loss
-||H e'||^2 / ||H e||^2 of the error e' after the step, H = I - P R.  A `ConvDiffMultigrid` uses it
+(||H e'||^2 + lam ||e'||^2) / (||H e||^2 + lam ||e||^2) of the error e' after the step, H = I - P R.  A `ConvDiffMultigrid` uses it
 through `set_learned`, with a per-application residual check that falls back to the plain cycle.
 """
 from __future__ import annotations
@@ -23,6 +23,7 @@ from .field import Device, Field
 
 IN_SIDE = 25   # network input region of a sample (points per side)
 PATCH = 16     # loss patch of a sample
+DEFAULT_LAMBDA = 1.0  # weight of the whole error beside its high-frequency part in the loss
 
 
 def param_count() -> int:
@@ -61,13 +62,15 @@ class SmootherSamples:
         return n.value
 
     def get(self, index: int):
-        """(inputs [3, 25, 25], target [16, 16], norm) of one sample, as float32 numpy values."""
+        """(inputs [3, 25, 25], tH [16, 16], tE [16, 16], nH, nE) of one sample, float32 values."""
         inp = np.empty(3 * IN_SIDE * IN_SIDE, dtype=np.float32)
-        tgt = np.empty(PATCH * PATCH, dtype=np.float32)
-        nrm = C.c_float()
+        tgt = np.empty(2 * PATCH * PATCH, dtype=np.float32)
+        nrm = np.empty(2, dtype=np.float32)
         check(L.lib().fx_lsm_data_get(self.h, int(index), inp.ctypes.data_as(C.POINTER(C.c_float)),
-                                      tgt.ctypes.data_as(C.POINTER(C.c_float)), C.byref(nrm)))
-        return inp.reshape(3, IN_SIDE, IN_SIDE), tgt.reshape(PATCH, PATCH), float(nrm.value)
+                                      tgt.ctypes.data_as(C.POINTER(C.c_float)),
+                                      nrm.ctypes.data_as(C.POINTER(C.c_float))))
+        t = tgt.reshape(2, PATCH, PATCH)
+        return inp.reshape(3, IN_SIDE, IN_SIDE), t[0], t[1], float(nrm[0]), float(nrm[1])
 
     def __del__(self):
         try:
@@ -98,21 +101,23 @@ class LearnedSmoother:
         p = np.ascontiguousarray(p, dtype=np.float32)
         check(L.lib().fx_lsm_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
 
-    def loss_grad(self, samples: SmootherSamples, indices: Sequence[int], want_grad: bool = True):
-        """(mean loss, gradient of the mean loss or None) over the given samples."""
+    def loss_grad(self, samples: SmootherSamples, indices: Sequence[int], want_grad: bool = True,
+                  lam: float = DEFAULT_LAMBDA):
+        """(mean loss with whole-error weight `lam`, its gradient or None) over the given samples."""
         idx = np.ascontiguousarray(np.asarray(indices, dtype=np.uint64))
         loss = C.c_double()
         g = np.empty(param_count(), dtype=np.float32) if want_grad else None
         check(L.lib().fx_lsm_loss_grad(self.h, samples.h, idx.ctypes.data_as(C.POINTER(C.c_size_t)), idx.size,
-                                       C.byref(loss),
+                                       float(lam), C.byref(loss),
                                        g.ctypes.data_as(C.POINTER(C.c_float)) if g is not None else None))
         return loss.value, g
 
     def train(self, samples: SmootherSamples, epochs: int, batch: int = 256, lr: float = 2e-3,
-              seed: int = 0) -> List[float]:
+              seed: int = 0, lam: float = DEFAULT_LAMBDA) -> List[float]:
         """Adam over `epochs` shuffles; returns the mean sample loss of each epoch."""
         out = (C.c_double * max(1, int(epochs)))()
-        check(L.lib().fx_lsm_train(self.h, samples.h, int(epochs), int(batch), float(lr), int(seed), out))
+        check(L.lib().fx_lsm_train(self.h, samples.h, int(epochs), int(batch), float(lr), float(lam), int(seed),
+                                   out))
         return [out[i] for i in range(int(epochs))]
 
     def smooth(self, op, x: Field, b: Field, omega: float = 0.8, steps: int = 1) -> None:

@@ -478,7 +478,8 @@ fx_precond *fx_cdmg_as_precond(fx_cdmg *mg);
  * step is the Jacobi sweep.  The network is trained on the GPU by the library's own forward,
  * backward and Adam kernels on samples cut from plain V-cycle iterates: the loss of a sample is
  * ||H e'||^2 / ||H e||^2, e' the error after the step and H = I - P R the part of an error that
- * the coarse grid cannot represent (full weighting R, bilinear P).
+ * the coarse grid cannot represent (full weighting R, bilinear P), plus lambda ||e'||^2 / ||e||^2
+ * (both parts normalised by the Jacobi-free denominator ||H e||^2 + lambda ||e||^2).
  * ------------------------------------------------------------------ */
 int fx_lsm_param_count(size_t *n);  /* 2913 */
 /* Parameters W1[16][3][9], b1[16], W2[16][16][9], b2[16], W3[16][9], b3: He-normal W1, W2 from
@@ -493,8 +494,8 @@ int fx_lsm_set_params(fx_lsm *m, const float *src, size_t n);
 int fx_lsm_smooth(fx_lsm *m, const fx_op *op, fx_buf *x, const fx_buf *b, double omega, size_t steps);
 /* Training samples on the device, up to `capacity` of them.  A sample is a 16 x 16 loss patch
  * whose first point (row, col) is even: the network inputs over the 25 x 25 region from
- * (row - 4, col - 4) (BF16, channel-major), the target t = (H e - omega H q) / s over the patch
- * and n = ||H e||^2 / s^2 (FP32). */
+ * (row - 4, col - 4) (BF16, channel-major); over the patch the targets tH = (H e - omega H q) / s
+ * and tE = (e - omega q) / s; and nH = ||H e||^2 / s^2, nE = ||e||^2 / s^2 (FP32). */
 int fx_lsm_data_create(fx_ctx *ctx, size_t capacity, fx_lsm_data **out);
 int fx_lsm_data_destroy(fx_lsm_data *d);
 int fx_lsm_data_size(const fx_lsm_data *d, size_t *n);
@@ -507,16 +508,17 @@ int fx_lsm_data_add_patches(fx_lsm_data *d, const fx_op *op, const fx_buf *x, co
  * patches_per_iterate samples at seeded random origins.  *added = samples stored. */
 int fx_lsm_data_add_problem(fx_lsm_data *d, const fx_op *op, const fx_buf *b, size_t iterates,
                             size_t patches_per_iterate, double omega, unsigned long long seed, size_t *added);
-/* Sample `index` back on the host: inputs[3 * 25 * 25] (the BF16 values, exactly), target[256], norm. */
+/* Sample `index` back on the host: inputs[3 * 25 * 25] (the BF16 values, exactly), target[512]
+ * (tH then tE), norm[2] (nH, nE). */
 int fx_lsm_data_get(const fx_lsm_data *d, size_t index, float *inputs, float *target, float *norm);
-/* Mean loss of the samples indices[0..count) and, when grad is not NULL, its gradient
- * grad[2913] with respect to the parameters (bitwise reproducible). */
-int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, size_t count, double *loss,
-                     float *grad);
-/* Adam (lr; beta 0.9 / 0.999, eps 1e-8) over `epochs` seeded shuffles of the samples in batches
- * of `batch`; epoch_loss[e] (may be NULL) = mean sample loss of epoch e, each batch's loss taken
- * before its step. */
-int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, double lr,
+/* Mean loss (weight lambda >= 0 on the whole error) of the samples indices[0..count) and, when
+ * grad is not NULL, its gradient grad[2913] with respect to the parameters (bitwise reproducible). */
+int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, size_t count, double lambda,
+                     double *loss, float *grad);
+/* Adam (lr; beta 0.9 / 0.999, eps 1e-8) on the loss with weight lambda, over `epochs` seeded
+ * shuffles of the samples in batches of `batch`; epoch_loss[e] (may be NULL) = mean sample loss of
+ * epoch e, each batch's loss taken before its step. */
+int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, double lr, double lambda,
                  unsigned long long seed, double *epoch_loss);
 /* Learned smoothing in a conv-diff multigrid: every level of at least min_points points except the
  * coarsest smooths with learned steps in place of the Jacobi sweeps (n_pre and n_post of them).

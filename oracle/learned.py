@@ -11,8 +11,8 @@ of the network and the loss, so that the GPU forward, backward and sample kernel
 - network: a1 = bf16(relu(conv(x, W1) + b1)), a2 = bf16(relu(conv(a1, W2) + b2)),
   c = conv(a2, W3) + b3 (cross-correlation, 3 x 3); the BF16 roundings pass gradients straight
   through, as the GPU backward does;
-- loss of a sample: ||t - H c||^2 / n over the 16 x 16 patch, H c = c - P R c with R full
-  weighting onto the even points and P bilinear interpolation.
+- loss of a sample: (||tH - H c||^2 + lam ||tE - c||^2) / (nH + lam nE) over the 16 x 16 patch,
+  H c = c - P R c with R full weighting onto the even points and P bilinear interpolation.
 """
 from __future__ import annotations
 
@@ -88,17 +88,19 @@ def h_apply(c: torch.Tensor) -> torch.Tensor:
     return c[:, 1:17, 1:17] - _bilinear(_fw(c))
 
 
-def loss_and_grad(params, inputs, targets, norms):
-    """Mean sample loss and its gradient (flat, FP64) for inputs [B, 3, 25, 25], targets [B, 16, 16],
-    norms [B]."""
+def loss_and_grad(params, inputs, t_h, t_e, n_h, n_e, lam):
+    """Mean sample loss and its gradient (flat, FP64) for inputs [B, 3, 25, 25], targets tH, tE
+    [B, 16, 16], norms nH, nE [B] and whole-error weight lam."""
     ps = [t.clone().requires_grad_(True) for t in unpack(params)]
     x = torch.as_tensor(np.asarray(inputs, dtype=np.float64))
-    t = torch.as_tensor(np.asarray(targets, dtype=np.float64))
-    n = torch.as_tensor(np.asarray(norms, dtype=np.float64))
+    th = torch.as_tensor(np.asarray(t_h, dtype=np.float64))
+    te = torch.as_tensor(np.asarray(t_e, dtype=np.float64))
+    n = torch.as_tensor(np.asarray(n_h, dtype=np.float64) + lam * np.asarray(n_e, dtype=np.float64))
     c = network(ps, x)[:, 0]
-    u = t - h_apply(c)
+    u = th - h_apply(c)
+    w = te - c[:, 1:17, 1:17]
     inv = torch.where(n > 0, 1.0 / n, torch.zeros_like(n))
-    loss = ((u * u).sum(dim=(1, 2)) * inv).mean()
+    loss = (((u * u).sum(dim=(1, 2)) + lam * (w * w).sum(dim=(1, 2))) * inv).mean()
     loss.backward()
     return float(loss.detach()), flatten([p.grad for p in ps])
 
@@ -122,8 +124,8 @@ def to_bf16(a: np.ndarray) -> np.ndarray:
 
 
 def extract(q, e, vx, vy, d, s, omega, dx, dy, y0, x0):
-    """One sample (inputs [3, 25, 25] as BF16 values, target [16, 16], norm) at loss origin (y0, x0)
-    of grids q, e, vx, vy, d [rows, cols] (FP64)."""
+    """One sample (inputs [3, 25, 25] as BF16 values, tH, tE [16, 16], nH, nE) at loss origin
+    (y0, x0) of grids q, e, vx, vy, d [rows, cols] (FP64)."""
     inp = to_bf16(inputs_of(q, vx, vy, d, s, dx, dy)[:, y0 - 4:y0 + 21, x0 - 4:x0 + 21])
     inv_s = 1.0 / s if s > 0 else 0.0
 
@@ -132,7 +134,9 @@ def extract(q, e, vx, vy, d, s, omega, dx, dy, y0, x0):
         return h_apply(c)[0].numpy()
 
     he, hq = hh(e), hh(q)
-    return inp, (he - omega * hq) * inv_s, float(np.sum(he * he) * inv_s * inv_s)
+    ep, qp = e[y0:y0 + T, x0:x0 + T], q[y0:y0 + T, x0:x0 + T]
+    return (inp, (he - omega * hq) * inv_s, (ep - omega * qp) * inv_s, float(np.sum(he * he) * inv_s * inv_s),
+            float(np.sum(ep * ep) * inv_s * inv_s))
 
 
 def smooth_step(params, x, b_minus_ax_over_d, vx, vy, d, omega, dx, dy):

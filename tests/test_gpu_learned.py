@@ -133,13 +133,14 @@ def test_samples_match_oracle(dev):
     q, d = _q_grid(oop, x0.ravel(), f, vx, vy, nu, h, N)
     s = float(np.sqrt(np.sum(q[1:-1, 1:-1] ** 2) / (n * n)))
     for k, (y0, x0_) in enumerate(origins):
-        inp, tgt, nrm = S.get(k)
-        wi, wt, wn = OL.extract(q, e0, vx.reshape(N, N), vy.reshape(N, N), d, s, omega, h, h, y0, x0_)
+        inp, th, te, nh, ne = S.get(k)
+        wi, wth, wte, wnh, wne = OL.extract(q, e0, vx.reshape(N, N), vy.reshape(N, N), d, s, omega, h, h, y0, x0_)
         # BF16 inputs: equal, or one BF16 step apart where FP64 rounding differs at a boundary
         assert np.all(np.abs(inp - wi) <= 2.0 ** -7 * np.abs(wi) + 1e-30)
         assert np.mean(inp == wi) > 0.99
-        assert rel_err(tgt.ravel().astype(np.float64), wt.ravel()) < 1e-6
-        assert abs(nrm - wn) <= 1e-6 * wn
+        assert rel_err(th.ravel().astype(np.float64), wth.ravel()) < 1e-6
+        assert rel_err(te.ravel().astype(np.float64), wte.ravel()) < 1e-6
+        assert abs(nh - wnh) <= 1e-6 * wnh and abs(ne - wne) <= 1e-6 * wne
 
 
 def test_loss_and_gradient_match_oracle(dev):
@@ -152,17 +153,18 @@ def test_loss_and_gradient_match_oracle(dev):
     lsm = LearnedSmoother(dev, seed=5)
     params = _random_params(lsm, 6)
     idx = list(range(24))
-    loss, grad = lsm.loss_grad(S, idx)
     data = [S.get(i) for i in idx]
-    wl, wg = OL.loss_and_grad(params, np.stack([d[0] for d in data]), np.stack([d[1] for d in data]),
-                              np.array([d[2] for d in data]))
-    assert abs(loss - wl) <= 1e-4 * wl
-    assert rel_err(grad.astype(np.float64), wg) < 2e-3
-    # every layer's gradient is live, and the same batch gives the same bits
-    for lo, hi in ((0, 432), (448, 2752), (2768, 2912)):
-        assert np.linalg.norm(wg[lo:hi]) > 0 and rel_err(grad[lo:hi].astype(np.float64), wg[lo:hi]) < 5e-3
-    l2, g2 = lsm.loss_grad(S, idx)
-    assert l2 == loss and np.array_equal(g2, grad)
+    for lam in (0.0, 1.0):
+        loss, grad = lsm.loss_grad(S, idx, lam=lam)
+        wl, wg = OL.loss_and_grad(params, *(np.stack([d[j] for d in data]) for j in range(3)),
+                                  np.array([d[3] for d in data]), np.array([d[4] for d in data]), lam)
+        assert abs(loss - wl) <= 1e-4 * wl
+        assert rel_err(grad.astype(np.float64), wg) < 2e-3
+        # every layer's gradient is live, and the same batch gives the same bits
+        for lo, hi in ((0, 432), (448, 2752), (2768, 2912)):
+            assert np.linalg.norm(wg[lo:hi]) > 0 and rel_err(grad[lo:hi].astype(np.float64), wg[lo:hi]) < 5e-3
+        l2, g2 = lsm.loss_grad(S, idx, lam=lam)
+        assert l2 == loss and np.array_equal(g2, grad)
 
 
 def test_training_beats_the_jacobi_step_and_learned_fgmres_converges(dev):

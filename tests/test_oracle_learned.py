@@ -23,12 +23,13 @@ def test_untrained_network_scores_the_jacobi_loss():
     p[:432] = rng.normal(0, 0.3, 432)
     p[448:2752] = rng.normal(0, 0.1, 2304)
     inp = OL.to_bf16(rng.uniform(-1, 1, (4, 3, 25, 25)))
-    tgt = rng.normal(size=(4, 16, 16))
-    nrm = np.array([3.0, 1.0, 0.5, 2.0])
-    loss, grad = OL.loss_and_grad(p, inp, tgt, nrm)
-    want = np.mean([(tgt[k] ** 2).sum() / nrm[k] for k in range(4)])
-    assert abs(loss - want) <= 1e-12 * want
-    assert np.all(grad[:2752] == 0) and np.any(grad[2768:] != 0)
+    th, te = rng.normal(size=(4, 16, 16)), rng.normal(size=(4, 16, 16))
+    nh, ne = np.array([3.0, 1.0, 0.5, 2.0]), np.array([1.0, 2.0, 4.0, 0.5])
+    for lam in (0.0, 0.7):
+        loss, grad = OL.loss_and_grad(p, inp, th, te, nh, ne, lam)
+        want = np.mean([((th[k] ** 2).sum() + lam * (te[k] ** 2).sum()) / (nh[k] + lam * ne[k]) for k in range(4)])
+        assert abs(loss - want) <= 1e-12 * want
+        assert np.all(grad[:2752] == 0) and np.any(grad[2768:] != 0)
 
 
 def test_sample_target_definition():
@@ -37,9 +38,11 @@ def test_sample_target_definition():
     q, e = rng.normal(size=(N, N)), rng.normal(size=(N, N))
     vx, vy = rng.normal(size=(N, N)), rng.normal(size=(N, N))
     d = np.abs(rng.normal(size=(N, N))) + 1.0
-    inp, tgt, nrm = OL.extract(q, e, vx, vy, d, 2.0, 0.8, 0.1, 0.1, 10, 12)
+    inp, th, te, nh, ne = OL.extract(q, e, vx, vy, d, 2.0, 0.8, 0.1, 0.1, 10, 12)
     he = OL.h_apply(torch.as_tensor(e[None, 9:28, 11:30].copy()))[0].numpy()
     hq = OL.h_apply(torch.as_tensor(q[None, 9:28, 11:30].copy()))[0].numpy()
-    assert np.allclose(tgt, (he - 0.8 * hq) / 2.0, rtol=0, atol=1e-14)
-    assert abs(nrm - (he ** 2).sum() / 4.0) < 1e-12 * nrm
+    assert np.allclose(th, (he - 0.8 * hq) / 2.0, rtol=0, atol=1e-14)
+    assert np.allclose(te, (e[10:26, 12:28] - 0.8 * q[10:26, 12:28]) / 2.0, rtol=0, atol=1e-14)
+    assert abs(nh - (he ** 2).sum() / 4.0) < 1e-12 * nh
+    assert abs(ne - (e[10:26, 12:28] ** 2).sum() / 4.0) < 1e-12 * ne
     assert inp.shape == (3, 25, 25) and np.array_equal(inp, OL.to_bf16(inp))
