@@ -23,7 +23,10 @@ from .field import Device, Field
 
 IN_SIDE = 25   # network input region of a sample (points per side)
 PATCH = 16     # loss patch of a sample
-DEFAULT_LAMBDA = 1.0  # weight of the whole error beside its high-frequency part in the loss
+# Weight of the whole error beside its high-frequency part in the loss.  0 by default: with a
+# positive weight the network chases the smooth error, which a local correction cannot remove,
+# and the trained cycles diverged (measured at 127^2 - 511^2, nu 1e-2 - 1e-4, weights 0.3 - 10).
+DEFAULT_LAMBDA = 0.0
 
 
 def param_count() -> int:
