@@ -64,7 +64,7 @@ _STRUCTS = {
     "fx_stats": FxStats, "fx_mg_vertex_opts": FxMgVertexOpts, "fx_mg_tuning": FxMgTuning,
 }
 _OPAQUE = {"fx_ctx", "fx_buf", "fx_precond", "fx_mg", "fx_cg", "fx_pipelined_cg", "fx_bicgstab",
-           "fx_gmres", "fx_graph", "fx_ir", "fx_fcg", "fx_fgmres", "fx_op", "fx_cdmg", "fx_lsm", "fx_lsm_data"}
+           "fx_gmres", "fx_graph", "fx_ir", "fx_fcg", "fx_fgmres", "fx_op", "fx_cdmg", "fx_lsm", "fx_lsm_data", "fx_batch"}
 _SCALARS = {
     "int": C.c_int, "size_t": C.c_size_t, "double": C.c_double, "float": C.c_float,
     "unsigned long long": C.c_ulonglong, "void": None, "char": C.c_char,

@@ -56,3 +56,61 @@ def gather_results(local: Dict[int, Any], n_problems: int, group=None) -> List[A
     if missing:
         raise RuntimeError(f"problems without a result: {missing[:8]}")
     return out
+
+
+class BatchSolver:
+    """Many independent steady convection-diffusion problems solved together on one GPU
+    (fx_batch_*; new): -nu Lap u + v.grad u = f (first-order upwind, Dirichlet 0) on square grids of
+    side 2^k + 1, each by right-preconditioned BiCGSTAB with the conv-diff V(2,2)-cycle, every
+    phase one launch over the whole batch (see fx_batch.cu).  Batch vectors are F64 `CudaBuffer`s
+    with every problem's grid one after the other (`offsets`)."""
+
+    def __init__(self, device, grid_sides: Sequence[int], nu: float, vx, vy, cycle_dtype=None,
+                 n_pre: int = 2, n_post: int = 2, omega: float = 0.8, coarse_max: int = 15,
+                 coarse_sweeps: int = 200, sigma: float = 0.0, coeff: float = 1.0):
+        import ctypes as C
+
+        from . import _lib as L
+        from .backend import check
+        from .core import DType
+        self._L, self._check, self._C = L, check, C
+        self.device = device
+        self.count = len(grid_sides)
+        sides = (C.c_size_t * self.count)(*[int(s) for s in grid_sides])
+        dt = DType.F64 if cycle_dtype is None else DType(cycle_dtype)
+        self._keep = (vx, vy)
+        out = C.c_void_p()
+        check(L.lib().fx_batch_create(device.backend().ctx, self.count, sides, float(nu), float(sigma), float(coeff),
+                                      vx.handle, vy.handle, int(dt), int(n_pre), int(n_post), float(omega),
+                                      int(coarse_max), int(coarse_sweeps), C.byref(out)))
+        self.h = out.value
+        offs = (C.c_size_t * (self.count + 1))()
+        lev = (C.c_size_t * self.count)()
+        check(L.lib().fx_batch_layout(self.h, offs, lev))
+        self.offsets = [offs[i] for i in range(self.count + 1)]
+        self.depths = [lev[i] for i in range(self.count)]
+
+    def apply(self, v, out) -> None:
+        self._check(self._L.lib().fx_batch_apply(self.h, v.handle, out.handle))
+
+    def precondition(self, z, r) -> None:
+        self._check(self._L.lib().fx_batch_precondition(self.h, z.handle, r.handle))
+
+    def bicgstab(self, x, b, rel_tol: float = 1e-10, max_iter: int = 200, use_graph: bool = True):
+        """Solve every problem; returns (per-problem SolveStats, batch iterations launched)."""
+        C = self._C
+        from ._lib import FxStats
+        from .solvers import _stats
+        st = (FxStats * self.count)()
+        run = C.c_size_t()
+        self._check(self._L.lib().fx_batch_bicgstab(self.h, x.handle, b.handle, float(rel_tol), int(max_iter),
+                                                    1 if use_graph else 0, st, C.byref(run)))
+        return [_stats(st[i]) for i in range(self.count)], run.value
+
+    def __del__(self):
+        try:
+            if self.h:
+                self._L.lib().fx_batch_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass

@@ -104,6 +104,7 @@ typedef struct fx_cdmg fx_cdmg;
 typedef struct fx_ir fx_ir;
 typedef struct fx_lsm fx_lsm;
 typedef struct fx_lsm_data fx_lsm_data;
+typedef struct fx_batch fx_batch;
 
 /* ------------------------------------------------------------------ */
 /* Context (HipBackend::new / singleton, backend-hip/src/backend.rs:103-264) */
@@ -527,6 +528,36 @@ int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, d
  * outlive the multigrid's use of it.  stats: checked applications and fallbacks so far. */
 int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, double fallback_ratio);
 int fx_cdmg_learned_stats(fx_cdmg *mg, unsigned long long *applications, unsigned long long *fallbacks);
+
+/* ------------------------------------------------------------------ */
+/* Batched solve (new; the reference solves one grid at a time, bicgstab.rs:218-346).  `count`
+ * independent steady problems sigma u + coeff (kappa Lap u + v.grad u) = f, kappa = -nu, each on
+ * its own square grid of side grid_side[p] = 2^k + 1 (ring included) over the unit square, with
+ * Dirichlet 0.  Vectors of the batch are F64 buffers holding every problem's grid one after the
+ * other (fx_batch_layout gives the offsets); vx and vy are such buffers, borrowed for the
+ * batch's life.  Each problem is solved by right-preconditioned BiCGSTAB with the conv-diff
+ * V-cycle of fx_cdmg_create_typed (cycle_dtype FX_F64 or FX_F32), every problem in the same
+ * launches: each phase of the algorithm is one launch over the whole batch, its blocks taking
+ * (problem, chunk) or (problem, tile) items from tables built here, so a launch fills the GPU
+ * with every problem's share.  The cycle equals fx_cdmg's bit for bit. */
+int fx_batch_create(fx_ctx *ctx, size_t count, const size_t *grid_side, double nu, double sigma, double coeff,
+                    const fx_buf *vx, const fx_buf *vy, int cycle_dtype, size_t n_pre, size_t n_post, double omega,
+                    size_t coarse_max, size_t coarse_sweeps, fx_batch **out);
+int fx_batch_destroy(fx_batch *b);
+/* offsets[count + 1]: where each problem's grid starts in a batch vector (and the total);
+ * levels[count] (may be NULL): each problem's multigrid depth */
+int fx_batch_layout(const fx_batch *b, size_t *offsets, size_t *levels);
+/* out = A v for every problem (synchronises) */
+int fx_batch_apply(fx_batch *b, const fx_buf *v, fx_buf *out);
+/* z = M r (one V-cycle from zero) for every problem (synchronises) */
+int fx_batch_precondition(fx_batch *b, fx_buf *z, const fx_buf *r);
+/* BiCGSTAB (bicgstab.rs:218-346, right-preconditioned by the batch's cycle) of every problem from
+ * its initial x, each to ||r_p|| < rel_tol ||b_p|| or max_iter iterations; stats[count] get each
+ * problem's iterations, residual and reason.  use_graph: each iteration of the whole batch is
+ * recorded once (per (x, b) pair) into a CUDA graph and replayed.  *iterations_run (may be
+ * NULL): batch iterations launched. */
+int fx_batch_bicgstab(fx_batch *b, fx_buf *x, const fx_buf *rhs, double rel_tol, size_t max_iter, int use_graph,
+                      fx_stats *stats, size_t *iterations_run);
 
 /* BiCGSTAB, GMRES(m) and flexible GMRES(m) on the operator (pc may be NULL): the same loops,
  * recurrences and stop tests as fx_bicgstab_solve*, fx_gmres_solve* and fx_fgmres_solve* */
