@@ -93,6 +93,12 @@ class BatchSolver:
     def apply(self, v, out) -> None:
         self._check(self._L.lib().fx_batch_apply(self.h, v.handle, out.handle))
 
+    def residual_norms(self, x, b):
+        """||b_p - A x_p|| of every problem (computed on the device)."""
+        out = (self._C.c_double * self.count)()
+        self._check(self._L.lib().fx_batch_residual_norms(self.h, x.handle, b.handle, out))
+        return [out[i] for i in range(self.count)]
+
     def precondition(self, z, r) -> None:
         self._check(self._L.lib().fx_batch_precondition(self.h, z.handle, r.handle))
 

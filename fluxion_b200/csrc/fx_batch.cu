@@ -225,6 +225,11 @@ __device__ __forceinline__ void bs_top(BState *S, double rr, double rho_new) {
     S->beta = (rho_new / S->rho) * (S->alpha / S->omega);
 }
 
+struct FinNorm2 {  // resid = ||r|| (the batch's residual check)
+    BState *S;
+    __device__ void operator()(int p, const double *v) const { S[p].resid = sqrt(v[0]); }
+};
+
 struct FinInit {
     BState *S;
     __device__ void operator()(int p, const double *v) const {
@@ -1093,6 +1098,22 @@ int fx_batch_apply(fx_batch *B, const fx_buf *v, fx_buf *out) {
                      BfAr{k, (const double *)v->ptr, (double *)out->ptr, (const double *)v->ptr, 0}, NoFinB{},
                      "batch_apply")));
     FX_CUDA(cudaStreamSynchronize(B->ctx->stream));
+    return FX_OK;
+}
+
+int fx_batch_residual_norms(fx_batch *B, const fx_buf *x, const fx_buf *b, double *norms) {
+    if (!B || !norms) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    FX_TRY(check_vec(B, x, "x"));
+    FX_TRY(check_vec(B, b, "b"));
+    fx_ctx *ctx = B->ctx;
+    FX_CUDA(cudaMemsetAsync(B->d_state, 0, B->np * sizeof(BState), ctx->stream));
+    // r = b - A x into the batch's r vector; ||r||^2 per problem into the state's resid slot
+    FX_TRY((bflat<2>(B, B->d_chunk0, B->nchunk0,
+                     BfInit{B->k0(), (const double *)x->ptr, (const double *)b->ptr, B->kv[0], B->kv[1]},
+                     FinNorm2{B->d_state}, "batch_residual_norm")));
+    FX_CUDA(cudaMemcpyAsync(B->h_state, B->d_state, B->np * sizeof(BState), cudaMemcpyDeviceToHost, ctx->stream));
+    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t p = 0; p < B->np; p++) norms[p] = B->h_state[p].resid;
     return FX_OK;
 }
 

@@ -35,6 +35,36 @@ constexpr int kDownFifo = 6;    // rows of raw loads in flight (a divisor of kSt
 constexpr int kUpFifo = 6;
 static_assert(kStripUnroll % kDownFifo == 0 && kStripUnroll % kUpFifo == 0, "FIFO depth must divide the unroll");
 
+// The FP64 kernels hold twice the register bytes per value.  Their block shape, FIFO depth and
+// minimum resident blocks per SM (the register cap of the launch bound) are set separately.
+#ifndef FX_STRIP_F64_WARPS
+#define FX_STRIP_F64_WARPS 8
+#endif
+#ifndef FX_STRIP_F64_UP_FIFO
+#define FX_STRIP_F64_UP_FIFO 6
+#endif
+#ifndef FX_STRIP_F64_DOWN_FIFO
+#define FX_STRIP_F64_DOWN_FIFO 6
+#endif
+#ifndef FX_STRIP_F64_UP_MINB
+#define FX_STRIP_F64_UP_MINB 1
+#endif
+#ifndef FX_STRIP_F64_DOWN_MINB
+#define FX_STRIP_F64_DOWN_MINB 1
+#endif
+template <typename T>
+__host__ __device__ constexpr int strip_warps() { return sizeof(T) == 8 ? FX_STRIP_F64_WARPS : kStripWarps; }
+template <typename T>
+__host__ __device__ constexpr int up_fifo() { return sizeof(T) == 8 ? FX_STRIP_F64_UP_FIFO : kUpFifo; }
+template <typename T>
+__host__ __device__ constexpr int down_fifo() { return sizeof(T) == 8 ? FX_STRIP_F64_DOWN_FIFO : kDownFifo; }
+template <typename T>
+__host__ __device__ constexpr int up_minb() { return sizeof(T) == 8 ? FX_STRIP_F64_UP_MINB : 1; }
+template <typename T>
+__host__ __device__ constexpr int down_minb() { return sizeof(T) == 8 ? FX_STRIP_F64_DOWN_MINB : 1; }
+static_assert(kStripUnroll % FX_STRIP_F64_UP_FIFO == 0 && kStripUnroll % FX_STRIP_F64_DOWN_FIFO == 0,
+              "FIFO depth must divide the unroll");
+
 struct StripGeom {
     int rows, cols;
     int nstrips;
@@ -80,14 +110,14 @@ using fast_t = std::integral_constant<bool, B>;
 constexpr int kDownOwn = 56;  // own columns per strip: lanes 2..29 (x1 -> x2 -> res -> FW: halo 4)
 
 template <typename T, typename TB>
-__global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const TB *__restrict__ b, T *__restrict__ x2g,
+__global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown(StripGeom G, const TB *__restrict__ b, T *__restrict__ x2g,
                                                              T *__restrict__ coarse, int ccols, VOp<T> op,
                                                              const int *skip) {
     grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
-    constexpr int D = kDownFifo, R = kStripUnroll;
+    constexpr int D = down_fifo<T>(), R = kStripUnroll;
     const int lane = threadIdx.x & 31;
-    const int item = blockIdx.x * kStripWarps + (threadIdx.x >> 5);
+    const int item = blockIdx.x * strip_warps<T>() + (threadIdx.x >> 5);
     if (item >= G.nitems) return;  // whole warps
     const int strip = item % G.nstrips, chunk = item / G.nstrips;
     const int rows = G.rows, cols = G.cols;
@@ -200,15 +230,15 @@ __global__ void __launch_bounds__(kStripWarps * 32) k_wdown(StripGeom G, const T
 constexpr int kUpOwn = 60;  // own columns per strip: lanes 1..30 (f -> x3 -> z: halo 2)
 
 template <typename T, typename TB, typename TZ, bool RZ, typename Fin>
-__global__ void __launch_bounds__(kStripWarps * 32) k_wup(StripGeom G, const T *__restrict__ x2g,
+__global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(StripGeom G, const T *__restrict__ x2g,
                                                            const T *__restrict__ e, int ccols,
                                                            const TB *__restrict__ b, TZ *__restrict__ z, VOp<T> op,
                                                            Fin fin, RedArgs<1> ra, const int *skip) {
     grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
-    constexpr int D = kUpFifo, R = kStripUnroll;
+    constexpr int D = up_fifo<T>(), R = kStripUnroll;
     const int lane = threadIdx.x & 31;
-    const int item = blockIdx.x * kStripWarps + (threadIdx.x >> 5);
+    const int item = blockIdx.x * strip_warps<T>() + (threadIdx.x >> 5);
     CSum acc[1] = {CSum{0.0, 0.0}};
     if (item < G.nitems) {  // idle warps still join the block reduction
         const int strip = item % G.nstrips, chunk = item / G.nstrips;
@@ -377,12 +407,12 @@ template <typename T, typename TB>
 int launch_wdown(fx_ctx *ctx, size_t rows, size_t cols, const TB *b, T *x2, T *coarse, size_t ccols,
                  const VOp<T> &op, const int *skip, int chunk_pct = 100) {
     static std::atomic<int> occ{0};
-    const long cap = strip_capacity((long)band_capacity(ctx, k_wdown<T, TB>, occ, kStripWarps * 32) * kStripWarps,
-                                    chunk_pct);
+    constexpr int W = strip_warps<T>();
+    const long cap = strip_capacity((long)band_capacity(ctx, k_wdown<T, TB>, occ, W * 32) * W, chunk_pct);
     const StripGeom G = strip_geom(rows, cols, kDownOwn, cap);
-    const int blocks = (G.nitems + kStripWarps - 1) / kStripWarps;
+    const int blocks = (G.nitems + W - 1) / W;
     timing_pre(ctx, "mg_down");
-    launch_pdl(ctx, k_wdown<T, TB>, blocks, kStripWarps * 32, 0, G, b, x2, coarse, (int)ccols, op, skip);
+    launch_pdl(ctx, k_wdown<T, TB>, blocks, W * 32, 0, G, b, x2, coarse, (int)ccols, op, skip);
     // reads b, writes the smoothed x2 and the restricted coarse rhs
     const double pts = (double)rows * (double)cols, cpts = (double)((rows - 1) / 2 + 1) * (double)ccols;
     timing_post(ctx, pts, pts * (sizeof(TB) + sizeof(T)) + cpts * sizeof(T));
@@ -393,13 +423,13 @@ template <typename T, typename TB, typename TZ, bool RZ, typename Fin>
 int launch_wup(fx_ctx *ctx, size_t rows, size_t cols, const T *x2, const T *e, size_t ccols, const TB *b, TZ *z,
                const VOp<T> &op, Fin fin, const int *skip, int chunk_pct = 100) {
     static std::atomic<int> occ{0};
-    const long cap = strip_capacity(
-        (long)band_capacity(ctx, k_wup<T, TB, TZ, RZ, Fin>, occ, kStripWarps * 32) * kStripWarps, chunk_pct);
+    constexpr int W = strip_warps<T>();
+    const long cap = strip_capacity((long)band_capacity(ctx, k_wup<T, TB, TZ, RZ, Fin>, occ, W * 32) * W, chunk_pct);
     const StripGeom G = strip_geom(rows, cols, kUpOwn, cap);
-    const int blocks = (G.nitems + kStripWarps - 1) / kStripWarps;
+    const int blocks = (G.nitems + W - 1) / W;
     if (RZ && blocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");
     timing_pre(ctx, "mg_up");
-    launch_pdl(ctx, k_wup<T, TB, TZ, RZ, Fin>, blocks, kStripWarps * 32, 0, G, x2, e, (int)ccols, b, z, op, fin,
+    launch_pdl(ctx, k_wup<T, TB, TZ, RZ, Fin>, blocks, W * 32, 0, G, x2, e, (int)ccols, b, z, op, fin,
                red_args<1>(ctx), skip);
     // reads x2, the coarse correction e and b, writes z
     const double pts = (double)rows * (double)cols, cpts = (double)((rows - 1) / 2 + 1) * (double)ccols;

@@ -549,6 +549,8 @@ int fx_batch_destroy(fx_batch *b);
 int fx_batch_layout(const fx_batch *b, size_t *offsets, size_t *levels);
 /* out = A v for every problem (synchronises) */
 int fx_batch_apply(fx_batch *b, const fx_buf *v, fx_buf *out);
+/* norms[count] = ||b_p - A x_p|| of every problem, computed on the device (synchronises) */
+int fx_batch_residual_norms(fx_batch *b, const fx_buf *x, const fx_buf *rhs, double *norms);
 /* z = M r (one V-cycle from zero) for every problem (synchronises) */
 int fx_batch_precondition(fx_batch *b, fx_buf *z, const fx_buf *r);
 /* BiCGSTAB (bicgstab.rs:218-346, right-preconditioned by the batch's cycle) of every problem from
