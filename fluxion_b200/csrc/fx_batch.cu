@@ -217,6 +217,10 @@ __device__ __forceinline__ void bs_top(BState *S, double rr, double rho_new) {
         bs_finish(S, FX_CONVERGED, S->iter, r_norm);
         return;
     }
+    if (!isfinite(r_norm)) {  // NaN / Inf in the problem: Breakdown rather than max_iter
+        bs_finish(S, FX_BREAKDOWN, S->iter, r_norm);
+        return;
+    }
     S->rho_new = rho_new;
     if (fabs(rho_new) < 1e-30) {
         bs_finish(S, FX_BREAKDOWN, S->iter, r_norm);

@@ -459,10 +459,21 @@ int fx_ctx_timing_end(fx_ctx *c, double *total_ms, unsigned long long *launches,
     return FX_OK;
 }
 
+// test hook: the next g_fail_allocs buffer allocations fail (fx_test_fail_allocations)
+static std::atomic<int> g_fail_allocs{0};
+
+int fx_test_fail_allocations(int count) {
+    g_fail_allocs.store(count < 0 ? 0 : count);
+    return FX_OK;
+}
+
 int fx_alloc(fx_ctx *ctx, size_t len, int dtype, fx_buf **out) {
     if (!ctx || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     if (dtype != FX_F32 && dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "unknown dtype");
     *out = nullptr;
+    for (int k = g_fail_allocs.load(); k > 0; k = g_fail_allocs.load())
+        if (g_fail_allocs.compare_exchange_weak(k, k - 1))
+            return fail(FX_ERR_BACKEND, "backend error: allocation failed (test hook)");
     fx_buf *b = new fx_buf();
     b->ctx = ctx;
     b->len = len;

@@ -817,6 +817,16 @@ struct SolverBase {
         FX_CUDA(cudaStreamSynchronize(ctx->stream));
         return FX_OK;
     }
+    // A residual that is not a finite number (a NaN or Inf in b, x or the operator) never passes
+    // the reference's stop test and would run to max_iter; the solve stops with Breakdown instead.
+    int stop_nonfinite() {
+        h_st->done = 1;
+        h_st->halt = 1;
+        h_st->reason = FX_BREAKDOWN;
+        FX_CUDA(cudaMemcpyAsync(&d_st->done, &h_st->done, 3 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        FX_CUDA(cudaStreamSynchronize(ctx->stream));
+        return FX_OK;
+    }
     int check_io(const fx_buf *x, const fx_buf *b) {
         FX_TRY(check_buf(x, "x"));
         FX_TRY(check_buf(b, "b"));
@@ -841,6 +851,7 @@ struct SolverBase {
             launched += nb;
             FX_TRY(read_state());
             if (h_st->done) return FX_OK;
+            if (!std::isfinite(h_st->resid)) return stop_nonfinite();
             // predict the iterations still needed from the mean reduction rate so far (r0: the
             // initial residual, recorded on the device by every solver's setup finaliser)
             const double r0 = h_st->r0 > 0 ? h_st->r0 : 1.0;
@@ -1404,6 +1415,10 @@ int ir_solve_impl(fx_ir *s, fx_buf *x, const fx_buf *b, double coeff, const fx_s
             H.reason = FX_CONVERGED;
             return FX_OK;
         }
+        if (!std::isfinite(rnorm)) {  // NaN / Inf: stop with Breakdown rather than run to max_outer
+            H.reason = FX_BREAKDOWN;
+            return FX_OK;
+        }
         if (k >= s->max_iter) {
             H.reason = FX_MAX_ITERATIONS;
             return FX_OK;
@@ -1865,6 +1880,10 @@ int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, cons
             st = {total_its, beta, FX_CONVERGED};
             break;
         }
+        if (!std::isfinite(beta)) {  // NaN / Inf in b, x or the operator: Breakdown, not max_iter
+            st = {total_its, beta, FX_BREAKDOWN};
+            break;
+        }
         FX_TRY(scale_into(V[0], V[0], 1.0 / beta));
         std::fill(s->grs.begin(), s->grs.end(), 0.0);
         s->grs[0] = beta;
@@ -1927,6 +1946,11 @@ int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, cons
             cur_resid = std::fabs(s->grs[k + 1]);
             total_its++;
             k++;
+            if (!std::isfinite(cur_resid)) {
+                st = {total_its, cur_resid, FX_BREAKDOWN};
+                finished = true;
+                break;
+            }
             if (cur_resid < s->tol) break;
             if (h_kp1_k <= 1e-30) break;
         }
@@ -2131,6 +2155,10 @@ int fgmres_solve_impl(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, co
             st = {total_its, beta, FX_CONVERGED};
             break;
         }
+        if (!std::isfinite(beta)) {  // NaN / Inf in b, x or the operator: Breakdown, not max_iter
+            st = {total_its, beta, FX_BREAKDOWN};
+            break;
+        }
         FX_TRY(scale_into(V[0], V[0], 1.0 / beta));
         std::fill(s->grs.begin(), s->grs.end(), 0.0);
         s->grs[0] = beta;
@@ -2187,6 +2215,11 @@ int fgmres_solve_impl(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, co
             cur_resid = std::fabs(s->grs[k + 1]);
             total_its++;
             k++;
+            if (!std::isfinite(cur_resid)) {
+                st = {total_its, cur_resid, FX_BREAKDOWN};
+                finished = true;
+                break;
+            }
             if (cur_resid < s->tol) break;
             if (h_kp1_k <= 1e-30) break;
         }

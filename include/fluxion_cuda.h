@@ -159,6 +159,10 @@ int fx_graph_destroy(fx_graph *graph);                    /* Drop for HipGraph :
 /* ------------------------------------------------------------------ */
 
 int fx_alloc(fx_ctx *ctx, size_t len, int dtype, fx_buf **out);
+/* Test hook (no counterpart in the reference): the next `count` buffer allocations (fx_alloc and
+ * everything built on it: uploads, solver and multigrid creation) fail with FX_ERR_BACKEND, as an
+ * out-of-memory would; 0 clears it.  Process-wide. */
+int fx_test_fail_allocations(int count);
 int fx_upload_f64(fx_ctx *ctx, const double *data, size_t len, fx_buf **out);
 int fx_upload_f32(fx_ctx *ctx, const float *data, size_t len, fx_buf **out);
 /* Non-owning view of existing device memory (interop); fx_free releases only the handle. */
