@@ -67,7 +67,10 @@ def parse():
     p.add_argument("--lanes", type=int, default=8, help="--mode batch: concurrent contexts (host threads)")
     p.add_argument("--pdl", type=int, default=1, choices=[0, 1],
                    help="--mode batch: programmatic dependent launch in the lanes' contexts")
-    p.add_argument("--autotune", action="store_true", help="--mode vcycle: autotune the cycle's layout first")
+    p.add_argument("--autotune", action="store_true",
+                   help="--mode vcycle: autotune the cycle's layout first; --mode batch: choose the batched "
+                        "solver's chunk size, sweep counts and cycle precision first (timed on a sample)")
+    p.add_argument("--tune-cache", default=None, help="JSON file that keeps autotuner choices between runs")
     p.add_argument("--mode", default="solve", choices=["solve", "vcycle", "batch", "convdiff", "learned"],
                    help="solve: the headline MG-PCG solve; vcycle: preconditioner applications alone "
                         "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target; batch: "
@@ -310,14 +313,26 @@ def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
         o += s * s
     out = torch.empty(tot, dtype=torch.float64, pin_memory=True).numpy()
     mg_dtype = DType.F32 if args.mg_dtype == "f32" else DType.F64
+    chunk, sweeps, tuned = 2048, 2, None
+    if args.autotune:  # before the timed region: work-item size, sweep counts and cycle precision
+        from fluxion_b200.autotune import TuneCache, tune_batch
+        t_tune = time.perf_counter()
+        tuned = tune_batch(dev, sides, nu, [host[i][1] for i in mine], [host[i][2] for i in mine],
+                           [host[i][3] for i in mine], sample=96, omega=OMEGA, coarse_max=COARSE_MAX,
+                           coarse_sweeps=COARSE_SWEEPS, cache=TuneCache(args.tune_cache))
+        tuned["tuning_s"] = time.perf_counter() - t_tune
+        chunk, sweeps = tuned["chunk"], tuned["sweeps"]
+        mg_dtype = DType.F32 if tuned["cycle_dtype"] == "f32" else DType.F64
 
     def once():
         VX, VY, F = be.allocate(tot, DType.F64), be.allocate(tot, DType.F64), be.allocate(tot, DType.F64)
         VX.write(xv)
         VY.write(yv)
         F.write(fv)
-        B = BatchSolver(dev, sides, nu, VX, VY, cycle_dtype=mg_dtype, omega=OMEGA, coarse_max=COARSE_MAX,
-                        coarse_sweeps=COARSE_SWEEPS)
+        B = BatchSolver(dev, sides, nu, VX, VY, cycle_dtype=mg_dtype, n_pre=sweeps, n_post=sweeps, omega=OMEGA,
+                        coarse_max=COARSE_MAX, coarse_sweeps=COARSE_SWEEPS)
+        if chunk != 2048:
+            B.set_chunk(chunk)
         X = be.allocate(tot, DType.F64)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -340,7 +355,9 @@ def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
         rel = float(rn[j] / max(host[i][4], 1e-300))
         res[i] = (sides[j] - 2, int(stats[j].iterations), bool(stats[j].converged()), solve_ms, rel, wall)
     return res, wall, {"batch_iterations_launched": run, "device_solve_ms": solve_ms,
-                       "points": tot, "launch_per_iteration": "one CUDA graph"}
+                       "points": tot, "launch_per_iteration": "one CUDA graph",
+                       "tuning": {"chunk": chunk, "sweeps": sweeps, "cycle_dtype": "f32" if mg_dtype == DType.F32 else
+                                  "f64", "autotuned": tuned}}
 
 
 def run_batch(args):
@@ -508,7 +525,7 @@ def _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist
         "solver": "batched (one launch per phase over the batch)" if args.batched else "lanes",
         "problems": args.batch, "n_gpus": world, "scaling": "strong", "lanes": lanes, "pdl": bool(args.pdl),
         **extra,
-        "vcycle_dtype": args.mg_dtype, "vcycle_replay": bool(args.replay),
+        "vcycle_dtype": extra.get("tuning", {}).get("cycle_dtype", args.mg_dtype), "vcycle_replay": bool(args.replay),
         "interior_sizes": {str(2 ** k - 1): int((ks == k).sum()) for k in range(k_lo, k_hi + 1)},
         "solves_per_s": args.batch / wall, "wall_s_excluding_host_data_generation": wall,
         "per_problem_ms_p50": float(np.percentile([r[5] * 1e3 for r in res], 50)),
@@ -516,7 +533,8 @@ def _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist
         "solve_ms_p50": float(np.percentile(ms, 50)), "solve_ms_p99": float(np.percentile(ms, 99)),
         "iterations_p50": float(np.percentile(its, 50)), "iterations_max": int(its.max()),
         "all_converged": ok, "max_true_rel_residual": max(r[4] for r in res),
-        "dtype": "f64" if args.mg_dtype == "f64" else "f64 (Krylov) / f32 (V-cycle)",
+        "dtype": "f64" if extra.get("tuning", {}).get("cycle_dtype", args.mg_dtype) == "f64"
+        else "f64 (Krylov) / f32 (V-cycle)",
         "data": "synthetic (seeded per problem), page-locked host arrays",
         "note": ("batched: per-problem times are the whole batch's (every problem finishes in the batch's "
                  "last launch)" if args.batched else

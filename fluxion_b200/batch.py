@@ -90,6 +90,10 @@ class BatchSolver:
         self.offsets = [offs[i] for i in range(self.count + 1)]
         self.depths = [lev[i] for i in range(self.count)]
 
+    def set_chunk(self, elements: int) -> None:
+        """Elements per flat work item of the batch's launches (no effect on the values)."""
+        self._check(self._L.lib().fx_batch_set_chunk(self.h, int(elements)))
+
     def apply(self, v, out) -> None:
         self._check(self._L.lib().fx_batch_apply(self.h, v.handle, out.handle))
 

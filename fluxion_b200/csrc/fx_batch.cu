@@ -31,7 +31,7 @@ using namespace fx;
 namespace {
 
 constexpr int kBT = 256;             // threads per block
-constexpr int kChunk = 8 * kBT;      // elements per flat work item
+constexpr int kChunkDefault = 8 * kBT;  // elements per flat work item (fx_batch_set_chunk changes it)
 constexpr int kTileB = 32;           // sweep-pair tile side (as k_cd_sweep2)
 constexpr int kTileX = kTileB + 4;   // x with a two-point halo
 constexpr int kTileY = kTileB + 2;   // first sweep with a one-point halo
@@ -689,6 +689,8 @@ struct fx_batch {
     double nu = 0, sigma = 0, coeff = 1, omega = 0.8;
     size_t n_pre = 2, n_post = 2, coarse_sweeps = 200;
     int nlev = 0;  // the deepest problem's level count
+    int chunk = kChunkDefault;  // elements per flat work item
+    std::vector<std::vector<int>> lv_side, lv_have, lv_smooth;  // per level: sides, problem lists
     std::vector<long long> off0;  // level-0 offsets (+ total at the end)
     long long total0 = 0;
     const fx_buf *vx = nullptr, *vy = nullptr;  // level-0 F64 fields (borrowed)
@@ -758,13 +760,13 @@ struct fx_batch {
 
 namespace {
 
-// chunk table of the given problems' arrays of side ns[p]
-std::vector<Chunk> make_chunks(const std::vector<int> &probs, const std::vector<int> &side) {
+// chunk table of the given problems' arrays of side ns[p], `chunk` elements per item
+std::vector<Chunk> make_chunks(const std::vector<int> &probs, const std::vector<int> &side, int chunk) {
     std::vector<Chunk> out;
     for (int p : probs) {
         const int n = side[p] * side[p];
-        const int first = (int)out.size(), count = (n + kChunk - 1) / kChunk;
-        for (int k = 0; k < count; k++) out.push_back(Chunk{p, k * kChunk, std::min(kChunk, n - k * kChunk), first, count});
+        const int first = (int)out.size(), count = (n + chunk - 1) / chunk;
+        for (int k = 0; k < count; k++) out.push_back(Chunk{p, k * chunk, std::min(chunk, n - k * chunk), first, count});
     }
     return out;
 }
@@ -776,6 +778,18 @@ int bflat(fx_batch *B, const Chunk *items, int n, F f, Fin fin, const char *what
     k_bflat<K, F, Fin><<<n, kBT, 0, B->ctx->stream>>>(items, f, fin, B->d_partials, B->d_tickets);
     timing_post(B->ctx, 0.0);
     return check_launch(B->ctx, what);
+}
+
+// (re)build the chunk tables of level l for the batch's chunk size
+int upload_chunks(fx_batch *B, int l) {
+    auto &D = B->lv[l];
+    const auto ch = make_chunks(B->lv_have[l], B->lv_side[l], B->chunk);
+    const auto sch = make_chunks(B->lv_smooth[l], B->lv_side[l], B->chunk);
+    FX_TRY(B->upload(&D.chunks, ch));
+    FX_TRY(B->upload(&D.smooth_chunks, sch));
+    D.nchunks = (int)ch.size();
+    D.nsmooth = (int)sch.size();
+    return FX_OK;
 }
 
 template <typename T>
@@ -808,11 +822,10 @@ int build_levels(fx_batch *B) {
         Lvl<T> *dl = nullptr;
         FX_TRY(B->upload(&dl, L[l]));
         D.lvl = dl;
-        const auto ch = make_chunks(have, side[l]), sch = make_chunks(smooth, side[l]);
-        FX_TRY(B->upload(&D.chunks, ch));
-        FX_TRY(B->upload(&D.smooth_chunks, sch));
-        D.nchunks = (int)ch.size();
-        D.nsmooth = (int)sch.size();
+        B->lv_side.push_back(side[l]);
+        B->lv_have.push_back(have);
+        B->lv_smooth.push_back(smooth);
+        FX_TRY(upload_chunks(B, l));
         std::vector<Tile> tiles;
         for (int p : smooth) {
             const int nt = (side[l][p] + kTileB - 1) / kTileB;
@@ -1056,7 +1069,7 @@ int fx_batch_create(fx_ctx *ctx, size_t count, const size_t *grid_side, double n
     if ((long long)vx->len != tot || (long long)vy->len != tot) return bad("velocity fields must hold every problem's grid");
     std::vector<int> all(count), side0(B->n0);
     for (size_t p = 0; p < count; p++) all[p] = (int)p;
-    const auto ch0 = make_chunks(all, side0);
+    const auto ch0 = make_chunks(all, side0, B->chunk);
     int st = B->upload(&B->d_chunk0, ch0);
     B->nchunk0 = (int)ch0.size();
     std::vector<Lvl<double>> l0(count);
@@ -1065,7 +1078,9 @@ int fx_batch_create(fx_ctx *ctx, size_t count, const size_t *grid_side, double n
         l0[p] = Lvl<double>{B->off0[p], B->n0[p], conv_consts<double>(h, h)};
     }
     if (st == FX_OK) st = B->upload(&B->d_lvl0_f64, l0);
-    size_t maxchunks = ch0.size();
+    // partials for the smallest chunk a batch may be given (fx_batch_set_chunk)
+    size_t maxchunks = 0;
+    for (size_t p = 0; p < count; p++) maxchunks += ((size_t)B->n0[p] * B->n0[p] + 255) / 256;
     if (st == FX_OK) st = B->dalloc(&B->d_partials, maxchunks * 4 * sizeof(double));
     if (st == FX_OK) st = B->dalloc(&B->d_tickets, count * sizeof(unsigned));
     if (st == FX_OK) st = B->dalloc(&B->d_state, count * sizeof(BState));
@@ -1080,6 +1095,24 @@ int fx_batch_create(fx_ctx *ctx, size_t count, const size_t *grid_side, double n
         return st;
     }
     *out = B;
+    return FX_OK;
+}
+
+int fx_batch_set_chunk(fx_batch *B, size_t elements) {
+    if (!B) return fail(FX_ERR_INVALID_ARGUMENT, "null batch");
+    if (elements < 256 || elements > 65536 || (elements % 256) != 0)
+        return fail(FX_ERR_INVALID_ARGUMENT, "batch: chunk must be a multiple of 256 elements in [256, 65536]");
+    FX_CUDA(cudaStreamSynchronize(B->ctx->stream));
+    B->chunk = (int)elements;
+    std::vector<int> all(B->np);
+    for (size_t p = 0; p < B->np; p++) all[p] = (int)p;
+    const auto ch0 = make_chunks(all, B->n0, B->chunk);
+    FX_TRY(B->upload(&B->d_chunk0, ch0));  // the old tables stay allocated until the batch goes
+    B->nchunk0 = (int)ch0.size();
+    for (int l = 0; l < B->nlev; l++) FX_TRY(upload_chunks(B, l));
+    if (B->step_exec) cudaGraphExecDestroy(B->step_exec);  // recorded with the old tables
+    B->step_exec = nullptr;
+    B->graph_key[0] = B->graph_key[1] = nullptr;
     return FX_OK;
 }
 

@@ -551,6 +551,9 @@ int fx_batch_destroy(fx_batch *b);
 /* offsets[count + 1]: where each problem's grid starts in a batch vector (and the total);
  * levels[count] (may be NULL): each problem's multigrid depth */
 int fx_batch_layout(const fx_batch *b, size_t *offsets, size_t *levels);
+/* Elements per flat work item of the batch's launches (a multiple of 256 in [256, 65536];
+ * 2048 at creation).  Changes no computed value; the autotuner picks it. */
+int fx_batch_set_chunk(fx_batch *b, size_t elements);
 /* out = A v for every problem (synchronises) */
 int fx_batch_apply(fx_batch *b, const fx_buf *v, fx_buf *out);
 /* norms[count] = ||b_p - A x_p|| of every problem, computed on the device (synchronises) */

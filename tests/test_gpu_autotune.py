@@ -63,3 +63,51 @@ def test_autotune_keeps_the_fastest_candidate(dev):
     z1 = Field.zeros(P.grid, DType.F64, dev)
     mg.precondition(z1, r)
     assert np.array_equal(z1.to_vec_f64(), z0.to_vec_f64())
+
+
+def test_batch_autotune_chooses_a_converging_candidate_and_caches_it(tmp_path):
+    """The batch tuner times whole solves of a sample for each (chunk, sweeps, cycle dtype), keeps
+    the fastest whose problems all converge, and a second call with the same key reads the JSON
+    cache instead of timing."""
+    import numpy as np
+    from fluxion_b200 import Device
+    from fluxion_b200.autotune import TuneCache, tune_batch
+    from fluxion_b200.workloads import poisson_uniform_rhs, stream_velocity
+    dev = Device.best()
+    sides = [33, 65, 129, 65, 33, 129, 65, 257]
+    vx, vy, f = [], [], []
+    for k, s in enumerate(sides):
+        a, b = stream_velocity(s - 2, 300 + k)
+        vx.append(a)
+        vy.append(b)
+        f.append(poisson_uniform_rhs(s - 2, 400 + k))
+    path = str(tmp_path / "tune.json")
+    best = tune_batch(dev, sides, 1e-2, vx, vy, f, sample=6, chunks=(1024, 4096), sweeps=(1, 2),
+                      dtypes=("f64", "f32"), cache=TuneCache(path))
+    assert not best["cached"] and len(best["candidates"]) == 8
+    assert any(c["ok"] for c in best["candidates"])
+    chosen = [c for c in best["candidates"] if c["chunk"] == best["chunk"] and c["sweeps"] == best["sweeps"]
+              and c["cycle_dtype"] == best["cycle_dtype"]][0]
+    assert chosen["ok"] and chosen["ms"] == min(c["ms"] for c in best["candidates"] if c["ok"])
+    again = tune_batch(dev, sides, 1e-2, vx, vy, f, sample=6, chunks=(1024, 4096), sweeps=(1, 2),
+                       dtypes=("f64", "f32"), cache=TuneCache(path))
+    assert again["cached"] and (again["chunk"], again["sweeps"], again["cycle_dtype"]) == \
+        (best["chunk"], best["sweeps"], best["cycle_dtype"])
+
+
+def test_vertex_mg_tuning_through_the_cache(tmp_path):
+    import numpy as np
+    from fluxion_b200 import DType, Device, Field, Multigrid
+    from fluxion_b200.autotune import TuneCache, tune_vertex_mg
+    from fluxion_b200.workloads import poisson_problem, poisson_uniform_rhs
+    dev = Device.best()
+    P = poisson_problem(1023)
+    mg = Multigrid.vertex(P.grid, None, dev, dtype=DType.F32)
+    r = Field.from_f64(P.grid, poisson_uniform_rhs(1023, 5), dev)
+    z = Field.zeros(P.grid, DType.F64, dev)
+    path = str(tmp_path / "mg.json")
+    a = tune_vertex_mg(mg, z, r, cache=TuneCache(path), reps=3, dtype="f32", coarse_max=15, coarse_sweeps=200)
+    mg2 = Multigrid.vertex(P.grid, None, dev, dtype=DType.F32)
+    b = tune_vertex_mg(mg2, z, r, cache=TuneCache(path), reps=3, dtype="f32", coarse_max=15, coarse_sweeps=200)
+    assert not a["cached"] and b["cached"]
+    assert mg2.get_tuning() == {"chunk_pct": a["chunk_pct"], "tail_top_points": a["tail_top_points"]}
