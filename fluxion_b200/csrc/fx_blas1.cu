@@ -22,6 +22,37 @@ using namespace fx;
 
 namespace {
 
+// F32 fast path of the BLAS-1 ops that stream whole vectors: with 4-byte elements one access per
+// thread and iteration keeps too few bytes in flight (axpy measured 0.75, dot2 0.61 of HBM), so when
+// every pointer is 16-byte aligned each thread moves four elements per access (float4).  fv takes
+// the vector index j (elements 4j .. 4j+3), fs the scalar index of the n % 4 tail elements, which
+// the first threads of the grid take.  Elementwise results equal the scalar path's; the sums are
+// deterministic for a given n.
+template <int K, typename V, typename S, typename Fin>
+__global__ void __launch_bounds__(kBlock) k_vec4(size_t n, V fv, S fs, Fin fin, RedArgs<K> ra) {
+    grid_dep_enter();
+    CSum acc[K > 0 ? K : 1];
+#pragma unroll
+    for (int k = 0; k < (K > 0 ? K : 1); k++) acc[k] = CSum{0.0, 0.0};
+    const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
+    const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (size_t j = gid; j < n4; j += stride) fv(j, acc);
+    if (4 * n4 + gid < n) fs(4 * n4 + gid, acc);
+    if constexpr (K > 0) grid_reduce<K>(acc, ra, fin);
+}
+
+bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+template <int K, typename V, typename S, typename Fin>
+int launch_vec4(fx_ctx *ctx, size_t n, V fv, S fs, Fin fin, const char *what) {
+    FlatGeom g = flat_geom(ctx, (n + 3) / 4);
+    if (g.blocks == 0) return FX_OK;
+    timing_pre(ctx, what);
+    launch_pdl(ctx, k_vec4<K, V, S, Fin>, g.blocks, kBlock, 0, n, fv, fs, fin, red_args<K>(ctx));
+    timing_post(ctx, (double)n);
+    return check_launch(ctx, what);
+}
+
 template <typename T>
 __device__ __forceinline__ T tmax(T a, T b) { return fmax(a, b); }
 template <>
@@ -133,6 +164,21 @@ int fx_axpy(fx_ctx *ctx, double alpha, const fx_buf *x, fx_buf *y) {
         const T *xp = (const T *)x->ptr;
         T *yp = (T *)y->ptr;
         const T a = (T)alpha;
+        if constexpr (sizeof(T) == 4) {
+            if (aligned16(xp) && aligned16(yp) && x->len >= 4096)
+                return launch_vec4<0>(
+                    ctx, x->len,
+                    [=] __device__(size_t j, CSum *) {
+                        const float4 xv = reinterpret_cast<const float4 *>(xp)[j];
+                        float4 yv = reinterpret_cast<float4 *>(yp)[j];
+                        yv.x = fx_fma(a, xv.x, yv.x);
+                        yv.y = fx_fma(a, xv.y, yv.y);
+                        yv.z = fx_fma(a, xv.z, yv.z);
+                        yv.w = fx_fma(a, xv.w, yv.w);
+                        reinterpret_cast<float4 *>(yp)[j] = yv;
+                    },
+                    [=] __device__(size_t i, CSum *) { yp[i] = fx_fma(a, xp[i], yp[i]); }, NoFin{}, "axpy");
+        }
         return launch_flat<0>(ctx, x->len, [=] __device__(size_t i, CSum *) { yp[i] = fx_fma(a, xp[i], yp[i]); },
                               NoFin{}, nullptr, "axpy");
     });
@@ -268,9 +314,28 @@ int fx_dot(fx_ctx *ctx, const fx_buf *x, const fx_buf *y, double *out) {
     FX_DISPATCH(x->dtype, {
         const T *xp = (const T *)x->ptr;
         const T *yp = (const T *)y->ptr;
-        FX_TRY(launch_flat<1>(ctx, x->len,
-                              [=] __device__(size_t i, CSum *acc) { csum_add_prod_t<T>(acc[0], xp[i], yp[i]); },
-                              StoreFin<1>{ctx->d_result}, nullptr, "dot"));
+        bool vec = false;
+        if constexpr (sizeof(T) == 4) {
+            if (aligned16(xp) && aligned16(yp) && x->len >= 4096) {
+                vec = true;
+                FX_TRY(launch_vec4<1>(
+                    ctx, x->len,
+                    [=] __device__(size_t j, CSum *acc) {
+                        const float4 a = reinterpret_cast<const float4 *>(xp)[j];
+                        const float4 b = reinterpret_cast<const float4 *>(yp)[j];
+                        csum_add_prod_t<float>(acc[0], a.x, b.x);
+                        csum_add_prod_t<float>(acc[0], a.y, b.y);
+                        csum_add_prod_t<float>(acc[0], a.z, b.z);
+                        csum_add_prod_t<float>(acc[0], a.w, b.w);
+                    },
+                    [=] __device__(size_t i, CSum *acc) { csum_add_prod_t<float>(acc[0], xp[i], yp[i]); },
+                    StoreFin<1>{ctx->d_result}, "dot"));
+            }
+        }
+        if (!vec)
+            FX_TRY(launch_flat<1>(ctx, x->len,
+                                  [=] __device__(size_t i, CSum *acc) { csum_add_prod_t<T>(acc[0], xp[i], yp[i]); },
+                                  StoreFin<1>{ctx->d_result}, nullptr, "dot"));
     });
     return read_results(ctx, 1, out);
 }
@@ -290,12 +355,40 @@ int fx_dot2(fx_ctx *ctx, const fx_buf *a, const fx_buf *b, const fx_buf *c, cons
         const T *bp = (const T *)b->ptr;
         const T *cp = (const T *)c->ptr;
         const T *dp = (const T *)d->ptr;
-        FX_TRY(launch_flat<2>(ctx, a->len,
-                              [=] __device__(size_t i, CSum *acc) {
-                                  csum_add_prod_t<T>(acc[0], ap[i], bp[i]);
-                                  csum_add_prod_t<T>(acc[1], cp[i], dp[i]);
-                              },
-                              StoreFin<2>{ctx->d_result}, nullptr, "dot2"));
+        bool vec = false;
+        if constexpr (sizeof(T) == 4) {
+            if (aligned16(ap) && aligned16(bp) && aligned16(cp) && aligned16(dp) && a->len >= 4096) {
+                vec = true;
+                FX_TRY(launch_vec4<2>(
+                    ctx, a->len,
+                    [=] __device__(size_t j, CSum *acc) {
+                        const float4 va = reinterpret_cast<const float4 *>(ap)[j];
+                        const float4 vb = reinterpret_cast<const float4 *>(bp)[j];
+                        const float4 vc = reinterpret_cast<const float4 *>(cp)[j];
+                        const float4 vd = reinterpret_cast<const float4 *>(dp)[j];
+                        csum_add_prod_t<float>(acc[0], va.x, vb.x);
+                        csum_add_prod_t<float>(acc[0], va.y, vb.y);
+                        csum_add_prod_t<float>(acc[0], va.z, vb.z);
+                        csum_add_prod_t<float>(acc[0], va.w, vb.w);
+                        csum_add_prod_t<float>(acc[1], vc.x, vd.x);
+                        csum_add_prod_t<float>(acc[1], vc.y, vd.y);
+                        csum_add_prod_t<float>(acc[1], vc.z, vd.z);
+                        csum_add_prod_t<float>(acc[1], vc.w, vd.w);
+                    },
+                    [=] __device__(size_t i, CSum *acc) {
+                        csum_add_prod_t<float>(acc[0], ap[i], bp[i]);
+                        csum_add_prod_t<float>(acc[1], cp[i], dp[i]);
+                    },
+                    StoreFin<2>{ctx->d_result}, "dot2"));
+            }
+        }
+        if (!vec)
+            FX_TRY(launch_flat<2>(ctx, a->len,
+                                  [=] __device__(size_t i, CSum *acc) {
+                                      csum_add_prod_t<T>(acc[0], ap[i], bp[i]);
+                                      csum_add_prod_t<T>(acc[1], cp[i], dp[i]);
+                                  },
+                                  StoreFin<2>{ctx->d_result}, nullptr, "dot2"));
     });
     double v[2];
     FX_TRY(read_results(ctx, 2, v));

@@ -142,6 +142,23 @@ def test_reductions_f32(be, n):
     assert be.dot(X, Y) == be.dot(X, Y)
 
 
+@pytest.mark.parametrize("n", [4099, 1 << 20])
+def test_axpy_f32_is_one_rounding(be, n):
+    """F32 axpy is fma(alpha, x, y) in single precision (one rounding), on the 16-byte vector path
+    and its scalar tail alike: equal to the exactly rounded FP64 result except where that double
+    rounding could differ (at most one ulp)."""
+    rng = np.random.default_rng(77 + n)
+    x, y = rand(rng, n).astype(np.float32), rand(rng, n).astype(np.float32)
+    a = np.float32(0.3712)
+    X, Y = be.upload_f32(x), be.upload_f32(y)
+    be.axpy(float(a), X, Y)
+    got = Y.to_numpy().astype(np.float32)
+    want = (np.float64(a) * x.astype(np.float64) + y.astype(np.float64)).astype(np.float32)
+    ulp = np.spacing(np.abs(want))
+    assert np.all(np.abs(got - want) <= ulp)
+    assert np.mean(got == want) > 0.999
+
+
 def test_compensated_dot_recovers_cancelled_terms(be):
     # +B and -B pairs cancel exactly; only the small terms survive.  A plain double sum
     # loses them, the compensated (twice-working-precision) sum must not.
