@@ -141,19 +141,36 @@ __global__ void __launch_bounds__(256) k_lsm_apply(Op A, const uint32_t *__restr
     const int r0 = blockIdx.y * kTile, c0 = blockIdx.x * kTile;
     const double s = scale[0], inv_s = scale[1];
 
-    // ---- input: 34 x 34 points from (r0 - 3, c0 - 3), zero outside the grid
-    for (int k = tid; k < kInRows * kBufW; k += 256) {
-        const int iy = k / kBufW, ix = k - iy * kBufW;
-        const int gr = r0 - 3 + iy, gc = c0 - 3 + ix;
-        float ch0 = 0.f, ch1 = 0.f, ch2 = 0.f;
-        if (gr >= 0 && gr < rows && gc >= 0 && gc < cols) {
-            const size_t i = (size_t)gr * cols + gc;
-            input_channels<T>(q[i], A.vxv(i), A.vyv(i), A.diag(i), inv_s, inv_dx, inv_dy, ch0, ch1, ch2);
+    // ---- input: 34 x 34 points from (r0 - 3, c0 - 3), zero outside the grid.  A thread's points
+    // are loaded first (all of them in flight at once), then turned into channels.
+    {
+        constexpr int kIt = (kInRows * kBufW + 255) / 256;
+        T qv[kIt], xv[kIt], yv[kIt], dv[kIt];
+#pragma unroll
+        for (int j = 0; j < kIt; j++) {
+            const int k = tid + j * 256;
+            const int iy = k / kBufW, ix = k - iy * kBufW;
+            const int gr = r0 - 3 + iy, gc = c0 - 3 + ix;
+            qv[j] = xv[j] = yv[j] = dv[j] = (T)0;
+            if (k < kInRows * kBufW && gr >= 0 && gr < rows && gc >= 0 && gc < cols) {
+                const size_t i = (size_t)gr * cols + gc;
+                qv[j] = q[i];
+                xv[j] = A.vxv(i);
+                yv[j] = A.vyv(i);
+                dv[j] = A.diag(i);
+            }
         }
-        uint2 v;
-        v.x = pack_bf16x2(ch0, ch1);
-        v.y = pack_bf16x2(ch2, 0.f);
-        *reinterpret_cast<uint2 *>(XB + (size_t)k * 8) = v;
+#pragma unroll
+        for (int j = 0; j < kIt; j++) {
+            const int k = tid + j * 256;
+            if (k >= kInRows * kBufW) break;
+            float ch0, ch1, ch2;  // zero for points outside the grid (all inputs zero there)
+            input_channels<T>(qv[j], xv[j], yv[j], dv[j], inv_s, inv_dx, inv_dy, ch0, ch1, ch2);
+            uint2 v;
+            v.x = pack_bf16x2(ch0, ch1);
+            v.y = pack_bf16x2(ch2, 0.f);
+            *reinterpret_cast<uint2 *>(XB + (size_t)k * 8) = v;
+        }
     }
     __syncthreads();
 
