@@ -573,8 +573,14 @@ def run_convdiff(args):
     ok = True
     for nu in [float(v) for v in args.nu.split(",")]:
         op = ConvDiffOperator(g, VX, VY, -nu, sigma=0.0, coeff=1.0)
+        def fg_cgs2():
+            s_ = FgmresSolver(g, dev, 30, 1e-10 * fnorm, 2000)
+            s_.set_orthogonalization("cgs2")
+            return s_
+
         arms = [(mdt, name, make) for mdt in (DType.F64, DType.F32) for name, make in (
             ("fgmres30", lambda: FgmresSolver(g, dev, 30, 1e-10 * fnorm, 2000)),
+            ("fgmres30_cgs2", fg_cgs2),
             ("gmres30", lambda: GmresSolver(g, dev, 30, 1e-10 * fnorm, 2000)),
             ("bicgstab", lambda: BiCgStabSolver(g, dev, 1e-10 * fnorm, 2000)))
             if mdt == DType.F64 or name != "gmres30"]

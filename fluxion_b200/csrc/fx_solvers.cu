@@ -2094,7 +2094,110 @@ int fcg_solve_impl(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const St
 
 struct fx_fgmres : fx_gmres {
     // bufs: 0..m the basis V, m+1 w, m+2 .. 2m+1 the directions Z
+    bool cgs2 = false;               // fx_fgmres_set_orthogonalization
+    double *d_cgs = nullptr;         // [2 (restart + 2)]: the two passes' coefficients
+    double *d_part = nullptr;        // [blocks][kCgsMax] block partials of the multi-dot
+    unsigned *d_ticket = nullptr;
+    ~fx_fgmres() {
+        if (d_cgs) cudaFree(d_cgs);
+        if (d_part) cudaFree(d_part);
+        if (d_ticket) cudaFree(d_ticket);
+    }
 };
+
+namespace {
+
+// ------------------------------------------------ classical Gram-Schmidt, twice (CGS2), for FGMRES
+//
+// Option (fx_fgmres_set_orthogonalization): the Arnoldi step orthogonalises w against the whole
+// basis v_0 .. v_k in three passes, each reading w and the basis once, instead of one modified
+// Gram-Schmidt pass per basis vector:
+//   pass 0: h1_j = v_j . w
+//   pass 1: w -= sum_j h1_j v_j, then h2_j = v_j . w (the same pass, from the updated element)
+//   pass 2: w -= sum_j h2_j v_j, then ||w||^2
+// and h_jk = h1_j + h2_j (Giraud, Langou, Rozloznik 2005: twice is enough).  The sums of a pass are
+// per-thread FP64 partials folded in a fixed order (block, then the blocks by a last-block
+// ticket), so the coefficients are deterministic.
+constexpr int kCgsMax = 32;  // basis vectors per pass (restart <= 32)
+
+struct CgsArgs {
+    double *w;
+    const double *v[kCgsMax];
+    int kb;                  // basis vectors v_0 .. v_{kb-1}
+    const double *coef;      // pass 1 / 2: the coefficients subtracted
+    double *out;             // pass 0 / 1: kb dots; pass 2: out[0] = ||w||^2
+    double *part;
+    unsigned *ticket;
+};
+
+template <int PASS>
+__global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
+    grid_dep_enter();
+    constexpr int NS = PASS == 2 ? 1 : kCgsMax;
+    double acc[NS];
+#pragma unroll
+    for (int j = 0; j < NS; j++) acc[j] = 0.0;
+    __shared__ double c[kCgsMax];
+    if (PASS > 0 && threadIdx.x < kCgsMax) c[threadIdx.x] = threadIdx.x < a.kb ? a.coef[threadIdx.x] : 0.0;
+    __syncthreads();
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double wv = a.w[i];
+        if (PASS > 0) {
+#pragma unroll
+            for (int j = 0; j < kCgsMax; j++)
+                if (j < a.kb) wv = fma(-c[j], a.v[j][i], wv);
+            a.w[i] = wv;
+        }
+        if (PASS == 2) {
+            acc[0] = fma(wv, wv, acc[0]);
+        } else {  // pass 1 reads each v_j[i] a second time, from L1 (a thread's values were just loaded)
+#pragma unroll
+            for (int j = 0; j < NS; j++)
+                if (j < a.kb) acc[j] = fma(a.v[j][i], wv, acc[j]);
+        }
+    }
+    // block: warp shuffles, then the warps in order; blocks: the last one folds in block order
+    __shared__ double sh[kBlock / 32][NS];
+    __shared__ bool is_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int ns = PASS == 2 ? 1 : a.kb;
+    for (int j = 0; j < ns; j++) {
+        double v = acc[j < NS ? j : 0];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) sh[wid][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < ns) {
+        double t = 0.0;
+        for (int k = 0; k < kBlock / 32; k++) t += sh[k][threadIdx.x];
+        a.part[(size_t)blockIdx.x * kCgsMax + threadIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    if (threadIdx.x < ns) {
+        CSum t{0.0, 0.0};
+        for (unsigned b = 0; b < gridDim.x; b++)
+            csum_add(t, ((volatile double *)a.part)[(size_t)b * kCgsMax + threadIdx.x]);
+        a.out[threadIdx.x] = csum_value(t);
+    }
+    if (threadIdx.x == 0) *a.ticket = 0u;
+}
+
+template <int PASS>
+int launch_cgs(fx_ctx *ctx, size_t n, const CgsArgs &a) {
+    FlatGeom g = flat_geom(ctx, n);
+    timing_pre(ctx, "fgmres_cgs2");
+    launch_pdl(ctx, k_cgs<PASS>, g.blocks, kBlock, 0, n, a);
+    timing_post(ctx, (double)n, (double)n * 8.0 * (a.kb + 1 + (PASS > 0 ? 1 : 0)));
+    return check_launch(ctx, "fgmres_cgs2");
+}
+
+}  // namespace
 
 namespace {
 
@@ -2178,18 +2281,46 @@ int fgmres_solve_impl(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, co
                 FX_TRY(zero_fill<T>(ctx, Z[k], n, nullptr));
                 FX_TRY(pc->apply(&zk, &vk, nullptr, true));
             }
-            // w = A z_k with w.v_0, then modified Gram-Schmidt with each dot fused into the AXPY
-            FX_TRY((launch_pt<T, 1>(ctx, RR, CC, Ld1<T>{Z[k]}, PtGmAv<T, MODE, true>{A, w, V[0]}, FinSlot{dh + 0},
-                                       nullptr, "fgmres_av")));
-            for (size_t j = 0; j <= k; j++) {
-                const T *vj = V[j];
-                const T *vn = j < k ? V[j + 1] : nullptr;
-                const double *hj = dh + j;
-                FX_TRY(launch_flat<1>(ctx, n, FlatGmMgs<T>{w, vj, vn, hj}, FinSlot{dh + j + 1}, nullptr, "fgmres_mgs"));
+            double h_kp1_k = 0.0;
+            if (s->cgs2) {  // w = A z_k, then CGS2 (three passes over the basis)
+                FX_TRY((launch_pt<T, 0>(ctx, RR, CC, Ld1<T>{Z[k]}, PtGmAv<T, MODE, false>{A, w, nullptr}, NoFin{},
+                                           nullptr, "fgmres_av")));
+                CgsArgs ca{};
+                ca.w = w;
+                ca.kb = (int)k + 1;
+                for (size_t j = 0; j <= k; j++) ca.v[j] = V[j];
+                ca.part = s->d_part;
+                ca.ticket = s->d_ticket;
+                double *h1 = s->d_cgs, *h2 = s->d_cgs + (m + 2);
+                ca.out = h1;
+                FX_TRY(launch_cgs<0>(ctx, n, ca));
+                ca.coef = h1;
+                ca.out = h2;
+                FX_TRY(launch_cgs<1>(ctx, n, ca));
+                ca.coef = h2;
+                ca.out = h2 + k + 1;
+                FX_TRY(launch_cgs<2>(ctx, n, ca));
+                std::vector<double> hv(2 * (m + 2));
+                FX_CUDA(cudaMemcpyAsync(hv.data(), s->d_cgs, 2 * (m + 2) * sizeof(double), cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+                FX_CUDA(cudaStreamSynchronize(ctx->stream));
+                for (size_t j = 0; j <= k; j++) H(j, k) = hv[j] + hv[m + 2 + j];
+                h_kp1_k = std::sqrt(hv[m + 2 + k + 1]);
+            } else {
+                // w = A z_k with w.v_0, then modified Gram-Schmidt with each dot fused into the AXPY
+                FX_TRY((launch_pt<T, 1>(ctx, RR, CC, Ld1<T>{Z[k]}, PtGmAv<T, MODE, true>{A, w, V[0]}, FinSlot{dh + 0},
+                                           nullptr, "fgmres_av")));
+                for (size_t j = 0; j <= k; j++) {
+                    const T *vj = V[j];
+                    const T *vn = j < k ? V[j + 1] : nullptr;
+                    const double *hj = dh + j;
+                    FX_TRY(launch_flat<1>(ctx, n, FlatGmMgs<T>{w, vj, vn, hj}, FinSlot{dh + j + 1}, nullptr,
+                                          "fgmres_mgs"));
+                }
+                FX_TRY(read_h(k));
+                for (size_t j = 0; j <= k; j++) H(j, k) = s->h_h[j];
+                h_kp1_k = std::sqrt(s->h_h[k + 1]);
             }
-            FX_TRY(read_h(k));
-            for (size_t j = 0; j <= k; j++) H(j, k) = s->h_h[j];
-            const double h_kp1_k = std::sqrt(s->h_h[k + 1]);
             H(k + 1, k) = h_kp1_k;
             if (h_kp1_k > 1e-30) FX_TRY(scale_into(V[k + 1], w, 1.0 / h_kp1_k));
             for (size_t j = 0; j < k; j++) {
@@ -3474,6 +3605,24 @@ int fx_fgmres_create(fx_ctx *ctx, const fx_grid *g, size_t restart, double tol, 
 }
 int fx_fgmres_destroy(fx_fgmres *s) {
     delete s;
+    return FX_OK;
+}
+int fx_fgmres_set_orthogonalization(fx_fgmres *s, int method) {
+    if (!s) return fail(FX_ERR_INVALID_ARGUMENT, "null solver");
+    if (method != 0 && method != 1) return fail(FX_ERR_INVALID_ARGUMENT, "method: 0 = MGS, 1 = CGS2");
+    if (method == 1 && s->restart > (size_t)kCgsMax)
+        return fail(FX_ERR_UNSUPPORTED, "CGS2 orthogonalisation needs restart <= 32");
+    if (method == 1 && !s->d_cgs) {
+        const size_t blocks = (size_t)s->ctx->num_sms * 8;  // flat_geom's cap
+        if (cudaMalloc(&s->d_cgs, 2 * (s->restart + 2) * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&s->d_part, blocks * kCgsMax * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&s->d_ticket, sizeof(unsigned)) != cudaSuccess ||
+            cudaMemset(s->d_ticket, 0, sizeof(unsigned)) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return fail(FX_ERR_BACKEND, "fgmres CGS2 scratch allocation failed");
+        }
+    }
+    s->cgs2 = method == 1;
     return FX_OK;
 }
 int fx_fgmres_set_params(fx_fgmres *s, double tol, size_t max_iter) {

@@ -531,6 +531,11 @@ class FgmresSolver(_Native):
     def name(self) -> str:
         return "FGMRES"
 
+    def set_orthogonalization(self, method: str) -> None:
+        """"mgs" (default, the reference's) or "cgs2" (classical Gram-Schmidt twice: three passes
+        over the basis per Arnoldi step; restart <= 32)."""
+        check(L.lib().fx_fgmres_set_orthogonalization(self.h, {"mgs": 0, "cgs2": 1}[method]))
+
 
 class GmresSolver(_Native):
     """gmres.rs:24-491: restarted GMRES(m) with modified Gram-Schmidt."""

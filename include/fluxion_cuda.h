@@ -428,6 +428,10 @@ int fx_fcg_solve_preconditioned(fx_fcg *s, fx_buf *x, const fx_buf *b, double co
 int fx_fgmres_create(fx_ctx *ctx, const fx_grid *g, size_t restart, double tol, size_t max_iter,
                      fx_fgmres **out);
 int fx_fgmres_destroy(fx_fgmres *s);
+/* Orthogonalisation of the Arnoldi step: 0 = modified Gram-Schmidt (default; the reference's,
+ * gmres.rs:185-189), 1 = classical Gram-Schmidt twice (CGS2: three passes over the basis per step
+ * instead of one per basis vector; restart <= 32).  New. */
+int fx_fgmres_set_orthogonalization(fx_fgmres *s, int method);
 int fx_fgmres_set_params(fx_fgmres *s, double tol, size_t max_iter);
 int fx_fgmres_solve(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                     const fx_boundaries *bc, fx_stats *out);

@@ -200,3 +200,23 @@ def test_multigrid_replays_its_recorded_cycle(dev):
         small = Grid.square(N - 2, 1.0)  # vectors of another extent are refused before any replay
         with pytest.raises(DimensionMismatch):
             mg.apply(Field.zeros(small, DType.F64, dev), Field.zeros(small, DType.F64, dev))
+
+
+@pytest.mark.parametrize("nu", [1e-2, 1e-3])
+def test_fgmres_cgs2_matches_oracle_mgs_solve(dev, nu):
+    """Flexible GMRES(30) with classical Gram-Schmidt twice (three passes over the basis per Arnoldi
+    step) reaches the oracle's MGS solve: same stop reason, iterations within one, solutions within
+    1e-8, the tolerance met on the residual the oracle recomputes."""
+    from fluxion_b200 import ConvDiffMultigrid, DType, FgmresSolver, Field
+    g, N, f, op, oop = _problem(127, dev, nu=nu)
+    tol = 1e-10 * np.linalg.norm(f)
+    b = Field.from_f64(g, f, dev)
+    x = Field.zeros(g, DType.F64, dev)
+    solver = FgmresSolver(g, dev, 30, tol, 300)
+    solver.set_orthogonalization("cgs2")
+    s = solver.solve_op(x, b, op, ConvDiffMultigrid(op))
+    xo = np.zeros(N * N)
+    it, _, reason = O.fgmres_solve_op(xo, f, oop, 30, tol, 300, O.CdMultigrid(oop))
+    assert s.converged() and reason == 0 and abs(s.iterations - it) <= 1, (s, it)
+    assert np.linalg.norm(O.op_apply(oop, x.to_vec_f64()) - f) < 1.01 * tol
+    assert rel_err(x.to_vec_f64(), xo) < 1e-8
