@@ -877,8 +877,55 @@ def main():
         return {"value": e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": N * N * 8,
                 "d2h_bytes_per_step": N * N * 8, "result_matches_device_run": bool(np.array_equal(u_host, want))}
 
-    e2e_plain = e2e(mg64, u64)
-    e2e_mixed = e2e(mg32, u32)
+    def e2e_pipelined(mg, want, nsteps):
+        """The same stream of solves with the copies overlapped: step k's f is uploaded on one copy
+        stream and step k-2's u read back on another while step k-1 solves (double-buffered b and
+        x, ordered by events).  Every step still uploads its f and reads back its u."""
+        up_s, down_s = torch.cuda.Stream(), torch.cuda.Stream()
+        bs = [b, Field.zeros(P.grid, DType.F64, dev)]
+        xs = [x, Field.zeros(P.grid, DType.F64, dev)]
+        outs = [torch.empty(N * N, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+        ev_up = [torch.cuda.Event() for _ in range(2)]
+        ev_down = [torch.cuda.Event() for _ in range(2)]
+        for e_ in ev_down:
+            e_.record(down_s)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        w0 = time.perf_counter()
+        for k in range(nsteps + 2):
+            if k < nsteps:  # upload of step k (its buffer's last reader, step k-2, has returned)
+                bs[k % 2].write_async(f_host, up_s.cuda_stream)
+                ev_up[k % 2].record(up_s)
+            j = k - 2
+            if 0 <= j < nsteps:  # read-back of step j (solved and returned)
+                xs[j % 2].copy_to_host_async(outs[j % 2], down_s.cuda_stream)
+                ev_down[j % 2].record(down_s)
+            j = k - 1
+            if 0 <= j < nsteps:  # solve of step j after its upload and the read-back that used its x
+                stream.wait_event(ev_up[j % 2])
+                stream.wait_event(ev_down[j % 2])
+                xs[j % 2].fill(0.0)
+                cg.solve_preconditioned(xs[j % 2], bs[j % 2], P.coeff, P.stencil, None, mg)
+        torch.cuda.synchronize()
+        e_ms = (time.perf_counter() - w0) * 1e3 / nsteps
+        if dist:
+            t = torch.tensor([e_ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        ok = all(bool(np.array_equal(o, want)) for o in outs)
+        return {"value": e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": N * N * 8,
+                "d2h_bytes_per_step": N * N * 8, "result_matches_device_run": ok,
+                "how": "a stream of solves through the public API: step k's upload and step k-2's read-back "
+                       "on two copy streams while step k-1 solves (pinned host memory, double-buffered)"}
+
+    e2e_plain_serial = e2e(mg64, u64)
+    e2e_mixed_serial = e2e(mg32, u32)
+    e2e_pipelined(mg64, u64, max(2, args.warmup))  # warm-up of the copy streams and buffers
+    e2e_plain = e2e_pipelined(mg64, u64, args.steps)
+    e2e_plain["serial"] = e2e_plain_serial
+    e2e_mixed = e2e_pipelined(mg32, u32, args.steps)
+    e2e_mixed["serial"] = e2e_mixed_serial
 
     # roofline of the dominant kernel, live over the timed plain solves
     roof = None

@@ -642,4 +642,30 @@ int fx_copy_to_host_f32(fx_ctx *ctx, const fx_buf *b, float *dst, size_t len) {
     return read_host(ctx, b, dst, FX_F32, len);
 }
 
+// Asynchronous copies between an F64 buffer and page-locked host memory, enqueued on `stream`
+// (NULL: the context's stream) without waiting; the caller orders them with events.
+int fx_write_f64_async(fx_ctx *ctx, fx_buf *b, const double *src, size_t len, void *stream) {
+    if (!ctx || !b || (!src && len)) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (b->dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "asynchronous copies take F64 buffers");
+    if (len != b->len)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "dimension mismatch: expected " + std::to_string(b->len) +
+                                                   ", got " + std::to_string(len));
+    if (!len) return FX_OK;
+    FX_CUDA(cudaMemcpyAsync(b->ptr, src, len * sizeof(double), cudaMemcpyHostToDevice,
+                            stream ? (cudaStream_t)stream : ctx->stream));
+    return FX_OK;
+}
+
+int fx_copy_to_host_f64_async(fx_ctx *ctx, const fx_buf *b, double *dst, size_t len, void *stream) {
+    if (!ctx || !b || (!dst && len)) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (b->dtype != FX_F64) return fail(FX_ERR_INVALID_ARGUMENT, "asynchronous copies take F64 buffers");
+    if (len != b->len)
+        return fail(FX_ERR_DIMENSION_MISMATCH, "destination length mismatch: expected " + std::to_string(b->len) +
+                                                   ", got " + std::to_string(len));
+    if (!len) return FX_OK;
+    FX_CUDA(cudaMemcpyAsync(dst, b->ptr, len * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream ? (cudaStream_t)stream : ctx->stream));
+    return FX_OK;
+}
+
 }  // extern "C"

@@ -11,7 +11,10 @@ from typing import Optional, Tuple
 
 import numpy as np
 
-from .backend import BackendUnavailable, CudaBackend, CudaBuffer
+import ctypes as C
+
+from . import _lib as L
+from .backend import BackendUnavailable, CudaBackend, CudaBuffer, check
 from .core import Boundaries, DimensionMismatch, DType, Grid, Stencil
 
 
@@ -120,6 +123,24 @@ class Field:
 
     def write(self, data) -> None:
         self.storage.write(np.asarray(data))
+
+    def write_async(self, data: np.ndarray, stream: int = 0) -> None:
+        """Enqueue the copy of a contiguous float64 host array (page-locked for a true DMA) into
+        this F64 field on `stream` (a cudaStream_t handle; 0 = the backend's stream) without
+        waiting (fx_write_f64_async).  The caller orders it against the solves with events."""
+        if data.dtype != np.float64 or not data.flags.c_contiguous:
+            raise TypeError("write_async takes a contiguous float64 array")
+        check(L.lib().fx_write_f64_async(self._b.ctx, self.storage.handle,
+                                         data.ctypes.data_as(C.POINTER(C.c_double)), data.size, stream or None))
+
+    def copy_to_host_async(self, out: np.ndarray, stream: int = 0) -> None:
+        """Enqueue the copy of this F64 field into a contiguous float64 host array on `stream`
+        without waiting (fx_copy_to_host_f64_async)."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise TypeError("copy_to_host_async takes a contiguous float64 array")
+        check(L.lib().fx_copy_to_host_f64_async(self._b.ctx, self.storage.handle,
+                                                out.ctypes.data_as(C.POINTER(C.c_double)), out.size,
+                                                stream or None))
 
     @property
     def _b(self) -> CudaBackend:

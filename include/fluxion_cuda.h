@@ -177,6 +177,12 @@ int fx_copy_to_host_f32(fx_ctx *ctx, const fx_buf *buf, float *dst, size_t len);
 /* Host -> existing buffer (no reallocation), converting to the buffer's dtype. */
 int fx_write_f64(fx_ctx *ctx, fx_buf *buf, const double *src, size_t len);
 int fx_write_f32(fx_ctx *ctx, fx_buf *buf, const float *src, size_t len);
+/* Asynchronous copies between an F64 buffer and page-locked host memory (new): enqueued on `stream`
+ * (a cudaStream_t; NULL = the context's stream), no wait.  The caller orders them against the
+ * library's work with events, so that uploads and read-backs of a stream of solves overlap the
+ * solves.  From pageable memory the driver copies synchronously. */
+int fx_write_f64_async(fx_ctx *ctx, fx_buf *buf, const double *src, size_t len, void *stream);
+int fx_copy_to_host_f64_async(fx_ctx *ctx, const fx_buf *buf, double *dst, size_t len, void *stream);
 
 /* ------------------------------------------------------------------ */
 /* Backend trait ops (crates/core/src/backend.rs)                      */

@@ -90,3 +90,33 @@ def test_pool_buffers_are_zeroed_and_follow_a_stream_switch():
     from fluxion_b200 import DimensionMismatch
     with pytest.raises(DimensionMismatch):
         v.copy_to_host(np.empty(data.size - 1))
+
+
+def test_async_copies_on_other_streams_ordered_by_events():
+    """fx_write_f64_async / fx_copy_to_host_f64_async on two copy streams, ordered against the
+    library's stream by events, move exactly the data (a round trip through an AXPY)."""
+    import torch
+    from fluxion_b200 import DType, Device, Field, Grid
+    dev = Device.Cuda(0)
+    be = dev.backend()
+    g = Grid.square(1025, 1.0 / 1024)
+    n = 1025 * 1025
+    src = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    src[:] = np.random.default_rng(9).uniform(-1, 1, n)
+    dst = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    lib = torch.cuda.ExternalStream(be.stream()) if be.stream() else torch.cuda.current_stream()
+    a, y = Field.zeros(g, DType.F64, dev), Field.zeros(g, DType.F64, dev)
+    y.fill(1.0)
+    be.synchronize()
+    a.write_async(src, up.cuda_stream)
+    e1 = torch.cuda.Event()
+    e1.record(up)
+    lib.wait_event(e1)
+    y.axpy(2.0, a)  # y = 1 + 2 src on the library's stream
+    e2 = torch.cuda.Event()
+    e2.record(lib)
+    down.wait_event(e2)
+    y.copy_to_host_async(dst, down.cuda_stream)
+    down.synchronize()
+    assert np.array_equal(dst, 1.0 + 2.0 * src)
