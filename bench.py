@@ -684,10 +684,13 @@ def run_learned(args):
         fnorm = float(np.linalg.norm(f))
         xr, sr, _ = solve(op, g, b, ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS), 1e-12 * fnorm)
         u_ref = xr.to_vec_f64()
-        for learned in (False, True):
+        # arms: the plain cycle; learned smoothing on every level of at least 1024 points; learned
+        # smoothing only on the levels of the training problems' sizes (at most 513^2 points)
+        for arm, lo, hi in (("plain", 0, 0), ("learned", 1024, 0), ("learned_levels_upto_513sq", 1024, 513 * 513)):
+            learned = arm != "plain"
             mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS)
             if learned:
-                mg.set_learned(lsm, min_points=1024, fallback_ratio=0.9)
+                mg.set_learned(lsm, min_points=lo, fallback_ratio=0.9, max_points=hi)
             x, st, ms = solve(op, g, b, mg, 1e-10 * fnorm)
             ax = Field.zeros(g, DType.F64, dev)
             op.apply(x, ax)
@@ -696,7 +699,7 @@ def run_learned(args):
             u = x.to_vec_f64()
             err = float(np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref))
             ok = ok and st.converged() and rel < 1e-10
-            r = {"nu": nu, "arm": "learned" if learned else "plain", "iterations": st.iterations,
+            r = {"nu": nu, "arm": arm, "iterations": st.iterations,
                  "converged": st.converged(), "ms": ms, "ms_per_iteration": ms / max(1, st.iterations),
                  "true_rel_residual": rel, "err_vs_fp64_reference_solve": err,
                  "reference_solve": {"iterations": sr.iterations, "tol": "1e-12 relative"}}

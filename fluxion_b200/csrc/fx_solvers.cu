@@ -2873,7 +2873,7 @@ struct fx_cdmg {
     // with the network; each application is checked and, when the learned cycle reduced
     // ||r|| by less than lsm_ratio, recomputed with the plain cycle
     const fx_lsm *lsm = nullptr;
-    size_t lsm_min_points = 0;
+    size_t lsm_min_points = 0, lsm_max_points = 0;  // 0: no upper bound
     double lsm_ratio = 0.9;
     double *d_lsm_scale = nullptr;          // [2]: s, 1 / s of the current learned step
     int *d_plain_skip = nullptr;            // 1: the plain recomputation is not needed
@@ -2933,7 +2933,8 @@ int cd_cycle(fx_cdmg *mg, T *x, const T *b, T *x_other, const int *skip, bool le
     auto smooth = [&](int l, size_t n) -> int {
         const CdLevel &L = mg->lv[l];
         const auto A = mg->level_op<T>(l);
-        if (learned && l < nl - 1 && L.rows * L.cols >= mg->lsm_min_points) {  // in place; oth[l] holds q
+        if (learned && l < nl - 1 && L.rows * L.cols >= mg->lsm_min_points &&
+            (!mg->lsm_max_points || L.rows * L.cols <= mg->lsm_max_points)) {  // in place; oth[l] holds q
             for (size_t k = 0; k < n; k++)
                 FX_TRY(lsm_step<T>(ctx, mg->lsm, A, cur[l], oth[l], rhs[l], omega, L.rows, L.cols, L.dx, L.dy,
                                    mg->d_lsm_scale, skip));
@@ -3827,13 +3828,21 @@ int fx_cdmg_set_replay(fx_cdmg *mg, int enabled) {
     return FX_OK;
 }
 
-int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, double fallback_ratio) {
+int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, size_t max_points, double fallback_ratio) {
     if (!mg) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     if (lsm && lsm->ctx->device != mg->ctx->device)
         return fail(FX_ERR_INVALID_ARGUMENT, "learned smoother lives on another device");
     if (lsm && !(fallback_ratio > 0.0)) return fail(FX_ERR_INVALID_ARGUMENT, "fallback ratio must be positive");
-    if (lsm && mg->lv[0].rows * mg->lv[0].cols < min_points)
-        return fail(FX_ERR_INVALID_ARGUMENT, "no level reaches min_points: the cycle would not use the network");
+    if (lsm) {
+        bool any = false;
+        for (size_t l = 0; l + 1 < mg->lv.size(); l++) {
+            const size_t pts = mg->lv[l].rows * mg->lv[l].cols;
+            any = any || (pts >= min_points && (!max_points || pts <= max_points));
+        }
+        if (!any)
+            return fail(FX_ERR_INVALID_ARGUMENT,
+                        "no level in [min_points, max_points]: the cycle would not use the network");
+    }
     FX_CUDA(cudaStreamSynchronize(mg->ctx->stream));
     mg->drop_replays();  // the recorded launch sequence changes
     if (lsm && !mg->d_lsm_scale) {
@@ -3844,6 +3853,7 @@ int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, doubl
     }
     mg->lsm = lsm;
     mg->lsm_min_points = min_points;
+    mg->lsm_max_points = max_points;
     mg->lsm_ratio = fallback_ratio;
     return FX_OK;
 }

@@ -422,14 +422,14 @@ class ConvDiffMultigrid(Preconditioner):
         (fx_cdmg_set_replay; off by default)."""
         check(L.lib().fx_cdmg_set_replay(self.h, 1 if enabled else 0))
 
-    def set_learned(self, smoother, min_points: int = 4096, fallback_ratio: float = 0.9) -> None:
-        """Smooth every level of at least `min_points` points (the coarsest excepted) with the
-        learned smoother (`fluxion_b200.learned.LearnedSmoother`) in place of the Jacobi sweeps;
-        each application whose ||r - A z|| exceeds fallback_ratio ||r|| is recomputed by the plain
-        cycle on the device (fx_cdmg_set_learned).  None switches it off."""
+    def set_learned(self, smoother, min_points: int = 4096, fallback_ratio: float = 0.9, max_points: int = 0) -> None:
+        """Smooth every level of `min_points` to `max_points` points (0: no bound; the coarsest
+        excepted) with the learned smoother (`fluxion_b200.learned.LearnedSmoother`) in place of the
+        Jacobi sweeps; each application whose ||r - A z|| exceeds fallback_ratio ||r|| is recomputed
+        by the plain cycle on the device (fx_cdmg_set_learned).  None switches it off."""
         self._lsm = smoother
         check(L.lib().fx_cdmg_set_learned(self.h, smoother.h if smoother is not None else None, int(min_points),
-                                          float(fallback_ratio)))
+                                          int(max_points), float(fallback_ratio)))
 
     def learned_stats(self):
         """(checked applications, fallbacks to the plain cycle) so far."""

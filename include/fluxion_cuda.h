@@ -535,12 +535,13 @@ int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, siz
  * epoch e, each batch's loss taken before its step. */
 int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, double lr, double lambda,
                  unsigned long long seed, double *epoch_loss);
-/* Learned smoothing in a conv-diff multigrid: every level of at least min_points points except the
- * coarsest smooths with learned steps in place of the Jacobi sweeps (n_pre and n_post of them).
+/* Learned smoothing in a conv-diff multigrid: every level of min_points to max_points points (0: no
+ * upper bound) except the coarsest smooths with learned steps in place of the Jacobi sweeps (n_pre and
+ * n_post of them).
  * Each application is checked on the device: when ||r - A z|| > fallback_ratio ||r|| the plain
  * cycle recomputes z (the flexible solvers accept either).  lsm NULL switches it off; lsm must
  * outlive the multigrid's use of it.  stats: checked applications and fallbacks so far. */
-int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, double fallback_ratio);
+int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, size_t max_points, double fallback_ratio);
 int fx_cdmg_learned_stats(fx_cdmg *mg, unsigned long long *applications, unsigned long long *fallbacks);
 
 /* ------------------------------------------------------------------ */
