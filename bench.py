@@ -422,7 +422,7 @@ def run_batch(args):
     if args.batched:
         res, wall, extra = run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist)
         lanes = 0
-        return _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist, lanes, extra)
+        return _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist, lanes, extra, host)
 
     def make_lane(k):
         dev = Device.Cuda(local_rank, lane=k)
@@ -499,10 +499,46 @@ def run_batch(args):
     wall = time.perf_counter() - t_begin
     if errors:
         raise errors[0]
-    return _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist, lanes, extra)
+    return _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist, lanes, extra, host)
 
 
-def _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist, lanes, extra):
+# Algorithmic bytes per grid point of one BiCGSTAB iteration with the conv-diff V(2,2)-cycle in
+# FP64 (fields x, b, vx, vy streamed once per pass): per cycle, level 0 = sweep pair 40 + residual
+# 40 + restriction 10 + prolongation 18 + sweep pair 40 = 148, x 4/3 for the coarser levels; two
+# cycles per iteration; the vector passes p 32, v = A p_hat 40, s 24, t = A s_hat 40, the update 64
+# and the two zero fills 16.
+BATCH_BYTES_PER_POINT_ITER = 2 * 148 * 4 / 3 + 216
+
+
+def batch_cpu_baseline(ks, host, sample_n=16):
+    """The oracle's BiCGSTAB + conv-diff V(2,2)-cycle (FP64, the same algorithm) on a sample of the
+    batch keeping its size mix, on all host threads; solves/s extrapolated to the whole batch by
+    points."""
+    from oracle import oracle as O
+    from fluxion_b200.autotune import _sample
+    O.set_threads(os.cpu_count() or 1)
+    sides = [int(2 ** k + 1) for k in ks]
+    idx = [i for i in _sample(sides, sample_n) if i in host]
+    t_tot, pts = 0.0, 0
+    for i in idx:
+        n, vx, vy, f, fnorm = host[i]
+        N, h = n + 2, 1.0 / (n + 1)
+        op = O.cd_op(N, N, h, h, np.ascontiguousarray(vx), np.ascontiguousarray(vy), kappa=None, kappa_s=-1e-2,
+                     sigma=0.0, coeff=1.0)
+        x = np.zeros(N * N)
+        t0 = time.perf_counter()
+        O.bicgstab_solve_op(x, np.ascontiguousarray(f), op, 1e-10 * fnorm, 200,
+                            O.CdMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS))
+        t_tot += time.perf_counter() - t0
+        pts += N * N
+    all_pts = sum(s * s for s in sides)
+    per_point_s = t_tot / max(1, pts)
+    return {"value": len(sides) / (per_point_s * all_pts), "unit": "solves/s", "cores": O.get_threads(),
+            "kind": "port", "sample": f"{len(idx)} problems keeping the batch's size mix ({t_tot:.1f} s), "
+                                      "extrapolated to the whole batch by grid points"}
+
+
+def _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist, lanes, extra, host=None):
     import torch
     from fluxion_b200.batch import gather_results
     if dist:  # the job's wall time is the slowest rank's; then one gather of the results
@@ -520,6 +556,21 @@ def _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist
     ms = np.array([r[3] for r in res])
     its = np.array([r[1] for r in res])
     ok = all(r[2] for r in res)
+    peak, peak_kind = measured_peaks()
+    roof = None
+    if args.batched and extra.get("device_solve_ms"):
+        # solve level: the algorithmic bytes of every problem's iterations over the batch's device time
+        byts = sum(BATCH_BYTES_PER_POINT_ITER * (r[1] + 1) * (r[0] + 2) ** 2 for r in res)
+        ach = byts / (extra["device_solve_ms"] * 1e-3) / 1e9
+        roof = {"kernel": "whole batched solve (all phases)", "bound": "hbm", "achieved": ach, "peak": peak,
+                "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind, "traffic": None,
+                "bytes_per_point_iteration": BATCH_BYTES_PER_POINT_ITER}
+    cpu = None
+    if not args.no_cpu and host is not None:
+        try:
+            cpu = batch_cpu_baseline(ks, host)
+        except Exception as e:  # reported, never required
+            cpu = {"value": None, "unit": "solves/s", "kind": "port", "sample": f"failed: {e}"}
     print(json.dumps({
         "mode": "batch", "workload": f"convdiff_batch_{args.batch}_k{k_lo}-{k_hi}_nu1e-2_bicgstab_cdmg",
         "solver": "batched (one launch per phase over the batch)" if args.batched else "lanes",
@@ -532,7 +583,7 @@ def _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist
         "per_problem_ms_p99": float(np.percentile([r[5] * 1e3 for r in res], 99)),
         "solve_ms_p50": float(np.percentile(ms, 50)), "solve_ms_p99": float(np.percentile(ms, 99)),
         "iterations_p50": float(np.percentile(its, 50)), "iterations_max": int(its.max()),
-        "all_converged": ok, "max_true_rel_residual": max(r[4] for r in res),
+        "all_converged": ok, "max_true_rel_residual": max(r[4] for r in res), "roofline": roof, "cpu_baseline": cpu,
         "dtype": "f64" if extra.get("tuning", {}).get("cycle_dtype", args.mg_dtype) == "f64"
         else "f64 (Krylov) / f32 (V-cycle)",
         "data": "synthetic (seeded per problem), page-locked host arrays",
