@@ -50,3 +50,30 @@ def read_raw(path: Union[str, os.PathLike], device=None):
     from .field import Field
     grid, data = read_raw_array(path)
     return Field.from_f64(grid, data, device)
+
+
+# Checkpoint of the learned smoother's parameters: an 8-byte magic, the parameter count as a
+# little-endian u64, then the FP32 master parameters in the library's order (W1, b1, W2, b2, W3, b3).
+_LSM_MAGIC = b"FXLSM001"
+
+
+def write_smoother_params(path: Union[str, os.PathLike], params: np.ndarray) -> None:
+    p = np.ascontiguousarray(params, dtype="<f4").ravel()
+    with open(path, "wb") as f:
+        f.write(_LSM_MAGIC)
+        f.write(struct.pack("<Q", p.size))
+        f.write(p.tobytes())
+
+
+def read_smoother_params(path: Union[str, os.PathLike]) -> np.ndarray:
+    with open(path, "rb") as f:
+        if f.read(8) != _LSM_MAGIC:
+            raise ValueError("not a learned-smoother checkpoint")
+        head = f.read(8)
+        if len(head) != 8:
+            raise EOFError("checkpoint shorter than its header")
+        (n,) = struct.unpack("<Q", head)
+        body = f.read(4 * n)
+        if len(body) != 4 * n:
+            raise EOFError(f"checkpoint holds {len(body) // 4} of {n} parameters")
+    return np.frombuffer(body, dtype="<f4").astype(np.float32)

@@ -123,6 +123,19 @@ class LearnedSmoother:
                                    out))
         return [out[i] for i in range(int(epochs))]
 
+    def save(self, path) -> None:
+        """Write the FP32 master parameters to a checkpoint file (fluxion_b200.io format)."""
+        from .io import write_smoother_params
+        write_smoother_params(path, self.params)
+
+    def load(self, path) -> None:
+        """Read parameters from a checkpoint (the optimiser state restarts)."""
+        from .io import read_smoother_params
+        p = read_smoother_params(path)
+        if p.size != param_count():
+            raise ValueError(f"checkpoint holds {p.size} parameters, the network has {param_count()}")
+        self.params = p
+
     def smooth(self, op, x: Field, b: Field, omega: float = 0.8, steps: int = 1) -> None:
         """`steps` learned smoothing steps on op x = b (x in place)."""
         check(L.lib().fx_lsm_smooth(self.h, op.h, x.storage.handle, b.storage.handle, float(omega), int(steps)))

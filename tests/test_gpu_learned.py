@@ -203,3 +203,22 @@ def test_training_beats_the_jacobi_step_and_learned_fgmres_converges(dev):
         assert np.linalg.norm(O.op_apply(oop, x.to_vec_f64()) - f) < 1.01 * tol
         its[name] = (st.iterations, mg.learned_stats() if name == "learned" else None)
     print("FGMRES(30) iterations (plain, learned [applications, fallbacks]):", its)
+
+
+def test_checkpoint_reload_gives_the_same_smoothing(dev, tmp_path):
+    from fluxion_b200 import Field
+    from fluxion_b200.learned import LearnedSmoother
+    n, nu = 61, 1e-2
+    g, N, h, vx, vy, f, op, oop = _cd(n, nu, dev, 17)
+    a = LearnedSmoother(dev, seed=5)
+    params = _random_params(a, 6)
+    a.save(tmp_path / "lsm.bin")
+    b = LearnedSmoother(dev, seed=99)
+    b.load(tmp_path / "lsm.bin")
+    assert np.array_equal(b.params, params)
+    outs = []
+    for m in (a, b):
+        x = Field.from_f64(g, np.zeros(N * N), dev)
+        m.smooth(op, x, Field.from_f64(g, f, dev), 0.8, 2)
+        outs.append(x.to_vec_f64())
+    assert np.array_equal(outs[0], outs[1])

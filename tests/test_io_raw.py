@@ -42,3 +42,21 @@ def test_errors(tmp_path):
     bad.write_bytes(struct.pack("<QQdd", 0, 4, 0.1, 0.1))
     with pytest.raises(InvalidGrid):
         read_raw_array(bad)
+
+
+def test_smoother_checkpoint_roundtrip(tmp_path):
+    import numpy as np
+    import pytest
+    from fluxion_b200.io import read_smoother_params, write_smoother_params
+    p = np.random.default_rng(1).normal(size=2913).astype(np.float32)
+    path = tmp_path / "lsm.bin"
+    write_smoother_params(path, p)
+    assert path.stat().st_size == 16 + 4 * 2913
+    assert np.array_equal(read_smoother_params(path), p)
+    raw = path.read_bytes()
+    (tmp_path / "bad.bin").write_bytes(b"XXXXXXXX" + raw[8:])
+    with pytest.raises(ValueError):
+        read_smoother_params(tmp_path / "bad.bin")
+    (tmp_path / "short.bin").write_bytes(raw[:100])
+    with pytest.raises(EOFError):
+        read_smoother_params(tmp_path / "short.bin")
