@@ -736,12 +736,17 @@ def run_learned(args):
         xr, sr, _ = solve(op, g, b, ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS), 1e-12 * fnorm)
         u_ref = xr.to_vec_f64()
         # arms: the plain cycle; learned smoothing on every level of at least 1024 points; learned
-        # smoothing only on the levels of the training problems' sizes (at most 513^2 points)
-        for arm, lo, hi in (("plain", 0, 0), ("learned", 1024, 0), ("learned_levels_upto_513sq", 1024, 513 * 513)):
+        # smoothing only on the levels of the training problems' sizes (at most 513^2 points), without
+        # and with a patience (3 fallbacks in a row switch the learned cycle off)
+        for arm, lo, hi, pat in (("plain", 0, 0, 0), ("learned", 1024, 0, 0),
+                                 ("learned_levels_upto_513sq", 1024, 513 * 513, 0),
+                                 ("learned_levels_upto_513sq_patience3", 1024, 513 * 513, 3)):
             learned = arm != "plain"
             mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS)
             if learned:
                 mg.set_learned(lsm, min_points=lo, fallback_ratio=0.9, max_points=hi)
+                if pat:
+                    mg.set_learned_patience(pat)
             x, st, ms = solve(op, g, b, mg, 1e-10 * fnorm)
             ax = Field.zeros(g, DType.F64, dev)
             op.apply(x, ax)
@@ -757,6 +762,8 @@ def run_learned(args):
             if learned:
                 apps, fb = mg.learned_stats()
                 r["learned_cycles"] = {"applications": apps, "fallbacks": fb}
+                if pat:
+                    r["learned_cycles"]["switched_off"] = mg.learned_disabled()
             runs.append(r)
             print(json.dumps(r), file=sys.stderr, flush=True)
     print(json.dumps({"mode": "learned", "workload": f"convdiff_{n}sq_fgmres30_learned_smoother",

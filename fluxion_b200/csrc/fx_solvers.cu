@@ -2134,11 +2134,14 @@ template <int PASS>
 __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
     grid_dep_enter();
     constexpr int NS = PASS == 2 ? 1 : kCgsMax;
+    const int kb = a.kb, ns = PASS == 2 ? 1 : kb;
+    // every index into acc is a compile-time constant (unrolled loops, predicated on kb), so the
+    // partials stay in registers
     double acc[NS];
 #pragma unroll
     for (int j = 0; j < NS; j++) acc[j] = 0.0;
     __shared__ double c[kCgsMax];
-    if (PASS > 0 && threadIdx.x < kCgsMax) c[threadIdx.x] = threadIdx.x < a.kb ? a.coef[threadIdx.x] : 0.0;
+    if (PASS > 0 && threadIdx.x < kCgsMax) c[threadIdx.x] = threadIdx.x < kb ? a.coef[threadIdx.x] : 0.0;
     __syncthreads();
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -2146,26 +2149,28 @@ __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
         if (PASS > 0) {
 #pragma unroll
             for (int j = 0; j < kCgsMax; j++)
-                if (j < a.kb) wv = fma(-c[j], a.v[j][i], wv);
+                if (j < kb) wv = fma(-c[j], a.v[j][i], wv);
             a.w[i] = wv;
         }
         if (PASS == 2) {
             acc[0] = fma(wv, wv, acc[0]);
-        } else {  // pass 1 reads each v_j[i] a second time, from L1 (a thread's values were just loaded)
+        } else {  // pass 1 reads each v_j[i] a second time, from L1 (the thread loaded it just before)
 #pragma unroll
             for (int j = 0; j < NS; j++)
-                if (j < a.kb) acc[j] = fma(a.v[j][i], wv, acc[j]);
+                if (j < kb) acc[j] = fma(a.v[j][i], wv, acc[j]);
         }
     }
-    // block: warp shuffles, then the warps in order; blocks: the last one folds in block order
+    // block: warp shuffles, then the warps in order
     __shared__ double sh[kBlock / 32][NS];
     __shared__ bool is_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int ns = PASS == 2 ? 1 : a.kb;
-    for (int j = 0; j < ns; j++) {
-        double v = acc[j < NS ? j : 0];
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (lane == 0) sh[wid][j] = v;
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+        if (j < ns) {
+            double v = acc[j];
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) sh[wid][j] = v;
+        }
     }
     __syncthreads();
     if (threadIdx.x < ns) {
@@ -2179,20 +2184,51 @@ __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    if (threadIdx.x < ns) {
+    // last block: warp w folds sums j = w, w + 8, ...; lane l takes blocks l, l + 32, ... (four
+    // loads in flight), then a fixed shuffle tree merges the lanes' compensated sums
+    const unsigned nb = gridDim.x;
+    for (int j = wid; j < ns; j += kBlock / 32) {
         CSum t{0.0, 0.0};
-        for (unsigned b = 0; b < gridDim.x; b++)
-            csum_add(t, ((volatile double *)a.part)[(size_t)b * kCgsMax + threadIdx.x]);
-        a.out[threadIdx.x] = csum_value(t);
+        unsigned b = lane;
+        for (; b + 96 < nb; b += 128) {
+            const double p0 = __ldcg(a.part + (size_t)b * kCgsMax + j);
+            const double p1 = __ldcg(a.part + (size_t)(b + 32) * kCgsMax + j);
+            const double p2 = __ldcg(a.part + (size_t)(b + 64) * kCgsMax + j);
+            const double p3 = __ldcg(a.part + (size_t)(b + 96) * kCgsMax + j);
+            csum_add(t, p0);
+            csum_add(t, p1);
+            csum_add(t, p2);
+            csum_add(t, p3);
+        }
+        for (; b < nb; b += 32) csum_add(t, __ldcg(a.part + (size_t)b * kCgsMax + j));
+        for (int off = 16; off > 0; off >>= 1) {
+            CSum o;
+            o.s = __shfl_down_sync(0xffffffffu, t.s, off);
+            o.c = __shfl_down_sync(0xffffffffu, t.c, off);
+            t = csum_merge(t, o);
+        }
+        if (lane == 0) a.out[j] = csum_value(t);
     }
     if (threadIdx.x == 0) *a.ticket = 0u;
 }
 
+// One wave of resident blocks (at most the partial buffer's num_sms * 8 rows): the fold in the
+// last block then reads a few hundred partials per sum.
 template <int PASS>
 int launch_cgs(fx_ctx *ctx, size_t n, const CgsArgs &a) {
-    FlatGeom g = flat_geom(ctx, n);
+    static std::atomic<int> occ_cache{0};
+    int occ = occ_cache.load(std::memory_order_relaxed);
+    if (!occ) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cgs<PASS>, kBlock, 0) != cudaSuccess || occ < 1)
+            occ = 1;
+        if (occ > 8) occ = 8;
+        occ_cache.store(occ, std::memory_order_relaxed);
+    }
+    size_t blocks = (n + kBlock - 1) / kBlock;
+    if (blocks > (size_t)ctx->num_sms * occ) blocks = (size_t)ctx->num_sms * occ;
+    if (blocks < 1) blocks = 1;
     timing_pre(ctx, "fgmres_cgs2");
-    launch_pdl(ctx, k_cgs<PASS>, g.blocks, kBlock, 0, n, a);
+    launch_pdl(ctx, k_cgs<PASS>, (int)blocks, kBlock, 0, n, a);
     timing_post(ctx, (double)n, (double)n * 8.0 * (a.kb + 1 + (PASS > 0 ? 1 : 0)));
     return check_launch(ctx, "fgmres_cgs2");
 }
@@ -2642,12 +2678,15 @@ struct FlatLsmCheck {
 };
 
 // plain_skip = (the learned cycle reduced ||r|| by at least `ratio`, or the solve is over);
-// counts applications and fallbacks while the solve runs
+// counts applications and fallbacks while the solve runs.  With a patience (state non-null),
+// `patience` fallbacks in a row switch the learned cycle off (state[1]).
 struct FinLsmCheck {
     double ratio2;
     const int *skip;
     int *plain_skip;
     unsigned long long *counts;  // [0] applications, [1] fallbacks
+    int *state;                  // LsmGate's [learned skip, off, fallbacks in a row], or null
+    int patience;
     __device__ void operator()(const double *v) const {
         const bool done = skip && *(volatile const int *)skip;
         const bool ok = v[1] <= ratio2 * v[0];
@@ -2655,7 +2694,29 @@ struct FinLsmCheck {
         if (!done) {
             counts[0] += 1;
             if (!ok) counts[1] += 1;
+            if (state) {
+                state[2] = ok ? 0 : state[2] + 1;
+                if (state[2] >= patience) state[1] = 1;
+            }
         }
+    }
+};
+
+// Gate of a learned application under a patience (one thread): the learned cycle and its check
+// run unless the solve is over or the learned cycle is off; when it is off, the plain cycle runs
+// alone (plain_skip 0) until the solve is over.
+struct FlatLsmGate {
+    const int *skip;
+    int *state;  // [0] learned skip (written here), [1] off, [2] fallbacks in a row
+    int *plain_skip;
+    __device__ __forceinline__ void operator()(size_t, CSum *) const {
+        const bool done = skip && *(volatile const int *)skip;
+        const bool off = state[1] != 0;
+        state[0] = (done || off) ? 1 : 0;
+        if (done)
+            *plain_skip = 1;
+        else if (off)
+            *plain_skip = 0;
     }
 };
 
@@ -2877,6 +2938,8 @@ struct fx_cdmg {
     double lsm_ratio = 0.9;
     double *d_lsm_scale = nullptr;          // [2]: s, 1 / s of the current learned step
     int *d_plain_skip = nullptr;            // 1: the plain recomputation is not needed
+    int lsm_patience = 0;                   // fallbacks in a row that switch the learned cycle off (0: never)
+    int *d_lsm_state = nullptr;             // FlatLsmGate's state
     unsigned long long *d_lsm_counts = nullptr;  // [2]: checked applications, fallbacks
     void drop_replays() {
         for (auto &g : replays) {
@@ -2889,6 +2952,7 @@ struct fx_cdmg {
         drop_replays();
         if (d_lsm_scale) cudaFree(d_lsm_scale);
         if (d_plain_skip) cudaFree(d_plain_skip);
+        if (d_lsm_state) cudaFree(d_lsm_state);
         if (d_lsm_counts) cudaFree(d_lsm_counts);
         for (auto &L : lv)
             for (fx_buf *f : {L.u, L.rhs, L.tmp, L.vx, L.vy, L.kappa}) fx_free(f);
@@ -3057,13 +3121,21 @@ int fx_cdmg::View::record(fx_buf *z, const fx_buf *r, const int *skip, bool z_ze
     };
     if (!mg->lsm) return run(false, skip, z_zero);
     // the learned cycle, its check, and the plain cycle where the check failed (all on the device)
-    FX_TRY(run(true, skip, z_zero));
+    const bool gated = mg->lsm_patience > 0;
+    const int *lskip = skip;
+    if (gated) {
+        FX_TRY(launch_flat<0>(ctx, 1, FlatLsmGate{skip, mg->d_lsm_state, mg->d_plain_skip}, NoFin{}, nullptr,
+                              "cdmg_learned_gate"));
+        lskip = mg->d_lsm_state;
+    }
+    FX_TRY(run(true, lskip, z_zero));
     const double ratio2 = mg->lsm_ratio * mg->lsm_ratio;
     FX_TRY((launch_flat<2>(ctx, n,
                            FlatLsmCheck{mg->level_op<double>(0), (const double *)z->ptr, (const double *)r->ptr,
                                         L0.rows, L0.cols},
-                           FinLsmCheck{ratio2, skip, mg->d_plain_skip, mg->d_lsm_counts}, nullptr,
-                           "cdmg_learned_check")));
+                           FinLsmCheck{ratio2, skip, mg->d_plain_skip, mg->d_lsm_counts,
+                                       gated ? mg->d_lsm_state : nullptr, mg->lsm_patience},
+                           gated ? lskip : nullptr, "cdmg_learned_check")));
     return run(false, mg->d_plain_skip, false);
 }
 
@@ -3855,6 +3927,29 @@ int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, size_
     mg->lsm_min_points = min_points;
     mg->lsm_max_points = max_points;
     mg->lsm_ratio = fallback_ratio;
+    if (mg->d_lsm_state) FX_CUDA(cudaMemset(mg->d_lsm_state, 0, 3 * sizeof(int)));
+    return FX_OK;
+}
+
+int fx_cdmg_set_learned_patience(fx_cdmg *mg, size_t patience) {
+    if (!mg) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (patience > (size_t)1 << 30) return fail(FX_ERR_INVALID_ARGUMENT, "patience out of range");
+    FX_CUDA(cudaStreamSynchronize(mg->ctx->stream));
+    if (!mg->d_lsm_state) FX_CUDA(cudaMalloc(&mg->d_lsm_state, 3 * sizeof(int)));
+    FX_CUDA(cudaMemset(mg->d_lsm_state, 0, 3 * sizeof(int)));
+    if ((int)patience != mg->lsm_patience) mg->drop_replays();  // the gate joins or leaves the sequence
+    mg->lsm_patience = (int)patience;
+    return FX_OK;
+}
+
+int fx_cdmg_learned_disabled(fx_cdmg *mg, int *disabled) {
+    if (!mg || !disabled) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    int st[3] = {0, 0, 0};
+    if (mg->d_lsm_state) {
+        FX_CUDA(cudaStreamSynchronize(mg->ctx->stream));
+        FX_CUDA(cudaMemcpy(st, mg->d_lsm_state, sizeof(st), cudaMemcpyDeviceToHost));
+    }
+    *disabled = st[1];
     return FX_OK;
 }
 

@@ -431,6 +431,17 @@ class ConvDiffMultigrid(Preconditioner):
         check(L.lib().fx_cdmg_set_learned(self.h, smoother.h if smoother is not None else None, int(min_points),
                                           int(max_points), float(fallback_ratio)))
 
+    def set_learned_patience(self, patience: int) -> None:
+        """After `patience` fallbacks in a row the learned cycle is switched off for good (until
+        set_learned or this call); 0 never switches it off (fx_cdmg_set_learned_patience)."""
+        check(L.lib().fx_cdmg_set_learned_patience(self.h, int(patience)))
+
+    def learned_disabled(self) -> bool:
+        """Whether the patience has switched the learned cycle off."""
+        d = C.c_int()
+        check(L.lib().fx_cdmg_learned_disabled(self.h, C.byref(d)))
+        return bool(d.value)
+
     def learned_stats(self):
         """(checked applications, fallbacks to the plain cycle) so far."""
         a, f = C.c_ulonglong(), C.c_ulonglong()

@@ -543,6 +543,12 @@ int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, d
  * outlive the multigrid's use of it.  stats: checked applications and fallbacks so far. */
 int fx_cdmg_set_learned(fx_cdmg *mg, const fx_lsm *lsm, size_t min_points, size_t max_points, double fallback_ratio);
 int fx_cdmg_learned_stats(fx_cdmg *mg, unsigned long long *applications, unsigned long long *fallbacks);
+/* Patience of the learned cycle (new): after `patience` fallbacks in a row the learned cycle is
+ * switched off, on the device, and the plain cycle alone runs from then on (no check); 0 (the
+ * default) never switches it off.  This call and fx_cdmg_set_learned switch it back on.
+ * fx_cdmg_learned_disabled reports whether it is off. */
+int fx_cdmg_set_learned_patience(fx_cdmg *mg, size_t patience);
+int fx_cdmg_learned_disabled(fx_cdmg *mg, int *disabled);
 
 /* ------------------------------------------------------------------ */
 /* Batched solve (new; the reference solves one grid at a time, bicgstab.rs:218-346).  `count`

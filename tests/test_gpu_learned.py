@@ -222,3 +222,32 @@ def test_checkpoint_reload_gives_the_same_smoothing(dev, tmp_path):
         m.smooth(op, x, Field.from_f64(g, f, dev), 0.8, 2)
         outs.append(x.to_vec_f64())
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_patience_switches_the_learned_cycle_off(dev):
+    """With a check no learned cycle passes and a patience of 2, the first two applications fall
+    back and the learned cycle is then off: every z is the plain cycle's, so the FGMRES solve is
+    the plain one bit for bit, and only two applications were checked."""
+    from fluxion_b200 import ConvDiffMultigrid, DType, FgmresSolver, Field
+    from fluxion_b200.learned import LearnedSmoother
+    g, N, h, vx, vy, f, op, oop = _cd(127, 1e-3, dev, 29)
+    lsm = LearnedSmoother(dev, seed=4)
+    _random_params(lsm, 10)
+    tol = 1e-10 * np.linalg.norm(f)
+    outs = []
+    for patience in (None, 2):
+        mg = ConvDiffMultigrid(op)
+        if patience:
+            mg.set_learned(lsm, min_points=1, fallback_ratio=1e-30)
+            mg.set_learned_patience(patience)
+        x = Field.zeros(g, DType.F64, dev)
+        st = FgmresSolver(g, dev, 30, tol, 300).solve_op(x, Field.from_f64(g, f, dev), op, mg)
+        outs.append((st.iterations, x.to_vec_f64()))
+        if patience:
+            assert st.converged()
+            assert mg.learned_disabled()
+            assert mg.learned_stats() == (2, 2)
+            mg.set_learned_patience(patience)  # switches it back on
+            assert not mg.learned_disabled()
+    assert outs[0][0] == outs[1][0]
+    assert np.array_equal(outs[0][1], outs[1][1])
