@@ -71,12 +71,13 @@ def parse():
                    help="--mode vcycle: autotune the cycle's layout first; --mode batch: choose the batched "
                         "solver's chunk size, sweep counts and cycle precision first (timed on a sample)")
     p.add_argument("--tune-cache", default=None, help="JSON file that keeps autotuner choices between runs")
-    p.add_argument("--mode", default="solve", choices=["solve", "vcycle", "batch", "convdiff", "learned"],
+    p.add_argument("--mode", default="solve", choices=["solve", "vcycle", "batch", "convdiff", "learned", "lsm_step"],
                    help="solve: the headline MG-PCG solve; vcycle: preconditioner applications alone "
                         "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target; batch: "
                         "1024 conv-diff problems; convdiff: convection-dominated conv-diff at --n; "
                         "learned: train the learned smoother, then FGMRES(30) with the learned vs the plain "
-                        "conv-diff cycle at --n")
+                        "conv-diff cycle at --n; lsm_step: learned smoothing steps alone at --n (a profiling "
+                        "target of the network kernel)")
     p.add_argument("--nu", default="1e-3,1e-4", help="--mode convdiff: viscosities, comma-separated")
     p.add_argument("--k-range", default="6,10",
                    help="--mode batch: interior sizes 2^k - 1 for k uniform in this inclusive range")
@@ -284,6 +285,67 @@ def run_vcycle(args):
     print(json.dumps({"mode": "vcycle", "workload": f"poisson_{n}sq_{args.mg_dtype}_vcycle", "steps": args.steps,
                       "warmup": args.warmup, "ms_per_vcycle": e0.elapsed_time(e1) / args.steps,
                       "levels": mg.depth(), "autotune": tuned, "per_launch_with_events": per}), flush=True)
+    return 0
+
+
+LSM_FLOPS_PER_POINT = 2 * (3 * 16 * 9 + 16 * 16 * 9 + 16 * 9)  # the network's MACs x 2, halos not counted
+
+
+def run_lsm_step(args):
+    """Time `steps` learned smoothing steps (the q / scale pass and the network with the update) on the
+    n^2 conv-diff problem after `warmup` untimed ones, with CUDA events on the library's stream, and
+    report the network pass's device time and its tensor roofline (5760 flop per point)."""
+    import ctypes as C
+
+    import torch
+    from fluxion_b200 import ConvDiffOperator, DType, Device, Field, Grid
+    from fluxion_b200 import _lib as L
+    from fluxion_b200.learned import LearnedSmoother
+    from fluxion_b200.workloads import poisson_uniform_rhs, stream_velocity
+
+    n = args.n
+    dev = Device.Cuda(0)
+    be = dev.backend()
+    stream = torch.cuda.Stream()
+    be.set_stream(stream.cuda_stream)
+    N, h = n + 2, 1.0 / (n + 1)
+    g = Grid.square(N, h)
+    vx, vy = stream_velocity(n, SEED + 3)
+    f = poisson_uniform_rhs(n, SEED + 4)
+    op = ConvDiffOperator(g, Field.from_f64(g, vx, dev), Field.from_f64(g, vy, dev), -1e-3, sigma=0.0, coeff=1.0)
+    lsm = LearnedSmoother(dev, seed=1)
+    p = lsm.params
+    p[-145:-1] = np.random.default_rng(SEED).normal(0.0, 0.2, 144)  # a non-zero last layer
+    lsm.params = p
+    x = Field.zeros(g, DType.F64, dev)
+    b = Field.from_f64(g, f, dev)
+    lsm.smooth(op, x, b, OMEGA, max(1, args.warmup))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    lsm.smooth(op, x, b, OMEGA, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1) / args.steps
+    L.lib().fx_ctx_timing_begin(be.ctx, b"lsm_apply")
+    lsm.smooth(op, x, b, OMEGA, 3)
+    cap = 8
+    ms, pts, byt, cnt = (C.c_double * cap)(), (C.c_double * cap)(), (C.c_double * cap)(), C.c_size_t()
+    L.lib().fx_ctx_timing_end_records(be.ctx, ms, pts, byt, cap, C.byref(cnt))
+    apply_ms = float(np.mean([ms[i] for i in range(cnt.value)])) if cnt.value else None
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak = float(json.load(fh)["bf16_tflops"])
+    except Exception:
+        peak = 1590.0
+    flops = LSM_FLOPS_PER_POINT * float(n) * float(n)
+    tf = flops / (apply_ms * 1e-3) / 1e12 if apply_ms else None
+    print(json.dumps({"mode": "lsm_step", "workload": f"learned_smoother_step_{n}sq", "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": step_ms, "network_pass_ms": apply_ms,
+                      "roofline": {"kernel": "k_lsm_apply", "bound": "tensor", "achieved": tf, "peak": peak,
+                                   "unit": "TFLOP/s", "frac": tf / peak if tf else None,
+                                   "flops_per_point": LSM_FLOPS_PER_POINT}}), flush=True)
     return 0
 
 
@@ -604,7 +666,7 @@ def run_convdiff(args):
     residual, so its true residual is reported beside it) and BiCGSTAB; FGMRES and BiCGSTAB
     again with the cycle in FP32 (the Krylov solver, its vectors and the residual stay FP64).  Device time with CUDA
     events around each solve; the true residual recomputed on the device.  These are the plain
-    Jacobi-multigrid arms; the learned smoother is not built."""
+    Jacobi-multigrid arms; the learned smoother's arms are --mode learned."""
     import torch
     from fluxion_b200 import (BiCgStabSolver, ConvDiffMultigrid, ConvDiffOperator, DType, Device, Field,
                               FgmresSolver, GmresSolver, Grid)
@@ -661,7 +723,8 @@ def run_convdiff(args):
             print(json.dumps(runs[-1]), flush=True, file=sys.stderr)
     print(json.dumps({"mode": "convdiff", "workload": f"convdiff_{n}sq_upwind_stream8", "n_interior": n,
                       "runs": runs, "dtype": "f64", "data": "synthetic (seeded)",
-                      "note": "plain Jacobi-multigrid arms; the learned smoother is not built"}), flush=True)
+                      "note": "plain Jacobi-multigrid arms (the learned smoother's are --mode learned)"}),
+          flush=True)
     return 0 if ok else 1
 
 
@@ -737,10 +800,10 @@ def run_learned(args):
         u_ref = xr.to_vec_f64()
         # arms: the plain cycle; learned smoothing on every level of at least 1024 points; learned
         # smoothing only on the levels of the training problems' sizes (at most 513^2 points), without
-        # and with a patience (3 fallbacks in a row switch the learned cycle off)
+        # and with a patience (8 fallbacks in a row switch the learned cycle off)
         for arm, lo, hi, pat in (("plain", 0, 0, 0), ("learned", 1024, 0, 0),
                                  ("learned_levels_upto_513sq", 1024, 513 * 513, 0),
-                                 ("learned_levels_upto_513sq_patience3", 1024, 513 * 513, 3)):
+                                 ("learned_levels_upto_513sq_patience8", 1024, 513 * 513, 8)):
             learned = arm != "plain"
             mg = ConvDiffMultigrid(op, 2, 2, OMEGA, COARSE_MAX, COARSE_SWEEPS)
             if learned:
@@ -787,6 +850,8 @@ def main():
         return run_convdiff(args)
     if args.mode == "learned":
         return run_learned(args)
+    if args.mode == "lsm_step":
+        return run_lsm_step(args)
 
     import torch
 

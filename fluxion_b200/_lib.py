@@ -13,7 +13,9 @@ import re
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfluxion_cuda.so")
+# FLUXION_CHECKED=1 loads the checked build (index checks recorded in device status words)
+LIB_PATH = os.path.join(HERE, "libfluxion_cuda_checked.so" if os.environ.get("FLUXION_CHECKED") == "1"
+                        else "libfluxion_cuda.so")
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "fluxion_cuda.h")
 
 FX_OK = 0
@@ -67,7 +69,7 @@ _OPAQUE = {"fx_ctx", "fx_buf", "fx_precond", "fx_mg", "fx_cg", "fx_pipelined_cg"
            "fx_gmres", "fx_graph", "fx_ir", "fx_fcg", "fx_fgmres", "fx_op", "fx_cdmg", "fx_lsm", "fx_lsm_data", "fx_batch"}
 _SCALARS = {
     "int": C.c_int, "size_t": C.c_size_t, "double": C.c_double, "float": C.c_float,
-    "unsigned long long": C.c_ulonglong, "void": None, "char": C.c_char,
+    "unsigned long long": C.c_ulonglong, "long long": C.c_longlong, "void": None, "char": C.c_char,
 }
 
 

@@ -6,6 +6,11 @@ and linked into ``fluxion_b200/libfluxion_cuda.so``.  Kernels are compiled with
 multiply-adds are the explicit ``fma`` calls that restate the reference's
 ``f64::mul_add``, which keeps F64 results bitwise comparable with the CPU path.
 The architecture can be overridden with ``FLUXION_CUDA_ARCH`` (e.g. ``sm_100a``).
+
+``build(checked=True)`` compiles the same sources with ``FX_CHECKED`` into
+``libfluxion_cuda_checked.so``: kernels that test every index they compute and record, never
+trap on, an out-of-range one (``fx_checked_status``).  ``FLUXION_CHECKED=1`` makes the package
+load it instead of the default library.
 """
 from __future__ import annotations
 
@@ -19,6 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfluxion_cuda.so")
+LIB_CHECKED = os.path.join(HERE, "libfluxion_cuda_checked.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
@@ -42,18 +48,20 @@ def _needs(obj: str, src: str, deps) -> bool:
     return any(os.path.getmtime(p) > t for p in [src, *deps])
 
 
-def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = False) -> str:
-    os.makedirs(BUILD_DIR, exist_ok=True)
+def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = False, checked: bool = False) -> str:
+    build_dir = os.path.join(BUILD_DIR, "checked") if checked else BUILD_DIR
+    lib = LIB_CHECKED if checked else LIB
+    os.makedirs(build_dir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     deps = sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [
         os.path.join(os.path.dirname(HERE), "include", "fluxion_cuda.h")]
     objs = []
     jobs = []
     for s in srcs:
-        o = os.path.join(BUILD_DIR, os.path.basename(s)[:-3] + ".o")
+        o = os.path.join(build_dir, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
         if force or _needs(o, s, deps):
-            cmd = [NVCC, *_arch_flags(), *COMMON, "-c", s, "-o", o]
+            cmd = [NVCC, *_arch_flags(), *COMMON, *(["-DFX_CHECKED"] if checked else []), "-c", s, "-o", o]
             if ptxas_verbose:
                 cmd += ["-Xptxas", "-v"]
             jobs.append(cmd)
@@ -71,14 +79,15 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
             list(ex.map(run, jobs))
-    if force or jobs or not os.path.exists(LIB):
-        link = [NVCC, *_arch_flags(), "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"]
+    if force or jobs or not os.path.exists(lib):
+        link = [NVCC, *_arch_flags(), "-shared", "-o", lib + ".tmp", *objs, "-lcudart"]
         if verbose:
             print(" ".join(link), flush=True)
         subprocess.run(link, check=True)
-        os.replace(LIB + ".tmp", LIB)
-    return LIB
+        os.replace(lib + ".tmp", lib)
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv, ptxas_verbose="--ptxas" in sys.argv))
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv, ptxas_verbose="--ptxas" in sys.argv,
+                checked="--checked" in sys.argv))

@@ -28,6 +28,8 @@
 
 using namespace fx;
 
+FX_CHECK_FILE(batch);
+
 namespace {
 
 constexpr int kBT = 256;             // threads per block
@@ -100,6 +102,21 @@ __device__ __forceinline__ void bs_finish(BState *S, int reason, long long iters
     S->resid = resid;
 }
 
+// points of problem p's level in a flat pass (the checked build's extent of its items): the level
+// of the functor's K0 (k) or LvlArgs (a) entries; functors with neither are not checked
+template <typename F>
+__device__ __forceinline__ auto bf_points_impl(const F &f, int p, int) -> decltype((long long)f.k.L[p].n) {
+    return (long long)f.k.L[p].n * f.k.L[p].n;
+}
+template <typename F>
+__device__ __forceinline__ auto bf_points_impl(const F &f, int p, long) -> decltype((long long)f.a.L[p].n) {
+    return (long long)f.a.L[p].n * f.a.L[p].n;
+}
+template <typename F>
+__device__ __forceinline__ long long bf_points_impl(const F &, int, ...) {
+    return 1LL << 62;
+}
+
 // ---------------------------------------------------------------- generic batched flat pass
 // One block per item of a chunk table; K compensated sums per problem, folded in item order by the
 // problem's last block (a per-problem ticket), which calls fin(problem, values).
@@ -111,7 +128,9 @@ __global__ void __launch_bounds__(kBT) k_bflat(const Chunk *__restrict__ items, 
     CSum acc[K > 0 ? K : 1];
 #pragma unroll
     for (int k = 0; k < (K > 0 ? K : 1); k++) acc[k] = CSum{0.0, 0.0};
-    f.run(c.prob, c.start + (int)threadIdx.x, c.start + c.len, kBT, acc);
+    // an item past its problem's level is not run (it still joins the problem's ticket)
+    const int hi = FX_IN((long long)c.start + c.len - 1, bf_points_impl(f, c.prob, 0)) ? c.start + c.len : c.start;
+    f.run(c.prob, c.start + (int)threadIdx.x, hi, kBT, acc);
     if constexpr (K > 0) {
         __shared__ bool is_last;
         block_reduce<K>(acc);
@@ -541,6 +560,7 @@ __global__ void __launch_bounds__(256) k_bsweep2(const Tile *__restrict__ tiles,
     T *out = outb + Lp.off;
     const int tid = threadIdx.x;
     const int r0 = tl.ty * kTileB, c0 = tl.tx * kTileB;
+    if (!(FX_IN(r0, rows) && FX_IN(c0, cols))) return;  // a tile of the table outside its problem's level
 #pragma unroll
     for (int j = 0; j < (kTileX * kTileX + 255) / 256; j++) {
         const int k = tid + j * 256;
@@ -605,6 +625,13 @@ __global__ void __launch_bounds__(1024) k_bcoarse(const int *__restrict__ probs,
     extern __shared__ unsigned char bsm[];
     const Lvl<T> &Lp = a.L[prob];
     const int rows = Lp.n, cols = Lp.n, n = rows * cols;
+#ifdef FX_CHECKED
+    {
+        unsigned dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (!(FX_IN(n - 1, kPts * (int)blockDim.x) && FX_IN(2LL * n - 1, dyn / sizeof(T)))) return;
+    }
+#endif
     T *s0 = reinterpret_cast<T *>(bsm);
     T *s1 = s0 + n;
     T *u = ub + Lp.off;

@@ -8,6 +8,8 @@
 
 #include "fx_internal.cuh"
 
+FX_CHECK_FILE(context);
+
 namespace fx {
 
 static thread_local std::string g_err;
@@ -227,6 +229,39 @@ FlatGeom flat_geom(fx_ctx *ctx, size_t n) {
     if (b > cap) b = cap;
     g.blocks = (int)b;
     return g;
+}
+
+// Registry of the checked build: the readers of the units' status words and the names of the
+// files holding checks (by hash).  Filled by static initialisers when the library loads; empty in
+// the default build.
+// test hook: one index check, no memory access (fx_test_check_index)
+__global__ void k_check_index(long long index, long long extent) {
+    if (threadIdx.x == 0) (void)FX_IN(index, extent);
+}
+
+struct CheckRegistry {
+    std::mutex mu;
+    std::vector<CheckReader> readers;
+    std::vector<std::pair<unsigned, std::string>> files;
+};
+static CheckRegistry &check_registry() {
+    static CheckRegistry r;
+    return r;
+}
+
+void check_register_unit(CheckReader reader) {
+    CheckRegistry &r = check_registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    r.readers.push_back(reader);
+}
+
+void check_register_file(unsigned hash, const char *name) {
+    CheckRegistry &r = check_registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    for (auto &f : r.files)
+        if (f.first == hash) return;
+    const char *base = std::strrchr(name, '/');
+    r.files.emplace_back(hash, base ? base + 1 : name);
 }
 
 int read_results(fx_ctx *ctx, int k, double *out) {
@@ -665,6 +700,52 @@ int fx_copy_to_host_f64_async(fx_ctx *ctx, const fx_buf *b, double *dst, size_t 
     if (!len) return FX_OK;
     FX_CUDA(cudaMemcpyAsync(dst, b->ptr, len * sizeof(double), cudaMemcpyDeviceToHost,
                             stream ? (cudaStream_t)stream : ctx->stream));
+    return FX_OK;
+}
+
+int fx_test_check_index(fx_ctx *ctx, long long index, long long extent) {
+    if (!ctx) return fail(FX_ERR_INVALID_ARGUMENT, "null context");
+    k_check_index<<<1, 32, 0, ctx->stream>>>(index, extent);
+    return check_launch(ctx, "test_check_index");
+}
+
+int fx_checked_build(void) {
+#ifdef FX_CHECKED
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+int fx_checked_status(fx_ctx *ctx, size_t *count, char *file, size_t file_cap, int *line, long long *index,
+                      long long *extent) {
+    if (!ctx || !count || !line || !index || !extent) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    *count = 0;
+    *line = 0;
+    *index = 0;
+    *extent = 0;
+    if (file && file_cap) file[0] = '\0';
+    FX_CUDA(cudaSetDevice(ctx->device));
+    FX_CUDA(cudaDeviceSynchronize());
+    CheckRegistry &r = check_registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    for (CheckReader rd : r.readers) {
+        CheckWord w{};
+        if (rd(&w)) return fail(FX_ERR_BACKEND, "reading a checked-build status word failed");
+        if (!w.code) continue;
+        if ((*count)++ == 0) {
+            *line = w.line;
+            *index = w.index;
+            *extent = w.extent;
+            if (file && file_cap) {
+                std::string name = "?";
+                for (auto &f : r.files)
+                    if (f.first == w.file) name = f.second;
+                std::strncpy(file, name.c_str(), file_cap - 1);
+                file[file_cap - 1] = '\0';
+            }
+        }
+    }
     return FX_OK;
 }
 

@@ -42,7 +42,75 @@ constexpr int kMaxSums = 4;
 constexpr int kBlock = 256;  // threads per block for grid kernels (8 warps)
 constexpr int kBandThreads = kBlock + 32;  // band kernels: 8 column warps + 1 halo warp
 
+// ------------------------------------------------------------------ checked build
+//
+// Compiled with FX_CHECKED (the separate libfluxion_cuda_checked.so), the kernels test the
+// indices they compute -- global offsets and shared-memory slots -- against the extent of the
+// array addressed before each access.  An access outside is not made (a load gives zero, a
+// store is dropped) and the first such event of each translation unit is written to that unit's
+// device status word: the source file (as a hash of its name), the line, the index and the
+// extent.  fx_checked_status reads and clears the words.  Nothing traps and nothing waits.  In
+// the default build FX_IN is the constant true and every check compiles away.
+struct CheckWord {
+    unsigned code;  // 0: clear; 1: an index was out of range
+    unsigned file;  // check_hash of the source file of the check
+    int line;
+    int pad;
+    long long index, extent;
+};
+
+__host__ __device__ constexpr unsigned check_hash(const char *s, unsigned h = 2166136261u) {
+    return *s ? check_hash(s + 1, (h ^ (unsigned char)*s) * 16777619u) : h;
+}
+
+// host: the readers of the units' words and the names of the files holding checks
+using CheckReader = int (*)(CheckWord *out);
+void check_register_unit(CheckReader reader);
+void check_register_file(unsigned hash, const char *name);
+
+#ifdef FX_CHECKED
+static __device__ CheckWord g_check_word;
+
+static __device__ __noinline__ void check_record(long long i, long long n, unsigned file, int line) {
+    if (atomicCAS(&g_check_word.code, 0u, 1u) == 0u) {
+        g_check_word.file = file;
+        g_check_word.line = line;
+        g_check_word.index = i;
+        g_check_word.extent = n;
+        __threadfence();
+    }
+}
+
+__device__ __forceinline__ bool check_in(long long i, long long n, unsigned file, int line) {
+    if ((unsigned long long)i < (unsigned long long)n) return true;
+    check_record(i, n, file, line);
+    return false;
+}
+
+#define FX_IN(i, n) (::fx::check_in((long long)(i), (long long)(n), ::fx::check_hash(__FILE__), __LINE__))
+
+// one reader per translation unit (it reads that unit's copy of the word, then clears it)
+static int check_read_unit(CheckWord *out) {
+    if (cudaMemcpyFromSymbol(out, g_check_word, sizeof(CheckWord)) != cudaSuccess) return 1;
+    const CheckWord zero{};
+    return cudaMemcpyToSymbol(g_check_word, &zero, sizeof(CheckWord)) != cudaSuccess;
+}
+struct CheckUnitReg {
+    CheckUnitReg() { check_register_unit(&check_read_unit); }
+};
+static CheckUnitReg g_check_unit_reg;
+struct CheckFileReg {
+    explicit CheckFileReg(const char *name) { check_register_file(check_hash(name), name); }
+};
+#define FX_CHECK_FILE(tag) static ::fx::CheckFileReg g_check_file_##tag(__FILE__)
+#else
+#define FX_IN(i, n) (true)
+#define FX_CHECK_FILE(tag) static_assert(true, "")
+#endif
+
 }  // namespace fx
+
+FX_CHECK_FILE(internal);
 
 struct fx_timing_rec {
     cudaEvent_t a, b;
@@ -484,7 +552,8 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader l
         for (int s = 0; s < CPT; s++) {
 #pragma unroll
             for (int q = 0; q < NL; q++) v[s][q] = (T)0;
-            if (r >= 0 && r < rows && valid[s]) ld.load((size_t)r * cols + col[s], v[s]);
+            if (r >= 0 && r < rows && valid[s] && FX_IN((size_t)r * cols + col[s], (size_t)rows * cols))
+                ld.load((size_t)r * cols + col[s], v[s]);
         }
     };
     auto load_aux = [&](int r, T (&a)[CPT][NA > 0 ? NA : 1]) {
@@ -494,7 +563,8 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader l
 #pragma unroll
                 for (int k = 0; k < NA; k++) {
                     a[s][k] = (T)0;
-                    if (point[s] && r < r1) a[s][k] = pt.aux(k)[(size_t)r * cols + col[s]];
+                    if (point[s] && r < r1 && FX_IN((size_t)r * cols + col[s], (size_t)rows * cols))
+                        a[s][k] = pt.aux(k)[(size_t)r * cols + col[s]];
                 }
             }
         }
@@ -504,7 +574,7 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader l
         T *row = ring[r & 7];
 #pragma unroll
         for (int s = 0; s < CPT; s++)
-            if (!halo_warp || s == 0) row[sidx[s]] = ld.combine(v[s]);
+            if ((!halo_warp || s == 0) && FX_IN(sidx[s], W)) row[sidx[s]] = ld.combine(v[s]);
     };
     auto compute_row = [&](int r, const T (&a)[CPT][NA > 0 ? NA : 1]) {
         const T *rn = ring[(r + 7) & 7];
@@ -514,7 +584,7 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader l
         const size_t rowoff = (size_t)r * cols;
 #pragma unroll
         for (int s = 0; s < CPT; s++) {
-            if (point[s]) {
+            if (point[s] && FX_IN(sidx[s] + 1, W) && FX_IN(rowoff + col[s], (size_t)rows * cols)) {
                 const int i = sidx[s];
                 const bool edge = i == 0;  // column 0: no west neighbours
                 Nb<T> nb;
@@ -616,12 +686,14 @@ __global__ void __launch_bounds__(kBlock) k_point(size_t rows, size_t cols, Load
     CSum acc[K > 0 ? K : 1];
 #pragma unroll
     for (int k = 0; k < (K > 0 ? K : 1); k++) acc[k] = CSum{0.0, 0.0};
+    const size_t n = rows * cols, stride = (size_t)gridDim.x * blockDim.x;
     auto val = [&](size_t j) -> T {
         T v[NL];
-        ld.load(j, v);
+#pragma unroll
+        for (int q = 0; q < NL; q++) v[q] = (T)0;
+        if (FX_IN(j, n)) ld.load(j, v);
         return ld.combine(v);
     };
-    const size_t n = rows * cols, stride = (size_t)gridDim.x * blockDim.x;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const size_t r = i / cols, c = i - r * cols;
         Nb<T> nb;

@@ -30,6 +30,8 @@
 
 #include "fx_internal.cuh"
 
+FX_CHECK_FILE(learned_h);
+
 namespace fx {
 namespace lsm {
 
@@ -152,7 +154,8 @@ __global__ void __launch_bounds__(256) k_lsm_apply(Op A, const uint32_t *__restr
             const int iy = k / kBufW, ix = k - iy * kBufW;
             const int gr = r0 - 3 + iy, gc = c0 - 3 + ix;
             qv[j] = xv[j] = yv[j] = dv[j] = (T)0;
-            if (k < kInRows * kBufW && gr >= 0 && gr < rows && gc >= 0 && gc < cols) {
+            if (k < kInRows * kBufW && gr >= 0 && gr < rows && gc >= 0 && gc < cols &&
+                FX_IN((long long)gr * cols + gc, (long long)rows * cols)) {
                 const size_t i = (size_t)gr * cols + gc;
                 qv[j] = q[i];
                 xv[j] = A.vxv(i);
@@ -308,6 +311,7 @@ __global__ void __launch_bounds__(256) k_lsm_apply(Op A, const uint32_t *__restr
                     const int gr = r0 + oy, gc = c0 + ox;
                     if (ox >= kTile || gr <= 0 || gc <= 0 || gr >= rows - 1 || gc >= cols - 1) continue;
                     const size_t i = (size_t)gr * cols + gc;
+                    if (!FX_IN(i, (long long)rows * cols)) continue;
                     const double c = (double)(acc[hm * 2] + b3);
                     x[i] = (T)((double)fx_fma(omega, q[i], x[i]) + s * c);
                 }

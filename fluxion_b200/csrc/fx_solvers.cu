@@ -20,6 +20,8 @@
 
 using namespace fx;
 
+FX_CHECK_FILE(solvers);
+
 // ---------------------------------------------------------------- device solver state
 
 namespace fx {
@@ -438,6 +440,13 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(T *u, const T *__restrict
     T *s0 = reinterpret_cast<T *>(smem_raw);
     T *s1 = s0 + rows * cols;
     const int n = rows * cols;
+#ifdef FX_CHECKED
+    {
+        unsigned dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (!(FX_IN(n - 1, kCoarsePts * (int)blockDim.x) && FX_IN(2LL * n - 1, dyn / sizeof(T)))) return;
+    }
+#endif
     int idx[kCoarsePts];
     bool inner[kCoarsePts];
     T bv[kCoarsePts];
@@ -2583,6 +2592,7 @@ __global__ void __launch_bounds__(256) k_lsm_extract(Op A, const double *__restr
     for (int k = tid; k < kPin * kPin; k += 256) {
         const int iy = k / kPin, ix = k - iy * kPin;
         const size_t i = (size_t)(y0 - 4 + iy) * cols + (x0 - 4 + ix);
+        if (!FX_IN((long long)(y0 - 4 + iy) * cols + (x0 - 4 + ix), (long long)rows * cols)) continue;
         float c0, c1, c2;
         input_channels<double>(q[i], A.vxv(i), A.vyv(i), A.diag(i), inv_s, inv_dx, inv_dy, c0, c1, c2);
         in[k] = __float2bfloat16_rn(c0);
@@ -2592,6 +2602,7 @@ __global__ void __launch_bounds__(256) k_lsm_extract(Op A, const double *__restr
     for (int k = tid; k < kP3 * kP3; k += 256) {
         const int y = k / kP3, x = k - y * kP3;
         const size_t i = (size_t)(y0 - 1 + y) * cols + (x0 - 1 + x);
+        if (!FX_IN((long long)(y0 - 1 + y) * cols + (x0 - 1 + x), (long long)rows * cols)) continue;
         se[k] = e[i];
         sq[k] = q[i];
     }
@@ -2774,7 +2785,9 @@ __global__ void __launch_bounds__(256) k_cd_sweep2(OpA<T, kModeCD> A, const T *_
         const int k = tid + j * 256;
         if (k >= kSw2X * kSw2X) break;
         const int gr = r0 - 2 + k / kSw2X, gc = c0 - 2 + k % kSw2X;
-        xs[k] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols) ? x[(size_t)gr * cols + gc] : (T)0;
+        xs[k] = (gr >= 0 && gr < rows && gc >= 0 && gc < cols && FX_IN((long long)gr * cols + gc, (long long)rows * cols))
+                    ? x[(size_t)gr * cols + gc]
+                    : (T)0;
     }
     __syncthreads();
 #pragma unroll
@@ -2812,6 +2825,7 @@ __global__ void __launch_bounds__(256) k_cd_sweep2(OpA<T, kModeCD> A, const T *_
         if (gr <= 0 || gc <= 0 || gr >= rows - 1 || gc >= cols - 1) continue;
         const size_t g = (size_t)gr * cols + gc;
         const int q = (lr + 1) * kSw2Y + (lc + 1);
+        if (!(FX_IN(g, (long long)rows * cols) && FX_IN(q + kSw2Y, kSw2Y * kSw2Y))) continue;
         Nb<T> nb;
         nb.c = ys[q];
         nb.n = ys[q - kSw2Y];
@@ -2852,6 +2866,13 @@ __global__ void __launch_bounds__(1024) k_cd_coarse(T *u, const T *__restrict__ 
     T *s0 = reinterpret_cast<T *>(smem_raw);
     T *s1 = s0 + rows * cols;
     const int n = rows * cols;
+#ifdef FX_CHECKED
+    {
+        unsigned dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (!(FX_IN(n - 1, kPts * (int)blockDim.x) && FX_IN(2LL * n - 1, dyn / sizeof(T)))) return;
+    }
+#endif
     int idx[kPts];
     bool inner[kPts];
     T bv[kPts], dv[kPts];

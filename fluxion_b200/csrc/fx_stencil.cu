@@ -6,6 +6,8 @@
 
 using namespace fx;
 
+FX_CHECK_FILE(stencil);
+
 namespace {
 
 // Boundary ring of apply_stencil / apply_stencil_var (ops.rs:796-843): top and bottom rows
@@ -16,26 +18,38 @@ template <typename T, bool VAR>
 __global__ void k_ring_values(const T *__restrict__ in, T *__restrict__ out, const T *__restrict__ coeff,
                               int rows, int cols, BcP B) {
     const int nring = 2 * cols + 2 * (rows - 2);
+    const long long n = (long long)rows * cols;
+    (void)n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nring; i += gridDim.x * blockDim.x) {
-        size_t idx;
-        double v;
+        size_t idx, nb;  // the point and its inward neighbour
+        int side;
+        double h;
         if (i < cols) {
             idx = i;
-            v = bc_value(B, 0, (double)in[idx], (double)in[idx + cols], B.dy);
+            nb = idx + cols;
+            side = 0;
+            h = B.dy;
         } else if (i < 2 * cols) {
             idx = (size_t)(rows - 1) * cols + (i - cols);
-            v = bc_value(B, 1, (double)in[idx], (double)in[idx - cols], B.dy);
+            nb = idx - cols;
+            side = 1;
+            h = B.dy;
         } else {
             const int j = i - 2 * cols;
             const size_t r = 1 + j / 2;
             if (j & 1) {
                 idx = r * cols + cols - 1;
-                v = bc_value(B, 3, (double)in[idx], (double)in[idx - 1], B.dx);
+                nb = idx - 1;
+                side = 3;
             } else {
                 idx = r * cols;
-                v = bc_value(B, 2, (double)in[idx], (double)in[idx + 1], B.dx);
+                nb = idx + 1;
+                side = 2;
             }
+            h = B.dx;
         }
+        if (!(FX_IN(idx, n) && FX_IN(nb, n))) continue;
+        const double v = bc_value(B, side, (double)in[idx], (double)in[nb], h);
         T o = (T)v;
         if (VAR) o = o * coeff[idx];
         out[idx] = o;
@@ -69,10 +83,12 @@ __global__ void __launch_bounds__(1024) k_lex_jacobi(T *x, const T *__restrict__
         for (int r = rlo + (int)threadIdx.x; r <= rhi; r += blockDim.x) {
             const int c = t - 2 * r;
             const size_t idx = (size_t)r * cols + c;
+            if (!FX_IN(idx, (long long)rows * cols)) continue;
             T ax = (T)0;
             for (int k = 0; k < P.ne_; k++) {
                 const int dr = P.gi[k] / 3 - 1, dc = P.gi[k] % 3 - 1;
-                ax = fx_fma((T)P.gw[k], x[idx + (long)dr * cols + dc], ax);
+                const long long j = (long long)idx + (long long)dr * cols + dc;
+                if (FX_IN(j, (long long)rows * cols)) ax = fx_fma((T)P.gw[k], x[j], ax);
             }
             const T residual = b[idx] - ax;
             x[idx] = fx_fma(om, id * residual, x[idx]);

@@ -12,6 +12,8 @@
 
 #include "fx_points.cuh"
 
+FX_CHECK_FILE(vcycle);
+
 namespace fx {
 
 template <typename T>
@@ -192,6 +194,19 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vtail(TailArgs<T> A, const 
     const int n1 = nlev > 1 ? A.rows[1] * A.cols[1] : 0;
     T *P = Y;       // coarser-level work buffers, inside Y
     T *Q = Y + n1;  // (n1 >= every coarser level; 2 n1 <= n0)
+#ifdef FX_CHECKED
+    {  // the layout the launcher sized: shared memory, register batches, the coarsest's points per thread
+        unsigned dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        long long words = 2LL * top_n;
+        for (int l = 1; l < nlev; l++) words += (l < nlev - 1 ? 2LL : 1LL) * A.rows[l] * A.cols[l];
+        const long long nco = (long long)A.rows[nlev - 1] * A.cols[nlev - 1];
+        bool ok = FX_IN(top_n - 1, (long long)KT * kTailThreads) && FX_IN(words - 1, dyn / sizeof(T)) &&
+                  FX_IN(nco - 1, 4LL * kTailThreads);
+        if (nlev > 1) ok = ok && FX_IN(2LL * n1 - 1, top_n);
+        if (!ok) return;  // uniform over the block: every thread tests the same values
+    }
+#endif
 
     // rhs / x2 of a coarser level l >= 1, packed after Y
     auto level_b = [&](int l) -> T * {

@@ -27,6 +27,8 @@
 
 #include "fx_vcycle.cuh"
 
+FX_CHECK_FILE(wcycle);
+
 namespace fx {
 
 constexpr int kStripWarps = 8;  // warps per block
@@ -131,6 +133,9 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
     const bool sta = own && ina, stb = own && inb;
     const bool cpt = own && ca >= 2 && ca <= cols - 3;  // coarse point (fr, ca) for even fr
     const int r0 = chunk * G.chunk_rows, r1 = min(r0 + G.chunk_rows, rows);  // r0 even
+    const long long nf = (long long)rows * cols, nc = (long long)((rows - 1) / 2 + 1) * ccols;  // extents
+    (void)nf;
+    (void)nc;
     // step q: b row q arrives; x1 row q; x2 row q-1; residual row q-2; full weighting of fine
     // row q-3 (even q-3 only)
     const int q_first = r0 - 3, q_last = r1 + 2;
@@ -145,8 +150,8 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
         fa[k] = (TB)0;
         fb[k] = (TB)0;
         if (row_in(q) && q <= q_last) {
-            if (ina) fa[k] = b[(size_t)q * cols + ca];
-            if (inb) fb[k] = b[(size_t)q * cols + cb];
+            if (ina && FX_IN((long long)q * cols + ca, nf)) fa[k] = b[(size_t)q * cols + ca];
+            if (inb && FX_IN((long long)q * cols + cb, nf)) fb[k] = b[(size_t)q * cols + cb];
         }
     }
 
@@ -170,8 +175,8 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
             x1b[s0] = (rin && inb) ? fx_fma(op.wd, bb, (T)0) : (T)0;
             const int qn = q + D;
             if (F || (row_in(qn) && qn <= q_last)) {
-                if (ina) fa[k % D] = b[ob];
-                if (inb) fb[k % D] = b[ob + 1];
+                if (ina && FX_IN(ob, nf)) fa[k % D] = b[ob];
+                if (inb && FX_IN(ob + 1, nf)) fb[k % D] = b[ob + 1];
             }
             ob += cols;
         }
@@ -186,8 +191,8 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
             x2a[s1] = va;
             x2b[s1] = vb;
             if (F || (rin && q - 1 >= r0 && q - 1 < r1)) {
-                if (sta) x2g[ox] = va;
-                if (stb) x2g[ox + 1] = vb;
+                if (sta && FX_IN(ox, nf)) x2g[ox] = va;
+                if (stb && FX_IN(ox + 1, nf)) x2g[ox + 1] = vb;
             }
             ox += cols;
         }
@@ -207,7 +212,7 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
         // onto coarse row (q-3) / 2 at coarse column ca / 2
         if (!(k & 1)) {  // q - 3 even (r0 even, so q_first odd)
             const int fr = q - 3;
-            if (cpt && (F || (fr >= r0 && fr < r1 && fr >= 2 && fr <= rows - 3))) {
+            if (cpt && (F || (fr >= r0 && fr < r1 && fr >= 2 && fr <= rows - 3)) && FX_IN(oc, nc)) {
                 const T e = (rsa[s1] + rsa[s2]) + (rwa[s0] + rsb[s0]);
                 const T d = (rwa[s1] + rsb[s1]) + (rwa[s2] + rsb[s2]);
                 coarse[oc] = ((T)4 * rsa[s0] + ((T)2 * e + d)) * (T)0.0625;
@@ -259,6 +264,9 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
         // steps with every row test true: q-2 >= max(r0, 1), q + D <= min(rows - 2, q_last)
         const int q_lo = max(r0, 1) + 2, q_hi = min(rows - 2, q_last) - D;
         const int m_last = (q_last >> 1) + 1;  // last coarse row any step reads
+        const long long nf = (long long)rows * cols, nc = (long long)crows * ccols;  // extents
+        (void)nf;
+        (void)nc;
         auto row_in = [&](int r) { return r >= 1 && r <= rows - 2; };
 
         // FIFO of D fine rows: raw x2 and b of both columns; per fine row pair (2m, 2m+1) of the
@@ -273,11 +281,11 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
             ba_[k] = (TB)0;
             bb_[k] = (TB)0;
             if (row_in(q) && q <= q_last) {
-                if (ina) {
+                if (ina && FX_IN(o, nf)) {
                     xa_[k] = x2g[o];
                     ba_[k] = b[o];
                 }
-                if (inb) {
+                if (inb && FX_IN(o + 1, nf)) {
                     xb_[k] = x2g[o + 1];
                     bb_[k] = b[o + 1];
                 }
@@ -287,8 +295,8 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
             v0 = (T)0;
             v1 = (T)0;
             if (m >= 0 && m < crows && m <= m_last) {
-                if (ce0) v0 = e[o];
-                if (ce1) v1 = e[o + 1];
+                if (ce0 && FX_IN(o, nc)) v0 = e[o];
+                if (ce1 && FX_IN(o + 1, nc)) v1 = e[o + 1];
             }
         };
         T c0a, c0b;  // coarse row q >> 1 of the current pair, columns kc, kc+1
@@ -337,11 +345,11 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
                 }
                 const int qn = q + D;
                 if (F) {
-                    if (ina) {
+                    if (ina && FX_IN(orow, nf)) {
                         xa_[k % D] = x2g[orow];
                         ba_[k % D] = b[orow];
                     }
-                    if (inb) {
+                    if (inb && FX_IN(orow + 1, nf)) {
                         xb_[k % D] = x2g[orow + 1];
                         bb_[k % D] = b[orow + 1];
                     }
@@ -368,13 +376,13 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
                 const int r = q - 2;
                 if (F || (row_in(r) && r >= r0 && r < r1)) {
                     TZ *row = z + oz;
-                    if (sta) {
+                    if (sta && FX_IN(oz, nf)) {
                         const TB bv = bwa[s2];
                         const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xa, x3a[s0], x3a[s1], wa, xb), xa);
                         row[0] = (TZ)v;
                         if (RZ) csum_fma(acc[0], (double)bv, (double)(TZ)v);
                     }
-                    if (stb) {
+                    if (stb && FX_IN(oz + 1, nf)) {
                         const TB bv = bwb[s2];
                         const T v = fx_fma(op.wd, (T)bv - op5v(op.a, xb, x3b[s0], x3b[s1], xa, eb), xb);
                         row[1] = (TZ)v;

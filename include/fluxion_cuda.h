@@ -594,6 +594,25 @@ int fx_gmres_solve_op(fx_gmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, 
 int fx_fgmres_solve_op(fx_fgmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc,
                        fx_stats *out);
 
+/* ------------------------------------------------------------------ */
+/* Checked build (new; the reference has no sanitizer mode).  libfluxion_cuda_checked.so is the
+ * same library compiled with FX_CHECKED: its kernels test every index they compute against the
+ * extent of the array addressed, skip an access outside it (a load gives zero, a store is
+ * dropped) and record the first such event of each source unit in a device status word.  It
+ * never traps.  fx_checked_build returns 1 in that library and 0 in the default one, whose checks
+ * are compiled away. */
+int fx_checked_build(void);
+/* Synchronises the context's device, then reads and clears the status words: *count = the number
+ * of units that recorded an out-of-range index since the last call, and for the first of them the
+ * source file of the check (file, NUL-terminated, at most file_cap bytes; may be NULL), its line,
+ * the index and the extent.  The default build reports count 0. */
+int fx_checked_status(fx_ctx *ctx, size_t *count, char *file, size_t file_cap, int *line, long long *index,
+                      long long *extent);
+/* Test hook: a kernel that tests `index` against `extent` with the checked build's check and
+ * makes no memory access, so an out-of-range pair is recorded (checked build) or nothing happens
+ * (default build). */
+int fx_test_check_index(fx_ctx *ctx, long long index, long long extent);
+
 #ifdef __cplusplus
 }
 #endif

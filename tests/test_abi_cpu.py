@@ -77,3 +77,16 @@ def test_device_lanes_are_distinct_values():
     d = Device.Cuda(0, lane=3)
     assert d.lane == 3 and d != Device.Cuda(0) and str(d) == "cuda:0/lane3"
     assert len({Device.Cuda(0, k) for k in range(4)}) == 4
+
+
+def test_checked_library_exports_the_same_symbols_and_says_so():
+    checked = os.path.join(ROOT, "fluxion_b200", "libfluxion_cuda_checked.so")
+    assert os.path.exists(checked), "libfluxion_cuda_checked.so not built"
+    out = subprocess.run(["nm", "-D", "--defined-only", checked], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r"\bT (fx_\w+)", out))
+    missing = [n for n in _declared() if n not in exported]
+    assert not missing, missing
+    # fx_checked_build touches no device: 1 in the checked library, 0 in the default one
+    assert C.CDLL(checked).fx_checked_build() == 1
+    assert L.lib().fx_checked_build() == (1 if os.environ.get("FLUXION_CHECKED") == "1" else 0)
