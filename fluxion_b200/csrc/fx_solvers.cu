@@ -2153,20 +2153,39 @@ __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
     if (PASS > 0 && threadIdx.x < kCgsMax) c[threadIdx.x] = threadIdx.x < kb ? a.coef[threadIdx.x] : 0.0;
     __syncthreads();
     const size_t stride = (size_t)gridDim.x * blockDim.x;
+    // the basis is read in batches of 8 vectors whose loads all issue before the first use, so
+    // each thread keeps 8 loads in flight (one at a time measured 0.18 of HBM bandwidth)
+    constexpr int kB = 8;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         double wv = a.w[i];
         if (PASS > 0) {
 #pragma unroll
-            for (int j = 0; j < kCgsMax; j++)
-                if (j < kb) wv = fma(-c[j], a.v[j][i], wv);
+            for (int j0 = 0; j0 < kCgsMax; j0 += kB) {
+                if (j0 < kb) {
+                    double vv[kB];
+#pragma unroll
+                    for (int t = 0; t < kB; t++) vv[t] = j0 + t < kb ? a.v[j0 + t][i] : 0.0;
+#pragma unroll
+                    for (int t = 0; t < kB; t++)
+                        if (j0 + t < kb) wv = fma(-c[j0 + t], vv[t], wv);
+                }
+            }
             a.w[i] = wv;
         }
         if (PASS == 2) {
             acc[0] = fma(wv, wv, acc[0]);
-        } else {  // pass 1 reads each v_j[i] a second time, from L1 (the thread loaded it just before)
+        } else {  // pass 1 reads each v_j[i] a second time (mostly from L2)
 #pragma unroll
-            for (int j = 0; j < NS; j++)
-                if (j < kb) acc[j] = fma(a.v[j][i], wv, acc[j]);
+            for (int j0 = 0; j0 < NS; j0 += kB) {
+                if (j0 < kb) {
+                    double vv[kB];
+#pragma unroll
+                    for (int t = 0; t < kB; t++) vv[t] = j0 + t < kb ? a.v[j0 + t][i] : 0.0;
+#pragma unroll
+                    for (int t = 0; t < kB; t++)
+                        if (j0 + t < kb) acc[j0 + t] = fma(vv[t], wv, acc[j0 + t]);
+                }
+            }
         }
     }
     // block: warp shuffles, then the warps in order

@@ -464,10 +464,10 @@ int launch_vtail(fx_ctx *ctx, const TailArgs<T> &A, size_t smem, const int *skip
 
 // blocks of `kernel` (of `threads` threads) resident on the whole GPU at once
 template <typename K>
-int band_capacity(fx_ctx *ctx, K kernel, std::atomic<int> &cache, int threads = kBandThreads) {
+int band_capacity(fx_ctx *ctx, K kernel, std::atomic<int> &cache, int threads = kBandThreads, size_t smem = 0) {
     int occ = cache.load(std::memory_order_relaxed);
     if (!occ) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, 0) != cudaSuccess || occ < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1)
             occ = 1;
         cache.store(occ, std::memory_order_relaxed);
     }

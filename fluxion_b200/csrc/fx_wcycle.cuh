@@ -23,7 +23,10 @@
 // bitwise equal to the unfused one.
 #pragma once
 
+#include <mutex>
 #include <type_traits>
+#include <utility>
+#include <vector>
 
 #include "fx_vcycle.cuh"
 
@@ -53,7 +56,11 @@ static_assert(kStripUnroll % kDownFifo == 0 && kStripUnroll % kUpFifo == 0, "FIF
 #define FX_STRIP_F64_DOWN_FIFO 3
 #endif
 #ifndef FX_STRIP_F64_UP_MINB
+#if !defined(FX_STRIP_ASYNC) || FX_STRIP_ASYNC
+#define FX_STRIP_F64_UP_MINB 4  // the row FIFO in shared memory leaves the up pass under 128 registers
+#else
 #define FX_STRIP_F64_UP_MINB 3
+#endif
 #endif
 #ifndef FX_STRIP_F64_DOWN_MINB
 #define FX_STRIP_F64_DOWN_MINB 4
@@ -70,6 +77,84 @@ template <typename T>
 __host__ __device__ constexpr int down_minb() { return sizeof(T) == 8 ? FX_STRIP_F64_DOWN_MINB : 1; }
 static_assert(kStripUnroll % FX_STRIP_F64_UP_FIFO == 0 && kStripUnroll % FX_STRIP_F64_DOWN_FIFO == 0,
               "FIFO depth must divide the unroll");
+
+// Row FIFOs in shared memory (FX_STRIP_ASYNC, the default): the raw loads of the rows ahead go to
+// shared memory by cp.async instead of to registers, so a deep prefetch costs no registers.  PF
+// rows are in flight per strip.  On the 4095^2 FP64 MG-PCG solve (one box, CUDA events): 4.91 ms
+// with the register FIFOs, 4.81 ms with PF = 6, 4.86 ms with PF = 8, 5.46 ms with PF = 12; the
+// level-0 down pass went from 87.5 to 69.1 us (PF = 8), and the FP64 up pass, out of its
+// register FIFO, fits 128 registers (16 warps per SM instead of 12).
+#ifndef FX_STRIP_ASYNC
+#define FX_STRIP_ASYNC 1
+#endif
+#ifndef FX_STRIP_F64_DOWN_PF
+#define FX_STRIP_F64_DOWN_PF 6
+#endif
+#ifndef FX_STRIP_F64_UP_PF
+#define FX_STRIP_F64_UP_PF 6
+#endif
+#ifndef FX_STRIP_F32_DOWN_PF
+#define FX_STRIP_F32_DOWN_PF 6
+#endif
+#ifndef FX_STRIP_F32_UP_PF
+#define FX_STRIP_F32_UP_PF 6
+#endif
+template <typename T>
+__host__ __device__ constexpr int down_pf() { return sizeof(T) == 8 ? FX_STRIP_F64_DOWN_PF : FX_STRIP_F32_DOWN_PF; }
+template <typename T>
+__host__ __device__ constexpr int up_pf() { return sizeof(T) == 8 ? FX_STRIP_F64_UP_PF : FX_STRIP_F32_UP_PF; }
+
+// One element (4 or 8 bytes) from global to shared memory, asynchronously; zero-filled when !valid
+// (nothing is read then: src-size 0, and the address given is `any`, a valid one).
+template <typename E>
+__device__ __forceinline__ void cp_async_elem(E *dst, const E *src, bool valid, const E *any) {
+    static_assert(sizeof(E) == 4 || sizeof(E) == 8, "4- or 8-byte elements");
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(valid ? src : any),
+                 "n"((int)sizeof(E)), "r"(valid ? (int)sizeof(E) : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// A lane's two columns of PF + 1 rows of one array in shared memory.  The caller commits one
+// cp.async group per step (every FIFO of the kernel in it) and waits for the group of the row it
+// reads; a step refills the slot the previous step read (its value is in registers by then), so
+// no copy lands in a slot that is still to be read.
+template <typename E, int PF>
+struct SmemFifo {
+    E *base;  // this lane's column pair in slot 0; slot s at base + 64 s
+    int rd, wr;
+    __device__ __forceinline__ void init(E *warp_base, int lane) {
+        base = warp_base + 2 * lane;
+        rd = 0;
+        wr = PF;
+    }
+    __device__ __forceinline__ void put_at(int slot, const E *src, bool va, bool vb, const E *any) {
+        cp_async_elem(base + slot * 64, src, va, any);
+        cp_async_elem(base + slot * 64 + 1, src + 1, vb, any);
+    }
+    __device__ __forceinline__ void put(const E *src, bool va, bool vb, const E *any) { put_at(wr, src, va, vb, any); }
+    __device__ __forceinline__ E a() const { return base[rd * 64]; }
+    __device__ __forceinline__ E b() const { return base[rd * 64 + 1]; }
+    __device__ __forceinline__ void advance() {
+        rd = rd == PF ? 0 : rd + 1;
+        wr = wr == PF ? 0 : wr + 1;
+    }
+};
+
+// dynamic shared memory of a strip launch: per warp, PF + 1 rows of 64 elements of each FIFO array
+template <typename T, typename TB>
+constexpr size_t wdown_smem() {
+    return FX_STRIP_ASYNC ? (size_t)strip_warps<T>() * (down_pf<T>() + 1) * 64 * sizeof(TB) : 0;
+}
+template <typename T, typename TB>
+constexpr size_t wup_smem() {
+    return FX_STRIP_ASYNC ? (size_t)strip_warps<T>() * (up_pf<T>() + 1) * 64 * (sizeof(T) + sizeof(TB)) : 0;
+}
 
 struct StripGeom {
     int rows, cols;
@@ -121,7 +206,8 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
                                                              const int *skip) {
     grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
-    constexpr int D = down_fifo<T>(), R = kStripUnroll;
+    [[maybe_unused]] constexpr int D = down_fifo<T>();
+    constexpr int R = kStripUnroll;
     const int lane = threadIdx.x & 31;
     const int item = blockIdx.x * strip_warps<T>() + (threadIdx.x >> 5);
     if (item >= G.nitems) return;  // whole warps
@@ -139,11 +225,26 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
     // step q: b row q arrives; x1 row q; x2 row q-1; residual row q-2; full weighting of fine
     // row q-3 (even q-3 only)
     const int q_first = r0 - 3, q_last = r1 + 2;
+    auto row_in = [&](int r) { return r >= 1 && r <= rows - 2; };
+#if FX_STRIP_ASYNC
+    constexpr int PF = down_pf<T>();
+    // steps with every row test true: q-3 >= max(r0, 2), q + PF <= min(rows - 2, q_last)
+    const int q_lo = max(r0, 2) + 3, q_hi = min(rows - 2, q_last) - PF;
+    extern __shared__ __align__(16) unsigned char strip_smem[];
+    SmemFifo<TB, PF> fifo;
+    fifo.init(reinterpret_cast<TB *>(strip_smem) + (threadIdx.x >> 5) * ((PF + 1) * 64), lane);
+#pragma unroll
+    for (int k = 0; k < PF; k++) {
+        const int q = q_first + k;
+        const long long o = (long long)q * cols + ca;
+        const bool rv = row_in(q) && q <= q_last;
+        fifo.put_at(k, b + o, rv && ina && FX_IN(o, nf), rv && inb && FX_IN(o + 1, nf), b);
+        cp_async_commit();
+    }
+#else
     // steps with every row test true: q-3 >= max(r0, 2), q + D <= min(rows - 2, q_last)
     const int q_lo = max(r0, 2) + 3, q_hi = min(rows - 2, q_last) - D;
-
     TB fa[D], fb[D];
-    auto row_in = [&](int r) { return r >= 1 && r <= rows - 2; };
 #pragma unroll
     for (int k = 0; k < D; k++) {
         const int q = q_first + k;
@@ -154,12 +255,17 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
             if (inb && FX_IN((long long)q * cols + cb, nf)) fb[k] = b[(size_t)q * cols + cb];
         }
     }
+#endif
 
     T bwa[3] = {}, bwb[3] = {}, x1a[3] = {}, x1b[3] = {}, x2a[3] = {}, x2b[3] = {};
     T rsa[3] = {}, rsb[3] = {}, rwa[3] = {};
     // element offsets of this lane's column ca, advanced one row per step: the rhs row being
     // fetched (q + D), the x2 row being stored (q - 1), and the coarse row of fine row q - 3
+#if FX_STRIP_ASYNC
+    long long ob = (long long)(q_first + PF) * cols + ca;
+#else
     long long ob = (long long)(q_first + D) * cols + ca;
+#endif
     long long ox = (long long)(q_first - 1) * cols + ca;
     long long oc = (long long)((q_first - 3) >> 1) * ccols + (ca >> 1);  // q_first - 3 even
     auto step = [&](int k, int q, auto fast) {
@@ -167,17 +273,30 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
         const int s0 = k % 3, s1 = (k + 2) % 3, s2 = (k + 1) % 3;  // slots of rows q, q-1, q-2
         // row q: rhs and x1 = w b (0 on the ring); refill with row q + D
         {
+#if FX_STRIP_ASYNC
+            cp_async_wait<PF - 1>();  // row q's group is complete
+            const T ba = (T)fifo.a(), bb = (T)fifo.b();
+#else
             const T ba = (T)fa[k % D], bb = (T)fb[k % D];
+#endif
             const bool rin = F || row_in(q);
             bwa[s0] = ba;
             bwb[s0] = bb;
             x1a[s0] = (rin && ina) ? fx_fma(op.wd, ba, (T)0) : (T)0;
             x1b[s0] = (rin && inb) ? fx_fma(op.wd, bb, (T)0) : (T)0;
+#if FX_STRIP_ASYNC
+            const int qn = q + PF;
+            const bool rv = F || (row_in(qn) && qn <= q_last);
+            fifo.put(b + ob, rv && ina && FX_IN(ob, nf), rv && inb && FX_IN(ob + 1, nf), b);
+            cp_async_commit();
+            fifo.advance();
+#else
             const int qn = q + D;
             if (F || (row_in(qn) && qn <= q_last)) {
                 if (ina && FX_IN(ob, nf)) fa[k % D] = b[ob];
                 if (inb && FX_IN(ob + 1, nf)) fb[k % D] = b[ob + 1];
             }
+#endif
             ob += cols;
         }
         // row q-1: x2
@@ -232,6 +351,9 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, down_minb<T>()) k_wdown
             }
         }
     }
+#if FX_STRIP_ASYNC
+    cp_async_wait<0>();  // no copy outlives the warp
+#endif
 }
 
 // ---------------------------------------------------------------- up
@@ -245,7 +367,12 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
                                                            Fin fin, RedArgs<1> ra, const int *skip) {
     grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;
-    constexpr int D = up_fifo<T>(), R = kStripUnroll;
+    [[maybe_unused]] constexpr int D = up_fifo<T>();
+    constexpr int R = kStripUnroll;
+#if FX_STRIP_ASYNC
+    constexpr int PF = up_pf<T>();
+    extern __shared__ __align__(16) unsigned char strip_smem[];
+#endif
     const int lane = threadIdx.x & 31;
     const int item = blockIdx.x * strip_warps<T>() + (threadIdx.x >> 5);
     CSum acc[1] = {CSum{0.0, 0.0}};
@@ -261,8 +388,13 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
         const int r0 = chunk * G.chunk_rows, r1 = min(r0 + G.chunk_rows, rows);  // r0 even
         // step q: F0 row q = x2 + P e; x3 row q-1; z row q-2
         const int q_first = r0 - 2, q_last = r1 + 1;  // q_first even
+#if FX_STRIP_ASYNC
+        // steps with every row test true: q-2 >= max(r0, 1), q + PF <= min(rows - 2, q_last)
+        const int q_lo = max(r0, 1) + 2, q_hi = min(rows - 2, q_last) - PF;
+#else
         // steps with every row test true: q-2 >= max(r0, 1), q + D <= min(rows - 2, q_last)
         const int q_lo = max(r0, 1) + 2, q_hi = min(rows - 2, q_last) - D;
+#endif
         const int m_last = (q_last >> 1) + 1;  // last coarse row any step reads
         const long long nf = (long long)rows * cols, nc = (long long)crows * ccols;  // extents
         (void)nf;
@@ -272,10 +404,34 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
         // FIFO of D fine rows: raw x2 and b of both columns; per fine row pair (2m, 2m+1) of the
         // unrolled step the coarse row m+1 at columns kc, kc+1, R rows ahead (row m is kept
         // from the previous pair)
-        T xa_[D], xb_[D], ea_[R / 2], eb_[R / 2];
+        T ea_[R / 2], eb_[R / 2];
+#if FX_STRIP_ASYNC
+        // x2 FIFOs of the block's warps, then their b FIFOs
+        SmemFifo<T, PF> fx;
+        SmemFifo<TB, PF> fbq;
+        fx.init(reinterpret_cast<T *>(strip_smem) + (threadIdx.x >> 5) * ((PF + 1) * 64), lane);
+        fbq.init(reinterpret_cast<TB *>(strip_smem + (size_t)strip_warps<T>() * (PF + 1) * 64 * sizeof(T)) +
+                     (threadIdx.x >> 5) * ((PF + 1) * 64),
+                 lane);
+        auto put_row = [&](int slot, int q, long long o, bool fast) {  // slot < 0: the FIFOs' next slot
+            const bool rv = fast || (row_in(q) && q <= q_last);
+            const bool va = rv && ina && FX_IN(o, nf), vb = rv && inb && FX_IN(o + 1, nf);
+            if (slot < 0) {
+                fx.put(x2g + o, va, vb, x2g);
+                fbq.put(b + o, va, vb, b);
+            } else {
+                fx.put_at(slot, x2g + o, va, vb, x2g);
+                fbq.put_at(slot, b + o, va, vb, b);
+            }
+            cp_async_commit();
+        };
+#else
+        T xa_[D], xb_[D];
         TB ba_[D], bb_[D];
+#endif
         // o: element offset of (q, ca) / (m, kc)
-        auto load_row = [&](int q, int k, long long o) {
+        [[maybe_unused]] auto load_row = [&](int q, int k, long long o) {
+#if !FX_STRIP_ASYNC
             xa_[k] = (T)0;
             xb_[k] = (T)0;
             ba_[k] = (TB)0;
@@ -290,6 +446,11 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
                     bb_[k] = b[o + 1];
                 }
             }
+#else
+            (void)q;
+            (void)k;
+            (void)o;
+#endif
         };
         auto load_coarse = [&](int m, T &v0, T &v1, long long o) {
             v0 = (T)0;
@@ -301,8 +462,13 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
         };
         T c0a, c0b;  // coarse row q >> 1 of the current pair, columns kc, kc+1
         load_coarse(q_first >> 1, c0a, c0b, (long long)(q_first >> 1) * ccols + kc);
+#if FX_STRIP_ASYNC
+#pragma unroll
+        for (int k = 0; k < PF; k++) put_row(k, q_first + k, (long long)(q_first + k) * cols + ca, false);
+#else
 #pragma unroll
         for (int k = 0; k < D; k++) load_row(q_first + k, k, (long long)(q_first + k) * cols + ca);
+#endif
 #pragma unroll
         for (int k = 0; k < R; k += 2) {
             const int m = ((q_first + k) >> 1) + 1;
@@ -310,7 +476,11 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
         }
         // running element offsets, advanced as the march goes: the fine row being fetched
         // (q + D), the coarse row fetched at odd steps ((q + R + 1) / 2), the z row (q - 2)
+#if FX_STRIP_ASYNC
+        long long orow = (long long)(q_first + PF) * cols + ca;
+#else
         long long orow = (long long)(q_first + D) * cols + ca;
+#endif
         long long oe = (long long)((q_first + R + 2) >> 1) * ccols + kc;
         long long oz = (long long)(q_first - 2) * cols + ca;
 
@@ -333,16 +503,29 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
                     pb = (T)0.5 * (e00 + e01);                    // v_eo
                 }
                 const bool rin = F || row_in(q);
+#if FX_STRIP_ASYNC
+                cp_async_wait<PF - 1>();  // row q's group is complete
+                fa[s0] = (rin && ina) ? fx.a() + pa : (T)0;
+                fb[s0] = (rin && inb) ? fx.b() + pb : (T)0;
+                bwa[s0] = fbq.a();
+                bwb[s0] = fbq.b();
+#else
                 fa[s0] = (rin && ina) ? xa_[k % D] + pa : (T)0;
                 fb[s0] = (rin && inb) ? xb_[k % D] + pb : (T)0;
                 bwa[s0] = ba_[k % D];
                 bwb[s0] = bb_[k % D];
+#endif
                 if (ro) {  // the pair is done: its lower coarse row becomes the upper one
                     c0a = e10;
                     c0b = e11;
                     load_coarse((q + R + 1) >> 1, ea_[k / 2], eb_[k / 2], oe);
                     oe += ccols;
                 }
+#if FX_STRIP_ASYNC
+                put_row(-1, q + PF, orow, F);
+                fx.advance();
+                fbq.advance();
+#else
                 const int qn = q + D;
                 if (F) {
                     if (ina && FX_IN(orow, nf)) {
@@ -356,6 +539,7 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
                 } else {
                     load_row(qn, k % D, orow);
                 }
+#endif
                 orow += cols;
             }
             // row q-1: x3
@@ -404,6 +588,9 @@ __global__ void __launch_bounds__(strip_warps<T>() * 32, up_minb<T>()) k_wup(Str
                 }
             }
         }
+#if FX_STRIP_ASYNC
+        cp_async_wait<0>();  // no copy outlives the warp
+#endif
     }
     if constexpr (RZ) grid_reduce<1>(acc, ra, fin);
 }
@@ -415,16 +602,35 @@ inline long strip_capacity(long resident_warps, int chunk_pct) {
     return cap < 1 ? 1 : cap;
 }
 
+// opt a strip kernel in to more than 48 KB of dynamic shared memory (the attribute is set per
+// device and kernel; setting it again is harmless, so the record only saves calls)
+template <typename K>
+int strip_smem_optin(K kernel, size_t smem) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void *, int>> done;
+    int dev = 0;
+    FX_CUDA(cudaGetDevice(&dev));
+    const std::pair<const void *, int> key{reinterpret_cast<const void *>(kernel), dev};
+    std::lock_guard<std::mutex> lk(mu);
+    for (const auto &d : done)
+        if (d == key) return FX_OK;
+    FX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    done.push_back(key);
+    return FX_OK;
+}
+
 template <typename T, typename TB>
 int launch_wdown(fx_ctx *ctx, size_t rows, size_t cols, const TB *b, T *x2, T *coarse, size_t ccols,
                  const VOp<T> &op, const int *skip, int chunk_pct = 100) {
     static std::atomic<int> occ{0};
     constexpr int W = strip_warps<T>();
-    const long cap = strip_capacity((long)band_capacity(ctx, k_wdown<T, TB>, occ, W * 32) * W, chunk_pct);
+    constexpr size_t smem = wdown_smem<T, TB>();
+    if (smem > 48 * 1024) FX_TRY(strip_smem_optin(k_wdown<T, TB>, smem));
+    const long cap = strip_capacity((long)band_capacity(ctx, k_wdown<T, TB>, occ, W * 32, smem) * W, chunk_pct);
     const StripGeom G = strip_geom(rows, cols, kDownOwn, cap);
     const int blocks = (G.nitems + W - 1) / W;
     timing_pre(ctx, "mg_down");
-    launch_pdl(ctx, k_wdown<T, TB>, blocks, W * 32, 0, G, b, x2, coarse, (int)ccols, op, skip);
+    launch_pdl(ctx, k_wdown<T, TB>, blocks, W * 32, smem, G, b, x2, coarse, (int)ccols, op, skip);
     // reads b, writes the smoothed x2 and the restricted coarse rhs
     const double pts = (double)rows * (double)cols, cpts = (double)((rows - 1) / 2 + 1) * (double)ccols;
     timing_post(ctx, pts, pts * (sizeof(TB) + sizeof(T)) + cpts * sizeof(T));
@@ -436,12 +642,15 @@ int launch_wup(fx_ctx *ctx, size_t rows, size_t cols, const T *x2, const T *e, s
                const VOp<T> &op, Fin fin, const int *skip, int chunk_pct = 100) {
     static std::atomic<int> occ{0};
     constexpr int W = strip_warps<T>();
-    const long cap = strip_capacity((long)band_capacity(ctx, k_wup<T, TB, TZ, RZ, Fin>, occ, W * 32) * W, chunk_pct);
+    constexpr size_t smem = wup_smem<T, TB>();
+    if (smem > 48 * 1024) FX_TRY(strip_smem_optin(k_wup<T, TB, TZ, RZ, Fin>, smem));
+    const long cap =
+        strip_capacity((long)band_capacity(ctx, k_wup<T, TB, TZ, RZ, Fin>, occ, W * 32, smem) * W, chunk_pct);
     const StripGeom G = strip_geom(rows, cols, kUpOwn, cap);
     const int blocks = (G.nitems + W - 1) / W;
     if (RZ && blocks > kMaxRedBlocks) return fail(FX_ERR_INVALID_ARGUMENT, "grid too large");
     timing_pre(ctx, "mg_up");
-    launch_pdl(ctx, k_wup<T, TB, TZ, RZ, Fin>, blocks, W * 32, 0, G, x2, e, (int)ccols, b, z, op, fin,
+    launch_pdl(ctx, k_wup<T, TB, TZ, RZ, Fin>, blocks, W * 32, smem, G, x2, e, (int)ccols, b, z, op, fin,
                red_args<1>(ctx), skip);
     // reads x2, the coarse correction e and b, writes z
     const double pts = (double)rows * (double)cols, cpts = (double)((rows - 1) / 2 + 1) * (double)ccols;
