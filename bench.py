@@ -71,13 +71,14 @@ def parse():
                    help="--mode vcycle: autotune the cycle's layout first; --mode batch: choose the batched "
                         "solver's chunk size, sweep counts and cycle precision first (timed on a sample)")
     p.add_argument("--tune-cache", default=None, help="JSON file that keeps autotuner choices between runs")
-    p.add_argument("--mode", default="solve", choices=["solve", "vcycle", "batch", "convdiff", "learned", "lsm_step"],
+    p.add_argument("--mode", default="solve", choices=["solve", "vcycle", "batch", "convdiff", "learned", "lsm_step", "micro"],
                    help="solve: the headline MG-PCG solve; vcycle: preconditioner applications alone "
                         "(the F32 V(2,2)-cycle on FP64 vectors), e.g. as a profiling target; batch: "
                         "1024 conv-diff problems; convdiff: convection-dominated conv-diff at --n; "
                         "learned: train the learned smoother, then FGMRES(30) with the learned vs the plain "
                         "conv-diff cycle at --n; lsm_step: learned smoothing steps alone at --n (a profiling "
-                        "target of the network kernel)")
+                        "target of the network kernel); micro: the stencil / AXPY / dual-dot microbenchmarks "
+                        "alone on an --n x --n grid")
     p.add_argument("--nu", default="1e-3,1e-4", help="--mode convdiff: viscosities, comma-separated")
     p.add_argument("--k-range", default="6,10",
                    help="--mode batch: interior sizes 2^k - 1 for k uniform in this inclusive range")
@@ -852,6 +853,16 @@ def main():
         return run_learned(args)
     if args.mode == "lsm_step":
         return run_lsm_step(args)
+    if args.mode == "micro":  # the microbenchmarks alone, on an --n^2 grid (a profiling target)
+        import torch
+        from fluxion_b200 import Device
+        be = Device.Cuda(0).backend()
+        stream = torch.cuda.Stream()
+        be.set_stream(stream.cuda_stream)
+        peak, _ = measured_peaks()
+        print(json.dumps({"mode": "micro", "n": args.n, "microbench": microbench(be, peak, args, stream, args.n)}),
+              flush=True)
+        return 0
 
     import torch
 
@@ -1127,12 +1138,11 @@ def main():
     return 0
 
 
-def microbench(be, peak, args, stream):
-    """Stencil / stencil-AXPY / AXPY / dual-dot on a 16384^2 grid (inputs far above L2)."""
+def microbench(be, peak, args, stream, n=16384):
+    """Stencil / stencil-AXPY / AXPY / dual-dot on an n^2 grid (16384^2 by default: inputs far above L2)."""
     import torch
     from fluxion_b200 import Boundaries, DType, Grid, Stencil
 
-    n = 16384
     g = Grid.square(n, 1.0 / (n - 1))
     st = Stencil.laplacian_2d_5pt(g.dx, g.dy)
     bc = Boundaries.zero_dirichlet()
