@@ -154,6 +154,24 @@ class CudaBuffer:
             check(L.lib().fx_write_f32(self.backend.ctx, self.handle,
                                        a.ctypes.data_as(C.POINTER(C.c_float)), a.size))
 
+    def write_async(self, data: np.ndarray, stream: int = 0) -> None:
+        """Enqueue the copy of a contiguous float64 host array (page-locked for a true DMA) into this
+        F64 buffer on `stream` (a cudaStream_t handle; 0 = the backend's stream) without waiting
+        (fx_write_f64_async).  The caller orders it against the work that reads it with events."""
+        if data.dtype != np.float64 or not data.flags.c_contiguous:
+            raise InvalidArgument("write_async takes a contiguous float64 array")
+        check(L.lib().fx_write_f64_async(self.backend.ctx, self.handle,
+                                         data.ctypes.data_as(C.POINTER(C.c_double)), data.size, stream or None))
+
+    def copy_to_host_async(self, out: np.ndarray, stream: int = 0) -> None:
+        """Enqueue the copy of this F64 buffer into a contiguous float64 host array on `stream`
+        without waiting (fx_copy_to_host_f64_async)."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise InvalidArgument("copy_to_host_async takes a contiguous float64 array")
+        check(L.lib().fx_copy_to_host_f64_async(self.backend.ctx, self.handle,
+                                                out.ctypes.data_as(C.POINTER(C.c_double)), out.size,
+                                                stream or None))
+
     def free(self) -> None:
         if self.handle:
             L.lib().fx_free(self.handle)

@@ -2139,72 +2139,99 @@ struct CgsArgs {
     unsigned *ticket;
 };
 
+// The grid walks tiles of kBlock elements.  In a tile, thread t first owns element t: in passes
+// 1 and 2 it reads w and the basis once and writes the updated w (loads in batches of 8, all
+// issued before the first use).  For the multi-dot (passes 0 and 1) warp q then owns the basis
+// vectors j = q, q + 8, q + 16, q + 24 and lane l the tile's elements l, l + 32, ..., with w from
+// shared memory: a thread keeps four partial sums, so the kernel needs few registers and many
+// resident warps keep the loads in flight.  (One element and 32 partial sums per thread measured
+// 0.42 of HBM bandwidth, latency-bound at 16 warps per SM.)  The sums of a basis vector are
+// added in a fixed order: over a warp's tiles, the lanes' shuffle tree, then the blocks.
 template <int PASS>
 __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
     grid_dep_enter();
-    constexpr int NS = PASS == 2 ? 1 : kCgsMax;
+    constexpr int kW = kBlock / 32;     // warps per block
+    constexpr int kJ = kCgsMax / kW;    // basis vectors per warp in the multi-dot
+    constexpr int kB = 8;               // loads per batch in the update
     const int kb = a.kb, ns = PASS == 2 ? 1 : kb;
-    // every index into acc is a compile-time constant (unrolled loops, predicated on kb), so the
-    // partials stay in registers
-    double acc[NS];
-#pragma unroll
-    for (int j = 0; j < NS; j++) acc[j] = 0.0;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     __shared__ double c[kCgsMax];
-    if (PASS > 0 && threadIdx.x < kCgsMax) c[threadIdx.x] = threadIdx.x < kb ? a.coef[threadIdx.x] : 0.0;
+    __shared__ const double *vp[kCgsMax];
+    __shared__ double sw[kBlock];
+    __shared__ double red[kW];
+    __shared__ bool is_last;
+    if (threadIdx.x < kCgsMax) {
+        c[threadIdx.x] = (PASS > 0 && threadIdx.x < kb) ? a.coef[threadIdx.x] : 0.0;
+        vp[threadIdx.x] = threadIdx.x < kb ? a.v[threadIdx.x] : nullptr;
+    }
     __syncthreads();
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    // the basis is read in batches of 8 vectors whose loads all issue before the first use, so
-    // each thread keeps 8 loads in flight (one at a time measured 0.18 of HBM bandwidth)
-    constexpr int kB = 8;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        double wv = a.w[i];
-        if (PASS > 0) {
+    double acc[kJ];
 #pragma unroll
-            for (int j0 = 0; j0 < kCgsMax; j0 += kB) {
-                if (j0 < kb) {
-                    double vv[kB];
+    for (int q = 0; q < kJ; q++) acc[q] = 0.0;
+    const size_t ntiles = (n + kBlock - 1) / kBlock;
+    for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const size_t i0 = tile * kBlock, i = i0 + threadIdx.x;
+        double wv = 0.0;
+        if (i < n) {
+            wv = a.w[i];
+            if (PASS > 0) {
 #pragma unroll
-                    for (int t = 0; t < kB; t++) vv[t] = j0 + t < kb ? a.v[j0 + t][i] : 0.0;
+                for (int j0 = 0; j0 < kCgsMax; j0 += kB) {
+                    if (j0 < kb) {
+                        double vv[kB];
 #pragma unroll
-                    for (int t = 0; t < kB; t++)
-                        if (j0 + t < kb) wv = fma(-c[j0 + t], vv[t], wv);
+                        for (int t = 0; t < kB; t++) vv[t] = j0 + t < kb ? vp[j0 + t][i] : 0.0;
+#pragma unroll
+                        for (int t = 0; t < kB; t++)
+                            if (j0 + t < kb) wv = fma(-c[j0 + t], vv[t], wv);
+                    }
                 }
+                a.w[i] = wv;
             }
-            a.w[i] = wv;
         }
         if (PASS == 2) {
             acc[0] = fma(wv, wv, acc[0]);
-        } else {  // pass 1 reads each v_j[i] a second time (mostly from L2)
+            continue;
+        }
+        sw[threadIdx.x] = wv;
+        __syncthreads();
 #pragma unroll
-            for (int j0 = 0; j0 < NS; j0 += kB) {
-                if (j0 < kb) {
-                    double vv[kB];
+        for (int e = 0; e < kBlock; e += 32) {
+            const size_t ie = i0 + e + lane;
+            if (ie < n) {
+                const double x = sw[e + lane];
+                double vv[kJ];
 #pragma unroll
-                    for (int t = 0; t < kB; t++) vv[t] = j0 + t < kb ? a.v[j0 + t][i] : 0.0;
-#pragma unroll
-                    for (int t = 0; t < kB; t++)
-                        if (j0 + t < kb) acc[j0 + t] = fma(vv[t], wv, acc[j0 + t]);
+                for (int q = 0; q < kJ; q++) {
+                    const int j = wid + kW * q;
+                    vv[q] = j < kb ? vp[j][ie] : 0.0;
                 }
+#pragma unroll
+                for (int q = 0; q < kJ; q++)
+                    if (wid + kW * q < kb) acc[q] = fma(vv[q], x, acc[q]);
             }
         }
+        __syncthreads();  // sw is rewritten by the next tile
     }
-    // block: warp shuffles, then the warps in order
-    __shared__ double sh[kBlock / 32][NS];
-    __shared__ bool is_last;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int j = 0; j < NS; j++) {
-        if (j < ns) {
-            double v = acc[j];
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            if (lane == 0) sh[wid][j] = v;
+    // block partials: basis vector j is one warp's (a shuffle tree); ||w||^2 is every thread's
+    if (PASS == 2) {
+        double v = acc[0];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) red[wid] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int k = 0; k < kW; k++) t += red[k];
+            a.part[(size_t)blockIdx.x * kCgsMax] = t;
         }
-    }
-    __syncthreads();
-    if (threadIdx.x < ns) {
-        double t = 0.0;
-        for (int k = 0; k < kBlock / 32; k++) t += sh[k][threadIdx.x];
-        a.part[(size_t)blockIdx.x * kCgsMax + threadIdx.x] = t;
+    } else {
+#pragma unroll
+        for (int q = 0; q < kJ; q++) {
+            double v = acc[q];
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            const int j = wid + kW * q;
+            if (lane == 0 && j < kb) a.part[(size_t)blockIdx.x * kCgsMax + j] = v;
+        }
     }
     __threadfence();
     __syncthreads();
@@ -2215,20 +2242,20 @@ __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
     // last block: warp w folds sums j = w, w + 8, ...; lane l takes blocks l, l + 32, ... (four
     // loads in flight), then a fixed shuffle tree merges the lanes' compensated sums
     const unsigned nb = gridDim.x;
-    for (int j = wid; j < ns; j += kBlock / 32) {
+    for (int j = wid; j < ns; j += kW) {
         CSum t{0.0, 0.0};
-        unsigned b = lane;
-        for (; b + 96 < nb; b += 128) {
-            const double p0 = __ldcg(a.part + (size_t)b * kCgsMax + j);
-            const double p1 = __ldcg(a.part + (size_t)(b + 32) * kCgsMax + j);
-            const double p2 = __ldcg(a.part + (size_t)(b + 64) * kCgsMax + j);
-            const double p3 = __ldcg(a.part + (size_t)(b + 96) * kCgsMax + j);
+        unsigned bb = lane;
+        for (; bb + 96 < nb; bb += 128) {
+            const double p0 = __ldcg(a.part + (size_t)bb * kCgsMax + j);
+            const double p1 = __ldcg(a.part + (size_t)(bb + 32) * kCgsMax + j);
+            const double p2 = __ldcg(a.part + (size_t)(bb + 64) * kCgsMax + j);
+            const double p3 = __ldcg(a.part + (size_t)(bb + 96) * kCgsMax + j);
             csum_add(t, p0);
             csum_add(t, p1);
             csum_add(t, p2);
             csum_add(t, p3);
         }
-        for (; b < nb; b += 32) csum_add(t, __ldcg(a.part + (size_t)b * kCgsMax + j));
+        for (; bb < nb; bb += 32) csum_add(t, __ldcg(a.part + (size_t)bb * kCgsMax + j));
         for (int off = 16; off > 0; off >>= 1) {
             CSum o;
             o.s = __shfl_down_sync(0xffffffffu, t.s, off);

@@ -3,12 +3,120 @@
 // smoothing primitives.  All grid kernels use the row-marching framework
 // (fx_internal.cuh): one HBM read per element of the marched field.
 #include "fx_points.cuh"
+#include "fx_wcycle.cuh"
 
 using namespace fx;
 
 FX_CHECK_FILE(stencil);
 
 namespace {
+
+// ------------------------------------------------ five-point stencil as a strip march
+//
+// apply_stencil and stencil_axpy with the five-point stencil (constant coefficient) take a leaner
+// path than the band march: a warp owns a strip of 64 columns (two per lane: lanes 1..30 own
+// theirs, lanes 0 and 31 hold the halo columns) and marches it down a chunk of rows.  Each lane
+// keeps its columns' rows q-2, q-1, q in registers; west / east neighbours come by one shuffle
+// each; the rows ahead (of x, and of y for the axpy) are copied into shared memory by cp.async,
+// 6 rows in flight.  No block barrier and no shared-memory ring: about a third of the band
+// march's instructions per point, which is what bounds the FP32 stencil (the band march measured
+// 0.64 of HBM bandwidth there with 69 % issue activity).  Every value is stencil_eval's
+// expression (ops.rs:923-935 nesting), so the result equals the band march's bit for bit.
+constexpr int kSOwn = 60;  // own columns per strip
+constexpr int kSWarps = 8;
+constexpr int kSPF = 6;    // rows in flight
+
+template <typename T, bool AXPY>
+constexpr size_t sstrip_smem() {
+    return (size_t)kSWarps * (AXPY ? 2 : 1) * (kSPF + 1) * 64 * sizeof(T);
+}
+
+template <typename T, bool AXPY>
+__global__ void __launch_bounds__(kSWarps * 32) k_sstrip(StripGeom G, const T *__restrict__ x, T *__restrict__ out,
+                                                         StencilP P, T alpha) {
+    grid_dep_enter();
+    extern __shared__ __align__(16) unsigned char ss_smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int item = blockIdx.x * kSWarps + w;
+    if (item >= G.nitems) return;  // whole warps
+    const int strip = item % G.nstrips, chunk = item / G.nstrips;
+    const int rows = G.rows, cols = G.cols;
+    const int ca = strip * kSOwn - 1 + 2 * lane, cb = ca + 1;
+    const bool lda = ca >= 0 && ca < cols, ldb = cb >= 0 && cb < cols;
+    const bool own = lane >= 1 && lane <= 30;
+    const bool sta = own && ca >= 1 && ca <= cols - 2, stb = own && cb >= 1 && cb <= cols - 2;
+    const int r0 = chunk * G.chunk_rows, r1 = min(r0 + G.chunk_rows, rows);
+    const int rlo = max(r0, 1), rhi = min(r1, rows - 1);  // output rows [rlo, rhi)
+    const long long n = (long long)rows * cols;
+    (void)n;
+    const T pc = (T)P.c, pn = (T)P.n, ps = (T)P.s, pw = (T)P.w, pe = (T)P.e;
+    SmemFifo<T, kSPF> fx;
+    SmemFifo<T, kSPF> fy;
+    fx.init(reinterpret_cast<T *>(ss_smem) + w * ((kSPF + 1) * 64), lane);
+    if (AXPY) fy.init(reinterpret_cast<T *>(ss_smem) + (kSWarps + w) * ((kSPF + 1) * 64), lane);
+    // step q: row q of x (and y) arrives, row q - 1 is computed; rows r0 - 1 .. r1 are read
+    const int qa = r0 - 1, qb = r1;
+    auto put = [&](int slot, int q) {
+        const bool rv = q >= 0 && q < rows && q <= qb;
+        const long long o = (long long)q * cols + ca;
+        const bool va = rv && lda && FX_IN(o, n), vb = rv && ldb && FX_IN(o + 1, n);
+        if (slot < 0) {
+            fx.put(x + o, va, vb, x);
+            if (AXPY) fy.put(out + o, va, vb, out);
+        } else {
+            fx.put_at(slot, x + o, va, vb, x);
+            if (AXPY) fy.put_at(slot, out + o, va, vb, out);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int k = 0; k < kSPF; k++) put(k, qa + k);
+    T xna = (T)0, xnb = (T)0, xca = (T)0, xcb = (T)0, yca = (T)0, ycb = (T)0;
+    long long o = (long long)(qa - 1) * cols + ca;  // element offset of (q - 1, ca)
+    for (int q = qa; q <= qb; q++) {
+        cp_async_wait<kSPF - 1>();  // row q's group is complete
+        const T xsa = fx.a(), xsb = fx.b();
+        T ysa = (T)0, ysb = (T)0;
+        if (AXPY) {
+            ysa = fy.a();
+            ysb = fy.b();
+        }
+        put(-1, q + kSPF);
+        fx.advance();
+        if (AXPY) fy.advance();
+        const int r = q - 1;
+        if (r >= rlo && r < rhi) {  // uniform over the warp
+            const T wa = shfl_w(xcb), eb = shfl_e(xca);
+            const T va = fx_fma(pc, xca, fx_fma(pn, xna, fx_fma(ps, xsa, fx_fma(pw, wa, pe * xcb))));
+            const T vb = fx_fma(pc, xcb, fx_fma(pn, xnb, fx_fma(ps, xsb, fx_fma(pw, xca, pe * eb))));
+            if (sta && FX_IN(o, n)) out[o] = AXPY ? fx_fma(alpha, va, yca) : va;
+            if (stb && FX_IN(o + 1, n)) out[o + 1] = AXPY ? fx_fma(alpha, vb, ycb) : vb;
+        }
+        xna = xca;
+        xnb = xcb;
+        xca = xsa;
+        xcb = xsb;
+        yca = ysa;
+        ycb = ysb;
+        o += cols;
+    }
+    cp_async_wait<0>();  // no copy outlives the warp
+}
+
+template <typename T, bool AXPY>
+int launch_sstrip(fx_ctx *ctx, size_t rows, size_t cols, const T *x, T *out, const StencilP &P, T alpha,
+                  const char *what) {
+    static std::atomic<int> occ{0};
+    constexpr size_t smem = sstrip_smem<T, AXPY>();
+    if (smem > 48 * 1024) FX_TRY(strip_smem_optin(k_sstrip<T, AXPY>, smem));
+    const long cap = (long)band_capacity(ctx, k_sstrip<T, AXPY>, occ, kSWarps * 32, smem) * kSWarps;
+    const StripGeom G = strip_geom(rows, cols, kSOwn, cap);
+    const int blocks = (G.nitems + kSWarps - 1) / kSWarps;
+    timing_pre(ctx, what);
+    launch_pdl(ctx, k_sstrip<T, AXPY>, blocks, kSWarps * 32, smem, G, x, out, P, alpha);
+    timing_post(ctx, (double)rows * (double)cols);
+    return check_launch(ctx, what);
+}
 
 // Boundary ring of apply_stencil / apply_stencil_var (ops.rs:796-843): top and bottom rows
 // (corners included) first, then the left and right columns of rows 1..rows-2; each value
@@ -127,11 +235,16 @@ int fx_apply_stencil(fx_ctx *ctx, const fx_buf *in, fx_buf *out, const fx_grid *
     FX_TRY(make_stencil(s, &P));
     FX_DISPATCH(in->dtype, {
         const size_t RR = g->rows, CC = g->cols;
-        FX_MODE_DISPATCH(P.mode, {
-            PtApply<T, MODE, false> pt{(T *)out->ptr, nullptr, P, B, (int)RR, (int)CC};
-            FX_TRY(launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)in->ptr}, pt, NoFin{}, nullptr,
-                                      "apply_stencil"));
-        });
+        if (P.mode == 5) {
+            FX_TRY((launch_sstrip<T, false>(ctx, RR, CC, (const T *)in->ptr, (T *)out->ptr, P, (T)0,
+                                            "apply_stencil")));
+        } else {
+            FX_MODE_DISPATCH(P.mode, {
+                PtApply<T, MODE, false> pt{(T *)out->ptr, nullptr, P, B, (int)RR, (int)CC};
+                FX_TRY(launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)in->ptr}, pt, NoFin{}, nullptr,
+                                          "apply_stencil"));
+            });
+        }
         return ring_values<T, false>(ctx, (const T *)in->ptr, (T *)out->ptr, nullptr, (int)RR, (int)CC, B);
     });
 }
@@ -165,6 +278,8 @@ int fx_stencil_axpy(fx_ctx *ctx, double alpha, const fx_buf *x, fx_buf *y, const
     FX_TRY(make_stencil(s, &P));
     FX_DISPATCH(x->dtype, {
         const size_t RR = g->rows, CC = g->cols;
+        if (P.mode == 5)
+            return launch_sstrip<T, true>(ctx, RR, CC, (const T *)x->ptr, (T *)y->ptr, P, (T)alpha, "stencil_axpy");
         FX_MODE_DISPATCH(P.mode, {
             PtAxpy<T, MODE> pt{(T *)y->ptr, P, (T)alpha, (int)RR, (int)CC};
             return launch_march<T, 0>(ctx, RR, CC, LoadArr<T>{(const T *)x->ptr}, pt, NoFin{}, nullptr,

@@ -80,24 +80,25 @@ static_assert(kStripUnroll % FX_STRIP_F64_UP_FIFO == 0 && kStripUnroll % FX_STRI
 
 // Row FIFOs in shared memory (FX_STRIP_ASYNC, the default): the raw loads of the rows ahead go to
 // shared memory by cp.async instead of to registers, so a deep prefetch costs no registers.  PF
-// rows are in flight per strip.  On the 4095^2 FP64 MG-PCG solve (one box, CUDA events): 4.91 ms
-// with the register FIFOs, 4.81 ms with PF = 6, 4.86 ms with PF = 8, 5.46 ms with PF = 12; the
-// level-0 down pass went from 87.5 to 69.1 us (PF = 8), and the FP64 up pass, out of its
-// register FIFO, fits 128 registers (16 warps per SM instead of 12).
+// rows are in flight per strip.  On the 4095^2 FP64 MG-PCG solve (CUDA events): 4.91 ms with the
+// register FIFOs, 4.81 ms with PF = 6, 4.86 ms with PF = 8, 5.46 ms with PF = 12 (one box); 4.64
+// against 4.82 ms for PF = 4 against 6 (another box, two alternating runs each).  The level-0 down
+// pass went from 87.5 to 69.1 us (PF = 8), and the FP64 up pass, out of its register FIFO, fits
+// 128 registers (16 warps per SM instead of 12).
 #ifndef FX_STRIP_ASYNC
 #define FX_STRIP_ASYNC 1
 #endif
 #ifndef FX_STRIP_F64_DOWN_PF
-#define FX_STRIP_F64_DOWN_PF 6
+#define FX_STRIP_F64_DOWN_PF 4
 #endif
 #ifndef FX_STRIP_F64_UP_PF
-#define FX_STRIP_F64_UP_PF 6
+#define FX_STRIP_F64_UP_PF 4
 #endif
 #ifndef FX_STRIP_F32_DOWN_PF
-#define FX_STRIP_F32_DOWN_PF 6
+#define FX_STRIP_F32_DOWN_PF 4
 #endif
 #ifndef FX_STRIP_F32_UP_PF
-#define FX_STRIP_F32_UP_PF 6
+#define FX_STRIP_F32_UP_PF 4
 #endif
 template <typename T>
 __host__ __device__ constexpr int down_pf() { return sizeof(T) == 8 ? FX_STRIP_F64_DOWN_PF : FX_STRIP_F32_DOWN_PF; }
