@@ -264,9 +264,15 @@ void check_register_file(unsigned hash, const char *name) {
     r.files.emplace_back(hash, base ? base + 1 : name);
 }
 
+// standalone reductions' results to mapped page-locked memory, written by the device (no copy
+// engine: a small cudaMemcpyAsync would queue behind any large transfer on the same engine)
+__global__ void k_results_out(const double *d, double *h, int k) {
+    if ((int)threadIdx.x < k) h[threadIdx.x] = d[threadIdx.x];
+}
+
 int read_results(fx_ctx *ctx, int k, double *out) {
-    FX_CUDA(cudaMemcpyAsync(ctx->h_result, ctx->d_result, k * sizeof(double), cudaMemcpyDeviceToHost,
-                            ctx->stream));
+    k_results_out<<<1, 32, 0, ctx->stream>>>(ctx->d_result, ctx->h_result_dev, k);
+    FX_TRY(check_launch(ctx, "results_out"));
     FX_CUDA(cudaStreamSynchronize(ctx->stream));
     for (int i = 0; i < k; i++) out[i] = ctx->h_result[i];
     return FX_OK;
@@ -316,7 +322,8 @@ int fx_ctx_create(int device, fx_ctx **out) {
         cudaMalloc(&c->d_partials, sizeof(double) * 2 * kMaxSums * (size_t)kMaxRedBlocks) != cudaSuccess ||
         cudaMalloc(&c->d_counter, sizeof(unsigned) * 4) != cudaSuccess ||
         cudaMalloc(&c->d_result, sizeof(double) * 8) != cudaSuccess ||
-        cudaMallocHost(&c->h_result, sizeof(double) * 8) != cudaSuccess ||
+        cudaHostAlloc(&c->h_result, sizeof(double) * 8, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&c->h_result_dev, c->h_result, 0) != cudaSuccess ||
         cudaMemset(c->d_counter, 0, sizeof(unsigned) * 4) != cudaSuccess) {
         std::string m = cudaGetErrorString(cudaGetLastError());
         fx_ctx_destroy(c);

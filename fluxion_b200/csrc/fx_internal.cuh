@@ -127,7 +127,8 @@ struct fx_ctx {
     double *d_partials = nullptr;  // [kMaxRedBlocks][2*kMaxSums]
     unsigned *d_counter = nullptr; // last-block ticket
     double *d_result = nullptr;    // results of standalone reductions [kMaxSums]
-    double *h_result = nullptr;    // pinned mirror
+    double *h_result = nullptr;    // mapped page-locked mirror
+    double *h_result_dev = nullptr; // its device address
     unsigned long long launches = 0;
     // per-kernel timing (fx_ctx_timing_begin / _end)
     bool timing = false;

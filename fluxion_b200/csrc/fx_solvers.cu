@@ -297,13 +297,6 @@ struct PtApplyOp {
     }
 };
 
-// Finalisers -------------------------------------------------------------------------
-
-struct FinStore1 {
-    double *dst;
-    __device__ void operator()(const double *v) const { *dst = v[0]; }
-};
-
 }  // namespace
 
 // ================================================================ multigrid
@@ -644,10 +637,16 @@ int reference_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b, bool x_zero) {
 
 namespace {
 
+// chunk percentage of the levels below the finest (0: the hierarchy's chunk_pct for every level)
+#ifndef FX_MID_CHUNK_PCT
+#define FX_MID_CHUNK_PCT 0
+#endif
+
 // Fused V(2,2)-cycle from a zero initial guess: per level one down and one up kernel, the
 // coarsest level solved in one block.  b0 / z0 are the finest-level rhs and result (TB / TZ
 // may be double while the cycle runs in T = float); with RZ the finest up kernel also
 // reduces r.z into `fin`.
+
 template <typename T, typename TB, typename TZ, bool RZ, typename Fin>
 int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
     fx_ctx *ctx = mg->ctx;
@@ -680,10 +679,11 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
         (top == nl - 1 ? mg->lv[top].rows * mg->lv[top].cols > 4096
                        : mg->lv[top].rows * mg->lv[top].cols > top_cap))
         return fail(FX_ERR_UNSUPPORTED, "coarsest level too large for the one-block solve");
+    const int mid_pct = FX_MID_CHUNK_PCT ? FX_MID_CHUNK_PCT : mg->chunk_pct;
     for (int l = 1; l < top; l++) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
         FX_TRY((launch_wdown<T, T>(ctx, L.rows, L.cols, (const T *)L.rhs->ptr, (T *)L.tmp->ptr, (T *)C.rhs->ptr,
-                                   C.cols, vop(l), skip, mg->chunk_pct)));
+                                   C.cols, vop(l), skip, mid_pct)));
     }
     {
         TailArgs<T> A{};
@@ -703,7 +703,7 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
         FX_TRY((launch_wup<T, T, T, false>(ctx, L.rows, L.cols, (const T *)L.tmp->ptr, (const T *)C.u->ptr, C.cols,
                                            (const T *)L.rhs->ptr, (T *)L.u->ptr, vop(l), NoFin{}, skip,
-                                           mg->chunk_pct)));
+                                           mid_pct)));
     }
     const MgLevel &L = mg->lv[0], &C = mg->lv[1];
     return launch_wup<T, TB, TZ, RZ>(ctx, L.rows, L.cols, (const T *)mg->tmp0->ptr, (const T *)C.u->ptr, C.cols, b0,
@@ -780,13 +780,28 @@ int fx_mg::View::apply(fx_buf *z, const fx_buf *r, const int *skip, bool z_zero)
 
 namespace {
 
+// The solver state moves between host and device without the copy engines: the device writes
+// it into mapped page-locked memory (k_state_out) and takes its initial value as a kernel
+// parameter (k_state_in).  A cudaMemcpyAsync of a few bytes queues on a copy engine behind
+// whatever large transfer that engine is doing: in a stream of solves whose 134 MB right-hand
+// sides and solutions are copied on other streams while the previous solve runs, every read-back
+// of the drive loop waited for a whole solution transfer.
+__global__ void k_state_in(DevState *d, DevState v) { *d = v; }
+__global__ void k_state_out(const DevState *d, DevState *h) { *h = *d; }
+__global__ void k_state_stop(DevState *d, int reason) {
+    d->done = 1;
+    d->halt = 1;
+    d->reason = reason;
+}
+
 struct SolverBase {
     fx_ctx *ctx = nullptr;
     fx_grid g{};
     double tol = 0;
     size_t max_iter = 0;
     DevState *d_st = nullptr;
-    DevState *h_st = nullptr;
+    DevState *h_st = nullptr;     // mapped page-locked memory
+    DevState *h_st_dev = nullptr; // its device address
     std::vector<fx_buf *> bufs;
     int dtype = FX_F64;  // of the solver's vectors (x, b and the work vectors)
     const fx_op *op = nullptr;  // set for the duration of a *_solve_op call
@@ -798,7 +813,8 @@ struct SolverBase {
         max_iter = mi;
         dtype = dt;
         FX_CUDA(cudaMalloc(&d_st, sizeof(DevState)));
-        FX_CUDA(cudaMallocHost(&h_st, sizeof(DevState)));
+        FX_CUDA(cudaHostAlloc(&h_st, sizeof(DevState), cudaHostAllocMapped));
+        FX_CUDA(cudaHostGetDevicePointer((void **)&h_st_dev, h_st, 0));
         for (int i = 0; i < nvec; i++) {
             fx_buf *b = nullptr;
             FX_TRY(fx_alloc(ctx, g.rows * g.cols, dt, &b));
@@ -818,11 +834,12 @@ struct SolverBase {
         s.tol = tol;
         s.max_iter = (long long)max_iter;
         *h_st = s;
-        FX_CUDA(cudaMemcpyAsync(d_st, h_st, sizeof(DevState), cudaMemcpyHostToDevice, ctx->stream));
-        return FX_OK;
+        k_state_in<<<1, 1, 0, ctx->stream>>>(d_st, s);
+        return check_launch(ctx, "state_in");
     }
     int read_state() {
-        FX_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+        k_state_out<<<1, 1, 0, ctx->stream>>>(d_st, h_st_dev);
+        FX_TRY(check_launch(ctx, "state_out"));
         FX_CUDA(cudaStreamSynchronize(ctx->stream));
         return FX_OK;
     }
@@ -832,7 +849,8 @@ struct SolverBase {
         h_st->done = 1;
         h_st->halt = 1;
         h_st->reason = FX_BREAKDOWN;
-        FX_CUDA(cudaMemcpyAsync(&d_st->done, &h_st->done, 3 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        k_state_stop<<<1, 1, 0, ctx->stream>>>(d_st, FX_BREAKDOWN);
+        FX_TRY(check_launch(ctx, "state_stop"));
         FX_CUDA(cudaStreamSynchronize(ctx->stream));
         return FX_OK;
     }

@@ -17,25 +17,39 @@ namespace {
 // path than the band march: a warp owns a strip of 64 columns (two per lane: lanes 1..30 own
 // theirs, lanes 0 and 31 hold the halo columns) and marches it down a chunk of rows.  Each lane
 // keeps its columns' rows q-2, q-1, q in registers; west / east neighbours come by one shuffle
-// each; the rows ahead (of x, and of y for the axpy) are copied into shared memory by cp.async,
-// 6 rows in flight.  No block barrier and no shared-memory ring: about a third of the band
-// march's instructions per point, which is what bounds the FP32 stencil (the band march measured
-// 0.64 of HBM bandwidth there with 69 % issue activity).  Every value is stencil_eval's
-// expression (ops.rs:923-935 nesting), so the result equals the band march's bit for bit.
+// each; the rows ahead (of x, and of y for the axpy) are loaded sstrip_d rows early into a
+// register FIFO.  The march is unrolled by that many rows, so every FIFO slot is a compile-time register, and a
+// step whose rows all lie inside the grid and the chunk takes a path without row tests.  No block
+// barrier and no shared-memory ring.  Every value is stencil_eval's expression (ops.rs:923-935
+// nesting), so the result equals the band march's bit for bit.
 constexpr int kSOwn = 60;  // own columns per strip
 constexpr int kSWarps = 8;
-constexpr int kSPF = 6;    // rows in flight
+// rows in flight (= the unroll): 6 for FP32, 4 for FP64 (6 spills under the register caps)
+#ifndef FX_SSTRIP_F32_D
+#define FX_SSTRIP_F32_D 6
+#endif
+template <typename T>
+__host__ __device__ constexpr int sstrip_d() {
+    return sizeof(T) == 4 ? FX_SSTRIP_F32_D : 4;
+}
+// FP64 five-point ops keep the band march (FX_SSTRIP_F64 = 1 switches them to the strip march):
+// on a 16384^2 grid the strip march gave 0.80 / 0.95 of HBM bandwidth for the FP64 stencil /
+// stencil-AXPY against the band march's 0.88 / 1.00, and 0.81 / 0.85 for FP32 against 0.64 / 0.62.
+#ifndef FX_SSTRIP_F64
+#define FX_SSTRIP_F64 0
+#endif
 
+// resident blocks per SM the launch bound asks for (the register cap: 64 / 85 / 85 / 128)
 template <typename T, bool AXPY>
-constexpr size_t sstrip_smem() {
-    return (size_t)kSWarps * (AXPY ? 2 : 1) * (kSPF + 1) * 64 * sizeof(T);
+constexpr int sstrip_minb() {
+    return sizeof(T) == 4 ? (AXPY ? 3 : 4) : (AXPY ? 2 : 3);
 }
 
 template <typename T, bool AXPY>
-__global__ void __launch_bounds__(kSWarps * 32) k_sstrip(StripGeom G, const T *__restrict__ x, T *__restrict__ out,
+__global__ void __launch_bounds__(kSWarps * 32, sstrip_minb<T, AXPY>()) k_sstrip(StripGeom G, const T *__restrict__ x, T *__restrict__ out,
                                                          StencilP P, T alpha) {
     grid_dep_enter();
-    extern __shared__ __align__(16) unsigned char ss_smem[];
+    constexpr int kSD = sstrip_d<T>();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int item = blockIdx.x * kSWarps + w;
     if (item >= G.nitems) return;  // whole warps
@@ -50,70 +64,80 @@ __global__ void __launch_bounds__(kSWarps * 32) k_sstrip(StripGeom G, const T *_
     const long long n = (long long)rows * cols;
     (void)n;
     const T pc = (T)P.c, pn = (T)P.n, ps = (T)P.s, pw = (T)P.w, pe = (T)P.e;
-    SmemFifo<T, kSPF> fx;
-    SmemFifo<T, kSPF> fy;
-    fx.init(reinterpret_cast<T *>(ss_smem) + w * ((kSPF + 1) * 64), lane);
-    if (AXPY) fy.init(reinterpret_cast<T *>(ss_smem) + (kSWarps + w) * ((kSPF + 1) * 64), lane);
-    // step q: row q of x (and y) arrives, row q - 1 is computed; rows r0 - 1 .. r1 are read
+    // step q: row q + kSD is fetched, row q leaves the FIFO, row q - 1 is computed; rows r0 - 1 .. r1
+    // are read
     const int qa = r0 - 1, qb = r1;
-    auto put = [&](int slot, int q) {
-        const bool rv = q >= 0 && q < rows && q <= qb;
-        const long long o = (long long)q * cols + ca;
-        const bool va = rv && lda && FX_IN(o, n), vb = rv && ldb && FX_IN(o + 1, n);
-        if (slot < 0) {
-            fx.put(x + o, va, vb, x);
-            if (AXPY) fy.put(out + o, va, vb, out);
-        } else {
-            fx.put_at(slot, x + o, va, vb, x);
-            if (AXPY) fy.put_at(slot, out + o, va, vb, out);
+    // steps with every row test true: q - 1 in [rlo, rhi) and q + kSD <= min(qb, rows - 1)
+    const int q_lo = rlo + 1, q_hi = min(rhi, min(qb, rows - 1) - kSD);
+    T fa[kSD], fb[kSD], ga[kSD], gb[kSD];  // FIFO rows of x (f) and y (g)
+    auto fetch = [&](int k, int q, long long o, bool fast) {
+        const bool rv = fast || (q >= 0 && q < rows && q <= qb);
+        if (!fast) {
+            fa[k] = fb[k] = (T)0;
+            if (AXPY) ga[k] = gb[k] = (T)0;
         }
-        cp_async_commit();
+        if (rv && lda && FX_IN(o, n)) {
+            fa[k] = x[o];
+            if (AXPY) ga[k] = out[o];
+        }
+        if (rv && ldb && FX_IN(o + 1, n)) {
+            fb[k] = x[o + 1];
+            if (AXPY) gb[k] = out[o + 1];
+        }
     };
 #pragma unroll
-    for (int k = 0; k < kSPF; k++) put(k, qa + k);
+    for (int k = 0; k < kSD; k++) fetch(k, qa + k, (long long)(qa + k) * cols + ca, false);
+    long long of = (long long)(qa + kSD) * cols + ca;  // element offset of (q + kSD, ca)
+    long long oo = (long long)(qa - 1) * cols + ca;    // element offset of (q - 1, ca)
     T xna = (T)0, xnb = (T)0, xca = (T)0, xcb = (T)0, yca = (T)0, ycb = (T)0;
-    long long o = (long long)(qa - 1) * cols + ca;  // element offset of (q - 1, ca)
-    for (int q = qa; q <= qb; q++) {
-        cp_async_wait<kSPF - 1>();  // row q's group is complete
-        const T xsa = fx.a(), xsb = fx.b();
+    auto step = [&](int k, int q, auto fast) {
+        constexpr bool F = decltype(fast)::value;
+        const T xsa = fa[k], xsb = fb[k];
         T ysa = (T)0, ysb = (T)0;
         if (AXPY) {
-            ysa = fy.a();
-            ysb = fy.b();
+            ysa = ga[k];
+            ysb = gb[k];
         }
-        put(-1, q + kSPF);
-        fx.advance();
-        if (AXPY) fy.advance();
-        const int r = q - 1;
-        if (r >= rlo && r < rhi) {  // uniform over the warp
+        fetch(k, q + kSD, of, F);
+        of += cols;
+        if (F || (q - 1 >= rlo && q - 1 < rhi)) {  // uniform over the warp
             const T wa = shfl_w(xcb), eb = shfl_e(xca);
             const T va = fx_fma(pc, xca, fx_fma(pn, xna, fx_fma(ps, xsa, fx_fma(pw, wa, pe * xcb))));
             const T vb = fx_fma(pc, xcb, fx_fma(pn, xnb, fx_fma(ps, xsb, fx_fma(pw, xca, pe * eb))));
-            if (sta && FX_IN(o, n)) out[o] = AXPY ? fx_fma(alpha, va, yca) : va;
-            if (stb && FX_IN(o + 1, n)) out[o + 1] = AXPY ? fx_fma(alpha, vb, ycb) : vb;
+            if (sta && FX_IN(oo, n)) out[oo] = AXPY ? fx_fma(alpha, va, yca) : va;
+            if (stb && FX_IN(oo + 1, n)) out[oo + 1] = AXPY ? fx_fma(alpha, vb, ycb) : vb;
         }
+        oo += cols;
         xna = xca;
         xnb = xcb;
         xca = xsa;
         xcb = xsb;
         yca = ysa;
         ycb = ysb;
-        o += cols;
+    };
+    for (int q0 = qa; q0 <= qb; q0 += kSD) {
+        if (q0 >= q_lo && q0 + kSD - 1 <= q_hi) {
+#pragma unroll
+            for (int k = 0; k < kSD; k++) step(k, q0 + k, fast_t<true>{});
+        } else {
+#pragma unroll
+            for (int k = 0; k < kSD; k++) {
+                if (q0 + k > qb) break;  // uniform over the warp
+                step(k, q0 + k, fast_t<false>{});
+            }
+        }
     }
-    cp_async_wait<0>();  // no copy outlives the warp
 }
 
 template <typename T, bool AXPY>
 int launch_sstrip(fx_ctx *ctx, size_t rows, size_t cols, const T *x, T *out, const StencilP &P, T alpha,
                   const char *what) {
     static std::atomic<int> occ{0};
-    constexpr size_t smem = sstrip_smem<T, AXPY>();
-    if (smem > 48 * 1024) FX_TRY(strip_smem_optin(k_sstrip<T, AXPY>, smem));
-    const long cap = (long)band_capacity(ctx, k_sstrip<T, AXPY>, occ, kSWarps * 32, smem) * kSWarps;
+    const long cap = (long)band_capacity(ctx, k_sstrip<T, AXPY>, occ, kSWarps * 32) * kSWarps;
     const StripGeom G = strip_geom(rows, cols, kSOwn, cap);
     const int blocks = (G.nitems + kSWarps - 1) / kSWarps;
     timing_pre(ctx, what);
-    launch_pdl(ctx, k_sstrip<T, AXPY>, blocks, kSWarps * 32, smem, G, x, out, P, alpha);
+    launch_pdl(ctx, k_sstrip<T, AXPY>, blocks, kSWarps * 32, 0, G, x, out, P, alpha);
     timing_post(ctx, (double)rows * (double)cols);
     return check_launch(ctx, what);
 }
@@ -235,7 +259,7 @@ int fx_apply_stencil(fx_ctx *ctx, const fx_buf *in, fx_buf *out, const fx_grid *
     FX_TRY(make_stencil(s, &P));
     FX_DISPATCH(in->dtype, {
         const size_t RR = g->rows, CC = g->cols;
-        if (P.mode == 5) {
+        if (P.mode == 5 && (sizeof(T) == 4 || FX_SSTRIP_F64)) {
             FX_TRY((launch_sstrip<T, false>(ctx, RR, CC, (const T *)in->ptr, (T *)out->ptr, P, (T)0,
                                             "apply_stencil")));
         } else {
@@ -278,7 +302,7 @@ int fx_stencil_axpy(fx_ctx *ctx, double alpha, const fx_buf *x, fx_buf *y, const
     FX_TRY(make_stencil(s, &P));
     FX_DISPATCH(x->dtype, {
         const size_t RR = g->rows, CC = g->cols;
-        if (P.mode == 5)
+        if (P.mode == 5 && (sizeof(T) == 4 || FX_SSTRIP_F64))
             return launch_sstrip<T, true>(ctx, RR, CC, (const T *)x->ptr, (T *)y->ptr, P, (T)alpha, "stencil_axpy");
         FX_MODE_DISPATCH(P.mode, {
             PtAxpy<T, MODE> pt{(T *)y->ptr, P, (T)alpha, (int)RR, (int)CC};
