@@ -84,12 +84,18 @@ def parse():
                    help="--mode batch: interior sizes 2^k - 1 for k uniform in this inclusive range")
     p.add_argument("--replay", type=int, default=0, choices=[0, 1],
                    help="--mode batch: record each hierarchy's cycle into a CUDA graph and replay it")
+    p.add_argument("--pipeline", type=int, default=4,
+                   help="--mode batch --batched 1: sub-batches (balanced by points) whose uploads, solves and "
+                        "read-backs overlap (1: upload all, solve all, read back all)")
     p.add_argument("--batched", type=int, default=1, choices=[0, 1],
                    help="--mode batch: 1 = the batched solver (every phase one launch over all problems, "
                         "graph-replayed iterations); 0 = independent solves on --lanes host threads")
     p.add_argument("--mg-dtype", default="f64", choices=["f64", "f32"],
                    help="--mode batch / vcycle: arithmetic of the V-cycle (the Krylov solver stays FP64)")
     return p.parse_args()
+
+
+NOMINAL_HBM_GBS = 7700.0  # B200 HBM3e, the nominal (HGX) figure, reported beside the measured one
 
 
 def measured_peaks():
@@ -351,14 +357,17 @@ def run_lsm_step(args):
 
 
 def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
-    """The batch through the batched solver: upload every problem's f, vx and vy from page-locked
-    host memory, build the batch (hierarchies and work tables), solve all problems by BiCGSTAB
-    with the conv-diff V-cycle (every phase one launch over the batch, each iteration replayed from
-    a CUDA graph), recompute every true residual on the device (the batch's operator) and read
-    the solutions back.  All of it is timed; the host data generation is not."""
+    """The batch through the batched solver, as a pipeline of --pipeline sub-batches (balanced by
+    points): every sub-batch's f, vx and vy are uploaded from page-locked host memory on a copy
+    stream at the start; sub-batch k is built (hierarchies and work tables) and solved by
+    BiCGSTAB with the conv-diff V-cycle (every phase one launch over the sub-batch, each
+    iteration replayed from a CUDA graph) once its upload has landed, while the later uploads
+    continue; its true residuals are computed on the device and its solutions read back on a
+    second copy stream while sub-batch k + 1 solves.  All of it is timed; the host data
+    generation is not."""
     import torch
     from fluxion_b200 import DType, Device
-    from fluxion_b200.batch import BatchSolver
+    from fluxion_b200.batch import BatchSolver, partition_by_points
 
     dev = Device.Cuda(local_rank)
     be = dev.backend()
@@ -366,15 +375,20 @@ def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
     be.set_stream(stream.cuda_stream)
     nu = 1e-2
     sides = [int(2 ** ks[i] + 1) for i in mine]
-    tot = sum(s * s for s in sides)
-    pin = torch.empty(3 * tot, dtype=torch.float64, pin_memory=True).numpy()
-    fv, xv, yv = pin[:tot], pin[tot:2 * tot], pin[2 * tot:]
-    o = 0
-    for i, s in zip(mine, sides):
-        n, vx, vy, f, _ = host[i]
-        fv[o:o + s * s], xv[o:o + s * s], yv[o:o + s * s] = f, vx, vy
-        o += s * s
-    out = torch.empty(tot, dtype=torch.float64, pin_memory=True).numpy()
+    nsub = max(1, min(int(args.pipeline), len(sides)))
+    parts = [p_ for p_ in partition_by_points([s_ * s_ for s_ in sides], nsub) if p_]
+    subs = []  # (local indices, sides, f, vx, vy, out) per sub-batch, host arrays page-locked
+    for part in parts:
+        sd = [sides[j] for j in part]
+        tot = sum(s_ * s_ for s_ in sd)
+        pin = torch.empty(4 * tot, dtype=torch.float64, pin_memory=True).numpy()
+        fv, xv, yv, out = pin[:tot], pin[tot:2 * tot], pin[2 * tot:3 * tot], pin[3 * tot:]
+        o = 0
+        for j, s_ in zip(part, sd):
+            _, vx, vy, f, _ = host[mine[j]]
+            fv[o:o + s_ * s_], xv[o:o + s_ * s_], yv[o:o + s_ * s_] = f, vx, vy
+            o += s_ * s_
+        subs.append((part, sd, fv, xv, yv, out))
     mg_dtype = DType.F32 if args.mg_dtype == "f32" else DType.F64
     chunk, sweeps, tuned = 2048, 2, None
     if args.autotune:  # before the timed region: work-item size, sweep counts and cycle precision
@@ -386,39 +400,60 @@ def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
         tuned["tuning_s"] = time.perf_counter() - t_tune
         chunk, sweeps = tuned["chunk"], tuned["sweeps"]
         mg_dtype = DType.F32 if tuned["cycle_dtype"] == "f32" else DType.F64
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
 
     def once():
-        VX, VY, F = be.allocate(tot, DType.F64), be.allocate(tot, DType.F64), be.allocate(tot, DType.F64)
-        VX.write(xv)
-        VY.write(yv)
-        F.write(fv)
-        B = BatchSolver(dev, sides, nu, VX, VY, cycle_dtype=mg_dtype, n_pre=sweeps, n_post=sweeps, omega=OMEGA,
-                        coarse_max=COARSE_MAX, coarse_sweeps=COARSE_SWEEPS)
-        if chunk != 2048:
-            B.set_chunk(chunk)
-        X = be.allocate(tot, DType.F64)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        stats, run = B.bicgstab(X, F, 1e-10, 200)
-        e1.record(stream)
-        rn = B.residual_norms(X, F)  # every true residual, on the device
-        X.copy_to_host_f64(out)
-        stream.synchronize()
-        return B, stats, run, e0.elapsed_time(e1), rn
+        bufs = []
+        for (_, sd, _, _, _, _) in subs:
+            tot = sum(s_ * s_ for s_ in sd)
+            bufs.append(tuple(be.allocate(tot, DType.F64) for _ in range(4)))  # VX, VY, F, X
+        up.wait_stream(stream)  # the buffers' allocation and zero fill come first
+        landed = []
+        for (_, _, fv, xv, yv, _), (VX, VY, F, _) in zip(subs, bufs):
+            VX.write_async(xv, up.cuda_stream)
+            VY.write_async(yv, up.cuda_stream)
+            F.write_async(fv, up.cuda_stream)
+            e_ = torch.cuda.Event()
+            e_.record(up)
+            landed.append(e_)
+        solve_ms, run_tot, per = 0.0, 0, []
+        keep = []
+        for (part, sd, _, _, _, out), (VX, VY, F, X), e_ in zip(subs, bufs, landed):
+            stream.wait_event(e_)
+            B = BatchSolver(dev, sd, nu, VX, VY, cycle_dtype=mg_dtype, n_pre=sweeps, n_post=sweeps, omega=OMEGA,
+                            coarse_max=COARSE_MAX, coarse_sweeps=COARSE_SWEEPS)
+            if chunk != 2048:
+                B.set_chunk(chunk)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            stats, run = B.bicgstab(X, F, 1e-10, 200)
+            e1.record(stream)
+            rn = B.residual_norms(X, F)  # every true residual, on the device (synchronises)
+            solve_ms += e0.elapsed_time(e1)
+            run_tot += run
+            down.wait_stream(stream)
+            X.copy_to_host_async(out, down.cuda_stream)
+            per.append((part, stats, rn))
+            keep.append(B)
+        down.synchronize()
+        return per, run_tot, solve_ms
 
-    once()  # warm-up (first-use costs of the library and the pool)
+    once()  # warm-up (first-use costs of the library, the pool and the copy streams)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    B, stats, run, solve_ms, rn = once()
+    per, run, solve_ms = once()
     wall = time.perf_counter() - t0
     res = {}
-    for j, i in enumerate(mine):
-        rel = float(rn[j] / max(host[i][4], 1e-300))
-        res[i] = (sides[j] - 2, int(stats[j].iterations), bool(stats[j].converged()), solve_ms, rel, wall)
+    for part, stats, rn in per:
+        for q, j in enumerate(part):
+            i = mine[j]
+            rel = float(rn[q] / max(host[i][4], 1e-300))
+            res[i] = (sides[j] - 2, int(stats[q].iterations), bool(stats[q].converged()), solve_ms, rel, wall)
     return res, wall, {"batch_iterations_launched": run, "device_solve_ms": solve_ms,
-                       "points": tot, "launch_per_iteration": "one CUDA graph",
+                       "points": sum(s_ * s_ for s_ in sides), "launch_per_iteration": "one CUDA graph",
+                       "pipeline_sub_batches": len(subs),
                        "tuning": {"chunk": chunk, "sweeps": sweeps, "cycle_dtype": "f32" if mg_dtype == DType.F32 else
                                   "f64", "autotuned": tuned}}
 
@@ -438,8 +473,8 @@ def run_batch(args):
     its norm read back, and the solution read back into the lane's page-locked host array.  Each
     lane keeps one BiCGSTAB object per grid size, created while warming up on one problem of
     every size.  Reports solves/s = problems / wall time of the whole batch, p50 / p99 of the
-    per-problem time and of the device solve time.  The persistent one-launch batched solver is
-    not built."""
+    per-problem time and of the device solve time.  `--batched 1` (the default) runs the batched
+    solver instead (run_batch_batched)."""
     import threading
 
     import torch
@@ -627,6 +662,7 @@ def _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist
         ach = byts / (extra["device_solve_ms"] * 1e-3) / 1e9
         roof = {"kernel": "whole batched solve (all phases)", "bound": "hbm", "achieved": ach, "peak": peak,
                 "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind, "traffic": None,
+                "nominal_peak": NOMINAL_HBM_GBS, "frac_of_nominal": ach / NOMINAL_HBM_GBS,
                 "bytes_per_point_iteration": BATCH_BYTES_PER_POINT_ITER}
     cpu = None
     if not args.no_cpu and host is not None:
@@ -650,8 +686,8 @@ def _batch_report(args, ks, k_lo, k_hi, res, wall, world, rank, local_rank, dist
         "dtype": "f64" if extra.get("tuning", {}).get("cycle_dtype", args.mg_dtype) == "f64"
         else "f64 (Krylov) / f32 (V-cycle)",
         "data": "synthetic (seeded per problem), page-locked host arrays",
-        "note": ("batched: per-problem times are the whole batch's (every problem finishes in the batch's "
-                 "last launch)" if args.batched else
+        "note": ("batched, in sub-batches whose uploads and read-backs overlap the other sub-batches' solves: "
+                 "per-problem times are the whole job's" if args.batched else
                  f"{lanes} host thread(s), one context and stream each, through the public API")}),
         flush=True)
     return 0 if ok else 1
@@ -876,7 +912,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from fluxion_b200 import CgSolver, DType, Device, Field, MixedPrecisionRefinement, Multigrid, PipelinedCgSolver
+    from fluxion_b200 import (CgSolver, DType, Device, FcgSolver, Field, InnerPcgF32, MixedPrecisionRefinement,
+                              Multigrid, PipelinedCgSolver)
     from fluxion_b200 import _lib as L
     from fluxion_b200.workloads import dst_poisson_solve, neg_laplacian_residual, poisson_modes_rhs, \
         poisson_problem
@@ -970,6 +1007,13 @@ def main():
     up = x.to_vec_f64()
     ir_ms, sti, _, _ = timed(mg32, args.steps, args.warmup, solver=ir)
     ui = x.to_vec_f64()
+    # FP64 flexible CG around inner FP32 V-cycle PCG solves (inner tol 1e-4): the outer Krylov
+    # space is kept where the refinement loop restarts
+    fcg = FcgSolver(P.grid, dev, tol, 50)
+    ipc = InnerPcgF32(P.grid, P.coeff, P.stencil, None, mg32, 1e-4, 100, dev)
+    fcg_ms, stf, _, _ = timed(ipc, args.steps, args.warmup, solver=fcg)
+    apps_f, inner_f = ipc.stats()
+    uf = x.to_vec_f64()
 
     # verification in FP64 (plain operator) and against the exact DST-I solve
     u_ref = dst_poisson_solve(f, n)
@@ -980,6 +1024,8 @@ def main():
     errp = float(np.linalg.norm(up - u_ref) / np.linalg.norm(u_ref))
     erri = float(np.linalg.norm(ui - u_ref) / np.linalg.norm(u_ref))
     rri = neg_laplacian_residual(ui, f, n) / fnorm
+    errf = float(np.linalg.norm(uf - u_ref) / np.linalg.norm(u_ref))
+    rrf = neg_laplacian_residual(uf, f, n) / fnorm
     rrp = neg_laplacian_residual(up, f, n) / fnorm
 
     # e2e: host f (pinned) -> solve -> host u (pinned), through the public API
@@ -1087,6 +1133,7 @@ def main():
                     traffic = float(ln.split(":")[1]) * top
         roof = {"kernel": dom + " (F64 cycle)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                "nominal_peak": NOMINAL_HBM_GBS, "frac_of_nominal": achieved / NOMINAL_HBM_GBS,
                 "algorithmic_bytes_per_launch": f_bytes, "bytes_per_point": f_bytes / top,
                 "grid_points_per_launch": top, "launches": len(fine), "avg_launch_ms": f_ms,
                 "all_levels": {"launches": len(ktime), "ms": all_ms,
@@ -1128,6 +1175,11 @@ def main():
                                          "inner_iterations": ir.last_inner_iterations, "rel_residual_fp64": rri,
                                          "err_vs_fp64_direct": erri,
                                          "solver": f"FP64 refinement, FP32 CG + F32 {SOLVER} inner to 1e-4"},
+            "fcg_fp64_outer_fp32_pcg_inner": {
+                "value": fcg_ms / 1e3, "unit": "s", "outer_iterations": int(stf.iterations),
+                "inner_iterations_per_solve": inner_f / max(1, args.steps + args.warmup),
+                "rel_residual_fp64": rrf, "err_vs_fp64_direct": errf,
+                "solver": f"FP64 flexible CG, inner FP32 CG + F32 {SOLVER} to 1e-4 per application"},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
             "gpu_launches": int(launches), "kernel_time_shares_ms": shares, "microbench": micro,
         }

@@ -14,7 +14,7 @@ __all__ = [
     "CudaBackend", "CudaBuffer", "BackendUnavailable", "InvalidArgument", "Device", "Field", "DeviceMismatch",
     "CgSolver", "CgStats", "PipelinedCgSolver", "BiCgStabSolver", "GmresSolver", "Multigrid", "SmootherKind",
     "Identity", "Preconditioner", "LinearSolver", "SolveStats", "ConvergenceReason",
-    "MixedPrecisionRefinement", "CudaGraph", "FcgSolver", "FgmresSolver", "InnerCg",
+    "MixedPrecisionRefinement", "CudaGraph", "FcgSolver", "FgmresSolver", "InnerCg", "InnerPcgF32",
     "ConvDiffOperator", "OperatorJacobi", "ConvDiffMultigrid",
     "CrankNicolsonSolver", "BdfSolver", "ImexSolver", "DiffusionSolver", "TimeScheme",
 ]
@@ -30,7 +30,7 @@ def __getattr__(name):
         from . import field
         return getattr(field, name)
     if name in ("CgSolver", "CgStats", "PipelinedCgSolver", "BiCgStabSolver", "GmresSolver", "Multigrid",
-                "MixedPrecisionRefinement", "FcgSolver", "FgmresSolver", "InnerCg",
+                "MixedPrecisionRefinement", "FcgSolver", "FgmresSolver", "InnerCg", "InnerPcgF32",
                 "ConvDiffOperator", "OperatorJacobi", "ConvDiffMultigrid", "SmootherKind", "Identity", "Preconditioner", "LinearSolver", "SolveStats",
                 "ConvergenceReason"):
         from . import solvers

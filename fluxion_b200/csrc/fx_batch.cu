@@ -743,8 +743,10 @@ struct fx_batch {
     double *d_partials = nullptr;
     unsigned *d_tickets = nullptr;
     BState *d_state = nullptr;
-    BState *h_state = nullptr;
-    int *d_count = nullptr, *h_count = nullptr;
+    // per-problem states and the active count reach mapped page-locked memory written by the
+    // device: no copy engine, so no wait behind a large transfer another stream has queued on it
+    BState *h_state = nullptr, *h_state_dev = nullptr;
+    int *h_count = nullptr, *h_count_dev = nullptr;
     // Krylov vectors (level-0 layout, F64): r, r_hat, p, v, s, t, p_hat, s_hat, tmp0 (the F64 cycle's partner)
     double *kv[9] = {};
     // graph of one iteration
@@ -1024,12 +1026,24 @@ int bicg_step(fx_batch *B, double *x) {
                     "batch_bicg_finish");
 }
 
-int read_active(fx_batch *B, int *active) {
-    k_bcount<<<1, 256, 0, B->ctx->stream>>>(B->d_state, (int)B->np, B->d_count);
-    FX_TRY(check_launch(B->ctx, "batch_count"));
-    FX_CUDA(cudaMemcpyAsync(B->h_count, B->d_count, sizeof(int), cudaMemcpyDeviceToHost, B->ctx->stream));
+__global__ void k_bstates_out(const BState *__restrict__ d, BState *h, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) h[i] = d[i];
+}
+
+// every problem's state into the mapped host array (synchronises)
+int states_out(fx_batch *B) {
+    const int n = (int)B->np;
+    k_bstates_out<<<(n + 255) / 256, 256, 0, B->ctx->stream>>>(B->d_state, B->h_state_dev, n);
+    FX_TRY(check_launch(B->ctx, "batch_states_out"));
     FX_CUDA(cudaStreamSynchronize(B->ctx->stream));
-    *active = *B->h_count;
+    return FX_OK;
+}
+
+int read_active(fx_batch *B, int *active) {
+    k_bcount<<<1, 256, 0, B->ctx->stream>>>(B->d_state, (int)B->np, B->h_count_dev);
+    FX_TRY(check_launch(B->ctx, "batch_count"));
+    FX_CUDA(cudaStreamSynchronize(B->ctx->stream));
+    *active = *(volatile int *)B->h_count;
     return FX_OK;
 }
 
@@ -1111,10 +1125,11 @@ int fx_batch_create(fx_ctx *ctx, size_t count, const size_t *grid_side, double n
     if (st == FX_OK) st = B->dalloc(&B->d_partials, maxchunks * 4 * sizeof(double));
     if (st == FX_OK) st = B->dalloc(&B->d_tickets, count * sizeof(unsigned));
     if (st == FX_OK) st = B->dalloc(&B->d_state, count * sizeof(BState));
-    if (st == FX_OK) st = B->dalloc(&B->d_count, sizeof(int));
     for (int k = 0; k < 9 && st == FX_OK; k++) st = B->dalloc(&B->kv[k], (size_t)tot * sizeof(double));
-    if (st == FX_OK && (cudaMallocHost(&B->h_state, count * sizeof(BState)) != cudaSuccess ||
-                        cudaMallocHost(&B->h_count, sizeof(int)) != cudaSuccess))
+    if (st == FX_OK && (cudaHostAlloc(&B->h_state, count * sizeof(BState), cudaHostAllocMapped) != cudaSuccess ||
+                        cudaHostGetDevicePointer((void **)&B->h_state_dev, B->h_state, 0) != cudaSuccess ||
+                        cudaHostAlloc(&B->h_count, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+                        cudaHostGetDevicePointer((void **)&B->h_count_dev, B->h_count, 0) != cudaSuccess))
         st = fail(FX_ERR_BACKEND, "batch: host allocation failed");
     if (st == FX_OK) st = B->dtype == FX_F64 ? build_levels<double>(B) : build_levels<float>(B);
     if (st != FX_OK) {
@@ -1175,8 +1190,7 @@ int fx_batch_residual_norms(fx_batch *B, const fx_buf *x, const fx_buf *b, doubl
     FX_TRY((bflat<2>(B, B->d_chunk0, B->nchunk0,
                      BfInit{B->k0(), (const double *)x->ptr, (const double *)b->ptr, B->kv[0], B->kv[1]},
                      FinNorm2{B->d_state}, "batch_residual_norm")));
-    FX_CUDA(cudaMemcpyAsync(B->h_state, B->d_state, B->np * sizeof(BState), cudaMemcpyDeviceToHost, ctx->stream));
-    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    FX_TRY(states_out(B));
     for (size_t p = 0; p < B->np; p++) norms[p] = B->h_state[p].resid;
     return FX_OK;
 }
@@ -1249,8 +1263,7 @@ int fx_batch_bicgstab(fx_batch *B, fx_buf *x, const fx_buf *b, double rel_tol, s
         FX_TRY(read_active(B, &active));
     }
     if (iterations_run) *iterations_run = run;
-    FX_CUDA(cudaMemcpyAsync(B->h_state, B->d_state, B->np * sizeof(BState), cudaMemcpyDeviceToHost, ctx->stream));
-    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    FX_TRY(states_out(B));
     for (size_t p = 0; p < B->np; p++) {
         const BState &S = B->h_state[p];
         stats[p].iterations = (size_t)S.iter;

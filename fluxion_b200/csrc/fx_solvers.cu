@@ -637,11 +637,6 @@ int reference_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b, bool x_zero) {
 
 namespace {
 
-// chunk percentage of the levels below the finest (0: the hierarchy's chunk_pct for every level)
-#ifndef FX_MID_CHUNK_PCT
-#define FX_MID_CHUNK_PCT 0
-#endif
-
 // Fused V(2,2)-cycle from a zero initial guess: per level one down and one up kernel, the
 // coarsest level solved in one block.  b0 / z0 are the finest-level rhs and result (TB / TZ
 // may be double while the cycle runs in T = float); with RZ the finest up kernel also
@@ -679,7 +674,7 @@ int fused_cycle(fx_mg *mg, const TB *b0, TZ *z0, Fin fin, const int *skip) {
         (top == nl - 1 ? mg->lv[top].rows * mg->lv[top].cols > 4096
                        : mg->lv[top].rows * mg->lv[top].cols > top_cap))
         return fail(FX_ERR_UNSUPPORTED, "coarsest level too large for the one-block solve");
-    const int mid_pct = FX_MID_CHUNK_PCT ? FX_MID_CHUNK_PCT : mg->chunk_pct;
+    const int mid_pct = mg->chunk_pct;
     for (int l = 1; l < top; l++) {
         const MgLevel &L = mg->lv[l], &C = mg->lv[l + 1];
         FX_TRY((launch_wdown<T, T>(ctx, L.rows, L.cols, (const T *)L.rhs->ptr, (T *)L.tmp->ptr, (T *)C.rhs->ptr,
@@ -3233,6 +3228,67 @@ namespace {
 // application is steps[k mod nsteps], so a schedule of different counts gives a
 // preconditioner that changes from one application to the next -- the case the flexible
 // solvers exist for; PCG and left-preconditioned GMRES lose their guarantees with it.
+// ------------------------------------------------ inner FP32 PCG preconditioner (new)
+//
+// z = the FP32 solution d of A d = r, by FP32 CG preconditioned by an FP32 V-cycle from d = 0 to
+// ||r - A d|| < rel_tol ||r|| (or max_iter): one pass casts r to FP32 and reduces ||r||^2, the
+// inner solve runs on FP32 vectors, one pass widens d into z.  It varies from one application
+// to the next (the inner stop depends on r), so it is for the flexible solvers (FCG, FGMRES),
+// which keep the outer Krylov information in FP64.
+
+struct FlatCastNorm {  // r32 = (float) r; ||r||^2
+    const double *r;
+    float *r32;
+    __device__ __forceinline__ void operator()(size_t i, CSum *acc) const {
+        const double v = r[i];
+        r32[i] = (float)v;
+        csum_fma(acc[0], v, v);
+    }
+};
+
+struct FlatWiden {  // z = (double) d
+    const float *d;
+    double *z;
+    __device__ __forceinline__ void operator()(size_t i, CSum *) const { z[i] = (double)d[i]; }
+};
+
+struct InnerPcgF32Pc : fx_precond {
+    fx_cg *cg = nullptr;  // FP32 CG: its vectors and state
+    fx_buf *r32 = nullptr, *d32 = nullptr;
+    fx_precond *inner = nullptr;  // FP32 V-cycle, borrowed
+    fx_grid g{};
+    double coeff = 0.0;
+    StencilP P{};
+    double rel_tol = 1e-4;
+    size_t max_iter = 100;
+    size_t total = 0, calls = 0;
+    ~InnerPcgF32Pc() override {
+        if (cg) fx_cg_destroy(cg);
+        if (r32) fx_free(r32);
+        if (d32) fx_free(d32);
+    }
+    int apply(fx_buf *z, const fx_buf *r, const int *, bool) override {
+        FX_TRY(check_same(z, r));
+        if (z->dtype != FX_F64 || z->len != g.rows * g.cols)
+            return fail(FX_ERR_INVALID_ARGUMENT, "inner FP32 PCG: vectors must be F64 fields of its grid");
+        const size_t n = z->len;
+        FX_TRY(launch_flat<1>(ctx, n, FlatCastNorm{(const double *)r->ptr, (float *)r32->ptr},
+                              StoreFin<1>{ctx->d_result}, nullptr, "inner_pcg_cast"));
+        double rr = 0.0;
+        FX_TRY(read_results(ctx, 1, &rr));
+        FX_TRY(zero_fill<float>(ctx, (float *)d32->ptr, n, nullptr));
+        calls++;
+        if (rr > 0.0 && std::isfinite(rr)) {
+            cg->tol = rel_tol * std::sqrt(rr);
+            cg->max_iter = max_iter;
+            SOLVER_MODE_DISPATCH(P, FX_TRY((cg_solve_impl<float, MODE>(cg, d32, r32, coeff, P, inner))));
+            total += (size_t)cg->h_st->iter;
+        }
+        return launch_flat<0>(ctx, n, FlatWiden{(const float *)d32->ptr, (double *)z->ptr}, NoFin{}, nullptr,
+                              "inner_pcg_widen");
+    }
+};
+
 struct InnerCgPc : fx_precond {
     fx_cg *cg = nullptr;
     fx_precond *inner = nullptr;
@@ -4204,6 +4260,41 @@ int fx_lsm_data_add_problem(fx_lsm_data *d, const fx_op *op, const fx_buf *b, si
     if (solver) fx_fgmres_destroy(solver);
     fx_cdmg_destroy(mg);
     return st;
+}
+
+int fx_precond_inner_pcg_f32(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st,
+                             const fx_boundaries *bc, fx_precond *inner_f32, double rel_tol, size_t max_iter,
+                             fx_precond **out) {
+    if (!ctx || !g || !st || !bc || !inner_f32 || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
+    if (!(rel_tol > 0.0 && rel_tol < 1.0)) return fail(FX_ERR_INVALID_ARGUMENT, "rel_tol must lie in (0, 1)");
+    if (max_iter < 1) return fail(FX_ERR_INVALID_ARGUMENT, "max_iter must be at least 1");
+    *out = nullptr;
+    InnerPcgF32Pc *p = new InnerPcgF32Pc();
+    p->ctx = ctx;
+    p->g = *g;
+    p->coeff = coeff;
+    p->inner = inner_f32;
+    p->rel_tol = rel_tol;
+    p->max_iter = max_iter;
+    int rc = prep_op(*g, st, bc, &p->P);
+    if (rc == FX_OK) rc = create_solver(ctx, g, 0.0, max_iter, 4, &p->cg, FX_F32);
+    if (rc == FX_OK) rc = fx_alloc(ctx, g->rows * g->cols, FX_F32, &p->r32);
+    if (rc == FX_OK) rc = fx_alloc(ctx, g->rows * g->cols, FX_F32, &p->d32);
+    if (rc != FX_OK) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return FX_OK;
+}
+
+int fx_precond_inner_pcg_f32_stats(const fx_precond *pc, size_t *applications, size_t *inner_iterations) {
+    const InnerPcgF32Pc *p = dynamic_cast<const InnerPcgF32Pc *>(pc);
+    if (!p || !applications || !inner_iterations)
+        return fail(FX_ERR_INVALID_ARGUMENT, "not an inner FP32 PCG preconditioner");
+    *applications = p->calls;
+    *inner_iterations = p->total;
+    return FX_OK;
 }
 
 int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st, const fx_boundaries *bc,

@@ -512,6 +512,43 @@ class InnerCg(Preconditioner):
             pass
 
 
+class InnerPcgF32(Preconditioner):
+    """Inner FP32 PCG preconditioner (new): z = the FP32 solution of (I + coeff S) d = r by CG
+    preconditioned by ``inner_f32`` (an FP32 `Multigrid.vertex`), from d = 0 to
+    ||r - A d|| < rel_tol ||r|| or max_iter iterations (fx_precond_inner_pcg_f32).  For
+    `FcgSolver` / `FgmresSolver`: FP64 outer Krylov, FP32 inner solves."""
+
+    def __init__(self, grid: Grid, coeff: float, stencil: Stencil, boundaries: Optional[Boundaries],
+                 inner_f32: Preconditioner, rel_tol: float = 1e-4, max_iter: int = 100,
+                 device: Optional[Device] = None):
+        self.device = device or Device.best()
+        self._inner = inner_f32  # kept alive: the native object borrows its handle
+        sc = StencilC(stencil)
+        g, bc = grid_c(grid), bcs_c(boundaries if boundaries is not None else Boundaries.zero_dirichlet())
+        out = C.c_void_p()
+        check(L.lib().fx_precond_inner_pcg_f32(self.device.backend().ctx, C.byref(g), float(coeff), sc.ptr,
+                                               C.byref(bc), inner_f32._handle(self.device), float(rel_tol),
+                                               int(max_iter), C.byref(out)))
+        self.h = out.value
+
+    def stats(self):
+        """(applications, inner FP32 CG iterations) so far."""
+        a, i = C.c_size_t(), C.c_size_t()
+        check(L.lib().fx_precond_inner_pcg_f32_stats(self.h, C.byref(a), C.byref(i)))
+        return a.value, i.value
+
+    def _handle(self, device: Device) -> int:
+        return self.h
+
+    def __del__(self):
+        try:
+            if self.h:
+                L.lib().fx_precond_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
 class FcgSolver(_Native):
     """Flexible CG (new; the reference has none): PCG with the Polak-Ribiere beta
     z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k) (Golub & Ye 1999; Notay 2000), safe with a

@@ -292,6 +292,15 @@ int fx_precond_apply(fx_precond *pc, fx_buf *z, const fx_buf *r);
 int fx_precond_inner_cg(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st,
                         const fx_boundaries *bc, const size_t *steps, size_t nsteps, fx_precond *inner,
                         fx_precond **out);
+/* Inner FP32 PCG preconditioner (new): z = (double) d, d the FP32 CG solution of (I + coeff S) d =
+ * (float) r from d = 0, preconditioned by inner_f32 (an FP32 vertex multigrid, borrowed; it must
+ * outlive this), stopped at ||r - A d|| < rel_tol ||r|| or max_iter iterations.  It varies between
+ * applications: a preconditioner for fx_fcg_* and fx_fgmres_* (FP64 outer Krylov, FP32 inner
+ * solves).  F64 vectors of grid g.  stats: applications and inner iterations so far. */
+int fx_precond_inner_pcg_f32(fx_ctx *ctx, const fx_grid *g, double coeff, const fx_stencil *st,
+                             const fx_boundaries *bc, fx_precond *inner_f32, double rel_tol, size_t max_iter,
+                             fx_precond **out);
+int fx_precond_inner_pcg_f32_stats(const fx_precond *pc, size_t *applications, size_t *inner_iterations);
 
 /* Multigrid::new / ::build (multigrid.rs:61-146): reference hierarchy (rows/2 per level,
  * Laplacian on each level, clamped 2x2 restriction, piecewise-constant prolongation,

@@ -442,3 +442,30 @@ def test_iterative_refinement_needs_a_single_precision_preconditioner(dev):
     ir = MixedPrecisionRefinement(P.grid, dev, 1e-8)
     with pytest.raises(Exception):
         ir.solve_preconditioned(x, b, P.coeff, P.stencil, None, Multigrid.vertex(P.grid, None, dev))
+
+
+@pytest.mark.parametrize("n", [511, 1023])
+def test_fcg_outer_fp32_pcg_inner_reaches_fp64_accuracy(dev, n):
+    """FP64 flexible CG around inner FP32 V-cycle PCG solves (inner tol 1e-4): rel. residual 1e-10
+    recomputed in FP64 with the plain operator, the FP64 direct solution to 1e-8, and fewer
+    outer steps than the refinement loop needs (the outer Krylov space is kept)."""
+    from fluxion_b200 import DType, FcgSolver, Field, InnerPcgF32, MixedPrecisionRefinement, Multigrid
+    from fluxion_b200.workloads import dst_poisson_solve, neg_laplacian_residual, poisson_problem, \
+        poisson_modes_rhs
+    P = poisson_problem(n)
+    f = poisson_modes_rhs(n, seed=31)
+    fn = float(np.linalg.norm(f))
+    b = Field.from_f64(P.grid, f, dev)
+    mg = Multigrid.vertex(P.grid, None, dev, dtype=DType.F32)
+    pc = InnerPcgF32(P.grid, P.coeff, P.stencil, None, mg, 1e-4, 100, dev)
+    x = Field.zeros(P.grid, DType.F64, dev)
+    s = FcgSolver(P.grid, dev, 1e-10 * fn, 50).solve_preconditioned(x, b, P.coeff, P.stencil, None, pc)
+    apps, inner = pc.stats()
+    assert s.converged() and 1 <= s.iterations <= 6 and apps >= s.iterations and inner >= apps
+    u = x.to_vec_f64()
+    assert neg_laplacian_residual(u, f, n) < 1.01e-10 * fn
+    assert rel_err(u, dst_poisson_solve(f, n)) < 1e-8
+    xi = Field.zeros(P.grid, DType.F64, dev)
+    si = MixedPrecisionRefinement(P.grid, dev, 1e-10 * fn, 20, 1e-4, 100).solve_preconditioned(
+        xi, b, P.coeff, P.stencil, None, mg)
+    assert si.converged() and s.iterations <= si.iterations
