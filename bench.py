@@ -358,8 +358,9 @@ def run_lsm_step(args):
 
 def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
     """The batch through the batched solver, as a pipeline of --pipeline sub-batches (balanced by
-    points): every sub-batch's f, vx and vy are uploaded from page-locked host memory on a copy
-    stream at the start; sub-batch k is built (hierarchies and work tables) and solved by
+    points): the first sub-batch's f, vx and vy are uploaded from page-locked host memory on a
+    copy stream, the others' once the first is built (its small table copies would otherwise
+    queue behind them on the copy engine); sub-batch k is built (hierarchies and work tables) and solved by
     BiCGSTAB with the conv-diff V-cycle (every phase one launch over the sub-batch, each
     iteration replayed from a CUDA graph) once its upload has landed, while the later uploads
     continue; its true residuals are computed on the device and its solutions read back on a
@@ -409,21 +410,28 @@ def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
             bufs.append(tuple(be.allocate(tot, DType.F64) for _ in range(4)))  # VX, VY, F, X
         up.wait_stream(stream)  # the buffers' allocation and zero fill come first
         landed = []
-        for (_, _, fv, xv, yv, _), (VX, VY, F, _) in zip(subs, bufs):
+
+        def upload(k):
+            (_, _, fv, xv, yv, _), (VX, VY, F, _) = subs[k], bufs[k]
             VX.write_async(xv, up.cuda_stream)
             VY.write_async(yv, up.cuda_stream)
             F.write_async(fv, up.cuda_stream)
             e_ = torch.cuda.Event()
             e_.record(up)
             landed.append(e_)
+
         solve_ms, run_tot, per = 0.0, 0, []
         keep = []
-        for (part, sd, _, _, _, out), (VX, VY, F, X), e_ in zip(subs, bufs, landed):
-            stream.wait_event(e_)
+        upload(0)
+        for k, ((part, sd, _, _, _, out), (VX, VY, F, X)) in enumerate(zip(subs, bufs)):
+            stream.wait_event(landed[k])
             B = BatchSolver(dev, sd, nu, VX, VY, cycle_dtype=mg_dtype, n_pre=sweeps, n_post=sweeps, omega=OMEGA,
                             coarse_max=COARSE_MAX, coarse_sweeps=COARSE_SWEEPS)
             if chunk != 2048:
                 B.set_chunk(chunk)
+            if k == 0:  # the other uploads go after the first build, whose small table copies would
+                for j in range(1, len(subs)):  # otherwise queue behind them on the copy engine
+                    upload(j)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             stats, run = B.bicgstab(X, F, 1e-10, 200)
