@@ -84,7 +84,7 @@ def parse():
                    help="--mode batch: interior sizes 2^k - 1 for k uniform in this inclusive range")
     p.add_argument("--replay", type=int, default=0, choices=[0, 1],
                    help="--mode batch: record each hierarchy's cycle into a CUDA graph and replay it")
-    p.add_argument("--pipeline", type=int, default=4,
+    p.add_argument("--pipeline", type=int, default=2,
                    help="--mode batch --batched 1: sub-batches (balanced by points) whose uploads, solves and "
                         "read-backs overlap (1: upload all, solve all, read back all)")
     p.add_argument("--batched", type=int, default=1, choices=[0, 1],

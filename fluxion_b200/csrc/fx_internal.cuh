@@ -490,8 +490,25 @@ constexpr int band_depth() {
     return S == 0 ? 8 : (S == 1 ? 6 : (S == 2 ? 4 : 2));
 }
 
+// Resident blocks per SM the band march's launch bound asks for (its register cap): 2, or the
+// point functor's MINB for FP64.  The CG direction and update passes ask for 4 (56 registers):
+// on the 4095^2 FP64 PCG solve pcg_dir went from 0.77 to 0.71 ms and the solve from 4.64 to 4.56
+// ms, while the plain stencil ops lose at 4 (0.89 -> 0.85 of HBM bandwidth), so they keep 2.
+template <typename P>
+__host__ __device__ constexpr auto point_minb(int) -> decltype(P::MINB, int()) {
+    return P::MINB;
+}
+template <typename P>
+__host__ __device__ constexpr int point_minb(long) {
+    return 2;
+}
+template <typename T, typename P>
+__host__ __device__ constexpr int march_minb() {
+    return sizeof(T) == 8 ? point_minb<P>(0) : 2;
+}
+
 template <typename T, int CPT, int D, int K, typename Loader, typename Point, typename Fin>
-__global__ void __launch_bounds__(kBandThreads, 2) k_march(MarchGeom G, Loader ld_in, Point pt_in, Fin fin,
+__global__ void __launch_bounds__(kBandThreads, march_minb<T, Point>()) k_march(MarchGeom G, Loader ld_in, Point pt_in, Fin fin,
                                                            RedArgs<K> ra, const int *skip) {
     grid_dep_enter();
     if (skip && *(volatile const int *)skip) return;

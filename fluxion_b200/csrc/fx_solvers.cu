@@ -954,6 +954,7 @@ struct FinCgInit {  // unpreconditioned: rs_old = r.r; loop-top test of iteratio
 template <typename T, int MODE>
 struct PtCgDir {
     static constexpr int NA = 0;
+    static constexpr int MINB = 4;  // FP64: 4 band blocks per SM (56 registers, no spill)
     OpA<T, MODE> A;
     T *p_new;
     __device__ __forceinline__ const T *aux(int) const { return nullptr; }
@@ -980,6 +981,7 @@ struct FinCgDir {  // alpha = rs_old / p.ap, breakdown test (cg.rs:133-142)
 template <typename T, int MODE>
 struct PtCgUpd {
     static constexpr int NA = 2;
+    static constexpr int MINB = 4;  // FP64: 4 band blocks per SM (56 registers, no spill)
     OpA<T, MODE> A;
     T *x, *r;
     const DevState *S;
