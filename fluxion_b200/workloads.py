@@ -1,5 +1,5 @@
 """Seeded synthetic workloads of the solve configurations, and the FP64 direct solve that
-judges their solutions.
+checks their solutions.
 
 Every generator returns row-major arrays with the boundary ring included.  The reference
 publishes no datasets for this path; these are the configurations' stated distributions:
@@ -94,7 +94,7 @@ def dst_poisson_solve(f_full: np.ndarray, n: int) -> np.ndarray:
 
 
 def neg_laplacian_residual(u_full: np.ndarray, f_full: np.ndarray, n: int) -> float:
-    """||f + Lap_h u||_2 over the interior, in FP64 with numpy (the plain-operator judge)."""
+    """||f + Lap_h u||_2 over the interior, in FP64 with numpy (the plain-operator check)."""
     h = 1.0 / (n + 1)
     u = u_full.reshape(n + 2, n + 2)
     f = f_full.reshape(n + 2, n + 2)
