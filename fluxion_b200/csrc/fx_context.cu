@@ -270,6 +270,18 @@ __global__ void k_results_out(const double *d, double *h, int k) {
     if ((int)threadIdx.x < k) h[threadIdx.x] = d[threadIdx.x];
 }
 
+__global__ void k_copy_out_f64(const double *d, double *h, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) h[i] = d[i];
+}
+
+int read_mapped(fx_ctx *ctx, const double *d, double *h_dev, size_t n) {
+    if (n > (1u << 20)) return fail(FX_ERR_INVALID_ARGUMENT, "read_mapped: at most 2^20 values");
+    k_copy_out_f64<<<1, 256, 0, ctx->stream>>>(d, h_dev, (int)n);
+    FX_TRY(check_launch(ctx, "copy_out"));
+    FX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return FX_OK;
+}
+
 int read_results(fx_ctx *ctx, int k, double *out) {
     k_results_out<<<1, 32, 0, ctx->stream>>>(ctx->d_result, ctx->h_result_dev, k);
     FX_TRY(check_launch(ctx, "results_out"));
@@ -732,6 +744,12 @@ int fx_checked_status(fx_ctx *ctx, size_t *count, char *file, size_t file_cap, i
     *index = 0;
     *extent = 0;
     if (file && file_cap) file[0] = '\0';
+    int prev = 0;
+    FX_CUDA(cudaGetDevice(&prev));
+    struct Restore {  // the caller's current device is left as it was
+        int d;
+        ~Restore() { cudaSetDevice(d); }
+    } restore{prev};
     FX_CUDA(cudaSetDevice(ctx->device));
     FX_CUDA(cudaDeviceSynchronize());
     CheckRegistry &r = check_registry();

@@ -786,6 +786,9 @@ struct StoreFin {
 };
 
 // Read K doubles of ctx->d_result back to the host (synchronising).
+// n device values into mapped page-locked memory (h_dev: its device address), written by a kernel
+// (no copy engine), then wait for them
+int read_mapped(fx_ctx *ctx, const double *d, double *h_dev, size_t n);
 int read_results(fx_ctx *ctx, int k, double *out);
 
 // ------------------------------------------------------------------ misc helpers

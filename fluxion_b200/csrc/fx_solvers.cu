@@ -1749,7 +1749,8 @@ int bicg_solve_impl(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, co
 struct fx_gmres : SolverBase {
     size_t restart = 30;
     double *d_h = nullptr;  // device column of dots
-    double *h_h = nullptr;
+    double *h_h = nullptr;      // mapped page-locked, 2 (restart + 2) values (CGS2 reads two columns)
+    double *h_h_dev = nullptr;  // its device address
     std::vector<double> hh, cc, ss, grs;
     std::vector<fx_buf *> vv;  // m+1 basis vectors (bufs[0..m]); w = bufs[m+1]
     ~fx_gmres() {
@@ -1851,9 +1852,7 @@ int gmres_solve_impl(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, cons
     fx_stats st{0, 0.0, FX_CONVERGED};
 
     auto read_h = [&](size_t k) -> int {
-        FX_CUDA(cudaMemcpyAsync(s->h_h, dh, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        FX_CUDA(cudaStreamSynchronize(ctx->stream));
-        return FX_OK;
+        return read_mapped(ctx, dh, s->h_h_dev, k + 2);
     };
     auto scale_into = [&](T *dst, const T *src, double f) -> int {  // copy_from + scale(f)
         return launch_flat<0>(ctx, n, FlatScaleInto<T>{dst, src, (T)f}, NoFin{}, nullptr, "gmres_scale");
@@ -2325,9 +2324,7 @@ int fgmres_solve_impl(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, co
     size_t total_its = 0;
     fx_stats st{0, 0.0, FX_CONVERGED};
     auto read_h = [&](size_t k) -> int {
-        FX_CUDA(cudaMemcpyAsync(s->h_h, dh, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        FX_CUDA(cudaStreamSynchronize(ctx->stream));
-        return FX_OK;
+        return read_mapped(ctx, dh, s->h_h_dev, k + 2);
     };
     auto scale_into = [&](T *dst, const T *src, double f) -> int {
         return launch_flat<0>(ctx, n, FlatScaleInto<T>{dst, src, (T)f}, NoFin{}, nullptr, "fgmres_scale");
@@ -2406,10 +2403,8 @@ int fgmres_solve_impl(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, co
                 ca.coef = h2;
                 ca.out = h2 + k + 1;
                 FX_TRY(launch_cgs<2>(ctx, n, ca));
-                std::vector<double> hv(2 * (m + 2));
-                FX_CUDA(cudaMemcpyAsync(hv.data(), s->d_cgs, 2 * (m + 2) * sizeof(double), cudaMemcpyDeviceToHost,
-                                        ctx->stream));
-                FX_CUDA(cudaStreamSynchronize(ctx->stream));
+                FX_TRY(read_mapped(ctx, s->d_cgs, s->h_h_dev, 2 * (m + 2)));
+                const double *hv = s->h_h;
                 for (size_t j = 0; j <= k; j++) H(j, k) = hv[j] + hv[m + 2 + j];
                 h_kp1_k = std::sqrt(hv[m + 2 + k + 1]);
             } else {
@@ -3728,7 +3723,8 @@ int fx_gmres_create(fx_ctx *ctx, const fx_grid *g, size_t restart, double tol, s
     s->ss.assign(restart, 0.0);
     s->grs.assign(restart + 1, 0.0);
     if (cudaMalloc(&s->d_h, (restart + 2) * sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&s->h_h, (restart + 2) * sizeof(double)) != cudaSuccess) {
+        cudaHostAlloc(&s->h_h, 2 * (restart + 2) * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&s->h_h_dev, s->h_h, 0) != cudaSuccess) {
         delete s;
         *out = nullptr;
         return fail(FX_ERR_BACKEND, "gmres scratch allocation failed");
@@ -3812,7 +3808,8 @@ int fx_fgmres_create(fx_ctx *ctx, const fx_grid *g, size_t restart, double tol, 
     s->ss.assign(restart, 0.0);
     s->grs.assign(restart + 1, 0.0);
     if (cudaMalloc(&s->d_h, (restart + 2) * sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&s->h_h, (restart + 2) * sizeof(double)) != cudaSuccess) {
+        cudaHostAlloc(&s->h_h, 2 * (restart + 2) * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&s->h_h_dev, s->h_h, 0) != cudaSuccess) {
         delete s;
         *out = nullptr;
         return fail(FX_ERR_BACKEND, "fgmres scratch allocation failed");
