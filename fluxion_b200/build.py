@@ -80,7 +80,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
             list(ex.map(run, jobs))
     if force or jobs or not os.path.exists(lib):
-        link = [NVCC, *_arch_flags(), "-shared", "-o", lib + ".tmp", *objs, "-lcudart"]
+        link = [NVCC, *_arch_flags(), "-shared", "-o", lib + ".tmp", *objs, "-lcudart", "-ldl"]
         if verbose:
             print(" ".join(link), flush=True)
         subprocess.run(link, check=True)

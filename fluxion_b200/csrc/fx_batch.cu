@@ -1208,6 +1208,7 @@ int fx_batch_precondition(fx_batch *B, fx_buf *z, const fx_buf *r) {
 
 int fx_batch_bicgstab(fx_batch *B, fx_buf *x, const fx_buf *b, double rel_tol, size_t max_iter, int use_graph,
                       fx_stats *stats, size_t *iterations_run) {
+    FX_RANGE("fx_batch_bicgstab");
     if (!B || !stats) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     FX_TRY(check_vec(B, x, "x"));
     FX_TRY(check_vec(B, b, "b"));

@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fluxion_cuda.h"
 
 // ------------------------------------------------------------------ errors
@@ -157,6 +159,16 @@ struct fx_buf {
 namespace fx {
 
 int check_launch(fx_ctx *ctx, const char *what);
+
+// NVTX range over a solve-level entry point: nsys / ncu timelines show each solve, cycle and
+// training run by name.  A no-op unless a tool attaches.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define FX_RANGE(name) ::fx::NvtxRange fx_nvtx_range_(name)
 bool capturing(cudaStream_t s);  // the stream is being captured into a graph
 
 // Programmatic dependent launch.  Kernels of the solve path are launched with programmatic

@@ -541,6 +541,7 @@ int fx_lsm_loss_grad(fx_lsm *m, const fx_lsm_data *d, const size_t *indices, siz
 
 int fx_lsm_train(fx_lsm *m, const fx_lsm_data *d, size_t epochs, size_t batch, double lr, double lambda,
                  unsigned long long seed, double *epoch_loss) {
+    FX_RANGE("fx_lsm_train");
     if (!m || !d) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     if (!(lambda >= 0.0)) return fail(FX_ERR_INVALID_ARGUMENT, "lambda must be non-negative");
     if (d->count == 0 || batch == 0) return fail(FX_ERR_INVALID_ARGUMENT, "no samples or zero batch");

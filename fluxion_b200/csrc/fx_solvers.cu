@@ -3332,6 +3332,7 @@ int fx_precond_destroy(fx_precond *pc) {
 }
 
 int fx_precond_apply(fx_precond *pc, fx_buf *z, const fx_buf *r) {
+    FX_RANGE("fx_precond_apply");
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     FX_TRY(check_buf(z, "z"));
     FX_TRY(check_buf(r, "r"));
@@ -3480,6 +3481,7 @@ int fx_mg_level_dims(const fx_mg *mg, size_t level, size_t *rows, size_t *cols) 
 }
 
 int fx_mg_v_cycle(fx_mg *mg, fx_buf *x, const fx_buf *b) {
+    FX_RANGE("fx_mg_v_cycle");
     if (!mg) return fail(FX_ERR_INVALID_ARGUMENT, "null multigrid");
     FX_TRY(check_buf(x, "x"));
     FX_TRY(check_buf(b, "b"));
@@ -3592,11 +3594,13 @@ static int cg_entry(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx
 
 int fx_cg_solve(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st, const fx_boundaries *bc,
                 fx_stats *out) {
+    FX_RANGE("fx_cg_solve");
     return cg_entry(s, x, b, coeff, st, bc, nullptr, out);
 }
 
 int fx_cg_solve_preconditioned(fx_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                                const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    FX_RANGE("fx_cg_solve_preconditioned");
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     return cg_entry(s, x, b, coeff, st, bc, pc, out);
 }
@@ -3618,6 +3622,7 @@ int fx_pipelined_cg_set_params(fx_pipelined_cg *s, double tol, size_t max_iter) 
 }
 int fx_pipelined_cg_solve(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                           const fx_boundaries *bc, fx_stats *out) {
+    FX_RANGE("fx_pipelined_cg_solve");
     if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     FX_TRY(s->check_io(x, b));
     StencilP P;
@@ -3630,6 +3635,7 @@ int fx_pipelined_cg_solve(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double
 int fx_pipelined_cg_solve_preconditioned(fx_pipelined_cg *s, fx_buf *x, const fx_buf *b, double coeff,
                                          const fx_stencil *st, const fx_boundaries *bc, fx_precond *pc,
                                          fx_stats *out) {
+    FX_RANGE("fx_pipelined_cg_solve_preconditioned");
     if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     FX_TRY(s->check_io(x, b));
@@ -3661,6 +3667,7 @@ int fx_ir_destroy(fx_ir *s) {
 }
 int fx_ir_solve_preconditioned(fx_ir *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                                const fx_boundaries *bc, fx_precond *pc, fx_stats *out, size_t *inner_iterations) {
+    FX_RANGE("fx_ir_solve_preconditioned");
     if (!s || !out) return fail(FX_ERR_INVALID_ARGUMENT, "null argument");
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     FX_TRY(check_buf(x, "x"));
@@ -3703,10 +3710,12 @@ static int bicg_entry(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, 
 }
 int fx_bicgstab_solve(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                       const fx_boundaries *bc, fx_stats *out) {
+    FX_RANGE("fx_bicgstab_solve");
     return bicg_entry(s, x, b, coeff, st, bc, nullptr, out);
 }
 int fx_bicgstab_solve_preconditioned(fx_bicgstab *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                                      const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    FX_RANGE("fx_bicgstab_solve_preconditioned");
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     return bicg_entry(s, x, b, coeff, st, bc, pc, out);
 }
@@ -3753,10 +3762,12 @@ static int gmres_entry(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, co
 }
 int fx_gmres_solve(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                    const fx_boundaries *bc, fx_stats *out) {
+    FX_RANGE("fx_gmres_solve");
     return gmres_entry(s, x, b, coeff, st, bc, nullptr, out);
 }
 int fx_gmres_solve_preconditioned(fx_gmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                                   const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    FX_RANGE("fx_gmres_solve_preconditioned");
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     return gmres_entry(s, x, b, coeff, st, bc, pc, out);
 }
@@ -3790,10 +3801,12 @@ static int fcg_entry(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const 
 }
 int fx_fcg_solve(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st, const fx_boundaries *bc,
                  fx_stats *out) {
+    FX_RANGE("fx_fcg_solve");
     return fcg_entry(s, x, b, coeff, st, bc, nullptr, out);
 }
 int fx_fcg_solve_preconditioned(fx_fcg *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                                 const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    FX_RANGE("fx_fcg_solve_preconditioned");
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     return fcg_entry(s, x, b, coeff, st, bc, pc, out);
 }
@@ -3856,10 +3869,12 @@ static int fgmres_entry(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, 
 }
 int fx_fgmres_solve(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                     const fx_boundaries *bc, fx_stats *out) {
+    FX_RANGE("fx_fgmres_solve");
     return fgmres_entry(s, x, b, coeff, st, bc, nullptr, out);
 }
 int fx_fgmres_solve_preconditioned(fx_fgmres *s, fx_buf *x, const fx_buf *b, double coeff, const fx_stencil *st,
                                    const fx_boundaries *bc, fx_precond *pc, fx_stats *out) {
+    FX_RANGE("fx_fgmres_solve_preconditioned");
     if (!pc) return fail(FX_ERR_INVALID_ARGUMENT, "null preconditioner");
     return fgmres_entry(s, x, b, coeff, st, bc, pc, out);
 }
@@ -3934,12 +3949,15 @@ static int op_entry(S *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_stats 
 }  // extern "C++"
 
 int fx_bicgstab_solve_op(fx_bicgstab *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc, fx_stats *out) {
+    FX_RANGE("fx_bicgstab_solve_op");
     return op_entry(s, x, b, op, out, [&] { return bicg_solve_impl<kModeCD>(s, x, b, op->coeff, StencilP{}, pc); });
 }
 int fx_gmres_solve_op(fx_gmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc, fx_stats *out) {
+    FX_RANGE("fx_gmres_solve_op");
     return op_entry(s, x, b, op, out, [&] { return gmres_solve_impl<kModeCD>(s, x, b, op->coeff, StencilP{}, pc); });
 }
 int fx_fgmres_solve_op(fx_fgmres *s, fx_buf *x, const fx_buf *b, const fx_op *op, fx_precond *pc, fx_stats *out) {
+    FX_RANGE("fx_fgmres_solve_op");
     return op_entry(s, x, b, op, out, [&] { return fgmres_solve_impl<kModeCD>(s, x, b, op->coeff, StencilP{}, pc); });
 }
 
