@@ -1156,9 +1156,10 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
-            t, iters, cores = oracle_solve(n, f)
+            runs = [oracle_solve(n, f) for _ in range(3)]  # best of 3
+            t, iters, cores = min(runs)
             cpu = {"value": t, "unit": "s", "cores": cores, "kind": "port",
-                   "sample": f"one full {n}^2 MG-PCG solve to 1e-10 ({iters} iterations), FP64"}
+                   "sample": f"best of 3 full {n}^2 MG-PCG solves to 1e-10 ({iters} iterations), FP64"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
 
