@@ -2153,13 +2153,14 @@ struct CgsArgs {
     unsigned *ticket;
 };
 
-// The grid walks tiles of kBlock elements.  In a tile, thread t first owns element t: in passes
-// 1 and 2 it reads w and the basis once and writes the updated w (loads in batches of 8, all
-// issued before the first use).  For the multi-dot (passes 0 and 1) warp q then owns the basis
-// vectors j = q, q + 8, q + 16, q + 24 and lane l the tile's elements l, l + 32, ..., with w from
-// shared memory: a thread keeps four partial sums, so the kernel needs few registers and many
-// resident warps keep the loads in flight.  (One element and 32 partial sums per thread measured
-// 0.42 of HBM bandwidth, latency-bound at 16 warps per SM.)  The sums of a basis vector are
+// The grid walks tiles of 2 kBlock elements.  In a tile, thread t first owns elements t and
+// t + kBlock: in passes 1 and 2 it reads w and the basis once and writes the updated w (loads in
+// batches of 8 per element, all issued before the first use).  For the multi-dot (passes 0 and 1)
+// warp q then owns the basis vectors j = q, q + 8, q + 16, q + 24 and lane l the tile's elements
+// l, l + 32, ..., two rows of 32 per step, with w from shared memory: a thread keeps four partial
+// sums, so the kernel needs few registers and many resident warps keep the loads in flight.  (One
+// element and 32 partial sums per thread measured 0.42 of HBM bandwidth, latency-bound at 16
+// warps per SM; one element per thread and tile, 0.63.)  The sums of a basis vector are
 // added in a fixed order: over a warp's tiles, the lanes' shuffle tree, then the blocks.
 template <int PASS>
 __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
@@ -2171,7 +2172,9 @@ __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     __shared__ double c[kCgsMax];
     __shared__ const double *vp[kCgsMax];
-    __shared__ double sw[kBlock];
+    constexpr int kU = 2;               // elements per thread in a tile (both phases keep 2x the loads in flight)
+    constexpr int kTile = kU * kBlock;
+    __shared__ double sw[kTile];
     __shared__ double red[kW];
     __shared__ bool is_last;
     if (threadIdx.x < kCgsMax) {
@@ -2182,48 +2185,65 @@ __global__ void __launch_bounds__(kBlock) k_cgs(size_t n, CgsArgs a) {
     double acc[kJ];
 #pragma unroll
     for (int q = 0; q < kJ; q++) acc[q] = 0.0;
-    const size_t ntiles = (n + kBlock - 1) / kBlock;
+    const size_t ntiles = (n + kTile - 1) / kTile;
     for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const size_t i0 = tile * kBlock, i = i0 + threadIdx.x;
-        double wv = 0.0;
-        if (i < n) {
-            wv = a.w[i];
-            if (PASS > 0) {
+        const size_t i0 = tile * kTile;
+        double wv[kU];
 #pragma unroll
-                for (int j0 = 0; j0 < kCgsMax; j0 += kB) {
-                    if (j0 < kb) {
-                        double vv[kB];
+        for (int u = 0; u < kU; u++) {
+            const size_t i = i0 + u * kBlock + threadIdx.x;
+            wv[u] = i < n ? a.w[i] : 0.0;
+        }
+        if (PASS > 0) {
 #pragma unroll
-                        for (int t = 0; t < kB; t++) vv[t] = j0 + t < kb ? vp[j0 + t][i] : 0.0;
+            for (int j0 = 0; j0 < kCgsMax; j0 += kB) {
+                if (j0 < kb) {
+                    double vv[kU][kB];
+#pragma unroll
+                    for (int u = 0; u < kU; u++) {
+                        const size_t i = i0 + u * kBlock + threadIdx.x;
+#pragma unroll
+                        for (int t = 0; t < kB; t++) vv[u][t] = (j0 + t < kb && i < n) ? vp[j0 + t][i] : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kU; u++)
 #pragma unroll
                         for (int t = 0; t < kB; t++)
-                            if (j0 + t < kb) wv = fma(-c[j0 + t], vv[t], wv);
-                    }
+                            if (j0 + t < kb) wv[u] = fma(-c[j0 + t], vv[u][t], wv[u]);
                 }
-                a.w[i] = wv;
+            }
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const size_t i = i0 + u * kBlock + threadIdx.x;
+                if (i < n) a.w[i] = wv[u];
             }
         }
         if (PASS == 2) {
-            acc[0] = fma(wv, wv, acc[0]);
+#pragma unroll
+            for (int u = 0; u < kU; u++) acc[0] = fma(wv[u], wv[u], acc[0]);
             continue;
         }
-        sw[threadIdx.x] = wv;
+#pragma unroll
+        for (int u = 0; u < kU; u++) sw[u * kBlock + threadIdx.x] = wv[u];
         __syncthreads();
 #pragma unroll
-        for (int e = 0; e < kBlock; e += 32) {
-            const size_t ie = i0 + e + lane;
-            if (ie < n) {
-                const double x = sw[e + lane];
-                double vv[kJ];
+        for (int e = 0; e < kTile; e += 64) {  // two 32-element rows of the tile per step
+            double vv[2][kJ], xs[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const size_t ie = i0 + e + 32 * h + lane;
+                xs[h] = sw[e + 32 * h + lane];
 #pragma unroll
                 for (int q = 0; q < kJ; q++) {
                     const int j = wid + kW * q;
-                    vv[q] = j < kb ? vp[j][ie] : 0.0;
+                    vv[h][q] = (j < kb && ie < n) ? vp[j][ie] : 0.0;
                 }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++)
 #pragma unroll
                 for (int q = 0; q < kJ; q++)
-                    if (wid + kW * q < kb) acc[q] = fma(vv[q], x, acc[q]);
-            }
+                    if (wid + kW * q < kb && i0 + e + 32 * h + lane < n) acc[q] = fma(vv[h][q], xs[h], acc[q]);
         }
         __syncthreads();  // sw is rewritten by the next tile
     }
@@ -2293,7 +2313,7 @@ int launch_cgs(fx_ctx *ctx, size_t n, const CgsArgs &a) {
         if (occ > 8) occ = 8;
         occ_cache.store(occ, std::memory_order_relaxed);
     }
-    size_t blocks = (n + kBlock - 1) / kBlock;
+    size_t blocks = (n + 2 * kBlock - 1) / (2 * kBlock);  // tiles of 2 kBlock elements
     if (blocks > (size_t)ctx->num_sms * occ) blocks = (size_t)ctx->num_sms * occ;
     if (blocks < 1) blocks = 1;
     timing_pre(ctx, "fgmres_cgs2");
