@@ -422,21 +422,26 @@ def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
 
         solve_ms, run_tot, per = 0.0, 0, []
         keep = []
+        host_ms = {"build": 0.0, "solve_and_check": 0.0}
         upload(0)
         for k, ((part, sd, _, _, _, out), (VX, VY, F, X)) in enumerate(zip(subs, bufs)):
             stream.wait_event(landed[k])
+            tb = time.perf_counter()
             B = BatchSolver(dev, sd, nu, VX, VY, cycle_dtype=mg_dtype, n_pre=sweeps, n_post=sweeps, omega=OMEGA,
                             coarse_max=COARSE_MAX, coarse_sweeps=COARSE_SWEEPS)
+            host_ms["build"] += (time.perf_counter() - tb) * 1e3
             if chunk != 2048:
                 B.set_chunk(chunk)
             if k == 0:  # the other uploads go after the first build, whose small table copies would
                 for j in range(1, len(subs)):  # otherwise queue behind them on the copy engine
                     upload(j)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ts = time.perf_counter()
             e0.record(stream)
             stats, run = B.bicgstab(X, F, 1e-10, 200)
             e1.record(stream)
             rn = B.residual_norms(X, F)  # every true residual, on the device (synchronises)
+            host_ms["solve_and_check"] += (time.perf_counter() - ts) * 1e3
             solve_ms += e0.elapsed_time(e1)
             run_tot += run
             down.wait_stream(stream)
@@ -444,14 +449,14 @@ def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
             per.append((part, stats, rn))
             keep.append(B)
         down.synchronize()
-        return per, run_tot, solve_ms
+        return per, run_tot, solve_ms, host_ms
 
     once()  # warm-up (first-use costs of the library, the pool and the copy streams)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    per, run, solve_ms = once()
+    per, run, solve_ms, host_ms = once()
     wall = time.perf_counter() - t0
     res = {}
     for part, stats, rn in per:
@@ -462,6 +467,7 @@ def run_batch_batched(args, ks, mine, host, world, rank, local_rank, dist):
     return res, wall, {"batch_iterations_launched": run, "device_solve_ms": solve_ms,
                        "points": sum(s_ * s_ for s_ in sides), "launch_per_iteration": "one CUDA graph",
                        "pipeline_sub_batches": len(subs),
+                       "host_wall_ms": {k_: round(v_, 1) for k_, v_ in host_ms.items()},
                        "tuning": {"chunk": chunk, "sweeps": sweeps, "cycle_dtype": "f32" if mg_dtype == DType.F32 else
                                   "f64", "autotuned": tuned}}
 

@@ -722,7 +722,7 @@ struct fx_batch {
     long long total0 = 0;
     const fx_buf *vx = nullptr, *vy = nullptr;  // level-0 F64 fields (borrowed)
     // device tables
-    std::vector<void *> dev_allocs;
+    std::vector<std::pair<void *, bool>> dev_allocs;  // (pointer, from the pool)
     Chunk *d_chunk0 = nullptr;  // level 0, every problem
     int nchunk0 = 0;
     struct LevelDev {
@@ -755,30 +755,24 @@ struct fx_batch {
     ~fx_batch() {
         if (ctx) cudaStreamSynchronize(ctx->stream);
         if (step_exec) cudaGraphExecDestroy(step_exec);
-        for (void *p : dev_allocs) cudaFree(p);
+        for (auto &a : dev_allocs) pool_free(ctx, a.first, a.second);
         if (h_state) cudaFreeHost(h_state);
         if (h_count) cudaFreeHost(h_count);
     }
     template <typename P>
-    int dalloc(P **p, size_t bytes) {
+    int dalloc(P **p, size_t bytes) {  // from the device's pool: a rebuilt batch reuses the memory
         void *q = nullptr;
-        if (bytes == 0) bytes = 16;
-        if (cudaMalloc(&q, bytes) != cudaSuccess) {
-            (void)cudaGetLastError();
-            return fail(FX_ERR_BACKEND, "batch: device allocation failed");
-        }
-        if (cudaMemset(q, 0, bytes) != cudaSuccess) {
-            cudaFree(q);
-            return fail(FX_ERR_BACKEND, "batch: memset failed");
-        }
-        dev_allocs.push_back(q);
+        bool pooled = false;
+        FX_TRY(pool_alloc(ctx, bytes, &q, &pooled));
+        dev_allocs.emplace_back(q, pooled);
         *p = (P *)q;
         return FX_OK;
     }
     template <typename P>
-    int upload(P **dst, const std::vector<P> &v) {
+    int upload(P **dst, const std::vector<P> &v) {  // ordered on the context's stream
         FX_TRY(dalloc(dst, v.size() * sizeof(P)));
-        if (!v.empty()) FX_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(P), cudaMemcpyHostToDevice));
+        if (!v.empty())
+            FX_CUDA(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(P), cudaMemcpyHostToDevice, ctx->stream));
         return FX_OK;
     }
     K0 k0() const {

@@ -57,6 +57,39 @@ static cudaMemPool_t device_pool(int device) {
     return pools[device];
 }
 
+int pool_alloc(fx_ctx *ctx, size_t bytes, void **out, bool *pooled) {
+    *out = nullptr;
+    *pooled = false;
+    if (bytes == 0) bytes = 16;
+    cudaMemPool_t pool = capturing(ctx->stream) ? nullptr : device_pool(ctx->device);
+    const cudaError_t e = pool ? cudaMallocFromPoolAsync(out, bytes, pool, ctx->stream) : cudaMalloc(out, bytes);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        *out = nullptr;
+        return fail(FX_ERR_BACKEND, std::string("device allocation failed: ") + cudaGetErrorString(e));
+    }
+    *pooled = pool != nullptr;
+    if (cudaMemsetAsync(*out, 0, bytes, ctx->stream) != cudaSuccess) {
+        (void)cudaGetLastError();
+        pool_free(ctx, *out, *pooled);
+        *out = nullptr;
+        return fail(FX_ERR_BACKEND, "memset failed");
+    }
+    return FX_OK;
+}
+
+void pool_free(fx_ctx *ctx, void *p, bool pooled) {
+    if (!p) return;
+    if (!pooled) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(p);
+    } else if (capturing(ctx->stream)) {
+        ctx->deferred_free.push_back(p);
+    } else {
+        cudaFreeAsync(p, ctx->stream);
+    }
+}
+
 bool capturing(cudaStream_t s) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {

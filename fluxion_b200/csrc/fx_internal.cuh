@@ -798,6 +798,11 @@ struct StoreFin {
 };
 
 // Read K doubles of ctx->d_result back to the host (synchronising).
+// Scratch arrays of a library object from the device's stream-ordered pool, ordered on the
+// context's stream and zero-filled (plain cudaMalloc while the stream is being captured);
+// pool_free releases them in stream order (or after the graph, during a capture).
+int pool_alloc(fx_ctx *ctx, size_t bytes, void **out, bool *pooled);
+void pool_free(fx_ctx *ctx, void *p, bool pooled);
 // n device values into mapped page-locked memory (h_dev: its device address), written by a kernel
 // (no copy engine), then wait for them
 int read_mapped(fx_ctx *ctx, const double *d, double *h_dev, size_t n);
