@@ -36,6 +36,16 @@ namespace fx {
 
 constexpr int kStripWarps = 8;  // warps per block
 constexpr int kStripUnroll = 6;  // the march is unrolled by 6 rows (= lcm(2, 3): row parity x 3-row windows)
+// Shortest row chunk of a warp (even).  A chunk shorter than the unroll never takes the
+// unrolled path without row tests, which costs instructions; but on the small levels, with
+// fewer warps than the GPU has SMs, each warp's march is pure latency (a step waits on
+// shuffles and dependent FP64 operations, with no other warp to hide them), and a chunk of
+// c rows takes c + 5 (down) or c + 4 (up) steps, so short chunks finish sooner.
+#ifndef FX_STRIP_MIN_CHUNK
+#define FX_STRIP_MIN_CHUNK 2
+#endif
+constexpr int kStripMinChunk = FX_STRIP_MIN_CHUNK;
+static_assert(kStripMinChunk >= 2 && kStripMinChunk % 2 == 0, "chunks start on even rows");
 constexpr int kDownFifo = 6;    // rows of raw loads in flight (a divisor of kStripUnroll)
 constexpr int kUpFifo = 6;
 static_assert(kStripUnroll % kDownFifo == 0 && kStripUnroll % kUpFifo == 0, "FIFO depth must divide the unroll");
@@ -171,12 +181,12 @@ inline StripGeom strip_geom(size_t rows, size_t cols, int useful, long capacity)
     G.cols = (int)cols;
     G.nstrips = (int)((cols - 1 + useful - 1) / useful);  // own ranges tile [0, cols - 1)
     if (G.nstrips < 1) G.nstrips = 1;
-    // one wave of resident warps; chunks of at least 6 rows (an unrolled step)
+    // one wave of resident warps; chunks of at least kStripMinChunk rows
     const long target = capacity;
     long chunks = target / G.nstrips;
     if (chunks < 1) chunks = 1;
     long cr = ((long)rows + chunks - 1) / chunks;
-    if (cr < kStripUnroll) cr = kStripUnroll;
+    if (cr < kStripMinChunk) cr = kStripMinChunk;
     cr = (cr + 1) & ~1L;
     G.chunk_rows = (int)cr;
     G.nitems = (int)(G.nstrips * (((long)rows + cr - 1) / cr));
