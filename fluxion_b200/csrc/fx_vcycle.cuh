@@ -113,72 +113,58 @@ __device__ __forceinline__ void jacobi_pts(const T *__restrict__ src, T *__restr
         if (cp[q] >= 0) dst[cp[q]] = v[q];
 }
 
-// Largest coarsest grid, ring included, that one warp solves from registers (F32 only: at
-// the 64 registers a thread of the 1024-thread tail may use, the F64 blocks spill and the
-// shared-memory sweeps are faster).
-constexpr int kWarpCoarseMax = 17;
+// Widest coarsest grid, ring included, that coarse_rows2 takes (a column per lane).
+constexpr int kRows2MaxCols = 32;
 
-// `sweeps` weighted-Jacobi sweeps from zero on a coarsest grid of at most 17 x 17 points, by
-// one warp with no barrier.  Lane l holds, in registers, the 4 x 2 block of rows
-// 1 + 4 (l >> 3) + i and columns 1 + 2 (l & 7) + j (i < 4, j < 2): the four block rows and
-// eight block columns cover rows and columns 1 .. 16.  Points that are not interior (the
-// ring, or outside the grid) are held at 0.  A block's outer neighbours come by shuffle from
-// lanes (l - 1), (l + 1), (l - 8) and (l + 8) mod 32.  Where that wraps around the block
-// layout it lands on layout row or column 16, which an interior of at most 15 x 15 leaves
-// empty, so those neighbours are 0, as the ring is.  The update is the expression of
-// jacobi_pts, so the result equals the shared-memory sweeps bit for bit.  out (rows x cols,
-// ring already 0) receives the interior.
+// `sweeps` weighted-Jacobi sweeps from zero on a coarsest grid of at most 32 columns and
+// 2 (kTailThreads / 32) + 2 rows.  Warp w owns grid rows 1 + 2w and 2 + 2w, lane l column l,
+// both values in registers.  West / east neighbours come by shuffle (columns past the grid
+// hold 0, as the ring does), the pair's inner neighbours from registers, and the rows above
+// and below from the neighbouring warps through shared memory: each sweep reads those two rows
+// from the current full-grid buffer and writes the warp's own two rows into the other one (P
+// and Q alternate, ring 0), then one named barrier joins the warps.  Per sweep a thread makes
+// two shared-memory loads and two stores, where the one-point-per-thread sweep makes five
+// loads.  The update is the expression of jacobi_pts, so the result equals it bit for bit, and
+// it lands in P for an even sweep count and in Q for an odd one.  Both buffers must hold zeros.
+// Measured on the 17 x 17 coarsest grid: 162 cycles a sweep at F32, against 182 for one warp
+// holding the whole grid in registers; at F64 it takes the same 250 cycles as the
+// one-point-per-thread sweeps, which stay in use there.
 template <typename T>
-__device__ __forceinline__ void coarse_warp(const T *B, T *out, int rows, int cols, const VOp<T> &op, int sweeps) {
+__device__ __forceinline__ void coarse_rows2(const T *B, T *P, T *Q, int rows, int cols, const VOp<T> &op,
+                                             int sweeps) {
     constexpr unsigned kAll = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int r0 = 1 + 4 * (lane >> 3), c0 = 1 + 2 * (lane & 7);
-    const int lw = (lane + 31) & 31, le = (lane + 1) & 31, ln = (lane + 24) & 31, ls = (lane + 8) & 31;
-    T x[4][2], b[4][2];
-    bool in[4][2];
+    const int nw = (rows - 1) / 2;  // warps holding rows: ceil((rows - 2) / 2)
+    const int warp = threadIdx.x >> 5, c = threadIdx.x & 31;
+    if (warp >= nw) return;
+    const int r0 = 1 + 2 * warp, n = rows * cols;
+    bool in[2];
+    T b[2], x[2];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            in[i][j] = r0 + i <= rows - 2 && c0 + j <= cols - 2;
-            b[i][j] = in[i][j] ? B[(r0 + i) * cols + c0 + j] : (T)0;
-            x[i][j] = (T)0;
-        }
-#pragma unroll 2  // two sweeps per pass let the compiler overlap one's shuffles with the other's math
-    for (int k = 0; k < sweeps; k++) {
-        T w[4], e[4], n[2], s[2];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            w[i] = __shfl_sync(kAll, x[i][1], lw);
-            e[i] = __shfl_sync(kAll, x[i][0], le);
-        }
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            n[j] = __shfl_sync(kAll, x[3][j], ln);
-            s[j] = __shfl_sync(kAll, x[0][j], ls);
-        }
-        T v[4][2];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 2; j++) {
-                const T c = x[i][j];
-                const T nn = i == 0 ? n[j] : x[i - 1][j];
-                const T ss = i == 3 ? s[j] : x[i + 1][j];
-                const T ww = j == 0 ? w[i] : x[i][0];
-                const T ee = j == 1 ? e[i] : x[i][1];
-                v[i][j] = in[i][j] ? fx_fma(op.wd, b[i][j] - op5v(op.a, c, nn, ss, ww, ee), c) : (T)0;
-            }
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 2; j++) x[i][j] = v[i][j];
+    for (int i = 0; i < 2; i++) {
+        const int r = r0 + i;
+        in[i] = r <= rows - 2 && c >= 1 && c <= cols - 2 && FX_IN(r * cols + c, n);
+        b[i] = in[i] ? B[r * cols + c] : (T)0;
+        x[i] = (T)0;
     }
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-            if (in[i][j]) out[(r0 + i) * cols + c0 + j] = x[i][j];
+    const int on = (r0 - 1) * cols + c, os = (r0 + 2) * cols + c;  // rows above and below the pair
+    const bool hn = c < cols && FX_IN(on, n), hs = r0 + 2 <= rows - 1 && c < cols && FX_IN(os, n);
+    const int o0 = r0 * cols + c, o1 = o0 + cols;
+    const int nthr = nw * 32;
+    for (int k = 0; k < sweeps; k++) {
+        const T *cur = (k & 1) ? Q : P;
+        T *nxt = (k & 1) ? P : Q;
+        const T xn = hn ? cur[on] : (T)0;
+        const T xs = hs ? cur[os] : (T)0;
+        const T w0 = __shfl_up_sync(kAll, x[0], 1), e0 = __shfl_down_sync(kAll, x[0], 1);
+        const T w1 = __shfl_up_sync(kAll, x[1], 1), e1 = __shfl_down_sync(kAll, x[1], 1);
+        const T v0 = in[0] ? fx_fma(op.wd, b[0] - op5v(op.a, x[0], xn, x[1], w0, e0), x[0]) : (T)0;
+        const T v1 = in[1] ? fx_fma(op.wd, b[1] - op5v(op.a, x[1], x[0], xs, w1, e1), x[1]) : (T)0;
+        x[0] = v0;
+        x[1] = v1;
+        if (in[0]) nxt[o0] = v0;
+        if (in[1]) nxt[o1] = v1;
+        asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory");
+    }
 }
 
 template <typename T>
@@ -316,10 +302,11 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vtail(TailArgs<T> A, const 
         __syncthreads();
     }
 
-    // ---- coarsest: `coarse_sweeps` weighted-Jacobi sweeps from zero.  Up to 17 x 17 points,
-    // warp 0 alone from registers; larger, P <-> Q in shared memory, each of the first warps
-    // owning up to 4 points (rhs in registers) and a named barrier joining them.  Either way
-    // the result lands in P for an even sweep count and in Q for an odd one.
+    // ---- coarsest: `coarse_sweeps` weighted-Jacobi sweeps from zero.  F32 grids of up to 32
+    // columns: a row pair per warp in registers (coarse_rows2); F64 and wider grids: P <-> Q in
+    // shared memory, each of the first warps owning up to 4 points (rhs in registers) and a
+    // named barrier joining them.  Either way the result lands in P for an even sweep count and
+    // in Q for an odd one.
     {
         const int l = nlev - 1, rows = A.rows[l], cols = A.cols[l], n = rows * cols;
         const VOp<T> op = A.op[l];
@@ -329,8 +316,8 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vtail(TailArgs<T> A, const 
             Q[p] = (T)0;
         }
         __syncthreads();
-        if (sizeof(T) == 4 && rows <= kWarpCoarseMax && cols <= kWarpCoarseMax) {
-            if (tid < 32) coarse_warp<T>(B, (A.coarse_sweeps & 1) ? Q : P, rows, cols, op, A.coarse_sweeps);
+        if (sizeof(T) == 4 && cols <= kRows2MaxCols && rows <= 2 * (kTailThreads / 32) + 2) {
+            coarse_rows2<T>(B, P, Q, rows, cols, op, A.coarse_sweeps);
         } else {
             // kPts points per thread: 1 while n fits the block (a predicated-off point still
             // costs its instructions every sweep), else 4 (n <= 4096)
